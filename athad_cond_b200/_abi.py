@@ -1,0 +1,197 @@
+"""ctypes description of the C ABI in include/athad_gpu.h.
+
+The shared library is the product; this module only describes its types and loads it.
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from enum import IntEnum
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libathad_gpu.so")
+
+
+class Status(IntEnum):
+    OK = 0
+    ERR_INVALID = 1
+    ERR_CUDA = 2
+    ERR_UNSUPPORTED = 3
+    ERR_OOM = 4
+    ERR_NONFINITE = 5
+    ERR_TIMEOUT = 6
+    ERR_NO_DEVICE = 7
+
+
+class Turb(IntEnum):
+    K_EPSILON = 1
+    K_OMEGA = 2
+    K_OMEGA_SST = 3
+
+
+class Wall(IntEnum):
+    MIRROR = 0
+    REFERENCE = 1
+
+
+FIELD_NAMES = [
+    "t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
+    "tn", "un", "vn", "wn", "cn", "cloudn", "icen", "grn", "co2n", "tken", "disn",
+    "p_dyn", "nue", "t_eq", "p_stat", "r_humid",
+    "S_c", "S_r", "S_i", "S_s", "S_g", "S_v",
+    "MC_t", "MC_q", "MC_v", "MC_w",
+    "aux_u", "aux_v", "aux_w",
+    "prod", "tke_source", "dis_source",
+    "S_c_c", "P_rain", "P_snow", "P_graupel", "Precipitation",
+    "r_dry",
+    "s", "s_u", "s_d", "M_u", "M_d",
+    "q_v_u", "q_c_u", "q_v_d",
+    "u_u", "v_u", "w_u", "u_d", "v_d", "w_d",
+    "E_u", "D_u", "E_d", "D_d",
+    "c_u", "e_l", "e_d", "e_p", "g_p",
+    "P_conv", "CloudBase", "LevelFreeSinking", "Deep_beg", "Deep_end",
+]
+FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
+NFIELDS = len(FIELD_NAMES)
+PROGNOSTIC = FIELD_NAMES[0:11]
+N_LEVEL = FIELD_NAMES[11:22]
+
+FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D"]
+FIELD2D = {n: i for i, n in enumerate(FIELD2D_NAMES)}
+PROFILE_NAMES = ["t_ref_level", "rho_base", "dlnrho_dr"]
+PROFILE = {n: i for i, n in enumerate(PROFILE_NAMES)}
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("im", ctypes.c_int32), ("jm", ctypes.c_int32), ("km", ctypes.c_int32)]
+
+
+_PARAM_INTS = [
+    "turb_model", "wall_mode", "poisson_metric_fix", "anelastic", "tracer_diff_flux",
+    "coriolis_nontrad", "metric_curvature", "metric_divergence",
+    "convection_perturbation", "convection_mode", "iter_prec", "pad0",
+]
+_PARAM_DOUBLES = [
+    "metric_r0", "re_turb",
+    "r_air", "g", "u_0", "cp_l", "t_0", "c_0", "L_atm", "zeta", "omega", "lamda", "lv", "ls",
+    "pr_turb", "sc_WaterVapour", "sc_CO2",
+    "r_Earth", "p_0", "t_00", "t_max_phys", "cloud_cap", "t_skin", "c_h2o_dry_top", "co2_0", "s_0",
+    "R_Air", "R_WaterVapour",
+    "M_bg", "R_bg", "R_mix",
+]
+
+
+class Params(ctypes.Structure):
+    _fields_ = ([("struct_size", ctypes.c_uint32)]
+                + [(n, ctypes.c_int32) for n in _PARAM_INTS]
+                + [(n, ctypes.c_double) for n in _PARAM_DOUBLES])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class StepScalars(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("diffusion_ramp", ctypes.c_double),
+                ("buoyancy_ramp", ctypes.c_double), ("write_diagnostics", ctypes.c_int32),
+                ("pad0", ctypes.c_int32)]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
+                ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
+                ("last_kernel_ms", ctypes.c_double)]
+
+
+# name -> (restype, argtypes); every symbol include/athad_gpu.h declares
+_P = ctypes.c_void_p
+_D = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "athad_default_params": (None, [ctypes.POINTER(Params)]),
+    "athad_abi_version": (ctypes.c_int32, []),
+    "athad_params_size": (ctypes.c_size_t, []),
+    "athad_create": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.POINTER(Params), ctypes.POINTER(_P)]),
+    "athad_destroy": (ctypes.c_int, [_P]),
+    "athad_last_error": (ctypes.c_char_p, [_P]),
+    "athad_set_stream": (ctypes.c_int, [_P, _P]),
+    "athad_synchronize": (ctypes.c_int, [_P]),
+    "athad_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(Grid)]),
+    "athad_upload": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_download": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_upload_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_download_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_upload_profile": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_download_profile": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_field_device_ptr": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_size_t)]),
+    "athad_fill": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_double]),
+    "athad_store_n_level": (ctypes.c_int, [_P]),
+    "athad_level_mean": (ctypes.c_int, [_P]),
+    "athad_rk4_step": (ctypes.c_int, [_P, ctypes.POINTER(StepScalars)]),
+    "athad_pressure_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "athad_saturation_adjust": (ctypes.c_int, [_P]),
+    "athad_densities": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "athad_moist_convection": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "athad_get_report": (ctypes.c_int, [_P, ctypes.POINTER(Report)]),
+}
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load libathad_gpu.so and bind every declared symbol.  Raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"athad_cond_b200: CUDA library {p} not found; run __graft_entry__.build() "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.athad_params_size() != ctypes.sizeof(Params):
+        raise RuntimeError("athad_cond_b200: athad_params layout mismatch between library and bindings")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def default_params() -> Params:
+    p = Params()
+    load_library().athad_default_params(ctypes.byref(p))
+    return p
+
+
+def config_params() -> Params:
+    """cli/config_cond.xml values without loading the library (same as athad_default_params)."""
+    p = Params()
+    p.struct_size = ctypes.sizeof(Params)
+    p.turb_model = Turb.K_OMEGA_SST
+    p.wall_mode = Wall.MIRROR
+    p.poisson_metric_fix = 1
+    p.convection_perturbation = 1
+    p.convection_mode = 1
+    p.iter_prec = 3
+    p.metric_r0 = -1.0
+    p.re_turb = 0.4 * 0.1 / 1.5e-5
+    vals = dict(r_air=40.8, g=9.8066, u_0=8.0, cp_l=1349.0, t_0=273.15, c_0=0.3464, L_atm=6287.5,
+                zeta=3.0, omega=0.000317, lamda=0.0262, lv=2520000.0, ls=2830000.0, pr_turb=0.9,
+                sc_WaterVapour=0.61, sc_CO2=0.96, r_Earth=6370.001, p_0=60000.0, t_00=236.15,
+                t_max_phys=2000.0, cloud_cap=0.05, t_skin=254.0, c_h2o_dry_top=0.00423,
+                co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5)
+    for k, v in vals.items():
+        setattr(p, k, v)
+    R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010
+    x = [0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0]
+    m_H2O, m_CO2 = x[0] * M_H2O, x[1] * M_CO2
+    m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031 + x[5] * 0.002016 + x[6] * 0.028010 + x[7] * 0.064066
+    M_mean = m_H2O + m_CO2 + m_bg
+    p.R_mix = R_STAR / M_mean
+    x_bg = x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
+    p.M_bg = (m_bg / x_bg) if x_bg > 0.0 else 0.028014
+    p.R_bg = R_STAR / p.M_bg
+    return p

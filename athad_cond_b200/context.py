@@ -1,0 +1,166 @@
+"""Python view of one device-resident model state (an athad_ctx).
+
+Mirrors the reference's call sites in cAtmosphereModel::run_3D_loop
+(atmosphere/cAtmosphereModel.cpp:1103-1724): each method is one of the in-place physics
+calls, named after the reference function it replaces.  Errors surface as AthadError with
+the library's own message, as the reference's `throw` would.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import FIELD, FIELD2D, PROFILE, Status
+
+
+class AthadError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = Status(status) if status in Status._value2member_map_ else status
+        super().__init__(f"{self.status!r}: {message}")
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class GpuAtmosphere:
+    """Device-resident state of one grid, driven through libathad_gpu.so."""
+
+    def __init__(self, im: int, jm: int, km: int, params: _abi.Params | None = None):
+        self.lib = _abi.load_library()
+        self.shape = (im, jm, km)
+        self.params = params if params is not None else _abi.default_params()
+        self.params.struct_size = ctypes.sizeof(_abi.Params)
+        self._grid = _abi.Grid(im, jm, km)
+        h = ctypes.c_void_p()
+        st = self.lib.athad_create(ctypes.byref(self._grid), ctypes.byref(self.params), ctypes.byref(h))
+        if st != 0:
+            raise AthadError(st, "athad_create failed")
+        self._h = h
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.athad_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            raise AthadError(st, self.lib.athad_last_error(self._h).decode())
+
+    @staticmethod
+    def footprint_bytes(im: int, jm: int, km: int) -> int:
+        g = _abi.Grid(im, jm, km)
+        return int(_abi.load_library().athad_footprint_bytes(ctypes.byref(g)))
+
+    def set_stream(self, cuda_stream_handle: int | None):
+        self._check(self.lib.athad_set_stream(self._h, ctypes.c_void_p(cuda_stream_handle or 0)))
+
+    def synchronize(self):
+        self._check(self.lib.athad_synchronize(self._h))
+
+    # ---- transfer ----
+    def upload(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"{name}: shape {a.shape} != {self.shape}")
+        self._check(self.lib.athad_upload(self._h, FIELD[name], _dptr(a), a.size))
+        # keep the buffer alive until the (possibly asynchronous) copy has been issued
+        self.synchronize()
+
+    def download(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(self.lib.athad_download(self._h, FIELD[name], _dptr(out), out.size))
+        return out
+
+    def upload_2d(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self._check(self.lib.athad_upload_2d(self._h, FIELD2D[name], _dptr(a), a.size))
+        self.synchronize()
+
+    def download_2d(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape[1:], dtype=np.float64)
+        self._check(self.lib.athad_download_2d(self._h, FIELD2D[name], _dptr(out), out.size))
+        return out
+
+    def upload_profile(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self._check(self.lib.athad_upload_profile(self._h, PROFILE[name], _dptr(a), a.size))
+        self.synchronize()
+
+    def download_profile(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape[0], dtype=np.float64)
+        self._check(self.lib.athad_download_profile(self._h, PROFILE[name], _dptr(out), out.size))
+        return out
+
+    def upload_state(self, state: dict):
+        for name, a in state.items():
+            if name in FIELD:
+                self.upload(name, a)
+            elif name in FIELD2D:
+                self.upload_2d(name, a)
+            elif name in PROFILE:
+                self.upload_profile(name, a)
+
+    def device_ptr(self, name: str):
+        p = ctypes.POINTER(ctypes.c_double)()
+        pitch = ctypes.c_size_t()
+        self._check(self.lib.athad_field_device_ptr(self._h, FIELD[name], ctypes.byref(p), ctypes.byref(pitch)))
+        return ctypes.cast(p, ctypes.c_void_p).value, int(pitch.value)
+
+    def fill(self, name: str, value: float):
+        self._check(self.lib.athad_fill(self._h, FIELD[name], float(value)))
+
+    # ---- the hot path (reference call sites of cAtmosphereModel::run_3D_loop) ----
+    def storeIntermediateData3D(self):
+        """UtilsAtm::storeIntermediateData3D (UtilsAtm.h:25-49)."""
+        self._check(self.lib.athad_store_n_level(self._h))
+
+    def computeLevelMeanTemperature(self):
+        """RungeKutta_Atm_Turb.cpp:24-41."""
+        self._check(self.lib.athad_level_mean(self._h))
+
+    def solveRungeKutta_Atmosphere_Turb(self, dt: float, diffusion_ramp: float = 1.0,
+                                        buoyancy_ramp: float = 1.0, write_diagnostics: bool = False):
+        """RungeKutta_Atm_Turb.cpp:44-273 (call site cAtmosphereModel.cpp:1509)."""
+        s = _abi.StepScalars(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0, 0)
+        self._check(self.lib.athad_rk4_step(self._h, ctypes.byref(s)))
+
+    def PressureSolverAtm_run(self, total_iter_count: int, n_sweeps: int = 1):
+        """PressureSolverAtm::run (PressureSolverAtm.h:27-669; call site cAtmosphereModel.cpp:1158)."""
+        self._check(self.lib.athad_pressure_sweep(self._h, n_sweeps, total_iter_count))
+
+    def project_initial_velocity(self, n_sweeps: int = 200, total_iter_count: int = 0):
+        """PressureSolverAtm::project_initial_velocity (PressureSolverAtm.h:686-767)."""
+        self._check(self.lib.athad_project_initial_velocity(self._h, n_sweeps, total_iter_count))
+
+    def SaturationAdjustment_run(self):
+        """SaturationAdjustment::run (SaturationAdjustment.h:25-45)."""
+        self._check(self.lib.athad_saturation_adjust(self._h))
+
+    def densities(self, set_water_profile: bool = False):
+        """ThermoAtm::densities (ThermoAtm.h:1436-1666)."""
+        self._check(self.lib.athad_densities(self._h, 1 if set_water_profile else 0))
+
+    def MoistConvection_run(self, iter_n: int):
+        """MoistConvection::run (MoistConvection.h:106-140)."""
+        self._check(self.lib.athad_moist_convection(self._h, iter_n))
+
+    def report(self) -> dict:
+        r = _abi.Report()
+        self._check(self.lib.athad_get_report(self._h, ctypes.byref(r)))
+        return {n: getattr(r, n) for n, _ in r._fields_}

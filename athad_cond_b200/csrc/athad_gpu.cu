@@ -1,0 +1,602 @@
+// athad_gpu.cu - the C ABI of include/athad_gpu.h: context lifetime, device-resident
+// state, host<->device transfer and the hot-path entry points.
+//
+// All device memory of a context is one allocation made at creation (fields, RK4 stage
+// buffers, the Poisson source, geometry tables, counters), so the hot path allocates
+// nothing and a context's HBM footprint is known before it is created.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <new>
+
+#include "kernels.cuh"
+#include "thermo.cuh"
+
+using namespace athad;
+
+namespace {
+
+constexpr int kNY = 11;   // prognostic fields t..dis
+
+struct Layout {
+    Dims d;
+    size_t field_elems;   // im*jm*pitch
+    size_t f2d_elems;     // jm*pitch
+    size_t n_fields;      // ATHAD_NFIELDS + internal 3-D buffers
+    size_t bytes;
+};
+
+constexpr int kInternal3D = 3 * kNY + 1;   // stage A, stage B, accumulator K, Poisson source
+
+size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+Layout make_layout(const athad_grid& g)
+{
+    Layout L;
+    L.d.im = g.im; L.d.jm = g.jm; L.d.km = g.km;
+    L.d.pitch = (int)round_up((size_t)g.km, 32);
+    L.d.plane = (long long)g.jm * L.d.pitch;
+    L.field_elems = round_up((size_t)g.im * L.d.plane, 64);
+    L.d.fstride = (long long)L.field_elems;
+    L.f2d_elems = round_up((size_t)g.jm * L.d.pitch, 64);
+    L.n_fields = ATHAD_NFIELDS + kInternal3D;
+    size_t b = L.n_fields * L.field_elems * sizeof(double);
+    b += ATHAD_NFIELDS2D * L.f2d_elems * sizeof(double);
+    b += ATHAD_NPROFILES * round_up((size_t)g.im, 64) * sizeof(double);
+    b += round_up((size_t)g.im * g.jm * sizeof(GeoIJ), 256);
+    b += round_up((size_t)g.im * g.jm * sizeof(PoiIJ), 256);
+    b += 4 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat
+    b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
+    b += 256;                                                                         // counters
+    L.bytes = b;
+    return L;
+}
+
+}  // namespace
+
+struct athad_ctx {
+    athad_grid grid{};
+    athad_params p{};
+    Layout L{};
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    char* slab = nullptr;
+    double* field[ATHAD_NFIELDS] = {};
+    double* stA[kNY] = {};
+    double* stB[kNY] = {};
+    double* stK[kNY] = {};
+    double* src = nullptr;
+    double* f2d[ATHAD_NFIELDS2D] = {};
+    double* prof[ATHAD_NPROFILES] = {};
+    GeoIJ* geo = nullptr;
+    PoiIJ* poi = nullptr;
+    double* sin_w = nullptr;
+    double* height = nullptr;
+    double* step_f = nullptr;
+    double* coslat = nullptr;
+    double* row_sum = nullptr;
+    double* row_cnt = nullptr;
+    unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
+    double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
+    std::vector<double> rad;
+    int64_t poisson_sweeps_since_reset = 0;
+    std::string err;
+};
+
+static athad_status fail(athad_ctx* c, athad_status s, const char* msg)
+{
+    if (c) c->err = msg;
+    return s;
+}
+
+static athad_status cuda_check(athad_ctx* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return ATHAD_OK;
+    if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? ATHAD_ERR_OOM : ATHAD_ERR_CUDA;
+}
+
+#define ATHAD_CHECK_LAUNCH(ctx, what)                                         \
+    do {                                                                      \
+        athad_status _s = cuda_check((ctx), cudaGetLastError(), (what));      \
+        if (_s != ATHAD_OK) return _s;                                        \
+    } while (0)
+
+extern "C" {
+
+int32_t athad_abi_version(void) { return ATHAD_ABI_VERSION; }
+size_t athad_params_size(void) { return sizeof(athad_params); }
+
+// cli/config_cond.xml values; composition resolved as AtmMixture::resolve (MixtureAtm.h:82-109)
+void athad_default_params(athad_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->struct_size = sizeof(athad_params);
+    p->turb_model = ATHAD_TURB_K_OMEGA_SST;
+    p->wall_mode = ATHAD_WALL_MIRROR;
+    p->poisson_metric_fix = 1;
+    p->convection_perturbation = 1;
+    p->convection_mode = 1;
+    p->iter_prec = 3;
+    p->metric_r0 = -1.0;                 // derive r_Earth*1e3/metricShellLength()
+    p->re_turb = 0.4 * 0.1 / 1.5e-5;     // TurbulenceAtm.h:26-35
+    p->r_air = 40.8; p->g = 9.8066; p->u_0 = 8.0; p->cp_l = 1349.0; p->t_0 = 273.15;
+    p->c_0 = 0.3464; p->L_atm = 6287.5; p->zeta = 3.0; p->omega = 0.000317; p->lamda = 0.0262;
+    p->lv = 2520000.0; p->ls = 2830000.0; p->pr_turb = 0.9; p->sc_WaterVapour = 0.61;
+    p->sc_CO2 = 0.96; p->r_Earth = 6370.001; p->p_0 = 60000.0; p->t_00 = 236.15;
+    p->t_max_phys = 2000.0; p->cloud_cap = 0.05; p->t_skin = 254.0; p->c_h2o_dry_top = 0.00423;
+    p->co2_0 = 0.6233; p->s_0 = 274515.75; p->R_Air = 296.8; p->R_WaterVapour = 461.5;
+    const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
+    const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
+                      + x[5] * 0.002016 + x[6] * 0.028010 + x[7] * 0.064066;
+    const double M_mean = m_H2O + m_CO2 + m_bg;
+    p->R_mix = thermo::R_STAR / M_mean;
+    const double x_bg = x[2] + x[3] + x[4] + x[5] + x[6] + x[7];
+    p->M_bg = (x_bg > 0.0) ? (m_bg / x_bg) : 0.028014;
+    p->R_bg = thermo::R_STAR / p->M_bg;
+}
+
+size_t athad_footprint_bytes(const athad_grid* grid)
+{
+    if (!grid || grid->im < 4 || grid->jm < 5 || grid->km < 5) return 0;
+    return make_layout(*grid).bytes;
+}
+
+const char* athad_last_error(const athad_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+athad_status athad_create(const athad_grid* grid, const athad_params* params, athad_ctx** out)
+{
+    if (!out) return ATHAD_ERR_INVALID;
+    *out = nullptr;
+    if (!grid || !params) return ATHAD_ERR_INVALID;
+    if (params->struct_size != sizeof(athad_params)) return ATHAD_ERR_INVALID;
+    if (grid->im < 4 || grid->jm < 5 || grid->km < 5 || grid->im > 1024) return ATHAD_ERR_INVALID;
+    if (params->turb_model < ATHAD_TURB_K_EPSILON || params->turb_model > ATHAD_TURB_K_OMEGA_SST)
+        return ATHAD_ERR_UNSUPPORTED;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return ATHAD_ERR_NO_DEVICE; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { cudaGetLastError(); return ATHAD_ERR_NO_DEVICE; }
+    if (prop.major != 10) return ATHAD_ERR_NO_DEVICE;   // built for sm_100a only
+
+    athad_ctx* c = new (std::nothrow) athad_ctx();
+    if (!c) return ATHAD_ERR_OOM;
+    c->grid = *grid;
+    c->p = *params;
+    c->L = make_layout(*grid);
+    const Layout& L = c->L;
+    const int im = grid->im, jm = grid->jm, km = grid->km;
+
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c; return ATHAD_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    if (cudaMalloc((void**)&c->slab, L.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return ATHAD_ERR_OOM;
+    }
+    // carve the slab
+    char* q = c->slab;
+    auto take = [&](size_t bytes) { char* r = q; q += round_up(bytes, 256); return r; };
+    for (int f = 0; f < ATHAD_NFIELDS; f++) c->field[f] = (double*)take(L.field_elems * sizeof(double));
+    for (int n = 0; n < kNY; n++) c->stA[n] = (double*)take(L.field_elems * sizeof(double));
+    for (int n = 0; n < kNY; n++) c->stB[n] = (double*)take(L.field_elems * sizeof(double));
+    for (int n = 0; n < kNY; n++) c->stK[n] = (double*)take(L.field_elems * sizeof(double));
+    c->src = (double*)take(L.field_elems * sizeof(double));
+    for (int f = 0; f < ATHAD_NFIELDS2D; f++) c->f2d[f] = (double*)take(L.f2d_elems * sizeof(double));
+    for (int f = 0; f < ATHAD_NPROFILES; f++) c->prof[f] = (double*)take(round_up((size_t)im, 64) * sizeof(double));
+    c->geo = (GeoIJ*)take((size_t)im * jm * sizeof(GeoIJ));
+    c->poi = (PoiIJ*)take((size_t)im * jm * sizeof(PoiIJ));
+    const size_t nmax = round_up((size_t)(im > jm ? im : jm), 64) * sizeof(double);
+    c->sin_w = (double*)take(nmax);
+    c->height = (double*)take(nmax);
+    c->step_f = (double*)take(nmax);
+    c->coslat = (double*)take(nmax);
+    c->row_sum = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
+    c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
+    c->counters = (unsigned long long*)take(256);
+    if ((size_t)(q - c->slab) > L.bytes) {
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        return ATHAD_ERR_INVALID;
+    }
+    // Every field starts at zero (the reference's Arrays are zero/one-initialised by
+    // resetArrays; the caller uploads the state it wants).
+    if (cudaMemsetAsync(c->slab, 0, L.bytes, c->stream) != cudaSuccess) {
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        return ATHAD_ERR_CUDA;
+    }
+
+    // ---- geometry, built on the host exactly as the reference builds it ----
+    const double pi180 = 180.0 / M_PI;                         // cAtmosphereModel.cpp:44
+    c->dr = 1.0 / (double)(im - 1);                            // :57
+    c->dthe = (180.0 / (double)(jm - 1)) / pi180;              // :46/:59 generalised
+    c->dphi = (360.0 / (double)(km - 1)) / pi180;              // :47/:60 generalised
+    std::vector<double> rad(im), the(jm);
+    rad[0] = 1.0;                                              // Array_1D::Coordinates running sum
+    for (int i = 1; i < im; i++) rad[i] = rad[i - 1] + c->dr;
+    the[0] = 0.0;
+    for (int j = 1; j < jm; j++) the[j] = the[j - 1] + c->dthe;
+    c->rad = rad;
+    std::vector<double> sin_w(jm), sin_f(jm), cos_t(jm), coslat(jm);
+    for (int j = 0; j < jm; j++) {   // mirror-exact tables
+        const int jj = (j < jm - 1 - j) ? j : jm - 1 - j;
+        sin_w[j] = std::sin(the[jj]);
+        if (j < jm - 1 - j) cos_t[j] = std::cos(the[j]);
+        else if (j > jm - 1 - j) cos_t[j] = -std::cos(the[jm - 1 - j]);
+        else cos_t[j] = 0.0;
+        sin_f[j] = sin_w[j] < 0.55 ? 0.55 : sin_w[j];
+        coslat[j] = std::cos((jj / (double)(jm - 1) - 0.5) * M_PI);   // ThermoAtm.h:1636
+    }
+    const double span = rad[im - 1] - rad[0];
+    c->shell_len = (span > 0.0) ? (std::exp(params->zeta * span) - 1.0) * params->L_atm / span
+                                : params->L_atm;                     // cAtmosphereModel.h:465-470
+    c->metric_r0 = (params->metric_r0 < 0.0)
+        ? ((c->shell_len > 0.0) ? params->r_Earth * 1.0e3 / c->shell_len : 0.0)
+        : params->metric_r0;                                          // cAtmosphereModel.cpp:382-399
+    auto rmet_of = [&](double rm) { return (c->metric_r0 > 0.0) ? (c->metric_r0 + (rm - rad[0])) : rm; };
+    std::vector<double> height(im), step(im);
+    const float hL = (float)params->L_atm;
+    for (int i = 0; i < im; i++)
+        height[i] = (double)(float)((std::exp(params->zeta * (rad[i] - rad[0])) - 1) * (double)hL);
+    for (int i = 0; i < im; i++) {   // SaturationAdjustment::computeSteps: float difference
+        const float h1 = (i + 1 <= im - 1) ? (float)height[i + 1] : -1.0f;
+        const float h0 = (float)height[i];
+        step[i] = (double)(float)(h1 - h0);
+    }
+    std::vector<GeoIJ> geo((size_t)im * jm);
+    std::vector<PoiIJ> poi((size_t)im * jm);
+    const double inv_dr2 = 1.0 / (c->dr * c->dr), inv_dthe2 = 1.0 / (c->dthe * c->dthe),
+                 inv_dphi2 = 1.0 / (c->dphi * c->dphi);
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++) {
+            GeoIJ& G = geo[(size_t)i * jm + j];
+            const double rm = rad[i];
+            G.exp_rm = 1.0 / (rm + 1.0);
+            G.exp_2_rm = G.exp_rm * G.exp_rm;
+            G.sinthe = sin_f[j];
+            G.sinthe2 = G.sinthe * G.sinthe;
+            G.costhe = cos_t[j];
+            const double rmet = rmet_of(rm);
+            const double rmet2 = rmet * rmet;
+            G.inv_rm = 1.0 / rmet;
+            G.inv_rm2 = 1.0 / rmet2;
+            G.inv_rmsinthe = 1.0 / (rmet * G.sinthe);
+            G.inv_rm2sinthe = G.inv_rm2 / G.sinthe;
+            G.inv_rm2sinthe2 = G.inv_rm2 / G.sinthe2;
+            G.costhe_inv_rm2sinthe = G.costhe * G.inv_rm2sinthe;
+            PoiIJ& P = poi[(size_t)i * jm + j];          // PressureSolverAtm.h:236-269
+            const double m_the = params->poisson_metric_fix ? G.inv_rm2 : G.inv_rm;
+            const double m_phi = params->poisson_metric_fix ? G.inv_rm2sinthe2 : G.inv_rmsinthe;
+            P.denom = 2.0 * G.exp_2_rm * inv_dr2 + 2.0 * m_the * inv_dthe2 + 2.0 * m_phi * inv_dphi2;
+            P.inv_denom = 1.0 / P.denom;
+            P.num1 = G.exp_2_rm * inv_dr2;
+            P.num2 = m_the * inv_dthe2;
+            P.num3 = m_phi * inv_dphi2;
+            P.exp_rm = G.exp_rm; P.exp_2_rm = G.exp_2_rm; P.inv_rm = G.inv_rm;
+            P.inv_rmsinthe = G.inv_rmsinthe; P.sinthe = G.sinthe; P.costhe = G.costhe;
+        }
+    athad_status s = ATHAD_OK;
+    s = cuda_check(c, cudaMemcpyAsync(c->geo, geo.data(), geo.size() * sizeof(GeoIJ), cudaMemcpyHostToDevice, c->stream), "geo");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->poi, poi.data(), poi.size() * sizeof(PoiIJ), cudaMemcpyHostToDevice, c->stream), "poi");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->sin_w, sin_w.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "sin_w");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->height, height.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "height");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_f, step.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->coslat, coslat.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "coslat");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
+    if (s != ATHAD_OK) {
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        return s;
+    }
+    *out = c;
+    return ATHAD_OK;
+}
+
+athad_status athad_destroy(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->slab);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return ATHAD_OK;
+}
+
+athad_status athad_set_stream(athad_ctx* ctx, void* s)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+    return ATHAD_OK;
+}
+
+athad_status athad_synchronize(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+// ---- transfer ---------------------------------------------------------------------------
+
+athad_status athad_upload(athad_ctx* ctx, athad_field f, const double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "upload: bad argument");
+    const Dims& d = ctx->L.d;
+    if (n != (size_t)d.im * d.jm * d.km) return fail(ctx, ATHAD_ERR_INVALID, "upload: size mismatch");
+    return cuda_check(ctx, cudaMemcpy2DAsync(ctx->field[f], d.pitch * sizeof(double), host, d.km * sizeof(double),
+                                             d.km * sizeof(double), (size_t)d.im * d.jm, cudaMemcpyHostToDevice,
+                                             ctx->stream), "upload");
+}
+
+athad_status athad_download(athad_ctx* ctx, athad_field f, double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "download: bad argument");
+    const Dims& d = ctx->L.d;
+    if (n != (size_t)d.im * d.jm * d.km) return fail(ctx, ATHAD_ERR_INVALID, "download: size mismatch");
+    athad_status s = cuda_check(ctx, cudaMemcpy2DAsync(host, d.km * sizeof(double), ctx->field[f], d.pitch * sizeof(double),
+                                                       d.km * sizeof(double), (size_t)d.im * d.jm, cudaMemcpyDeviceToHost,
+                                                       ctx->stream), "download");
+    if (s != ATHAD_OK) return s;
+    return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "download sync");
+}
+
+athad_status athad_upload_2d(athad_ctx* ctx, athad_field2d f, const double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NFIELDS2D) return fail(ctx, ATHAD_ERR_INVALID, "upload_2d: bad argument");
+    const Dims& d = ctx->L.d;
+    if (n != (size_t)d.jm * d.km) return fail(ctx, ATHAD_ERR_INVALID, "upload_2d: size mismatch");
+    return cuda_check(ctx, cudaMemcpy2DAsync(ctx->f2d[f], d.pitch * sizeof(double), host, d.km * sizeof(double),
+                                             d.km * sizeof(double), (size_t)d.jm, cudaMemcpyHostToDevice, ctx->stream),
+                      "upload_2d");
+}
+
+athad_status athad_download_2d(athad_ctx* ctx, athad_field2d f, double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NFIELDS2D) return fail(ctx, ATHAD_ERR_INVALID, "download_2d: bad argument");
+    const Dims& d = ctx->L.d;
+    if (n != (size_t)d.jm * d.km) return fail(ctx, ATHAD_ERR_INVALID, "download_2d: size mismatch");
+    athad_status s = cuda_check(ctx, cudaMemcpy2DAsync(host, d.km * sizeof(double), ctx->f2d[f], d.pitch * sizeof(double),
+                                                       d.km * sizeof(double), (size_t)d.jm, cudaMemcpyDeviceToHost,
+                                                       ctx->stream), "download_2d");
+    if (s != ATHAD_OK) return s;
+    return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "download_2d sync");
+}
+
+athad_status athad_upload_profile(athad_ctx* ctx, athad_profile f, const double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NPROFILES) return fail(ctx, ATHAD_ERR_INVALID, "upload_profile: bad argument");
+    if (n != (size_t)ctx->grid.im) return fail(ctx, ATHAD_ERR_INVALID, "upload_profile: size mismatch");
+    return cuda_check(ctx, cudaMemcpyAsync(ctx->prof[f], host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                      "upload_profile");
+}
+
+athad_status athad_download_profile(athad_ctx* ctx, athad_profile f, double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NPROFILES) return fail(ctx, ATHAD_ERR_INVALID, "download_profile: bad argument");
+    if (n != (size_t)ctx->grid.im) return fail(ctx, ATHAD_ERR_INVALID, "download_profile: size mismatch");
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(host, ctx->prof[f], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                                     ctx->stream), "download_profile");
+    if (s != ATHAD_OK) return s;
+    return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "download_profile sync");
+}
+
+athad_status athad_field_device_ptr(athad_ctx* ctx, athad_field f, double** ptr, size_t* pitch)
+{
+    if (!ctx || !ptr || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "field_device_ptr: bad argument");
+    *ptr = ctx->field[f];
+    if (pitch) *pitch = (size_t)ctx->L.d.pitch;
+    return ATHAD_OK;
+}
+
+athad_status athad_fill(athad_ctx* ctx, athad_field f, double value)
+{
+    if (!ctx || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "fill: bad argument");
+    launch_fill(ctx->L.d, ctx->field[f], value, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "fill");
+    return ATHAD_OK;
+}
+
+// ---- hot path -----------------------------------------------------------------------------
+
+athad_status athad_store_n_level(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    const size_t bytes = ctx->L.field_elems * sizeof(double);
+    for (int n = 0; n < kNY; n++) {
+        athad_status s = cuda_check(ctx, cudaMemcpyAsync(ctx->field[ATHAD_TN + n], ctx->field[ATHAD_T + n], bytes,
+                                                         cudaMemcpyDeviceToDevice, ctx->stream), "store_n_level");
+        if (s != ATHAD_OK) return s;
+    }
+    return ATHAD_OK;
+}
+
+athad_status athad_level_mean(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    launch_level_mean(ctx->L.d, ctx->field[ATHAD_T], ctx->sin_w, ctx->prof[ATHAD_PROF_T_REF_LEVEL], ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "level_mean");
+    return ATHAD_OK;
+}
+
+athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
+{
+    if (!ctx || !s) return fail(ctx, ATHAD_ERR_INVALID, "rk4_step: bad argument");
+    const athad_params& p = ctx->p;
+    athad_status st = athad_level_mean(ctx);
+    if (st != ATHAD_OK) return st;
+    RK4Args a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    a.geo = ctx->geo;
+    a.t_ref = ctx->prof[ATHAD_PROF_T_REF_LEVEL];
+    a.dlnrho = ctx->prof[ATHAD_PROF_DLNRHO_DR];
+    for (int n = 0; n < kNY; n++) a.Yn[n] = ctx->field[ATHAD_TN + n];
+    for (int n = 0; n < kNY; n++) a.K[n] = ctx->stK[n];
+    a.p_dyn = ctx->field[ATHAD_P_DYN]; a.nue = ctx->field[ATHAD_NUE];
+    a.t_eq = ctx->field[ATHAD_T_EQ]; a.p_stat = ctx->field[ATHAD_P_STAT]; a.r_humid = ctx->field[ATHAD_R_HUMID];
+    a.S_c = ctx->field[ATHAD_S_C]; a.S_r = ctx->field[ATHAD_S_R]; a.S_i = ctx->field[ATHAD_S_I];
+    a.S_s = ctx->field[ATHAD_S_S]; a.S_g = ctx->field[ATHAD_S_G]; a.S_v = ctx->field[ATHAD_S_V];
+    a.MC_t = ctx->field[ATHAD_MC_T]; a.MC_q = ctx->field[ATHAD_MC_Q];
+    a.MC_v = ctx->field[ATHAD_MC_V]; a.MC_w = ctx->field[ATHAD_MC_W];
+    a.aux_u = ctx->field[ATHAD_AUX_U]; a.aux_v = ctx->field[ATHAD_AUX_V]; a.aux_w = ctx->field[ATHAD_AUX_W];
+    a.prod = ctx->field[ATHAD_PROD]; a.tke_source = ctx->field[ATHAD_TKE_SOURCE];
+    a.dis_source = ctx->field[ATHAD_DIS_SOURCE];
+    a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_2dthe = 1.0 / (2.0 * ctx->dthe); a.inv_2dphi = 1.0 / (2.0 * ctx->dphi);
+    a.inv_dr2 = 1.0 / (ctx->dr * ctx->dr); a.inv_dthe2 = 1.0 / (ctx->dthe * ctx->dthe);
+    a.inv_dphi2 = 1.0 / (ctx->dphi * ctx->dphi);
+    a.dt = s->dt; a.half_dt = 0.5 * s->dt; a.dt_sixth = s->dt / 6.0;
+    a.diffusion_ramp = s->diffusion_ramp; a.buoyancy_ramp = s->buoyancy_ramp;
+    a.tke_max_nd = 1000.0 / (p.u_0 * p.u_0);                   // RungeKutta_Atm_Turb.cpp:67-68
+    a.force_nd = p.omega * ctx->shell_len / p.u_0;              // RHS_Atm_Turb.cpp:445
+    a.coeff_energy_p = p.u_0 * p.u_0 / (p.cp_l * p.t_0);       // RHS_Atm_Turb.cpp:366-372
+    a.coeff_energy = 1.0 / (p.c_0 * p.cp_l * p.t_0);
+    a.coeff_MC_vel = p.L_atm / (p.u_0 * p.u_0);
+    a.coeff_MC_q = p.L_atm / (p.u_0 * p.c_0);
+    a.coeff_MC_t = p.L_atm / (p.u_0 * p.t_0);
+    a.lv = p.lv; a.ls = p.ls; a.g = p.g; a.u_0 = p.u_0; a.L_atm = p.L_atm; a.re_turb = p.re_turb;
+    a.pr_turb = p.pr_turb; a.sc_WaterVapour = p.sc_WaterVapour; a.sc_CO2 = p.sc_CO2;
+    a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
+    a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
+    a.write_diag = s->write_diagnostics;
+    for (int stage = 1; stage <= 4; stage++) {
+        for (int n = 0; n < kNY; n++) {
+            double* cur = ctx->field[ATHAD_T + n];
+            a.Yin[n] = (stage == 1) ? cur : (stage == 3) ? ctx->stB[n] : ctx->stA[n];
+            a.Yout[n] = (stage == 1 || stage == 3) ? ctx->stA[n] : (stage == 2) ? ctx->stB[n] : cur;
+            a.Ybnd[n] = ctx->stB[n];
+        }
+        launch_rk4_stage(stage, a, ctx->stream);
+        ATHAD_CHECK_LAUNCH(ctx, "rk4 stage");
+    }
+    return ATHAD_OK;
+}
+
+static PoissonArgs poisson_args(athad_ctx* ctx, int total_iter_count)
+{
+    PoissonArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    a.poi = ctx->poi;
+    a.dlnrho = ctx->prof[ATHAD_PROF_DLNRHO_DR];
+    a.aux_u = ctx->field[ATHAD_AUX_U]; a.aux_v = ctx->field[ATHAD_AUX_V]; a.aux_w = ctx->field[ATHAD_AUX_W];
+    a.src = ctx->src;
+    a.p = ctx->field[ATHAD_P_DYN];
+    a.counters = ctx->counters;
+    a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_2dthe = 1.0 / (2.0 * ctx->dthe); a.inv_2dphi = 1.0 / (2.0 * ctx->dphi);
+    a.anelastic = ctx->p.anelastic; a.metric_div = ctx->p.metric_divergence;
+    a.ceiling = (total_iter_count > 300) ? 3.0 : 10.0;          // PressureSolverAtm.h:583
+    return a;
+}
+
+athad_status athad_pressure_sweep(athad_ctx* ctx, int32_t n_sweeps, int32_t total_iter_count)
+{
+    if (!ctx || n_sweeps < 0) return fail(ctx, ATHAD_ERR_INVALID, "pressure_sweep: bad argument");
+    if (n_sweeps == 0) return ATHAD_OK;
+    PoissonArgs a = poisson_args(ctx, total_iter_count);
+    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), ctx->stream), "counters");
+    if (s != ATHAD_OK) return s;
+    launch_poisson_prepare(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "poisson prepare");
+    for (int i = 0; i < n_sweeps; i++) {
+        launch_poisson_sweep(a, ctx->stream);
+        ATHAD_CHECK_LAUNCH(ctx, "poisson sweep");
+    }
+    ctx->poisson_sweeps_since_reset = n_sweeps;
+    return ATHAD_OK;
+}
+
+athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps, int32_t total_iter_count)
+{
+    if (!ctx || n_sweeps < 0) return fail(ctx, ATHAD_ERR_INVALID, "project_initial_velocity: bad argument");
+    const size_t bytes = ctx->L.field_elems * sizeof(double);
+    athad_status s = ATHAD_OK;
+    for (int n = 0; n < 3 && s == ATHAD_OK; n++)               // PressureSolverAtm.h:694-704
+        s = cuda_check(ctx, cudaMemcpyAsync(ctx->field[ATHAD_AUX_U + n], ctx->field[ATHAD_U + n], bytes,
+                                            cudaMemcpyDeviceToDevice, ctx->stream), "project copy");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaMemsetAsync(ctx->field[ATHAD_P_DYN], 0, bytes, ctx->stream), "project zero");
+    if (s != ATHAD_OK) return s;
+    s = athad_pressure_sweep(ctx, n_sweeps, total_iter_count);
+    if (s != ATHAD_OK) return s;
+    PoissonArgs a = poisson_args(ctx, total_iter_count);
+    launch_project_correct(a, ctx->field[ATHAD_U], ctx->field[ATHAD_V], ctx->field[ATHAD_W], ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "project correct");
+    const int zero_fields[4] = {ATHAD_P_DYN, ATHAD_AUX_U, ATHAD_AUX_V, ATHAD_AUX_W};   // :752-762
+    for (int n = 0; n < 4 && s == ATHAD_OK; n++)
+        s = cuda_check(ctx, cudaMemsetAsync(ctx->field[zero_fields[n]], 0, bytes, ctx->stream), "project clear");
+    return s;
+}
+
+static ColumnArgs column_args(athad_ctx* ctx)
+{
+    ColumnArgs a;
+    std::memset(&a, 0, sizeof a);
+    const athad_params& p = ctx->p;
+    a.d = ctx->L.d;
+    a.height = ctx->height; a.step_f = ctx->step_f;
+    double** F = ctx->field;
+    a.t = F[ATHAD_T]; a.c = F[ATHAD_C]; a.cloud = F[ATHAD_CLOUD]; a.ice = F[ATHAD_ICE]; a.gr = F[ATHAD_GR];
+    a.co2 = F[ATHAD_CO2]; a.p_stat = F[ATHAD_P_STAT]; a.r_humid = F[ATHAD_R_HUMID]; a.r_dry = F[ATHAD_R_DRY];
+    a.S_c_c = F[ATHAD_S_C_C]; a.P_rain = F[ATHAD_P_RAIN]; a.P_snow = F[ATHAD_P_SNOW];
+    a.P_graupel = F[ATHAD_P_GRAUPEL]; a.Precipitation = F[ATHAD_PRECIPITATION];
+    a.S_v = F[ATHAD_S_V]; a.S_c = F[ATHAD_S_C]; a.S_i = F[ATHAD_S_I]; a.S_r = F[ATHAD_S_R];
+    a.S_s = F[ATHAD_S_S]; a.S_g = F[ATHAD_S_G];
+    a.t_top_init = ctx->f2d[ATHAD_2D_T_TOP_INIT]; a.p_stat_landscape = ctx->f2d[ATHAD_2D_P_STAT_LANDSCAPE];
+    a.rho_base = ctx->prof[ATHAD_PROF_RHO_BASE]; a.dlnrho = ctx->prof[ATHAD_PROF_DLNRHO_DR];
+    a.row_sum = ctx->row_sum; a.row_cnt = ctx->row_cnt; a.coslat = ctx->coslat;
+    a.counters = ctx->counters + 2;
+    a.t_0 = p.t_0; a.t_00 = p.t_00; a.t_max_phys = p.t_max_phys; a.cloud_cap = p.cloud_cap;
+    a.M_bg = p.M_bg; a.R_bg = p.R_bg; a.R_mix = p.R_mix; a.r_air = p.r_air; a.g = p.g; a.t_skin = p.t_skin;
+    a.c_h2o_dry_top = p.c_h2o_dry_top;
+    a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_dr = 1.0 / ctx->dr;
+    return a;
+}
+
+athad_status athad_saturation_adjust(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    ColumnArgs a = column_args(ctx);
+    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters + 2, 0, sizeof(unsigned long long), ctx->stream), "counters");
+    if (s != ATHAD_OK) return s;
+    launch_saturation_adjust(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "saturation_adjust");
+    return ATHAD_OK;
+}
+
+athad_status athad_densities(athad_ctx* ctx, int32_t set_water_profile)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    ColumnArgs a = column_args(ctx);
+    a.set_water_profile = set_water_profile ? 1 : 0;
+    launch_densities(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "densities");
+    return ATHAD_OK;
+}
+
+athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n)
+{
+    (void)iter_n;
+    return fail(ctx, ATHAD_ERR_UNSUPPORTED, "moist_convection: not built yet");
+}
+
+athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
+{
+    if (!ctx || !out) return fail(ctx, ATHAD_ERR_INVALID, "get_report: bad argument");
+    unsigned long long h[3] = {0, 0, 0};
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, ctx->stream), "report");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "report sync");
+    if (s != ATHAD_OK) return s;
+    std::memset(out, 0, sizeof *out);
+    out->poisson_src_cells = (int64_t)h[0] * ctx->poisson_sweeps_since_reset;
+    out->poisson_src_clamped = (int64_t)h[1] * ctx->poisson_sweeps_since_reset;
+    out->satadj_ceiling_hits = (int64_t)h[2];
+    return ATHAD_OK;
+}
+
+}  // extern "C"

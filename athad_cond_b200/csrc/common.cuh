@@ -1,0 +1,61 @@
+// common.cuh - device-side helpers shared by the sm_100a kernels of the ATHAD_COND
+// hot path: comparison helpers with the C++ standard library's exact semantics, the
+// IEEE non-finite test of lib/Utils.h:121-125, field addressing and the launch-time
+// constants every kernel receives by value.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/athad_gpu.h"
+
+#define ATHAD_HD __host__ __device__ __forceinline__
+
+namespace athad {
+
+// std::max / std::min / std::clamp exactly: (a < b) ? b : a etc.  fmax/fmin differ on NaN
+// and signed zero, and the reference's results depend on which operand survives.
+ATHAD_HD double smax(double a, double b) { return (a < b) ? b : a; }
+ATHAD_HD double smin(double a, double b) { return (b < a) ? b : a; }
+ATHAD_HD double sclamp(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
+
+ATHAD_HD bool is_finite_bits(double v)
+{
+#ifdef __CUDA_ARCH__
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+#else
+    unsigned long long b;
+    __builtin_memcpy(&b, &v, sizeof b);
+#endif
+    return (b & 0x7FF0000000000000ULL) != 0x7FF0000000000000ULL;
+}
+
+// safe_clamp of RungeKutta_Atm_Turb.cpp:76-81
+ATHAD_HD double safe_clamp(double v, double lo, double hi)
+{
+    if (!is_finite_bits(v)) return lo;
+    return (v < lo) ? lo : (v > hi) ? hi : v;
+}
+
+// Per-(i,j) metric factors of cAtmosphereModel::CellGeometry (cAtmosphereModel.h:170-178),
+// built on the host once per context exactly as RungeKutta_Atm_Turb.cpp:104-135 builds
+// them, with mirror-symmetric sin/cos tables.
+struct GeoIJ {
+    double exp_rm, exp_2_rm, sinthe, sinthe2, costhe;
+    double inv_rm, inv_rm2, inv_rmsinthe, inv_rm2sinthe, inv_rm2sinthe2, costhe_inv_rm2sinthe;
+};
+
+// Grid extents and the strides of a pitched field: element (i,j,k) is at
+// ((i*jm + j)*pitch + k).
+struct Dims {
+    int im, jm, km;
+    int pitch;            // row length in elements (>= km, multiple of 32)
+    long long plane;      // jm * pitch
+    long long fstride;    // im * jm * pitch: distance between consecutive fields
+};
+
+ATHAD_HD long long idx3(const Dims& d, int i, int j, int k)
+{
+    return ((long long)i * d.jm + j) * d.pitch + k;
+}
+
+}  // namespace athad

@@ -1,0 +1,295 @@
+// k_columns.cu - per-cell and per-column moist physics of the ATHAD_COND atmosphere on
+// sm_100a: SaturationAdjustment::run (SaturationAdjustment.h:25-459) and
+// ThermoAtm::densities (ThermoAtm.h:1436-1666), flat terrain.
+//
+// Both are FP64-pipe bound (IAPWS transcendentals inside a Newton iteration, a sequential
+// column ODE), so they run one thread per cell / per column with k on threadIdx.x for
+// coalesced access; the column reduction that builds rho_bar uses a fixed-order warp
+// reduction and pairs rows j and jm-1-j so it is deterministic and mirror-invariant.
+#include "kernels.cuh"
+#include "thermo.cuh"
+
+namespace athad {
+
+using namespace thermo;
+
+// IceSchemeCommon::evaporateWhereImpossible, IceSchemeCommon.h:121-190
+__device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, double t_u,
+                                           double& cv, double& cld, double& ic, double& T_nd)
+{
+    const double co2 = a.co2[c];
+    const double q_cond = smax(0.0, cld) + smax(0.0, ic) + smax(0.0, a.gr[c]);
+    if (q_cond > 0.0) {
+        const double c_max = smax(0.0, 1.0 - co2);
+        const double c_new = smin(c_max, cv + q_cond);
+        const double q_used = smax(0.0, c_new - cv);
+        cv = c_new;
+        cld = 0.0; ic = 0.0;
+        a.gr[c] = 0.0;
+        if (t_u < T_CRIT) {
+            const double cp_loc = cp_of(cv, co2, t_u, a.M_bg);
+            if (cp_loc > 0.0) {
+                double T_new = t_u - latent_heat(t_u) * q_used / cp_loc;
+                if (T_new < 1.0) T_new = 1.0;
+                T_nd = T_new / a.t_0;
+            }
+        }
+    }
+    {
+        const double rho = smax(1.0e-6, a.r_humid[c]);
+        const double q_p = smax(0.0, a.P_rain[c]) / (1.6 * rho)
+                         + smax(0.0, a.P_snow[c]) / (0.96 * rho)
+                         + smax(0.0, a.P_graupel[c]) / (2.0 * rho);
+        if (q_p > 0.0) {
+            const double c_max = smax(0.0, 1.0 - co2);
+            cv = smin(c_max, cv + q_p);
+        }
+    }
+    a.P_rain[c] = 0.0; a.P_snow[c] = 0.0; a.P_graupel[c] = 0.0; a.Precipitation[c] = 0.0;
+    a.S_v[c] = 0.0; a.S_c[c] = 0.0; a.S_i[c] = 0.0; a.S_r[c] = 0.0; a.S_s[c] = 0.0;
+    a.S_g[c] = 0.0; a.S_c_c[c] = 0.0;
+}
+
+// adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
+// Neither reads a neighbour, so the two passes of the reference fuse into one.
+__global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    bool hit = false;
+    if (k < d.km) {
+        const long long c = idx3(d, i, j, k);
+        double cv = a.c[c], cld = a.cloud[c], ic = a.ice[c], T_nd = a.t[c];
+        const double co2 = a.co2[c], p_local = a.p_stat[c];
+        const double inv_t_0 = 1.0 / a.t_0;
+        const double fade_K = 5.0;
+        double S_c_c = a.S_c_c[c];
+        if (i == 0) S_c_c = 0.0;
+        if (i >= 1 && i < d.im - 1) {
+            S_c_c = 0.0;
+            const double q_v_old = smax(0.0, cv), q_c_old = smax(0.0, cld), q_i_old = smax(0.0, ic);
+            double T = T_nd * a.t_0;
+            if (T < T_CRIT) {
+                const double t_range_inv = 1.0 / (a.t_0 - a.t_00);
+                const double dt_dim = a.step_f[i] / 1.6;
+                const double M_other = M_nonwater(cv, co2, a.M_bg);
+                const double q_sat0 = saturation_mass_fraction(saturation_pressure_auto(T), p_local, M_other);
+                const double alpha_entry = 1.0 / (1.0 + exp(-(T - a.t_00) / fade_K));
+                if ((q_v_old > q_sat0 && alpha_entry > 0.01) ||
+                    (q_v_old < q_sat0 && (q_c_old > 1e-12 || q_i_old > 1e-12))) {
+                    double q_v_b = q_v_old, q_c_b = q_c_old, q_i_b = q_i_old;
+                    double q_v_hyp = q_v_b;
+                    const double T_original = T_nd * a.t_0;
+                    for (int iter = 1; iter <= 20; iter++) {
+                        const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
+                        const double DEP = 1.0 - CND;
+                        double d_q_v = q_v_hyp - q_v_b;
+                        if (d_q_v > 0) {
+                            const double max_evap = q_c_b + q_i_b;
+                            if (d_q_v > max_evap) d_q_v = max_evap;
+                        }
+                        const double d_cnd = d_q_v * CND, d_dep = d_q_v * DEP;
+                        q_v_b += d_q_v;
+                        q_c_b = smax(0.0, q_c_b - d_cnd);
+                        q_i_b = smax(0.0, q_i_b - d_dep);
+                        const double cp_loc = cp_of(q_v_b, co2, T, a.M_bg);
+                        T -= (latent_heat(T) * d_cnd + latent_heat_sublimation(T) * d_dep) / cp_loc;
+                        const double E_sat = saturation_pressure(T);
+                        const double E_Ice = sublimation_pressure(T);
+                        const double q_sat = saturation_mass_fraction(E_sat, p_local, M_other);
+                        const double q_Ice = saturation_mass_fraction(E_Ice, p_local, M_other);
+                        const double q_sum = q_c_b + q_i_b;
+                        const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
+                                                                  : ((T >= a.t_0) ? q_sat : q_Ice);
+                        const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
+                        const double L_cnd = latent_heat(T);
+                        const double L_dep = latent_heat_sublimation(T);
+                        const double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other)
+                                          + DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
+                        const double omega = 1.0 / (1.0 + Gain);
+                        q_v_hyp = q_v_b + omega * (q_v_target - q_v_b);
+                        if (fabs(q_v_b / q_v_hyp - 1.0) <= 1.0e-6) break;
+                    }
+                    q_c_b = smax(0.0, q_c_b);
+                    q_i_b = smax(0.0, q_i_b);
+                    if (T > T_CRIT) T = T_CRIT;
+                    if (!isnan(T) && !isnan(q_v_b)) {
+                        S_c_c = alpha_entry * (q_c_b - q_c_old) / dt_dim;
+                        cv = q_v_old + alpha_entry * (q_v_b - q_v_old);
+                        cld = q_c_old + alpha_entry * (q_c_b - q_c_old);
+                        ic = q_i_old + alpha_entry * (q_i_b - q_i_old);
+                        T_nd = (T_original + alpha_entry * (T - T_original)) * inv_t_0;
+                    }
+                    if (T < a.t_00) { cld = 0.0; ic = 0.0; }
+                }
+            }
+        }
+        a.S_c_c[c] = S_c_c;
+        // ---- clampAndFade ----
+        if (cv < 0.0) cv = 0.0;
+        if (cld < 0.0) cld = 0.0;
+        if (ic < 0.0) ic = 0.0;
+        const double c_max = smax(0.0, 1.0 - co2);
+        if (cv > c_max) { cv = c_max; hit = true; }
+        double T_dim = T_nd * a.t_0;
+        if (T_dim > a.t_max_phys) { T_dim = a.t_max_phys; T_nd = a.t_max_phys * inv_t_0; }
+        const double M_o = M_nonwater(cv, co2, a.M_bg);
+        const double q_s = saturation_mass_fraction_at(T_dim, p_local, M_o);
+        if (T_dim >= T_CRIT || q_s >= 1.0) {
+            evaporate_where_impossible(a, c, T_dim, cv, cld, ic, T_nd);
+        } else {
+            const double q_sat = q_s;   // same arguments as the second evaluation (:419-423)
+            if (cv > q_sat) {
+                const double excess = cv - q_sat;
+                cv = q_sat;
+                if (T_dim >= a.t_00) {
+                    cld += excess;
+                    T_dim += latent_heat(T_dim) * excess / cp_of(cv, co2, T_dim, a.M_bg);
+                } else {
+                    ic += excess;
+                    T_dim += latent_heat_sublimation(T_dim) * excess / cp_of(cv, co2, T_dim, a.M_bg);
+                }
+                if (T_dim > a.t_max_phys) T_dim = a.t_max_phys;
+                T_nd = T_dim * inv_t_0;
+            }
+            if (cld > a.cloud_cap) cld = a.cloud_cap;
+            if (ic > a.cloud_cap) ic = a.cloud_cap;
+            const double alpha = 1.0 / (1.0 + exp(-(T_dim - a.t_00) / fade_K));
+            cv *= alpha; cld *= alpha; ic *= alpha;
+        }
+        a.c[c] = cv; a.cloud[c] = cld; a.ice[c] = ic; a.t[c] = T_nd;
+    }
+    const unsigned nh = __popc(__ballot_sync(0xffffffffu, hit));
+    if ((threadIdx.x & 31) == 0 && nh && a.counters) atomicAdd(a.counters, (unsigned long long)nh);
+}
+
+void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st)
+{
+    const dim3 block(128), grid((a.d.km + 127) / 128, a.d.jm, a.d.im);
+    saturation_adjust_kernel<<<grid, block, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------------------------------
+// densities: one thread per column, ThermoAtm.h:1484-1614
+__global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k >= d.km) return;
+    const double p_sl_factor = 1e-2 * a.r_air * a.R_mix;
+    double T_prev = smax(180.0, a.t[idx3(d, 0, j, k)] * a.t_0);
+    double p_prev = p_sl_factor * T_prev;
+    double q_sat_min = 1.0;
+    double q_v_p = 0.0, q_c_p = 0.0;   // c and co2 of level i-1 (after any rewrite)
+    for (int i = 0; i < d.im; i++) {
+        const long long c = idx3(d, i, j, k);
+        const double q_v = a.c[c];
+        const double q_c = a.co2[c];
+        const double R_loc = R_of(q_v, q_c, a.R_bg);
+        double T_i, p_i;
+        if (i == 0) {
+            T_i = T_prev; p_i = p_prev;
+        } else {
+            const double dz = a.height[i] - a.height[i - 1];
+            const double cp_loc = cp_of(q_v_p, q_c_p, T_prev, a.M_bg);
+            const double M_nw = M_nonwater(q_v_p, q_c_p, a.M_bg);
+            const double q_s = saturation_mass_fraction_at(T_prev, p_prev, M_nw);
+            const double gamma = (q_v_p >= 0.99 * q_s)
+                ? moist_lapse(T_prev, p_prev, M_nw, cp_loc, R_loc, a.g)
+                : a.g / cp_loc;
+            const double T_ad = T_prev - gamma * dz;
+            T_i = smax(a.t_skin, T_ad);
+            const double T_mean = 0.5 * (T_prev + T_i);
+            p_i = p_prev * exp(-a.g * dz / (R_loc * T_mean));
+        }
+        a.t[c] = T_i / a.t_0;
+        a.p_stat[c] = p_i;
+        double q_v_now = q_v;
+        if (a.set_water_profile && i > 0) {
+            const double M_nw_i = M_nonwater(q_v, q_c, a.M_bg);
+            const double q_s_i = saturation_mass_fraction_at(T_i, p_i, M_nw_i);
+            if (q_s_i < q_sat_min) q_sat_min = q_s_i;
+            q_v_now = smax(q_sat_min, a.c_h2o_dry_top);
+            a.c[c] = q_v_now;
+        }
+        const double water_factor = smax(0.5, 1.0 - a.cloud[c] - a.ice[c]);
+        a.r_humid[c] = 1e2 * p_i / (R_loc * T_i * water_factor);
+        const double R_dry_loc = R_of(0.0, q_c, a.R_bg);
+        a.r_dry[c] = 1e2 * p_i / (R_dry_loc * T_i);
+        T_prev = T_i; p_prev = p_i;
+        q_v_p = q_v_now; q_c_p = q_c;
+    }
+    const long long c2 = (long long)j * d.pitch + k;
+    a.t_top_init[c2] = a.t[idx3(d, d.im - 1, j, k)];
+    a.p_stat_landscape[c2] = a.p_stat[idx3(d, 0, j, k)];
+}
+
+// per-(i,j) row sums of the positive densities, fixed warp order (one warp per row)
+__global__ void __launch_bounds__(256) densities_rowsum_kernel(const ColumnArgs a)
+{
+    const Dims& d = a.d;
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= d.im * d.jm) return;
+    const int i = row / d.jm, j = row % d.jm;
+    const double* r = a.r_humid + idx3(d, i, j, 0);
+    double s = 0.0, q = 0.0;
+    for (int k = lane; k < d.km; k += 32) {
+        const double v = r[k];
+        if (v > 0.0) { s += v; q += 1.0; }
+    }
+    for (int off = 16; off >= 1; off >>= 1) {
+        s = s + __shfl_xor_sync(0xffffffffu, s, off);
+        q = q + __shfl_xor_sync(0xffffffffu, q, off);
+    }
+    if (lane == 0) { a.row_sum[row] = s; a.row_cnt[row] = q; }
+}
+
+// rho_bar(i) and its log-derivative, ThermoAtm.h:1629-1660; one thread per level
+__global__ void densities_profile_kernel(const ColumnArgs a)
+{
+    const Dims& d = a.d;
+    const int i = threadIdx.x;
+    if (i < d.im) {
+        double num = 0.0, den = 0.0;
+        for (int j = 0; j <= d.jm / 2; j++) {
+            const int jr = d.jm - 1 - j;
+            if (jr < j) break;
+            const double cl = a.coslat[j];
+            const double s0 = a.row_sum[i * d.jm + j], c0 = a.row_cnt[i * d.jm + j];
+            if (jr != j) {
+                num += cl * (s0 + a.row_sum[i * d.jm + jr]);
+                den += cl * (c0 + a.row_cnt[i * d.jm + jr]);
+            } else {
+                num += cl * s0;
+                den += cl * c0;
+            }
+        }
+        const double rb = (den > 0.0) ? num / den : 0.0;
+        a.rho_base[i] = rb;
+        a.row_sum[i * d.jm] = (rb > 0.0) ? log(rb) : 0.0;   // reuse as lnrho store
+    }
+    __syncthreads();
+    if (i < d.im) {
+        const double inv_2dr = a.inv_2dr, inv_dr = a.inv_dr;
+        double v = 0.0;
+        if (i >= 1 && i < d.im - 1) v = (a.row_sum[(i + 1) * d.jm] - a.row_sum[(i - 1) * d.jm]) * inv_2dr;
+        else if (i == 0 && d.im > 1) v = (a.row_sum[1 * d.jm] - a.row_sum[0]) * inv_dr;
+        else if (i == d.im - 1 && d.im > 1) v = (a.row_sum[(d.im - 1) * d.jm] - a.row_sum[(d.im - 2) * d.jm]) * inv_dr;
+        a.dlnrho[i] = v;
+    }
+}
+
+void launch_densities(const ColumnArgs& a, cudaStream_t st)
+{
+    const Dims& d = a.d;
+    densities_column_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
+    const int rows = d.im * d.jm;
+    densities_rowsum_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a);
+    densities_profile_kernel<<<1, ((d.im + 31) / 32) * 32, 0, st>>>(a);
+}
+
+}  // namespace athad

@@ -1,0 +1,212 @@
+// k_poisson.cu - pressure-Poisson relaxation of the ATHAD_COND atmosphere on sm_100a.
+//
+// Replaces PressureSolverAtm::run (PressureSolverAtm.h:27-594) for flat terrain, and the
+// gradient correction of PressureSolverAtm::project_initial_velocity (:713-749).
+//
+// The provisional velocity aux_u/v/w does not change while the pressure relaxes, so its
+// clamped divergence (the Poisson source) is formed once per call into a scratch field;
+// every red-black sweep then streams p and that source only.  Within one colour every
+// cell reads only cells of the other colour, so the in-place update is order-independent
+// and the result equals the serial red-black sweep bit for bit.
+#include "kernels.cuh"
+
+namespace athad {
+
+// aux radial boundary, PressureSolverAtm.h:106-121.  c43 and c13 are `const int` members
+// initialised from 4.0/3.0 and 1.0/3.0 (cAtmosphereModel.h:158): 1 and 0.
+__global__ void poisson_aux_bc_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1) return;
+    const long long c0 = idx3(d, 0, j, k), c1 = idx3(d, 1, j, k), c2 = idx3(d, 2, j, k);
+    const long long t0 = idx3(d, d.im - 1, j, k), t1 = idx3(d, d.im - 2, j, k), t2 = idx3(d, d.im - 3, j, k);
+    const double c43 = 1.0, c13 = 0.0;
+    if (a.anelastic) {
+        a.aux_u[c0] = 0.0;
+        a.aux_u[t0] = 0.0;
+    } else {
+        a.aux_u[c0] = c43 * a.aux_u[c1] - c13 * a.aux_u[c2];
+        a.aux_u[t0] = c43 * a.aux_u[t1] - c13 * a.aux_u[t2];
+    }
+    a.aux_v[c0] = c43 * a.aux_v[c1] - c13 * a.aux_v[c2];
+    a.aux_v[t0] = c43 * a.aux_v[t1] - c13 * a.aux_v[t2];
+    a.aux_w[c0] = c43 * a.aux_w[c1] - c13 * a.aux_w[c2];
+    a.aux_w[t0] = c43 * a.aux_w[t1] - c13 * a.aux_w[t2];
+}
+
+// clamped divergence source, PressureSolverAtm.h:415-473 (central differences)
+__global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    bool fluid = (k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1 && i >= 1 && i < d.im - 1);
+    bool clamped = false;
+    if (fluid) {
+        const long long c = idx3(d, i, j, k);
+        const PoiIJ P = a.poi[i * d.jm + j];
+        const long long sI = d.plane, sJ = d.pitch;
+        const double du_dr = (__ldg(a.aux_u + c + sI) - __ldg(a.aux_u + c - sI)) * a.inv_2dr;
+        const double dv_dthe = (__ldg(a.aux_v + c + sJ) - __ldg(a.aux_v + c - sJ)) * a.inv_2dthe;
+        const double dw_dphi = (__ldg(a.aux_w + c + 1) - __ldg(a.aux_w + c - 1)) * a.inv_2dphi;
+        double div_src = du_dr * P.exp_rm + dv_dthe * P.inv_rm + dw_dphi * P.inv_rmsinthe;
+        if (a.anelastic) div_src += __ldg(a.aux_u + c) * __ldg(a.dlnrho + i) * P.exp_rm;
+        if (a.metric_div)
+            div_src += (2.0 * __ldg(a.aux_u + c) + __ldg(a.aux_v + c) * P.costhe / P.sinthe) * P.inv_rm;
+        const double src_max = P.denom * 2.0;   // p_dyn_cap = 2 (:148)
+        if (!is_finite_bits(div_src)) div_src = 0.0;
+        else if (div_src > src_max) { div_src = src_max; clamped = true; }
+        else if (div_src < -src_max) { div_src = -src_max; clamped = true; }
+        a.src[c] = div_src;
+    }
+    // warp-aggregated counters
+    const unsigned nf = __popc(__ballot_sync(0xffffffffu, fluid));
+    const unsigned nc = __popc(__ballot_sync(0xffffffffu, clamped));
+    if ((threadIdx.x & 31) == 0 && a.counters) {
+        if (nf) atomicAdd(a.counters + 0, (unsigned long long)nf);
+        if (nc) atomicAdd(a.counters + 1, (unsigned long long)nc);
+    }
+}
+
+// one colour of the red-black sweep, PressureSolverAtm.h:225-486 (update :475-480)
+template <int COLOUR>
+__global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1) return;
+    if (((i + j + k) & 1) != COLOUR) return;
+    const long long c = idx3(d, i, j, k);
+    const PoiIJ P = a.poi[i * d.jm + j];
+    const long long sI = d.plane, sJ = d.pitch;
+    const double* p = a.p;
+    const double pip = p[c + sI], pim = p[c - sI];
+    const double num_a = a.anelastic ? P.exp_2_rm * __ldg(a.dlnrho + i) * a.inv_2dr : 0.0;
+    a.p[c] = ((pip + pim) * P.num1
+            + (p[c + sJ] + p[c - sJ]) * P.num2
+            + (p[c + 1] + p[c - 1]) * P.num3
+            + (pip - pim) * num_a
+            - __ldg(a.src + c)) * P.inv_denom;
+}
+
+// radial boundary (PressureSolverAtm.h:504-526): p[0] = 1*p[1] - 0*p[2], lid copy
+__global__ void poisson_bc_radial_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k >= d.km) return;
+    double* p = a.p;
+    p[idx3(d, 0, j, k)] = 1.0 * p[idx3(d, 1, j, k)] - 0.0 * p[idx3(d, 2, j, k)];
+    p[idx3(d, d.im - 1, j, k)] = p[idx3(d, d.im - 2, j, k)];
+}
+
+// pole copy (:535-541)
+__global__ void poisson_bc_pole_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (k >= d.km) return;
+    double* p = a.p;
+    p[idx3(d, i, 0, k)] = p[idx3(d, i, 1, k)];
+    p[idx3(d, i, d.jm - 1, k)] = p[idx3(d, i, d.jm - 2, k)];
+}
+
+// seam average (:544-552)
+__global__ void poisson_bc_seam_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= d.jm) return;
+    double* row = a.p + idx3(d, i, j, 0);
+    const double r0 = 1.0 * row[1] - 0.0 * row[2];
+    const double r1 = 1.0 * row[d.km - 2] - 0.0 * row[d.km - 3];
+    const double m = (r0 + r1) / 2.0;
+    row[0] = m;
+    row[d.km - 1] = m;
+}
+
+// |p_dyn| ceiling (:583-594); writes only where the value changes
+__global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.km || j >= d.jm) return;
+    const long long c = idx3(d, i, j, k);
+    const double v = a.p[c];
+    if (!is_finite_bits(v)) a.p[c] = 0.0;
+    else if (v > a.ceiling) a.p[c] = a.ceiling;
+    else if (v < -a.ceiling) a.p[c] = -a.ceiling;
+}
+
+void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st)
+{
+    const Dims& d = a.d;
+    poisson_aux_bc_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
+    const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
+    poisson_src_kernel<<<grid, block, 0, st>>>(a);
+}
+
+void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
+{
+    const Dims& d = a.d;
+    const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
+    poisson_colour_kernel<0><<<grid, block, 0, st>>>(a);
+    poisson_colour_kernel<1><<<grid, block, 0, st>>>(a);
+    poisson_bc_radial_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
+    poisson_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
+    poisson_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
+    poisson_ceiling_kernel<<<grid, block, 0, st>>>(a);
+}
+
+// gradient correction of project_initial_velocity, PressureSolverAtm.h:728-749
+__global__ void __launch_bounds__(256) project_correct_kernel(PoissonArgs a, double* u, double* v, double* w)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1) return;
+    const long long c = idx3(d, i, j, k);
+    const PoiIJ P = a.poi[i * d.jm + j];
+    const long long sI = d.plane, sJ = d.pitch;
+    const double* p = a.p;
+    const double dpdr = (p[c + sI] - p[c - sI]) * a.inv_2dr;
+    const double dpdthe = (p[c + sJ] - p[c - sJ]) * a.inv_2dthe;
+    const double dpdphi = (p[c + 1] - p[c - 1]) * a.inv_2dphi;
+    u[c] -= dpdr * P.exp_rm;
+    v[c] -= dpdthe * P.inv_rm;
+    w[c] -= dpdphi * P.inv_rmsinthe;
+}
+
+void launch_project_correct(const PoissonArgs& a, double* u, double* v, double* w, cudaStream_t st)
+{
+    const Dims& d = a.d;
+    const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
+    project_correct_kernel<<<grid, block, 0, st>>>(a, u, v, w);
+}
+
+// ---------------------------------------------------------------------------------------
+__global__ void fill_kernel(Dims d, double* dst, double v)
+{
+    const long long n = d.fstride;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x)
+        dst[q] = v;
+}
+
+void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st)
+{
+    fill_kernel<<<148 * 4, 256, 0, st>>>(d, dst, v);
+}
+
+}  // namespace athad

@@ -1,0 +1,396 @@
+// k_rk4.cu - RK4 time step of the ATHAD_COND atmosphere on sm_100a.
+//
+// Replaces cAtmosphereModel::solveRungeKutta_Atmosphere_Turb (RungeKutta_Atm_Turb.cpp:44-273)
+// and cAtmosphereModel::RHS_Atmosphere_Turb (RHS_Atm_Turb.cpp:31-1080) for flat terrain.
+//
+// Structure: one launch per RK4 stage, one thread per cell of the full grid, k (longitude)
+// on threadIdx.x so every field access of a warp is one coalesced 256-byte row segment;
+// the 7-point star stencil reads its i+-1 and j+-1 neighbours from rows that neighbouring
+// warps of the same CTA / plane also read, so they hit L1/L2 and DRAM sees each field about
+// once per stage.  Stage semantics are Jacobi (each stage reads the previous stage's state
+// everywhere); the accumulator K = k1 + 2 k2 + 2 k3 is formed in the reference's exact
+// summation order so the final combination rounds as RungeKutta_Atm_Turb.cpp:253-263 does.
+//
+// Mirror symmetry: every theta-direction expression is written so that row j and row
+// jm-1-j round identically (second differences sum the two neighbours first; the trig
+// tables are mirror-exact), and the level mean pairs rows j and jm-1-j.  The result of a
+// mirror-symmetric state is therefore bit-for-bit mirror symmetric.
+#include "kernels.cuh"
+
+namespace athad {
+
+// ---------------------------------------------------------------------------------------
+// computeLevelMeanTemperature (RungeKutta_Atm_Turb.cpp:24-41).  One CTA per level i.  Each
+// row sum is a 32-lane strided partial sum reduced by xor butterfly; rows j and jm-1-j are
+// added before weighting, so the mean of a mirrored field is identical.
+__global__ void __launch_bounds__(256) level_mean_kernel(Dims d, const double* __restrict__ t,
+                                                         const double* __restrict__ sin_w,
+                                                         double* __restrict__ out)
+{
+    extern __shared__ double rows[];   // [jm]
+    const int i = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int j = warp; j < d.jm; j += nwarp) {
+        const double* row = t + idx3(d, i, j, 0);
+        double s = 0.0;
+        for (int k = lane; k < d.km; k += 32) s += __ldg(row + k);
+        for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) rows[j] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0, wsum = 0.0;
+        const int half = d.jm / 2;
+        for (int j = 0; j < half; j++) {
+            sum += sin_w[j] * (rows[j] + rows[d.jm - 1 - j]);
+            wsum += 2.0 * sin_w[j] * (double)d.km;
+        }
+        if (d.jm & 1) {
+            sum += sin_w[half] * rows[half];
+            wsum += sin_w[half] * (double)d.km;
+        }
+        out[i] = (wsum > 0.0) ? sum / wsum : 1.0;
+    }
+}
+
+void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
+                       cudaStream_t st)
+{
+    level_mean_kernel<<<d.im, 256, sizeof(double) * d.jm, st>>>(d, t, sin_w, out);
+}
+
+// ---------------------------------------------------------------------------------------
+// minmod slope limiter, RHS_Atm_Turb.cpp:26-28
+__device__ __forceinline__ double minmod(double a, double b)
+{
+    return (a * b <= 0.0) ? 0.0 : (fabs(a) < fabs(b) ? a : b);
+}
+
+// Central derivatives of one field at one cell (RHS_Atm_Turb.cpp:121-123, 223-225, 327-329).
+struct Der {
+    double c;                       // centre value
+    double d1r, d2r, d1t, d2t, d1p, d2p;
+    double ar, at, ap;              // minmod-limited advective gradients
+};
+
+template <bool LIMIT>
+__device__ __forceinline__ Der derivs(const double* __restrict__ F, long long c, long long sI,
+                                      long long sJ, const RK4Args& a)
+{
+    const double f0 = __ldg(F + c);
+    const double fip = __ldg(F + c + sI), fim = __ldg(F + c - sI);
+    const double fjp = __ldg(F + c + sJ), fjm = __ldg(F + c - sJ);
+    const double fkp = __ldg(F + c + 1), fkm = __ldg(F + c - 1);
+    Der r;
+    r.c = f0;
+    r.d1r = (fip - fim) * a.inv_2dr;
+    r.d2r = (fip - 2.0 * f0 + fim) * a.inv_dr2;
+    r.d1t = (fjp - fjm) * a.inv_2dthe;
+    r.d2t = ((fjp + fjm) - 2.0 * f0) * a.inv_dthe2;     // mirror-exact form
+    r.d1p = (fkp - fkm) * a.inv_2dphi;
+    r.d2p = (fkp - 2.0 * f0 + fkm) * a.inv_dphi2;
+    if (LIMIT) {   // RHS_Atm_Turb.cpp:788-814; inv_dr = 2 * inv_2dr as in :762-764
+        r.ar = minmod(f0 - fim, fip - f0) * (2.0 * a.inv_2dr);
+        r.at = minmod(f0 - fjm, fjp - f0) * (2.0 * a.inv_2dthe);
+        r.ap = minmod(f0 - fkm, fkp - f0) * (2.0 * a.inv_2dphi);
+    } else {
+        r.ar = r.d1r; r.at = r.d1t; r.ap = r.d1p;
+    }
+    return r;
+}
+
+// Stage update of one field (RungeKutta_Atm_Turb.cpp:167-182, 199-209, 226-236, 253-263).
+// Field n: 0 t, 1 u, 2 v, 3 w, 4 c, 5 cloud, 6 ice, 7 gr, 8 co2, 9 tke, 10 dis.
+template <int STAGE>
+__device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long c, double kn)
+{
+    const double yn = __ldg(a.Yn[n] + c);
+    double kk, coef;
+    if (STAGE == 1) {
+        a.K[n][c] = kn;
+        kk = kn; coef = a.half_dt;
+    } else if (STAGE < 4) {
+        const double acc = a.K[n][c] + 2.0 * kn;
+        a.K[n][c] = acc;
+        kk = kn; coef = (STAGE == 3) ? a.dt : a.half_dt;
+    } else {
+        kk = a.K[n][c] + kn; coef = a.dt_sixth;
+    }
+    const double y = yn + kk * coef;
+    double out;
+    if (n >= 4 && n <= 7) out = smax(0.0, y);
+    else if (n == 9) out = safe_clamp(y, 0.0, a.tke_max_nd);
+    else if (n == 10) out = smax(1.0e-10, y);
+    else out = y;
+    a.Yout[n][c] = out;
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.km || j >= d.jm) return;
+    const long long c = idx3(d, i, j, k);
+    const bool interior = (i > 0 && i < d.im - 1 && j > 0 && j < d.jm - 1 && k > 0 && k < d.km - 1);
+    if (!interior) {
+        // Boundary cells are not integrated (the reference loops run over the interior);
+        // the stage buffers carry their current value so interior stencils can read them.
+        if (STAGE == 1) {
+#pragma unroll
+            for (int n = 0; n < 11; n++) {
+                const double v = __ldg(a.Yin[n] + c);
+                a.Yout[n][c] = v;
+                a.Ybnd[n][c] = v;
+            }
+        }
+        return;
+    }
+    const long long sI = d.plane, sJ = d.pitch;
+    const GeoIJ G = a.geo[i * d.jm + j];
+    const double exp_rm = G.exp_rm, exp_2_rm = G.exp_2_rm;
+    const double sinthe = G.sinthe, sinthe2 = G.sinthe2, costhe = G.costhe;
+    const double inv_rm = G.inv_rm, inv_rm2 = G.inv_rm2, inv_rmsinthe = G.inv_rmsinthe;
+    const double inv_rm2sinthe = G.inv_rm2sinthe, inv_rm2sinthe2 = G.inv_rm2sinthe2;
+    const double cos_rm2sin = G.costhe_inv_rm2sinthe;
+
+    // velocities
+    const Der U = derivs<true>(a.Yin[1], c, sI, sJ, a);
+    const Der V = derivs<true>(a.Yin[2], c, sI, sJ, a);
+    const Der W = derivs<true>(a.Yin[3], c, sI, sJ, a);
+    const double u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
+    // pressure gradient
+    const double* P = a.p_dyn;
+    const double dpdr = (__ldg(P + c + sI) - __ldg(P + c - sI)) * a.inv_2dr;
+    const double dpdthe = (__ldg(P + c + sJ) - __ldg(P + c - sJ)) * a.inv_2dthe;
+    const double dpdphi = (__ldg(P + c + 1) - __ldg(P + c - 1)) * a.inv_2dphi;
+    const double nue_ijk = __ldg(a.nue + c);
+
+    // ---- turbulence: production (RHS_Atm_Turb.cpp:528-561) ----
+    const Der TK = derivs<false>(a.Yin[9], c, sI, sJ, a);
+    const Der DI = derivs<false>(a.Yin[10], c, sI, sJ, a);
+    const double tke_ijk = TK.c, dis_ijk = DI.c;
+    double prod;
+    {
+        const double dudr_s = U.d1r * exp_rm, dvdr_s = V.d1r * exp_rm, dwdr_s = W.d1r * exp_rm;
+        const double dudthe_s = U.d1t * inv_rm, dvdthe_s = V.d1t * inv_rm, dwdthe_s = W.d1t * inv_rm;
+        const double dudphi_s = U.d1p * inv_rmsinthe, dvdphi_s = V.d1p * inv_rmsinthe,
+                     dwdphi_s = W.d1p * inv_rmsinthe;
+        const double dis_here = smax(dis_ijk, 1.0e-10);
+        const double tke_here = smax(tke_ijk, 0.0);
+        const double nue_max = 1000.0 / (a.u_0 * a.L_atm);
+        double cnue = (a.turb_model == ATHAD_TURB_K_EPSILON) ? 0.028 * tke_here * tke_here / dis_here
+                                                            : tke_here / dis_here;
+        cnue = smin(cnue, nue_max);
+        const double der = 0.66667 * (dudr_s + dvdthe_s + dwdphi_s);
+        prod = smax(0.0,
+              (cnue * (2.0 * dudr_s - der) - 0.66667 * tke_ijk) * dudr_s
+            + (cnue * (dudthe_s + dvdr_s)) * dudthe_s
+            + (cnue * (dudphi_s + dwdr_s)) * dudphi_s
+            + (cnue * (2.0 * dvdthe_s - der) - 0.66667 * tke_ijk) * dvdthe_s
+            + (cnue * (dvdr_s + dudthe_s)) * dvdr_s
+            + (cnue * (dvdphi_s + dwdthe_s)) * dvdphi_s
+            + (cnue * (2.0 * dwdphi_s - der) - 0.66667 * tke_ijk) * dwdphi_s
+            + (cnue * (dwdr_s + dudphi_s)) * dwdr_s
+            + (cnue * (dwdthe_s + dvdphi_s)) * dwdthe_s);
+    }
+    // ---- closures (RHS_Atm_Turb.cpp:563-721) ----
+    double diffusion_t_re, diffusion_vel_re, diffusion_tke_re, diffusion_dis_re;
+    double tke_source, dis_source;
+    {
+        const double inv_re = 1.0 / a.re_turb;
+        diffusion_t_re = (inv_re + nue_ijk) / a.pr_turb;
+        diffusion_vel_re = inv_re + nue_ijk;
+        const double tke_s = smax(tke_ijk, 1.0e-10), dis_s = smax(dis_ijk, 1.0e-10);
+        const double dis_src_max = 20.0 * dis_s * dis_s, tke_src_max = 20.0 * tke_s * dis_s;
+        if (a.turb_model == ATHAD_TURB_K_EPSILON) {
+            diffusion_tke_re = inv_re + nue_ijk / 1.0;
+            diffusion_dis_re = inv_re + nue_ijk / 1.3;
+            const double P_k = prod, Y_k = dis_s;
+            const double P_w = 1.35 * (dis_s / tke_s) * P_k;
+            const double Y_w = 1.80 * dis_s * dis_s / tke_s;
+            tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
+            dis_source = sclamp(P_w - Y_w, -dis_src_max, dis_src_max);
+        } else if (a.turb_model == ATHAD_TURB_K_OMEGA) {
+            diffusion_tke_re = inv_re + 0.6 * nue_ijk;
+            diffusion_dis_re = inv_re + 0.5 * nue_ijk;
+            const double P_k = smin(prod, 20.0 * 0.09 * tke_s * dis_s);
+            const double Y_k = 0.09 * tke_s * dis_s;
+            const double P_w = 0.52 * (dis_s / tke_s) * P_k;
+            const double Y_w = 0.0708 * dis_s * dis_s;
+            const double cross = TK.d1r * DI.d1r + TK.d1t * inv_rm * DI.d1t * inv_rm
+                               + TK.d1p * inv_rmsinthe * DI.d1p * inv_rmsinthe;
+            const double sig_d = (cross <= 0.0) ? 0.0 : 0.125;
+            const double D_w = sig_d * cross / dis_s;
+            tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
+            dis_source = sclamp(P_w - Y_w + D_w, -dis_src_max, dis_src_max);
+        } else {   // k-omega SST
+            const double bet_star = 0.09, sig_w2 = 1.168;
+            // wall distance, RHS_Atm_Turb.cpp:640-671 (flat terrain: min(i, j, k));
+            // ATHAD_WALL_MIRROR measures the meridional distance to the nearer pole
+            double d_j = (double)j;
+            if (a.wall_mode == ATHAD_WALL_MIRROR) { const int jr = d.jm - 1 - j; if (jr < j) d_j = (double)jr; }
+            const double d_k = (double)k;
+            double d_close = (double)i;
+            if (d_j <= d_close) d_close = d_j;
+            if (d_k <= d_close) d_close = d_k;
+            const double cross = TK.d1r * DI.d1r + TK.d1t * inv_rm * DI.d1t * inv_rm
+                               + TK.d1p * inv_rmsinthe * DI.d1p * inv_rmsinthe;
+            const double CD_kw = smax((2.0 * sig_w2) / dis_ijk * cross, 1.0e-20);
+            const double nue_air_nd = 1.5e-5 / (a.u_0 * a.L_atm);
+            const double arg1 = smin(smax(
+                sqrt(tke_ijk) / (bet_star * dis_ijk * d_close),
+                (500.0 * nue_air_nd) / (d_close * d_close * dis_ijk)),
+                (4.0 * sig_w2 * tke_ijk) / (CD_kw * d_close * d_close));
+            const double F1 = tanh(pow(arg1, 4.0));
+            const double bk = F1 * 1.176 + (1.0 - F1) * 1.0;
+            const double bw = F1 * 2.0 + (1.0 - F1) * sig_w2;
+            diffusion_tke_re = inv_re + nue_ijk / bk;
+            diffusion_dis_re = inv_re + nue_ijk / bw;
+            const double P_k = smin(prod, 20.0 * bet_star * tke_s * dis_s);
+            const double Y_k = bet_star * tke_s * dis_s;
+            const double P_w = (F1 * 0.413 + (1.0 - F1) * 0.2) * P_k * dis_s / tke_s;
+            const double Y_w = (F1 * 0.0333 + (1.0 - F1) * 0.0368) * dis_s * dis_s;
+            const double D_w = 2.0 * (1.0 - F1) * sig_w2 / dis_s * cross;
+            tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
+            dis_source = sclamp(P_w - Y_w + D_w, -dis_src_max, dis_src_max);
+        }
+        diffusion_t_re *= a.diffusion_ramp;
+        diffusion_vel_re *= a.diffusion_ramp;
+        diffusion_tke_re *= a.diffusion_ramp;
+        diffusion_dis_re *= a.diffusion_ramp;
+    }
+
+    // ---- transport / diffusion / assembly (RHS_Atm_Turb.cpp:748-1079) ----
+    const double u_exp = u_ijk * exp_rm, v_invrm = v_ijk * inv_rm, w_invrs = w_ijk * inv_rmsinthe;
+    const double two_over_rm_exp = 2.0 * inv_rm * exp_rm;
+    const double v_metric = (1.0 + costhe * costhe / sinthe2) * inv_rm2;
+    const double dpdr_exp = dpdr * exp_rm, dpdthe_invrm = dpdthe * inv_rm, dpdphi_invrs = dpdphi * inv_rmsinthe;
+    const double nontrad = a.nontrad ? 1.0 : 0.0;
+    const double coriolis_rad = nontrad * 2.0 * sinthe * w_ijk;
+    const double coriolis_the = 2.0 * costhe * w_ijk;
+    const double coriolis_phi = -2.0 * (costhe * v_ijk + nontrad * sinthe * u_ijk);
+    double tr_u = u_exp * U.ar + v_invrm * U.at + w_invrs * U.ap;
+    double tr_v = u_exp * V.ar + v_invrm * V.at + w_invrs * V.ap;
+    double tr_w = u_exp * W.ar + v_invrm * W.at + w_invrs * W.ap;
+    if (a.curvature) {
+        const double cotanthe = costhe / sinthe;
+        tr_u += -(v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
+        tr_v += (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
+        tr_w += (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
+    }
+    const double diffusion_u = (U.d2r * exp_2_rm + 2.0 * u_ijk * inv_rm2
+        + U.d2t * inv_rm2 + 4.0 * U.d1r * inv_rm * exp_rm
+        + U.d1t * cos_rm2sin + U.d2p * inv_rm2sinthe2) * diffusion_vel_re;
+    const double diffusion_v = (V.d2r * exp_2_rm + V.d1r * two_over_rm_exp
+        + V.d2t * inv_rm2 + V.d1t * cos_rm2sin
+        - v_metric * v_ijk + V.d2p * inv_rm2sinthe2
+        + 2.0 * U.d1t * inv_rm2
+        - W.d1p * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
+    const double diffusion_w = (W.d2r * exp_2_rm + W.d1r * two_over_rm_exp
+        + W.d2t * inv_rm2 + W.d1t * cos_rm2sin
+        - v_metric * w_ijk + W.d2p * inv_rm2sinthe2
+        + 2.0 * U.d1p * inv_rm2sinthe
+        + V.d1p * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
+
+    // temperature
+    const Der T = derivs<true>(a.Yin[0], c, sI, sJ, a);
+    const double t_ijk = T.c;
+    const double r_h = __ldg(a.r_humid + c);
+    const double rhs_u = -dpdr_exp - tr_u + diffusion_u
+        + a.buoyancy_ramp * 1.0 * a.g * a.dt / a.u_0 * (t_ijk - __ldg(a.t_ref + i))
+        + 1.0 * a.force_nd * coriolis_rad;
+    double drag_profile = 1.0 - (double)(i - 0) / 5.0;
+    if (drag_profile < 0.0) drag_profile = 0.0;
+    if (drag_profile > 1.0) drag_profile = 1.0;
+    const double surf_drag = (1.0 / 86400.0 * a.L_atm / a.u_0 * a.dt) * drag_profile;
+    const double rhs_v = -dpdthe_invrm - tr_v + diffusion_v
+        + 1.0 * a.force_nd * coriolis_the
+        + a.coeff_MC_vel * __ldg(a.MC_v + c)
+        - surf_drag * v_ijk;
+    const double rhs_w = -dpdphi_invrs - tr_w + diffusion_w
+        + 1.0 * a.force_nd * coriolis_phi
+        + a.coeff_MC_vel * __ldg(a.MC_w + c)
+        - surf_drag * w_ijk;
+    stage_update<STAGE>(a, 1, c, rhs_u);
+    stage_update<STAGE>(a, 2, c, rhs_v);
+    stage_update<STAGE>(a, 3, c, rhs_w);
+    if (STAGE == 4) {
+        a.aux_u[c] = rhs_u + dpdr_exp;
+        a.aux_v[c] = rhs_v + dpdthe_invrm;
+        a.aux_w[c] = rhs_w + dpdphi_invrs;
+        if (a.write_diag) {
+            a.prod[c] = prod;
+            a.tke_source[c] = tke_source;
+            a.dis_source[c] = dis_source;
+        }
+    }
+    {
+        const double pressure_t = a.coeff_energy_p * (u_exp * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
+        const double tr_t = u_exp * T.ar + v_invrm * T.at + w_invrs * T.ap;
+        const double diffusion_t = (T.d2r * exp_2_rm + T.d1r * two_over_rm_exp
+            + T.d2t * inv_rm2 + T.d1t * cos_rm2sin + T.d2p * inv_rm2sinthe2) * diffusion_t_re;
+        double rhs_t = pressure_t - tr_t + diffusion_t
+            + a.coeff_MC_t * __ldg(a.MC_t + c)
+            + a.coeff_energy * (__ldg(a.S_c + c) + __ldg(a.S_r + c)) * a.lv * r_h
+            + a.coeff_energy * (__ldg(a.S_i + c) + __ldg(a.S_s + c) + __ldg(a.S_g + c)) * a.ls * r_h;
+        // Held-Suarez relaxation, RHS_Atm_Turb.cpp:977-992
+        const double k_a = 1.0 / (4.0 * 86400.0), k_s = 1.0 / (0.4 * 86400.0), sigma_b = 0.7;
+        const double p_surf = __ldg(a.p_stat + idx3(d, 0, j, k));
+        const double sigma = (p_surf > 0.0) ? __ldg(a.p_stat + c) / p_surf : 0.0;
+        double bl = (sigma - sigma_b) / (1.0 - sigma_b);
+        if (bl < 0.0) bl = 0.0;
+        const double cos4lat = sinthe2 * sinthe2;
+        const double k_T = k_a + (k_s - k_a) * bl * cos4lat;
+        rhs_t -= (k_T * a.L_atm / a.u_0) * (t_ijk - __ldg(a.t_eq + c));
+        stage_update<STAGE>(a, 0, c, rhs_t);
+    }
+    // moisture and tracers (RHS_Atm_Turb.cpp:911-934, 1059-1072)
+    const double dlnrho_dr_i = a.tracer_diff_flux ? __ldg(a.dlnrho + i) * exp_2_rm : 0.0;
+    const double diff_prec_re_inv = 1.0 / (a.sc_WaterVapour * a.re_turb);
+    const double diff_co2_re_inv = 1.0 / (a.sc_CO2 * a.re_turb);
+#pragma unroll 1
+    for (int n = 4; n <= 8; n++) {
+        const Der Q = (n <= 6) ? derivs<true>(a.Yin[n], c, sI, sJ, a) : derivs<false>(a.Yin[n], c, sI, sJ, a);
+        const double coef = (n == 8) ? diff_co2_re_inv : diff_prec_re_inv;
+        const double tr = u_exp * Q.ar + v_invrm * Q.at + w_invrs * Q.ap;
+        const double dif = (Q.d2r * exp_2_rm + Q.d1r * two_over_rm_exp
+            + Q.d2t * inv_rm2 + Q.d1t * cos_rm2sin
+            + Q.d2p * inv_rm2sinthe2
+            + Q.d1r * dlnrho_dr_i) * coef;
+        double rhs;
+        if (n == 4)      rhs = -tr + dif + 1.0 * __ldg(a.S_v + c) * r_h + a.coeff_MC_q * __ldg(a.MC_q + c);
+        else if (n == 5) rhs = -tr + dif + 1.0 * __ldg(a.S_c + c) * r_h;
+        else if (n == 6) rhs = -tr + dif + 1.0 * __ldg(a.S_i + c) * r_h;
+        else if (n == 7) rhs = -tr + dif + 1.0 * __ldg(a.S_g + c) * r_h;
+        else             rhs = -tr + dif;
+        stage_update<STAGE>(a, n, c, rhs);
+    }
+    // tke and omega/epsilon (RHS_Atm_Turb.cpp:936-942, 1074-1075)
+    {
+        const double tr_tke = u_exp * TK.d1r + v_invrm * TK.d1t + w_invrs * TK.d1p;
+        const double tr_dis = u_exp * DI.d1r + v_invrm * DI.d1t + w_invrs * DI.d1p;
+        const double diffusion_tke = (TK.d2r * exp_2_rm + TK.d1r * two_over_rm_exp
+            + TK.d2t * inv_rm2 + TK.d1t * cos_rm2sin + TK.d2p * inv_rm2sinthe2) * diffusion_tke_re;
+        const double diffusion_dis = (DI.d2r * exp_2_rm + DI.d1r * two_over_rm_exp
+            + DI.d2t * inv_rm2 + DI.d1t * cos_rm2sin + DI.d2p * inv_rm2sinthe2) * diffusion_dis_re;
+        stage_update<STAGE>(a, 9, c, -tr_tke + diffusion_tke + tke_source);
+        stage_update<STAGE>(a, 10, c, -tr_dis + diffusion_dis + dis_source);
+    }
+}
+
+void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((a.d.km + 31) / 32, (a.d.jm + 3) / 4, a.d.im);
+    switch (stage) {
+        case 1: rk4_stage_kernel<1><<<grid, block, 0, st>>>(a); break;
+        case 2: rk4_stage_kernel<2><<<grid, block, 0, st>>>(a); break;
+        case 3: rk4_stage_kernel<3><<<grid, block, 0, st>>>(a); break;
+        default: rk4_stage_kernel<4><<<grid, block, 0, st>>>(a); break;
+    }
+}
+
+}  // namespace athad

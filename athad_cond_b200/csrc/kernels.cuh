@@ -1,0 +1,88 @@
+// kernels.cuh - launch interface of the sm_100a kernels of the ATHAD_COND hot path.
+// Every launcher issues on the given stream and returns without synchronising.
+#pragma once
+
+#include "common.cuh"
+
+namespace athad {
+
+// Argument block of the RK4 stage kernels.  Field pointers are pitched device arrays.
+struct RK4Args {
+    Dims d;
+    const GeoIJ* geo;          // [im*jm]
+    const double* t_ref;       // [im]   level-mean temperature
+    const double* dlnrho;      // [im]   d ln rho_bar / d rad.z
+    const double* Yin[11];     // stage state read (stencil)
+    double*       Yout[11];    // stage state written
+    const double* Yn[11];      // time level n
+    double*       K[11];       // RK4 accumulator k1 + 2 k2 + 2 k3
+    double*       Ybnd[11];    // stage 1 only: second stage buffer that receives the boundary
+    const double* p_dyn;
+    const double* nue;
+    const double* t_eq;
+    const double* p_stat;
+    const double* r_humid;
+    const double* S_c; const double* S_r; const double* S_i; const double* S_s;
+    const double* S_g; const double* S_v;
+    const double* MC_t; const double* MC_q; const double* MC_v; const double* MC_w;
+    double* aux_u; double* aux_v; double* aux_w;
+    double* prod; double* tke_source; double* dis_source;
+    // constants
+    double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
+    double dt, half_dt, dt_sixth, diffusion_ramp, buoyancy_ramp, tke_max_nd, force_nd;
+    double coeff_energy_p, coeff_energy, coeff_MC_vel, coeff_MC_q, coeff_MC_t;
+    double lv, ls, g, u_0, L_atm, re_turb, pr_turb, sc_WaterVapour, sc_CO2;
+    int turb_model, wall_mode, nontrad, curvature, tracer_diff_flux, write_diag;
+};
+
+void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
+                       cudaStream_t st);
+void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st);
+
+// Per-(i,j) coefficients of the 7-point Poisson operator, PressureSolverAtm.h:236-269,
+// computed on the host once per context.
+struct PoiIJ {
+    double denom, inv_denom, num1, num2, num3;
+    double exp_rm, exp_2_rm, inv_rm, inv_rmsinthe, sinthe, costhe;
+};
+
+struct PoissonArgs {
+    Dims d;
+    const PoiIJ* poi;           // [im*jm]
+    const double* dlnrho;       // [im] (anelastic)
+    double* aux_u; double* aux_v; double* aux_w;
+    double* src;                // clamped divergence source (scratch field)
+    double* p;
+    unsigned long long* counters;   // [2] fluid cells, clamped sources
+    double inv_2dr, inv_2dthe, inv_2dphi;
+    int anelastic, metric_div;
+    double ceiling;
+};
+void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st);   // aux BC + source
+void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st);     // colours + BCs + ceiling
+void launch_project_correct(const PoissonArgs& a, double* u, double* v, double* w, cudaStream_t st);
+
+// Column physics
+struct ColumnArgs {
+    Dims d;
+    const double* height;      // [im] layer heights (float-rounded, as the reference)
+    const double* step_f;      // [im] SaturationAdjustment step (float difference)
+    double* t; double* c; double* cloud; double* ice; double* gr; double* co2;
+    double* p_stat; double* r_humid; double* r_dry;
+    double* S_c_c; double* P_rain; double* P_snow; double* P_graupel; double* Precipitation;
+    double* S_v; double* S_c; double* S_i; double* S_r; double* S_s; double* S_g;
+    double* t_top_init; double* p_stat_landscape;   // 2-D, pitched rows [jm][pitch]
+    double* rho_base; double* dlnrho;               // [im]
+    double* row_sum; double* row_cnt;               // scratch [im*jm]
+    const double* coslat;                           // [jm] mirror-symmetric weights
+    unsigned long long* counters;
+    double t_0, t_00, t_max_phys, cloud_cap, M_bg, R_bg, R_mix, r_air, g, t_skin, c_h2o_dry_top;
+    double inv_2dr, inv_dr;
+    int set_water_profile;
+};
+void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st);
+void launch_densities(const ColumnArgs& a, cudaStream_t st);
+
+void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st);
+
+}  // namespace athad

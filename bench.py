@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the ATHAD_COND model-iteration hot path on B200.
+
+One step = one model iteration of cAtmosphereModel::run_3D_loop restricted to the hot path,
+at the reference cadence (cAtmosphereModel.cpp:1156-1509): the RK4 step every iteration, one
+pressure-Poisson sweep every 4th, saturation adjustment, moist convection and the column
+densities every 2nd, and the time-level copy (storeIntermediateData3D) that closes it.
+Metric: grid-point RK4 steps per second = im*jm*km * steps / time.
+
+Workload: the 41 x 181 x 361 grid of the reference's second configuration (plain FP64), a
+seeded synthetic state with the reference's shapes and value ranges.  The inputs (about
+40 fields of 21 MB) are far larger than the 126 MB L2, so no flush is needed between steps.
+
+--gpus N > 1 (under torchrun): independent replicas, one per GPU (the path has no
+cross-replica exchange), weak scaling; value = all ranks' grid-point steps / max time.
+--impl reference: the reference's CPU path timed on the host cores (see cpu_reference()).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = (41, 181, 361)
+# fields the reference's off-path modules (boundary conditions, filters, turbulence, ice
+# scheme, radiation) write between hot-path calls: uploaded every step in the end-to-end
+# measurement; and the fields they read back afterwards.
+E2E_UP = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "nue",
+          "S_c", "S_r", "S_i", "S_s", "S_g", "S_v", "t_eq"]
+E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "p_dyn"]
+# algorithmic FP64 fields moved per grid point by one RK4 step (level mean: 1 read; stage 1:
+# 37 reads + 22 writes; stages 2-3: 48 + 22; stage 4: 48 + 14)
+RK4_FIELDS_PER_POINT = 1 + 59 + 70 + 70 + 62
+
+
+def iteration(g, it: int, dt: float):
+    """One model iteration at the reference cadence."""
+    if it % 4 == 0:
+        g.PressureSolverAtm_run(total_iter_count=it)
+    if it % 2 == 0:
+        g.SaturationAdjustment_run()
+        g.densities()
+    g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0))
+    g.storeIntermediateData3D()
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(seconds_budget: float = 20.0):
+    """The oracle (single-threaded C restatement of the reference path) on a bounded
+    sample: whole model iterations of the same grid until the budget is used."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from athad_cond_b200 import make_state
+    from athad_cond_b200._abi import config_params
+    from oracle_binding import OracleState
+    im, jm, km = GRID
+    o = OracleState(make_state(im, jm, km, seed=20261203), config_params())
+    t0 = time.perf_counter()
+    it = 0
+    while True:
+        it += 1
+        if it % 4 == 0:
+            o.pressure_sweep(1, it)
+        if it % 2 == 0:
+            o.saturation_adjust()
+            o.densities()
+        o.rk4(dt=4e-5, buoyancy_ramp=min(1.0, it / 300.0))
+        o.store_n_level()
+        el = time.perf_counter() - t0
+        if el >= seconds_budget or it >= 8:
+            break
+    val = im * jm * km * it / el
+    return {"value": val, "unit": "grid-point RK4 steps/s", "cores": 1, "kind": "port",
+            "sample": f"{it} model iterations of {im}x{jm}x{km} through the C oracle "
+                      f"(-O2, 1 thread), {el:.1f} s"}
+
+
+def reference_arm(args):
+    """The reference's CPU path for the same metric and grid.  Until the reference itself
+    is built (it supports only its compiled-in 61x181x361 grid), this times the C
+    restatement of it (the oracle) on a bounded sample of each step."""
+    b = cpu_baseline(seconds_budget=20.0)
+    im, jm, km = GRID
+    return {"impl": "reference", "metric": "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)",
+            "value": b["value"], "unit": b["unit"], "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"plain FP64 model iteration, {im}x{jm}x{km} grid", "grid": [im, jm, km]},
+            "cpu_baseline": b,
+            "e2e": {"value": b["value"], "unit": b["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_ours(args, rank, world, device):
+    import numpy as np
+    import torch
+    from athad_cond_b200 import GpuAtmosphere, make_state
+    from athad_cond_b200._abi import config_params
+
+    im, jm, km = GRID
+    pts = im * jm * km
+    p = config_params()
+    st = make_state(im, jm, km, seed=20261203 + rank)
+    g = GpuAtmosphere(im, jm, km, p)
+    g.upload_state(st)
+    stream = torch.cuda.Stream(device=device)
+    g.set_stream(stream.cuda_stream)
+    dt = 4e-5
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        iteration(g, it, dt)
+    g.synchronize()
+    # ---- device-timed region ----
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    rk_ev = []
+    with ClockSampler(device.index if device.index is not None else 0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            it += 1
+            if it % 4 == 0:
+                g.PressureSolverAtm_run(total_iter_count=it)
+            if it % 2 == 0:
+                g.SaturationAdjustment_run()
+                g.densities()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0))
+            b.record(stream)
+            rk_ev.append((a, b))
+            g.storeIntermediateData3D()
+        ev1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
+    rk_ms = [a.elapsed_time(b) for a, b in rk_ev]
+    if dist:
+        tdist.barrier()
+        t = torch.tensor([ms], device=device)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- end to end through the C ABI with host buffers ----
+    host_up = {n: torch.from_numpy(st[n]).pin_memory() for n in E2E_UP}
+    host_down = {n: torch.empty(GRID, dtype=torch.float64).pin_memory() for n in E2E_DOWN}
+    lib = g.lib
+    from athad_cond_b200._abi import FIELD
+    e2e_steps = max(4, min(args.steps, 40))
+    g.synchronize()
+    if dist:
+        tdist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        it += 1
+        for n in E2E_UP:
+            h = host_up[n]
+            lib.athad_upload(g._h, FIELD[n], ctypes.cast(h.data_ptr(), ctypes.POINTER(ctypes.c_double)), h.numel())
+        iteration(g, it, dt)
+        for n in E2E_DOWN:
+            h = host_down[n]
+            lib.athad_download(g._h, FIELD[n], ctypes.cast(h.data_ptr(), ctypes.POINTER(ctypes.c_double)), h.numel())
+    e1.record(stream)
+    stream.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=device)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    ok = all(np.isfinite(host_down[n].numpy()).all() for n in ("t", "u", "p_dyn"))
+    g.close()
+    peak, peak_kind = measured_peaks()
+    rk_avg = sum(rk_ms) / len(rk_ms)
+    alg_bytes = RK4_FIELDS_PER_POINT * 8.0 * pts
+    achieved = alg_bytes / (rk_avg * 1e-3) / 1e9
+    res = {
+        "value": pts * args.steps * world / (ms * 1e-3),
+        "ms_per_step": ms / args.steps,
+        "e2e_value": pts * e2e_steps * world / (e2e_ms * 1e-3),
+        "h2d": 8 * pts * len(E2E_UP), "d2h": 8 * pts * len(E2E_DOWN),
+        "rk4_ms": rk_avg, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+        "clocks": clk.summary(), "finite": ok,
+        "launches_per_step": None,
+    }
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    im, jm, km = GRID
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        line = reference_arm(args)
+        print(json.dumps(line))
+        return
+
+    import torch
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=device)
+    r = run_ours(args, rank, world, device)
+    base = cpu_baseline() if (rank == 0 and world == 1) else None
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank != 0:
+        return
+    # kernel launches per step of our own kernels, averaged over the cadence cycle:
+    # RK4 = level mean + 4 stages; pressure = aux BC + source + 2 colours + 3 BCs + ceiling;
+    # saturation adjustment 1; densities 3
+    launches = args.steps * 5 + (args.steps // 4) * 8 + (args.steps // 2) * 4
+    line = {
+        "metric": "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)",
+        "value": r["value"], "unit": "grid-point steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plain FP64 model iteration, {im}x{jm}x{km} grid "
+                               "(RK4 every step, pressure sweep every 4th, saturation adjustment "
+                               "and densities every 2nd)",
+                   "grid": [im, jm, km], "points": im * jm * km,
+                   "l2": "inputs larger than L2 (about 40 fields x 21 MB per step), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": r["e2e_value"], "unit": "grid-point steps/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
+                     "frac": r["achieved"] / r["peak"], "traffic": None,
+                     "kernel": "rk4 step (level mean + 4 stage launches)",
+                     "peak_source": r["peak_kind"]},
+        "cpu_baseline": base,
+        "gpu_launches": launches,
+        "clocks": r["clocks"],
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+/*
+ * athad_gpu.h - C ABI of the B200 (sm_100a) implementation of the ATHAD_COND model
+ * iteration hot path.
+ *
+ * The reference has no plugin or FFI interface for this path: the physics classes are
+ * friends of cAtmosphereModel that mutate its public Array members in place
+ * (atmosphere/cAtmosphereModel.h:52-67, 536-662).  Each entry point below replaces one
+ * of those in-place calls; the reference call site it stands in for is cited beside it.
+ *
+ * Conventions
+ *   - Host buffers are caller-owned, packed FP64, (i, j, k) order with k (longitude)
+ *     fastest: exactly the element order of the reference's Array::x[i][j][k] rows
+ *     (lib/Array.cpp:62-71).  n = im*jm*km for 3-D fields.
+ *   - Device state is owned by the context and stays resident between calls; a caller
+ *     only uploads what changed on the host and downloads what it needs to read.
+ *   - Every call returns an athad_status; nothing throws across the ABI.  A failing
+ *     call leaves a message readable with athad_last_error().
+ *   - One host thread per context.  All work of a context is issued on one CUDA stream
+ *     (its own, or the one given to athad_set_stream), so calls are ordered.
+ *   - Terrain is flat (no land cells, i_topography == 0), which is the configuration
+ *     the reference runs (cli/config_cond.xml, InitValues_Atm.cpp init_topography).
+ */
+#ifndef ATHAD_GPU_H
+#define ATHAD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATHAD_ABI_VERSION 1
+
+typedef enum athad_status {
+    ATHAD_OK              = 0,
+    ATHAD_ERR_INVALID     = 1,  /* bad argument (null pointer, size mismatch, bad id)  */
+    ATHAD_ERR_CUDA        = 2,  /* a CUDA runtime call failed                          */
+    ATHAD_ERR_UNSUPPORTED = 3,  /* a configuration this build does not implement       */
+    ATHAD_ERR_OOM         = 4,  /* device allocation failed / budget exceeded          */
+    ATHAD_ERR_NONFINITE   = 5,  /* a kernel's status word reported non-finite input    */
+    ATHAD_ERR_TIMEOUT     = 6,  /* a bounded device-side wait gave up                  */
+    ATHAD_ERR_NO_DEVICE   = 7   /* no CUDA device, or not an sm_100 device             */
+} athad_status;
+
+/* Grid: im radial levels, jm colatitude rows (pole to pole, both poles stored),
+ * km longitudes (both seam meridians stored).  cAtmosphereModel.h:162 fixes these at
+ * 61 x 181 x 361; here they are run-time values (dr = 1/(im-1), dtheta = pi/(jm-1),
+ * dphi = 2 pi/(km-1), the generalisation of cAtmosphereModel.cpp:46-60). */
+typedef struct athad_grid {
+    int32_t im, jm, km;
+} athad_grid;
+
+/* Turbulence closures of RHS_Atm_Turb.cpp:563-721 (turb_model in the XML). */
+typedef enum athad_turb_model {
+    ATHAD_TURB_K_EPSILON   = 1,
+    ATHAD_TURB_K_OMEGA     = 2,
+    ATHAD_TURB_K_OMEGA_SST = 3
+} athad_turb_model;
+
+/* Wall distance of the k-omega-SST blending function (RHS_Atm_Turb.cpp:640-671).
+ * With flat terrain the reference's scan reduces to d = min(i, j, k): it measures the
+ * meridional distance from the NORTH pole only, which breaks north-south mirror
+ * symmetry by construction.  MIRROR measures it from the nearer pole,
+ * min(i, min(j, jm-1-j), k), and is the default; REFERENCE reproduces the reference. */
+typedef enum athad_wall_mode {
+    ATHAD_WALL_MIRROR    = 0,
+    ATHAD_WALL_REFERENCE = 1
+} athad_wall_mode;
+
+/* Model constants and switches.  Every double is the cAtmosphereModel member of the
+ * same name (atmosphere/AtmosphereParams.h.inc, values from cli/config_cond.xml) unless
+ * noted.  athad_default_params() fills the values of cli/config_cond.xml. */
+typedef struct athad_params {
+    uint32_t struct_size;        /* sizeof(athad_params), checked by athad_create     */
+    int32_t  turb_model;         /* athad_turb_model                                  */
+    int32_t  wall_mode;          /* athad_wall_mode                                   */
+    int32_t  poisson_metric_fix; /* ATM_POISSON_METRIC_FIX, default 1 (PressureSolverAtm.h:173) */
+    int32_t  anelastic;          /* ATM_ANELASTIC, default 0 (PressureSolverAtm.h:92)  */
+    int32_t  tracer_diff_flux;   /* ATM_TRACER_DIFF_FLUX, default 0 (RHS_Atm_Turb.cpp:906) */
+    int32_t  coriolis_nontrad;   /* ATOM_CORIOLIS_NONTRAD, default 0 (lib/Utils.h:54)  */
+    int32_t  metric_curvature;   /* ATOM_METRIC_CURVATURE, default 0 (lib/Utils.h:92)  */
+    int32_t  metric_divergence;  /* ATOM_METRIC_DIVERGENCE, default 0 (lib/Utils.h:98) */
+    int32_t  convection_perturbation; /* XML, 1 */
+    int32_t  convection_mode;    /* XML, 1 */
+    int32_t  iter_prec;          /* XML, 3 */
+    int32_t  pad0;
+    /* metric radius in rad.z units; 0 = off.  The reference default (ATM_METRIC_RADIUS
+     * unset) is r_Earth*1e3/metricShellLength() (cAtmosphereModel.cpp:382-399); the
+     * value 0 reproduces ATM_METRIC_RADIUS=0. */
+    double metric_r0;
+    double re_turb;              /* TurbulenceAtm.h:35: 0.4 * 0.1 / 1.5e-5            */
+    double r_air, g, u_0, cp_l, t_0, c_0, L_atm, zeta, omega, lamda, lv, ls;
+    double pr_turb, sc_WaterVapour, sc_CO2;
+    double r_Earth, p_0, t_00, t_max_phys, cloud_cap, t_skin, c_h2o_dry_top, co2_0, s_0;
+    double R_Air, R_WaterVapour;
+    /* composition resolved from the configured mole fractions, AtmMixture::resolve
+     * (MixtureAtm.h:82-109), i.e. cAtmosphereModel::m_comp */
+    double M_bg, R_bg, R_mix;
+} athad_params;
+
+/* 3-D fields, one per cAtmosphereModel Array member of the same name. */
+typedef enum athad_field {
+    /* prognostic state (current level) */
+    ATHAD_T = 0, ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_C, ATHAD_CLOUD, ATHAD_ICE, ATHAD_GR,
+    ATHAD_CO2, ATHAD_TKE, ATHAD_DIS,
+    /* time level n (storeIntermediateData3D, UtilsAtm.h:25-49) */
+    ATHAD_TN, ATHAD_UN, ATHAD_VN, ATHAD_WN, ATHAD_CN, ATHAD_CLOUDN, ATHAD_ICEN, ATHAD_GRN,
+    ATHAD_CO2N, ATHAD_TKEN, ATHAD_DISN,
+    /* inputs of the right-hand side */
+    ATHAD_P_DYN, ATHAD_NUE, ATHAD_T_EQ, ATHAD_P_STAT, ATHAD_R_HUMID,
+    ATHAD_S_C, ATHAD_S_R, ATHAD_S_I, ATHAD_S_S, ATHAD_S_G, ATHAD_S_V,
+    ATHAD_MC_T, ATHAD_MC_Q, ATHAD_MC_V, ATHAD_MC_W,
+    /* provisional velocity (RHS_Atm_Turb.cpp:1077-1079), source of the Poisson solve */
+    ATHAD_AUX_U, ATHAD_AUX_V, ATHAD_AUX_W,
+    /* turbulence diagnostics written by the last RK4 stage (RHS_Atm_Turb.cpp:551, 628) */
+    ATHAD_PROD, ATHAD_TKE_SOURCE, ATHAD_DIS_SOURCE,
+    /* saturation adjustment / microphysics fields (SaturationAdjustment.h,
+     * IceSchemeCommon.h:121-190) */
+    ATHAD_S_C_C, ATHAD_P_RAIN, ATHAD_P_SNOW, ATHAD_P_GRAUPEL, ATHAD_PRECIPITATION,
+    /* densities (ThermoAtm.h:1436-1666) */
+    ATHAD_R_DRY,
+    /* moist convection (MoistConvection.h) */
+    ATHAD_MC_S, ATHAD_MC_S_U, ATHAD_MC_S_D, ATHAD_M_U, ATHAD_M_D,
+    ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_Q_V_D,
+    ATHAD_U_U, ATHAD_V_U, ATHAD_W_U, ATHAD_U_D, ATHAD_V_D, ATHAD_W_D,
+    ATHAD_E_U, ATHAD_D_U, ATHAD_E_D, ATHAD_D_D,
+    ATHAD_C_U, ATHAD_E_L, ATHAD_E_DD, ATHAD_E_P, ATHAD_G_P,
+    ATHAD_P_CONV, ATHAD_CLOUD_BASE, ATHAD_LEVEL_FREE_SINKING, ATHAD_DEEP_BEG, ATHAD_DEEP_END,
+    ATHAD_NFIELDS
+} athad_field;
+
+/* 2-D (jm x km) fields. */
+typedef enum athad_field2d {
+    ATHAD_2D_T_TOP_INIT = 0,        /* cAtmosphereModel::t_top_init                  */
+    ATHAD_2D_P_STAT_LANDSCAPE,      /* Array_2D p_stat_landscape                      */
+    ATHAD_2D_EVAPORATION,           /* Array_2D Evaporation (MoistConvection input)   */
+    ATHAD_2D_Q_SENSIBLE,            /* Array_2D Q_sensible_2D (MoistConvection input) */
+    ATHAD_NFIELDS2D
+} athad_field2d;
+
+/* 1-D (im) profiles. */
+typedef enum athad_profile {
+    ATHAD_PROF_T_REF_LEVEL = 0,     /* computeLevelMeanTemperature, RK4.cpp:24-41     */
+    ATHAD_PROF_RHO_BASE,            /* m_rho_base, ThermoAtm.h:1629-1646               */
+    ATHAD_PROF_DLNRHO_DR,           /* m_dlnrho_dr, ThermoAtm.h:1652-1659              */
+    ATHAD_NPROFILES
+} athad_profile;
+
+/* Per-iteration scalars of run_3D_loop (cAtmosphereModel.cpp:1109-1131). */
+typedef struct athad_step_scalars {
+    double dt;               /* dt = dt_visc (or dt_inviscid in the spin-up)           */
+    double diffusion_ramp;   /* diffusion_ramp in [0,1]                                */
+    double buoyancy_ramp;    /* min(1, total_iter_count / 300)                         */
+    int32_t write_diagnostics; /* 1: store prod/tke_source/dis_source of stage 4       */
+    int32_t pad0;
+} athad_step_scalars;
+
+/* Counters a call leaves behind (read with athad_get_report). */
+typedef struct athad_report {
+    int64_t poisson_src_cells;     /* fluid cells of the last pressure sweep(s)          */
+    int64_t poisson_src_clamped;   /* of which the divergence source hit p_dyn_cap       */
+    int64_t satadj_ceiling_hits;   /* c > 1 - co2 clamps in clampAndFade                  */
+    int64_t nonfinite_inputs;      /* non-finite values found by the last input check    */
+    double  last_kernel_ms;        /* device time of the last timed entry point          */
+} athad_report;
+
+typedef struct athad_ctx athad_ctx;
+
+/* ---- lifetime -------------------------------------------------------------- */
+
+/* Fill p with the cli/config_cond.xml values and the reference's default switches. */
+void athad_default_params(athad_params* p);
+int32_t athad_abi_version(void);
+size_t athad_params_size(void);
+
+/* Create a context on the current CUDA device; allocates every field once. */
+athad_status athad_create(const athad_grid* grid, const athad_params* params, athad_ctx** out);
+athad_status athad_destroy(athad_ctx* ctx);
+const char*  athad_last_error(const athad_ctx* ctx);
+/* Issue all further work on this stream (a cudaStream_t passed as void*); NULL = the
+ * context's own stream. */
+athad_status athad_set_stream(athad_ctx* ctx, void* cuda_stream);
+athad_status athad_synchronize(athad_ctx* ctx);
+/* Device bytes held by a context of this grid (admission by HBM footprint). */
+size_t athad_footprint_bytes(const athad_grid* grid);
+
+/* ---- state transfer --------------------------------------------------------- */
+
+athad_status athad_upload(athad_ctx* ctx, athad_field f, const double* host, size_t n);
+athad_status athad_download(athad_ctx* ctx, athad_field f, double* host, size_t n);
+athad_status athad_upload_2d(athad_ctx* ctx, athad_field2d f, const double* host, size_t n);
+athad_status athad_download_2d(athad_ctx* ctx, athad_field2d f, double* host, size_t n);
+athad_status athad_upload_profile(athad_ctx* ctx, athad_profile f, const double* host, size_t n);
+athad_status athad_download_profile(athad_ctx* ctx, athad_profile f, double* host, size_t n);
+/* Device address and row pitch (in elements, >= km) of a field: element (i,j,k) is at
+ * ptr[(i*jm + j)*pitch + k].  For zero-copy adapters and device-side consumers. */
+athad_status athad_field_device_ptr(athad_ctx* ctx, athad_field f, double** ptr, size_t* pitch);
+/* Fill a field with a constant on the device. */
+athad_status athad_fill(athad_ctx* ctx, athad_field f, double value);
+
+/* ---- the hot path ----------------------------------------------------------- */
+
+/* storeIntermediateData3D(1.0) (UtilsAtm.h:25-49; call sites cAtmosphereModel.cpp:667,
+ * 1647): the n-level fields := the current ones. */
+athad_status athad_store_n_level(athad_ctx* ctx);
+
+/* cAtmosphereModel::computeLevelMeanTemperature (RungeKutta_Atm_Turb.cpp:24-41):
+ * fills the t_ref_level profile from t.  Mirror-symmetric, deterministic order. */
+athad_status athad_level_mean(athad_ctx* ctx);
+
+/* cAtmosphereModel::solveRungeKutta_Atmosphere_Turb (RungeKutta_Atm_Turb.cpp:44-273)
+ * with RHS_Atmosphere_Turb (RHS_Atm_Turb.cpp:31-1080); call site
+ * cAtmosphereModel.cpp:1509.  Computes t_ref_level, then the four RK4 stages over the
+ * interior cells with Jacobi stage semantics (every stage reads the previous stage's
+ * state everywhere).  Updates t..dis, aux_u/v/w and, with write_diagnostics, the stage-4
+ * prod/tke_source/dis_source. */
+athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s);
+
+/* PressureSolverAtm::run (PressureSolverAtm.h:27-669); call site
+ * cAtmosphereModel.cpp:1158.  n_sweeps red-black Gauss-Seidel sweeps of the pressure
+ * Poisson equation with the source from aux_u/v/w, each followed by the boundary
+ * conditions and the |p_dyn| ceiling.  total_iter_count selects the ceiling (10, or 3
+ * after iteration 300). */
+athad_status athad_pressure_sweep(athad_ctx* ctx, int32_t n_sweeps, int32_t total_iter_count);
+
+/* PressureSolverAtm::project_initial_velocity (PressureSolverAtm.h:686-767); call site
+ * cAtmosphereModel.cpp:665. */
+athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
+                                            int32_t total_iter_count);
+
+/* SaturationAdjustment::run (SaturationAdjustment.h:25-45); call sites
+ * cAtmosphereModel.cpp:574, 1218. */
+athad_status athad_saturation_adjust(athad_ctx* ctx);
+
+/* ThermoAtm::densities (ThermoAtm.h:1436-1666); call sites cAtmosphereModel.cpp:567
+ * (set_water_profile = 1), 634, 1418. */
+athad_status athad_densities(athad_ctx* ctx, int32_t set_water_profile);
+
+/* MoistConvection::run (MoistConvection.h:106-140); call sites cAtmosphereModel.cpp:599,
+ * 1247. */
+athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n);
+
+/* Counters of the last calls. */
+athad_status athad_get_report(athad_ctx* ctx, athad_report* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATHAD_GPU_H */

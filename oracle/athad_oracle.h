@@ -1,0 +1,130 @@
+/*
+ * athad_oracle.h - CPU restatement of the ATHAD_COND model-iteration hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared against; it
+ * is never linked into, loaded by or called from the product.  Only tests/, the smoke()
+ * entry point and the cpu_baseline leg of bench.py use it.
+ *
+ * Plain C99, FP64, compiled without -ffast-math and with -ffp-contract=off so every
+ * operation rounds as written.  Each function cites the reference file:line it follows.
+ *
+ * Two semantics are available through the `compat` argument:
+ *   compat = 0  the semantics the CUDA path implements: Jacobi RK4 stages, trig tables
+ *               and theta second differences written so that the result is exactly
+ *               north-south mirror symmetric, a pairwise (mirror-invariant) level mean.
+ *   compat = 1  the reference's own semantics, operation for operation: the in-place,
+ *               cell-by-cell RK4 sweep of RungeKutta_Atm_Turb.cpp:99-266 in serial order
+ *               (OMP_NUM_THREADS=1), the reference's trig tables and expression order.
+ *               Used to pin this restatement against the reference built from source.
+ *
+ * The field pointers are packed host arrays in (i, j, k) order, k fastest, indexed by
+ * the athad_field enumeration of include/athad_gpu.h (re-declared here as plain ints so
+ * this file does not include product headers).
+ */
+#ifndef ATHAD_ORACLE_H
+#define ATHAD_ORACLE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_params {
+    uint32_t struct_size;
+    int32_t  turb_model, wall_mode, poisson_metric_fix, anelastic, tracer_diff_flux;
+    int32_t  coriolis_nontrad, metric_curvature, metric_divergence;
+    int32_t  convection_perturbation, convection_mode, iter_prec, pad0;
+    double metric_r0, re_turb;
+    double r_air, g, u_0, cp_l, t_0, c_0, L_atm, zeta, omega, lamda, lv, ls;
+    double pr_turb, sc_WaterVapour, sc_CO2;
+    double r_Earth, p_0, t_00, t_max_phys, cloud_cap, t_skin, c_h2o_dry_top, co2_0, s_0;
+    double R_Air, R_WaterVapour;
+    double M_bg, R_bg, R_mix;
+} or_params;
+
+typedef struct or_step {
+    double dt, diffusion_ramp, buoyancy_ramp;
+    int32_t write_diagnostics, pad0;
+} or_step;
+
+/* field ids, identical numbering to athad_field */
+enum {
+    OF_T = 0, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR, OF_CO2, OF_TKE, OF_DIS,
+    OF_TN, OF_UN, OF_VN, OF_WN, OF_CN, OF_CLOUDN, OF_ICEN, OF_GRN, OF_CO2N, OF_TKEN, OF_DISN,
+    OF_P_DYN, OF_NUE, OF_T_EQ, OF_P_STAT, OF_R_HUMID,
+    OF_S_C, OF_S_R, OF_S_I, OF_S_S, OF_S_G, OF_S_V,
+    OF_MC_T, OF_MC_Q, OF_MC_V, OF_MC_W,
+    OF_AUX_U, OF_AUX_V, OF_AUX_W,
+    OF_PROD, OF_TKE_SOURCE, OF_DIS_SOURCE,
+    OF_S_C_C, OF_P_RAIN, OF_P_SNOW, OF_P_GRAUPEL, OF_PRECIPITATION,
+    OF_R_DRY,
+    OF_MC_S, OF_MC_S_U, OF_MC_S_D, OF_M_U, OF_M_D,
+    OF_Q_V_U, OF_Q_C_U, OF_Q_V_D,
+    OF_U_U, OF_V_U, OF_W_U, OF_U_D, OF_V_D, OF_W_D,
+    OF_E_U, OF_D_U, OF_E_D, OF_D_D,
+    OF_C_U, OF_E_L, OF_E_DD, OF_E_P, OF_G_P,
+    OF_P_CONV, OF_CLOUD_BASE, OF_LEVEL_FREE_SINKING, OF_DEEP_BEG, OF_DEEP_END,
+    OF_NFIELDS
+};
+enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_N };
+enum { OFP_T_REF_LEVEL = 0, OFP_RHO_BASE, OFP_DLNRHO_DR, OFP_N };
+
+size_t or_params_size(void);
+int    or_nfields(void);
+
+/* computeLevelMeanTemperature, RungeKutta_Atm_Turb.cpp:24-41 */
+void or_level_mean(int im, int jm, int km, const or_params* p, int compat,
+                   double* const* f, double* const* prof);
+
+/* solveRungeKutta_Atmosphere_Turb + RHS_Atmosphere_Turb, RungeKutta_Atm_Turb.cpp:44-273,
+ * RHS_Atm_Turb.cpp:31-1080.  Returns 0, or -1 on a configuration the restatement does
+ * not cover. */
+int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int compat,
+           double* const* f, double* const* prof);
+
+/* PressureSolverAtm::run, PressureSolverAtm.h:27-594.  counters[0] = fluid cells,
+ * counters[1] = clamped sources (may be NULL). */
+void or_pressure_sweep(int im, int jm, int km, const or_params* p, int compat,
+                       int n_sweeps, int total_iter_count, double* const* f,
+                       double* const* prof, int64_t* counters);
+
+/* PressureSolverAtm::project_initial_velocity, PressureSolverAtm.h:686-767 */
+void or_project_initial_velocity(int im, int jm, int km, const or_params* p, int compat,
+                                 int n_sweeps, int total_iter_count, double* const* f,
+                                 double* const* prof);
+
+/* SaturationAdjustment::run, SaturationAdjustment.h:25-459.  counters[0] = ceiling hits */
+void or_saturation_adjust(int im, int jm, int km, const or_params* p, int compat,
+                          double* const* f, int64_t* counters);
+
+/* ThermoAtm::densities, ThermoAtm.h:1436-1666 */
+void or_densities(int im, int jm, int km, const or_params* p, int compat,
+                  int set_water_profile, double* const* f, double* const* f2,
+                  double* const* prof);
+
+/* MoistConvection::run, MoistConvection.h:106-140 */
+int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, int iter_n,
+                        double* const* f, double* const* f2);
+
+/* storeIntermediateData3D, UtilsAtm.h:25-49 */
+void or_store_n_level(int im, int jm, int km, double* const* f);
+
+/* Thermodynamics (SaturationH2O.h, MixtureAtm.h), exposed for the known-answer tests. */
+double or_saturation_pressure(double T);
+double or_sublimation_pressure(double T);
+double or_latent_heat(double T);
+double or_saturation_mass_fraction(double E, double p, double M_other);
+double or_dew_point(double e);
+double or_dqsat_dT(double T, double p, double M_other);
+double or_moist_lapse(double T, double p, double M_other, double cp, double R_mix, double g);
+double or_cp_of(double c, double co2, double T, double M_bg);
+double or_R_of(double c, double co2, double R_bg);
+double or_M_nonwater(double c, double co2, double M_bg);
+void   or_resolve(const double* x8, double* out7);   /* M_mean, R_mix, q_H2O, q_CO2, q_bg, M_bg, R_bg */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,141 @@
+"""ctypes binding of the oracle (oracle/liboracle.so), the CPU checker of the tests.
+
+Test infrastructure: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg
+use it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from athad_cond_b200._abi import FIELD, FIELD_NAMES, FIELD2D_NAMES, PROFILE_NAMES, Params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+        _lib = ctypes.CDLL(LIB)
+        _lib.or_params_size.restype = ctypes.c_size_t
+        assert _lib.or_params_size() == ctypes.sizeof(Params), "oracle params layout differs"
+        _lib.or_nfields.restype = ctypes.c_int
+        assert _lib.or_nfields() == len(FIELD_NAMES)
+        for name in ["or_saturation_pressure", "or_sublimation_pressure", "or_latent_heat",
+                     "or_dew_point"]:
+            fn = getattr(_lib, name)
+            fn.restype = ctypes.c_double
+            fn.argtypes = [ctypes.c_double]
+        _lib.or_saturation_mass_fraction.restype = ctypes.c_double
+        _lib.or_saturation_mass_fraction.argtypes = [ctypes.c_double] * 3
+        _lib.or_dqsat_dT.restype = ctypes.c_double
+        _lib.or_dqsat_dT.argtypes = [ctypes.c_double] * 3
+        _lib.or_moist_lapse.restype = ctypes.c_double
+        _lib.or_moist_lapse.argtypes = [ctypes.c_double] * 6
+        _lib.or_cp_of.restype = ctypes.c_double
+        _lib.or_cp_of.argtypes = [ctypes.c_double] * 4
+        _lib.or_R_of.restype = ctypes.c_double
+        _lib.or_R_of.argtypes = [ctypes.c_double] * 3
+        _lib.or_M_nonwater.restype = ctypes.c_double
+        _lib.or_M_nonwater.argtypes = [ctypes.c_double] * 3
+    return _lib
+
+
+class Step(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("diffusion_ramp", ctypes.c_double),
+                ("buoyancy_ramp", ctypes.c_double), ("write_diagnostics", ctypes.c_int32),
+                ("pad0", ctypes.c_int32)]
+
+
+def _ptrs(state: dict, names, shape):
+    arr = (ctypes.POINTER(ctypes.c_double) * len(names))()
+    keep = []
+    for q, n in enumerate(names):
+        a = state.get(n)
+        if a is None:
+            a = np.zeros(shape)
+            state[n] = a
+        assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], n
+        keep.append(a)
+        arr[q] = a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return arr, keep
+
+
+class OracleState:
+    """Host copy of every field, advanced by the oracle in place."""
+
+    def __init__(self, state: dict, params: Params):
+        any_ = next(iter(v for k, v in state.items() if k in FIELD))
+        self.shape = any_.shape
+        self.params = params
+        im, jm, km = self.shape
+        self.f = {n: np.array(state[n], dtype=np.float64, copy=True) if n in state else np.zeros(self.shape)
+                  for n in FIELD_NAMES}
+        self.f2 = {n: np.array(state[n], dtype=np.float64, copy=True) if n in state else np.zeros((jm, km))
+                   for n in FIELD2D_NAMES}
+        self.prof = {n: np.array(state[n], dtype=np.float64, copy=True) if n in state else np.zeros(im)
+                     for n in PROFILE_NAMES}
+
+    def _args(self):
+        self._F, self._kf = _ptrs(self.f, FIELD_NAMES, self.shape)
+        self._F2, self._k2 = _ptrs(self.f2, FIELD2D_NAMES, self.shape[1:])
+        self._P, self._kp = _ptrs(self.prof, PROFILE_NAMES, (self.shape[0],))
+        return self._F, self._F2, self._P
+
+    def rk4(self, dt=4e-5, diffusion_ramp=1.0, buoyancy_ramp=1.0, write_diagnostics=False, compat=0):
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        s = Step(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0, 0)
+        r = lib().or_rk4(im, jm, km, ctypes.byref(self.params), ctypes.byref(s), compat, F, P)
+        assert r == 0
+
+    def level_mean(self, compat=0):
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        lib().or_level_mean(im, jm, km, ctypes.byref(self.params), compat, F, P)
+
+    def pressure_sweep(self, n_sweeps=1, total_iter_count=4, compat=0):
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        cnt = (ctypes.c_int64 * 2)()
+        lib().or_pressure_sweep(im, jm, km, ctypes.byref(self.params), compat, n_sweeps,
+                                total_iter_count, F, P, cnt)
+        return int(cnt[0]), int(cnt[1])
+
+    def project_initial_velocity(self, n_sweeps=200, total_iter_count=0, compat=0):
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        lib().or_project_initial_velocity(im, jm, km, ctypes.byref(self.params), compat, n_sweeps,
+                                          total_iter_count, F, P)
+
+    def saturation_adjust(self, compat=0):
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        cnt = (ctypes.c_int64 * 1)()
+        lib().or_saturation_adjust(im, jm, km, ctypes.byref(self.params), compat, F, cnt)
+        return int(cnt[0])
+
+    def densities(self, set_water_profile=False, compat=0):
+        F, F2, P = self._args()
+        im, jm, km = self.shape
+        lib().or_densities(im, jm, km, ctypes.byref(self.params), compat, 1 if set_water_profile else 0,
+                           F, F2, P)
+
+    def moist_convection(self, iter_n, compat=0):
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        return lib().or_moist_convection(im, jm, km, ctypes.byref(self.params), compat, iter_n, F, F2)
+
+    def store_n_level(self):
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_store_n_level(im, jm, km, F)

@@ -1,0 +1,205 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on identical seeded
+states, and exact north-south mirror symmetry of the CUDA results.
+
+Tolerances (relative to the field's max magnitude, FP64):
+  * Poisson sweep, project_initial_velocity, level mean: bit-identical (no
+    transcendentals; both sides round every operation as written).
+  * RK4 step: 1e-12 (the SST blending function calls tanh/pow, whose last bit differs
+    between CUDA and glibc).
+  * saturation adjustment, densities: 1e-11 (IAPWS exp/pow chains inside a Newton
+    iteration / a column ODE).
+"""
+import numpy as np
+import pytest
+
+from athad_cond_b200 import GpuAtmosphere, make_state, mirror
+from athad_cond_b200._abi import FIELD_NAMES, config_params, Wall, Turb
+from oracle_binding import OracleState
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(11, 21, 41), (21, 91, 181)]
+PROG = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis"]
+ANTI = {"v", "vn", "aux_v", "MC_v"}
+
+
+def relerr(a, b):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def gpu_with(state, params):
+    im, jm, km = state["t"].shape
+    g = GpuAtmosphere(im, jm, km, params)
+    g.upload_state(state)
+    return g
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+@pytest.mark.parametrize("wall", [Wall.MIRROR, Wall.REFERENCE])
+def test_rk4_step_matches_oracle(grid, wall):
+    p = config_params()
+    p.wall_mode = wall
+    st = make_state(*grid, seed=7)
+    o = OracleState(st, p)
+    o.rk4(dt=4e-5, diffusion_ramp=1.0, buoyancy_ramp=0.5, write_diagnostics=True)
+    with gpu_with(st, p) as g:
+        g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5, write_diagnostics=True)
+        for n in PROG + ["aux_u", "aux_v", "aux_w", "prod", "tke_source", "dis_source"]:
+            e = relerr(g.download(n), o.f[n])
+            assert e <= 1e-12, (n, e)
+        tr = g.download_profile("t_ref_level")
+        assert np.array_equal(tr, o.prof["t_ref_level"])
+
+
+@pytest.mark.parametrize("turb", [Turb.K_EPSILON, Turb.K_OMEGA])
+def test_rk4_other_closures(turb):
+    p = config_params()
+    p.turb_model = turb
+    st = make_state(11, 21, 41, seed=3)
+    o = OracleState(st, p)
+    o.rk4()
+    with gpu_with(st, p) as g:
+        g.solveRungeKutta_Atmosphere_Turb(4e-5)
+        for n in PROG:
+            assert relerr(g.download(n), o.f[n]) <= 1e-12, n
+
+
+def test_rk4_switches():
+    p = config_params()
+    p.coriolis_nontrad = 1
+    p.metric_curvature = 1
+    p.tracer_diff_flux = 1
+    p.metric_r0 = 0.0
+    st = make_state(11, 21, 41, seed=5)
+    st["dlnrho_dr"] = np.linspace(-1.0, -3.0, 11)
+    o = OracleState(st, p)
+    o.rk4()
+    with gpu_with(st, p) as g:
+        g.solveRungeKutta_Atmosphere_Turb(4e-5)
+        for n in PROG:
+            assert relerr(g.download(n), o.f[n]) <= 1e-12, n
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_rk4_mirror_symmetry_exact(grid):
+    p = config_params()
+    st = make_state(*grid, seed=11, symmetric=True)
+    with gpu_with(st, p) as g:
+        for it in range(3):
+            g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.2)
+            g.storeIntermediateData3D()
+        for n in PROG + ["aux_u", "aux_v", "aux_w"]:
+            a = g.download(n)
+            assert np.array_equal(a, mirror(a, n in ANTI)), n
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_pressure_sweep_bit_exact(grid):
+    p = config_params()
+    st = make_state(*grid, seed=13)
+    rng = np.random.default_rng(1)
+    for n in ("aux_u", "aux_v", "aux_w"):
+        st[n] = 1e-3 * rng.standard_normal(st["t"].shape)
+    st["aux_v"][:, 3, 5] = 1e6       # one clamped source
+    o = OracleState(st, p)
+    cells, clamped = o.pressure_sweep(n_sweeps=3, total_iter_count=400)
+    with gpu_with(st, p) as g:
+        g.PressureSolverAtm_run(total_iter_count=400, n_sweeps=3)
+        for n in ("p_dyn", "aux_u", "aux_v", "aux_w"):
+            assert np.array_equal(g.download(n), o.f[n]), n
+        r = g.report()
+        assert r["poisson_src_cells"] == cells and r["poisson_src_clamped"] == clamped
+
+
+def test_pressure_sweep_anelastic_and_divergence():
+    p = config_params()
+    p.anelastic = 1
+    p.metric_divergence = 1
+    p.poisson_metric_fix = 0
+    st = make_state(11, 21, 41, seed=17)
+    st["dlnrho_dr"] = np.linspace(-1.0, -3.0, 11)
+    rng = np.random.default_rng(2)
+    for n in ("aux_u", "aux_v", "aux_w"):
+        st[n] = 1e-3 * rng.standard_normal(st["t"].shape)
+    o = OracleState(st, p)
+    o.pressure_sweep(n_sweeps=2, total_iter_count=4)
+    with gpu_with(st, p) as g:
+        g.PressureSolverAtm_run(total_iter_count=4, n_sweeps=2)
+        assert np.array_equal(g.download("p_dyn"), o.f["p_dyn"])
+
+
+def test_project_initial_velocity_bit_exact():
+    p = config_params()
+    st = make_state(11, 21, 41, seed=19)
+    o = OracleState(st, p)
+    o.project_initial_velocity(n_sweeps=20)
+    with gpu_with(st, p) as g:
+        g.project_initial_velocity(n_sweeps=20)
+        for n in ("u", "v", "w", "p_dyn", "aux_u"):
+            assert np.array_equal(g.download(n), o.f[n]), n
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_saturation_adjust_matches_oracle(grid):
+    p = config_params()
+    st = make_state(*grid, seed=23)
+    im = grid[0]
+    # drive part of the column supersaturated / subsaturated with condensate, and make some
+    # cells supercritical or superheated so every branch of clampAndFade runs
+    st["c"] = st["c"] * 1.5
+    st["cloud"][im // 2:, :, ::3] += 2e-3
+    st["t"][1, :, ::5] = 700.0 / 273.15
+    st["P_rain"][:, :, ::7] = 1e-5
+    st["co2"][2, :, ::11] = 0.99
+    o = OracleState(st, p)
+    hits = o.saturation_adjust()
+    with gpu_with(st, p) as g:
+        g.SaturationAdjustment_run()
+        for n in ("t", "c", "cloud", "ice", "gr", "S_c_c", "P_rain", "S_v"):
+            assert relerr(g.download(n), o.f[n]) <= 1e-11, n
+        assert g.report()["satadj_ceiling_hits"] == hits
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+@pytest.mark.parametrize("set_water", [False, True])
+def test_densities_matches_oracle(grid, set_water):
+    p = config_params()
+    st = make_state(*grid, seed=29)
+    o = OracleState(st, p)
+    o.densities(set_water_profile=set_water)
+    with gpu_with(st, p) as g:
+        g.densities(set_water_profile=set_water)
+        for n in ("t", "p_stat", "r_humid", "r_dry", "c"):
+            assert relerr(g.download(n), o.f[n]) <= 1e-11, n
+        for n in ("t_top_init", "p_stat_landscape"):
+            assert relerr(g.download_2d(n), o.f2[n]) <= 1e-11, n
+        for n in ("rho_base", "dlnrho_dr"):
+            assert relerr(g.download_profile(n), o.prof[n]) <= 1e-11, n
+
+
+def test_cadence_loop_matches_oracle():
+    """Ten model iterations at the reference cadence: RK4 every iteration, one pressure
+    sweep every 4th, saturation adjustment + densities every 2nd (run_3D_loop,
+    cAtmosphereModel.cpp:1156-1509)."""
+    p = config_params()
+    grid = (11, 21, 41)
+    st = make_state(*grid, seed=31)
+    o = OracleState(st, p)
+    with gpu_with(st, p) as g:
+        for it in range(1, 11):
+            br = min(1.0, it / 300.0)
+            if it % 4 == 0:
+                o.pressure_sweep(1, it)
+                g.PressureSolverAtm_run(it)
+            if it % 2 == 0:
+                o.saturation_adjust()
+                g.SaturationAdjustment_run()
+                o.densities()
+                g.densities()
+            o.rk4(dt=4e-5, buoyancy_ramp=br)
+            g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, br)
+            o.store_n_level()
+            g.storeIntermediateData3D()
+        for n in PROG + ["p_dyn", "p_stat", "r_humid"]:
+            assert relerr(g.download(n), o.f[n]) <= 1e-10, n
