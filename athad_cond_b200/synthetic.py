@@ -114,7 +114,7 @@ def make_state(im: int, jm: int, km: int, seed: int = 20261203, symmetric: bool 
         a = st.get(name)
         if a is None:
             a = np.zeros((im, jh, km))
-        a = np.ascontiguousarray(np.broadcast_to(a, (im, jh, km)), dtype=np.float64)
+        a = np.array(np.broadcast_to(a, (im, jh, km)), dtype=np.float64, copy=True)
         if symmetric:
             full = np.empty((im, jm, km))
             full[:, :jh, :] = a

@@ -84,6 +84,9 @@ void or_level_mean(int im, int jm, int km, const or_params* p, int compat,
 int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int compat,
            double* const* f, double* const* prof);
 
+void or_rhs_cell_at(int im, int jm, int km, const or_params* p, const or_step* s, int compat,
+                    double* const* f, double* const* prof, int i, int j, int k, double* out);
+
 /* PressureSolverAtm::run, PressureSolverAtm.h:27-594.  counters[0] = fluid cells,
  * counters[1] = clamped sources (may be NULL). */
 void or_pressure_sweep(int im, int jm, int km, const or_params* p, int compat,

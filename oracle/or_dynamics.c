@@ -504,9 +504,20 @@ int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int com
     const double* nu = f[OF_NUE];
 
     if (compat) {
-        /* in place, cell by cell, serial (i, j, k) order: RungeKutta_Atm_Turb.cpp:99-266 */
-        for (int i = 1; i < im - 1; i++)
-            for (int j = 1; j < jm - 1; j++) {
+        /* In place, cell by cell: RungeKutta_Atm_Turb.cpp:99-266.  compat = 1 is the serial
+         * (i, j, k) order.  compat = T > 1 reproduces the reference run with T OpenMP threads:
+         * `collapse(2) schedule(static)` gives thread t one contiguous range of the (i, j)
+         * rows, all ranges advance together, so where two ranges meet the later thread's
+         * first rows are finished before the earlier thread reaches its last rows.  Running
+         * the ranges one after another in reverse order reproduces exactly that. */
+        const int T = compat;
+        const long nrows = (long)(im - 2) * (jm - 2);
+        const long q = nrows / T, rem = nrows % T;
+        for (int th = T - 1; th >= 0; th--) {
+            const long r0 = th * q + (th < rem ? th : rem);
+            const long r1 = r0 + q + (th < rem ? 1 : 0);
+            for (long r = r0; r < r1; r++) {
+                const int i = 1 + (int)(r / (jm - 2)), j = 1 + (int)(r % (jm - 2));
                 cgeo G;
                 make_cgeo(&g, p, i, j, &G);
                 for (int k = 1; k < km - 1; k++) {
@@ -532,6 +543,7 @@ int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int com
                     }
                 }
             }
+        }
         or_geom_free(&g);
         return 0;
     }
@@ -754,4 +766,25 @@ void or_store_n_level(int im, int jm, int km, double* const* f)
 {
     const size_t n = (size_t)im * jm * km;
     for (int q = 0; q < 11; q++) memcpy(f[OF_TN + q], f[OF_T + q], n * sizeof(double));
+}
+
+/* RHS_Atmosphere_Turb at one interior cell of the current state (t_ref_level taken from
+ * prof), with the reference's expression order when compat != 0.  out = rhs_t..rhs_dis,
+ * aux_u/v/w, prod, tke_source, dis_source. */
+void or_rhs_cell_at(int im, int jm, int km, const or_params* p, const or_step* s, int compat,
+                    double* const* f, double* const* prof, int i, int j, int k, double* out)
+{
+    or_geom g;
+    or_geom_init(&g, im, jm, km, p, compat);
+    cgeo G;
+    make_cgeo(&g, p, i, j, &G);
+    const double* Y[NY];
+    for (int q = 0; q < NY; q++) Y[q] = f[OF_T + q];
+    rhs_out o;
+    rhs_cell(&g, p, s, compat ? 1 : 0, i, j, k, &G, Y, f[OF_P_DYN], f[OF_NUE], f,
+             prof[OFP_T_REF_LEVEL], prof[OFP_DLNRHO_DR], &o);
+    for (int q = 0; q < NY; q++) out[q] = o.k[q];
+    out[11] = o.aux[0]; out[12] = o.aux[1]; out[13] = o.aux[2];
+    out[14] = o.prod; out[15] = o.tke_source; out[16] = o.dis_source;
+    or_geom_free(&g);
 }

@@ -1,0 +1,385 @@
+// ref_harness.cpp - a C entry layer around the unmodified reference, so the tests can run
+// the reference's own hot-path functions on a state they choose and read the results.
+// TEST INFRASTRUCTURE ONLY (the checker of the oracle); built into oracle/_ref/ by
+// oracle/ref/Makefile from the reference sources where they lie.
+//
+// The reference keeps its model state in private members of cAtmosphereModel and runs its
+// physics through friend classes.  To reach them without editing the reference, the
+// standard headers are included first and the access specifiers are then widened for the
+// reference headers only.  Object layout does not depend on access, so this TU and the
+// reference's own objects agree on every member's address.
+#include <algorithm>
+#include <cassert>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <csignal>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fenv.h>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <sys/stat.h>
+#include <sys/types.h>
+#include <tuple>
+#include <vector>
+#include <omp.h>
+#include "tinyxml2.h"
+
+#define private public
+#define protected public
+#include "cAtmosphereModel.h"
+// MoistConvection.h defines two non-inline globals that cAtmosphereModel.cpp defines too;
+// give this TU's copies their own names (same initialisers).
+#define eps_u harness_eps_u
+#define del_u harness_del_u
+#include "MoistConvection.h"
+#undef eps_u
+#undef del_u
+#include "ZeroCatIceScheme.h"
+#include "OneCatIceScheme.h"
+#include "TwoCatIceScheme.h"
+#include "ThreeCatIceScheme.h"
+#include "SaturationAdjustment.h"
+#include "VelocityInitializer.h"
+#include "PressureSolverAtm.h"
+#include "ThermoAtm.h"
+#include "UtilsAtm.h"
+#include "BC_Atm.h"
+#include "TurbulenceAtm.h"
+#undef private
+#undef protected
+
+namespace {
+
+struct NullBuf : std::streambuf {
+    int overflow(int c) override { return c; }
+};
+NullBuf g_null;
+std::streambuf* g_saved = nullptr;
+
+Array* field3(cAtmosphereModel* m, const std::string& n)
+{
+#define F(name) if (n == #name) return &m->name;
+    F(t) F(u) F(v) F(w) F(c) F(cloud) F(ice) F(gr) F(co2) F(tke) F(dis)
+    F(tn) F(un) F(vn) F(wn) F(cn) F(cloudn) F(icen) F(grn) F(co2n) F(tken) F(disn)
+    F(p_dyn) F(nue) F(t_eq) F(p_stat) F(r_humid)
+    F(S_c) F(S_r) F(S_i) F(S_s) F(S_g) F(S_v)
+    F(MC_t) F(MC_q) F(MC_v) F(MC_w)
+    F(aux_u) F(aux_v) F(aux_w)
+    F(prod) F(tke_source) F(dis_source)
+    F(S_c_c) F(P_rain) F(P_snow) F(P_graupel) F(Precipitation)
+    F(r_dry)
+    F(s) F(s_u) F(s_d) F(M_u) F(M_d) F(q_v_u) F(q_c_u) F(q_v_d)
+    F(u_u) F(v_u) F(w_u) F(u_d) F(v_d) F(w_d)
+    F(E_u) F(D_u) F(E_d) F(D_d)
+    F(c_u) F(e_l) F(e_d) F(e_p) F(g_p)
+    F(P_conv) F(CloudBase) F(LevelFreeSinking) F(Deep_beg) F(Deep_end)
+    F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
+    F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
+#undef F
+    return nullptr;
+}
+
+Array_2D* field2(cAtmosphereModel* m, const std::string& n)
+{
+    if (n == "p_stat_landscape") return &m->p_stat_landscape;
+    if (n == "Evaporation") return &m->Evaporation;
+    if (n == "Q_sensible_2D") return &m->Q_sensible_2D;
+    return nullptr;
+}
+
+std::vector<double>* profile(cAtmosphereModel* m, const std::string& n)
+{
+    if (n == "t_ref_level") return &m->t_ref_level;
+    if (n == "rho_base") return &m->m_rho_base;
+    if (n == "dlnrho_dr") return &m->m_dlnrho_dr;
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_dims(int* im, int* jm, int* km)
+{
+    *im = cAtmosphereModel::im; *jm = cAtmosphereModel::jm; *km = cAtmosphereModel::km;
+}
+
+void ref_set_threads(int n) { omp_set_num_threads(n); }
+
+void ref_quiet(int q)
+{
+    if (q && !g_saved) g_saved = std::cout.rdbuf(&g_null);
+    if (!q && g_saved) { std::cout.rdbuf(g_saved); g_saved = nullptr; }
+}
+
+// xml == NULL: the compiled-in defaults (SetDefaultConfig, cAtmosphereDefaults.cpp.inc),
+// which are the values of cli/config_cond.xml, then the composition LoadConfig would resolve.
+void* ref_new(const char* xml)
+{
+    cAtmosphereModel* m = new cAtmosphereModel();
+    if (xml) m->LoadConfig(xml);
+    else m->initComposition();
+    return m;
+}
+
+void ref_delete(void* p) { delete (cAtmosphereModel*)p; }
+
+// The reference's initial state: RunTimeSlice (cAtmosphereModel.cpp:468-668) for Ma = 0
+// without its file output, the printed diagnostics and the standard-atmosphere dew-point
+// diagnostic (standAtm_DewPoint_HumidRel, a 60-step bisection per cell that no hot-path
+// function reads), then the Held-Suarez target snapshot of run_3D_loop (:750-753).
+int ref_init_state(void* p)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->m_current_time = m->m_time_list.insert(0).first;
+    UtilsAtm(*m).resetArrays();
+    m->dt = m->dt_visc;
+    m->iter_n = 0;
+    m->total_iter_count = 0;
+    if (m->turb_model.empty() || m->turb_model == "none") m->turb_model = "laminar";
+    m->use_turbulence_model = (m->turb_model != "laminar");
+    m->use_k_epsilon_turbulence_model = (m->turb_model == "k_epsilon");
+    m->use_k_omega_turbulence_model = (m->turb_model == "k_omega");
+    m->use_k_omega_SST_turbulence_model = (m->turb_model == "k_omega_SST");
+    m->initGridCoordinates();
+    m->initMetricRadius();
+    m->init_layer_heights();
+    m->init_tropopause_layers();
+    m->read_Atmosphere_Surface_Data(0);
+    m->LandOceanFraction();
+    if (!m->use_NASA_velocity) VelocityInitializer(*m).compute();
+    BC_Atm(*m).bcVelSurfSur();
+    AtomUtils::damp_wiggles(m->u, &m->i_topography, true, true, true);
+    AtomUtils::damp_wiggles(m->v, &m->i_topography, true, true, true);
+    AtomUtils::damp_wiggles(m->w, &m->i_topography, true, true, true);
+    m->initTemperatureData(0);
+    AtomUtils::damp_wiggles(m->t, &m->i_topography, true, true, true);
+    m->t_top_init.assign(m->jm, std::vector<double>(m->km, 0.0));
+    for (int j = 0; j < m->jm; j++)
+        for (int k = 0; k < m->km; k++) m->t_top_init[j][k] = m->t.x[m->im - 1][j][k];
+    m->initWaterWapour();
+    for (int pass = 0; pass < 2; pass++) {
+        ThermoAtm(*m).co2Atmosphere();
+        ThermoAtm(*m).densities(true);
+    }
+    m->initCloudIce();
+    SaturationAdjustment(*m).run();
+    AtomUtils::damp_wiggles(m->ice, &m->i_topography, true, true, true);
+    AtomUtils::damp_wiggles(m->c, &m->i_topography, true, true, true);
+    AtomUtils::damp_wiggles(m->cloud, &m->i_topography, true, true, true);
+    ThermoAtm(*m).precipitableWater();
+    switch (m->CategoryIceScheme) {
+        case 0: ZeroCatIceScheme(*m).run(); break;
+        case 1: OneCatIceScheme(*m).run(); break;
+        case 2: TwoCatIceScheme(*m).run(); break;
+        case 3: ThreeCatIceScheme(*m).run(); break;
+        default: break;
+    }
+    AtomUtils::damp_wiggles(m->P_rain, &m->i_topography, true, true, true);
+    AtomUtils::damp_wiggles(m->P_snow, &m->i_topography, true, true, true);
+    MoistConvection(*m).run(m->iter_n);
+    for (Array* a : {&m->P_conv, &m->E_u, &m->M_u, &m->q_v_u, &m->q_c_u, &m->E_d, &m->M_d, &m->q_v_d})
+        AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
+    if (m->turb_model != "laminar") {
+        TurbulenceAtm(*m).init();
+        TurbulenceAtm(*m).run();
+        for (Array* a : {&m->tke, &m->dis, &m->nue, &m->prod, &m->tke_source, &m->dis_source})
+            AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
+    }
+    UtilsAtm(*m).precipitationSum();
+    ThermoAtm(*m).co2Atmosphere();
+    ThermoAtm(*m).co2Column(true);
+    ThermoAtm(*m).waterBudget(true);
+    ThermoAtm(*m).densities();
+    ThermoAtm(*m).forces();
+    ThermoAtm(*m).waterVapourEvaporation();
+    ThermoAtm(*m).latentSensibleHeat();
+    ThermoAtm(*m).vegetationLand();
+    BC_Atm(*m).bcRadius();
+    BC_Atm(*m).bcTheta();
+    BC_Atm(*m).bcPhi();
+    BC_Atm(*m).bcScalarSurfSur();
+    BC_Atm(*m).bcSolidGround();
+    PressureSolverAtm(*m).project_initial_velocity(200);
+    UtilsAtm(*m).storeIntermediateData3D(1.0);
+    for (int i = 0; i < m->im; i++)
+        for (int j = 0; j < m->jm; j++)
+            for (int k = 0; k < m->km; k++) m->t_eq.x[i][j][k] = m->t.x[i][j][k];
+    return 0;
+}
+
+int ref_get3(void* p, const char* name, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    Array* a = field3(m, name);
+    if (!a || !a->x) return -1;
+    size_t q = 0;
+    for (int i = 0; i < m->im; i++)
+        for (int j = 0; j < m->jm; j++) {
+            std::memcpy(out + q, a->x[i][j], sizeof(double) * m->km);
+            q += m->km;
+        }
+    return 0;
+}
+
+int ref_set3(void* p, const char* name, const double* in)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    Array* a = field3(m, name);
+    if (!a || !a->x) return -1;
+    size_t q = 0;
+    for (int i = 0; i < m->im; i++)
+        for (int j = 0; j < m->jm; j++) {
+            std::memcpy(a->x[i][j], in + q, sizeof(double) * m->km);
+            q += m->km;
+        }
+    return 0;
+}
+
+int ref_get2(void* p, const char* name, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    if (std::string(name) == "t_top_init") {
+        if ((int)m->t_top_init.size() != m->jm) return -1;
+        for (int j = 0; j < m->jm; j++)
+            for (int k = 0; k < m->km; k++) out[(size_t)j * m->km + k] = m->t_top_init[j][k];
+        return 0;
+    }
+    Array_2D* a = field2(m, name);
+    if (!a || !a->y) return -1;
+    for (int j = 0; j < m->jm; j++)
+        for (int k = 0; k < m->km; k++) out[(size_t)j * m->km + k] = a->y[j][k];
+    return 0;
+}
+
+int ref_set2(void* p, const char* name, const double* in)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    if (std::string(name) == "t_top_init") {
+        m->t_top_init.assign(m->jm, std::vector<double>(m->km, 0.0));
+        for (int j = 0; j < m->jm; j++)
+            for (int k = 0; k < m->km; k++) m->t_top_init[j][k] = in[(size_t)j * m->km + k];
+        return 0;
+    }
+    Array_2D* a = field2(m, name);
+    if (!a || !a->y) return -1;
+    for (int j = 0; j < m->jm; j++)
+        for (int k = 0; k < m->km; k++) a->y[j][k] = in[(size_t)j * m->km + k];
+    return 0;
+}
+
+int ref_getp(void* p, const char* name, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    std::vector<double>* v = profile(m, name);
+    if (!v || (int)v->size() != m->im) return -1;
+    std::memcpy(out, v->data(), sizeof(double) * m->im);
+    return 0;
+}
+
+int ref_setp(void* p, const char* name, const double* in)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    std::vector<double>* v = profile(m, name);
+    if (!v) return -1;
+    v->assign(in, in + m->im);
+    return 0;
+}
+
+// scalars the run loop sets before the hot-path calls (cAtmosphereModel.cpp:1109-1131)
+void ref_set_scalars(void* p, double dt, double diffusion_ramp, double buoyancy_ramp,
+                     int total_iter_count, int iter_n)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->dt = dt;
+    m->diffusion_ramp = diffusion_ramp;
+    m->buoyancy_ramp = buoyancy_ramp;
+    m->total_iter_count = total_iter_count;
+    m->iter_n = iter_n;
+}
+
+// a few derived constants, for the tests to compare with their own derivation
+void ref_constants(void* p, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    out[0] = m->re_turb;
+    out[1] = m->m_metric_r0;
+    out[2] = m->metricShellLength();
+    out[3] = m->m_comp.M_bg;
+    out[4] = m->m_comp.R_bg;
+    out[5] = m->m_comp.R_mix;
+    out[6] = m->dt_visc;
+}
+
+void ref_rk4(void* p) { ((cAtmosphereModel*)p)->solveRungeKutta_Atmosphere_Turb(); }
+void ref_pressure(void* p) { PressureSolverAtm(*(cAtmosphereModel*)p).run(false); }
+void ref_project(void* p, int n) { PressureSolverAtm(*(cAtmosphereModel*)p).project_initial_velocity(n); }
+void ref_satadj(void* p) { SaturationAdjustment(*(cAtmosphereModel*)p).run(); }
+void ref_densities(void* p, int set_water) { ThermoAtm(*(cAtmosphereModel*)p).densities(set_water != 0); }
+void ref_moist(void* p, int iter_n)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->iter_n = iter_n;
+    MoistConvection(*m).run(iter_n);
+}
+void ref_store(void* p) { UtilsAtm(*(cAtmosphereModel*)p).storeIntermediateData3D(1.0); }
+void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
+
+// RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4
+// driver builds (RungeKutta_Atm_Turb.cpp:92-135).  out = rhs_t..rhs_dis (11), aux_u/v/w,
+// prod, tke_source, dis_source.
+void ref_rhs_cell(void* p, int i, int j, int k, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    cAtmosphereModel::CellGeometry geo;
+    geo.rm = m->rad.z[i];
+    geo.rm2 = geo.rm * geo.rm;
+    geo.exp_rm = 1.0 / (geo.rm + 1.0);
+    geo.exp_2_rm = geo.exp_rm * geo.exp_rm;
+    double st = sin(m->the.z[j]);
+    if (st < 0.55) st = 0.55;
+    geo.sinthe = st;
+    geo.sinthe2 = geo.sinthe * geo.sinthe;
+    geo.costhe = cos(m->the.z[j]);
+    const double rmet = m->metricRadius(geo.rm);
+    const double rmet2 = rmet * rmet;
+    geo.inv_rm = 1.0 / rmet;
+    geo.inv_rm2 = 1.0 / rmet2;
+    geo.inv_rmsinthe = 1.0 / (rmet * geo.sinthe);
+    geo.inv_rm2sinthe = geo.inv_rm2 / geo.sinthe;
+    geo.inv_rm2sinthe2 = geo.inv_rm2 / geo.sinthe2;
+    geo.costhe_inv_rm2sinthe = geo.costhe * geo.inv_rm2sinthe;
+    geo.inv_2dr = 1.0 / (2.0 * m->dr);
+    geo.inv_2dthe = 1.0 / (2.0 * m->dthe);
+    geo.inv_2dphi = 1.0 / (2.0 * m->dphi);
+    geo.inv_dr2 = 1.0 / (m->dr * m->dr);
+    geo.inv_dthe2 = 1.0 / (m->dthe * m->dthe);
+    geo.inv_dphi2 = 1.0 / (m->dphi * m->dphi);
+    if ((int)m->t_ref_level.size() != m->im) m->computeLevelMeanTemperature();
+    m->RHS_Atmosphere_Turb(i, j, k, geo);
+    const Array* r[11] = {&m->rhs_t, &m->rhs_u, &m->rhs_v, &m->rhs_w, &m->rhs_c, &m->rhs_cloud,
+                          &m->rhs_ice, &m->rhs_g, &m->rhs_co2, &m->rhs_tke, &m->rhs_dis};
+    for (int q = 0; q < 11; q++) out[q] = r[q]->x[i][j][k];
+    out[11] = m->aux_u.x[i][j][k];
+    out[12] = m->aux_v.x[i][j][k];
+    out[13] = m->aux_w.x[i][j][k];
+    out[14] = m->prod.x[i][j][k];
+    out[15] = m->tke_source.x[i][j][k];
+    out[16] = m->dis_source.x[i][j][k];
+}
+
+}  // extern "C"

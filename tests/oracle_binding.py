@@ -98,6 +98,15 @@ class OracleState:
         r = lib().or_rk4(im, jm, km, ctypes.byref(self.params), ctypes.byref(s), compat, F, P)
         assert r == 0
 
+    def rhs_cell(self, i, j, k, dt=4e-5, diffusion_ramp=1.0, buoyancy_ramp=1.0, compat=0):
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        s = Step(dt, diffusion_ramp, buoyancy_ramp, 0, 0)
+        out = (ctypes.c_double * 17)()
+        lib().or_rhs_cell_at(im, jm, km, ctypes.byref(self.params), ctypes.byref(s), compat, F, P,
+                             int(i), int(j), int(k), out)
+        return np.array(list(out))
+
     def level_mean(self, compat=0):
         F, _, P = self._args()
         im, jm, km = self.shape

@@ -1,0 +1,102 @@
+"""ctypes binding of the reference itself, built from its sources into oracle/_ref/ by
+oracle/ref/Makefile (test infrastructure: it pins the oracle)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def lib_path(variant: str = "pin") -> str:
+    return os.path.join(REF_DIR, variant, "libathad_ref.so")
+
+
+def available(variant: str = "pin") -> bool:
+    return os.path.exists(lib_path(variant))
+
+
+class Reference:
+    """One cAtmosphereModel of the reference (grid fixed at 61 x 181 x 361)."""
+
+    def __init__(self, variant: str = "pin", quiet: bool = True, threads: int | None = None):
+        self.lib = ctypes.CDLL(lib_path(variant))
+        L = self.lib
+        L.ref_new.restype = ctypes.c_void_p
+        L.ref_new.argtypes = [ctypes.c_char_p]
+        for n in ["ref_init_state", "ref_rk4", "ref_pressure", "ref_satadj", "ref_store",
+                  "ref_level_mean", "ref_delete"]:
+            getattr(L, n).argtypes = [ctypes.c_void_p]
+        for n in ["ref_get3", "ref_set3", "ref_get2", "ref_set2", "ref_getp", "ref_setp"]:
+            getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+            getattr(L, n).restype = ctypes.c_int
+        L.ref_project.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_densities.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_moist.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_set_scalars.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.ref_rhs_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_double)]
+        L.ref_constants.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_quiet.argtypes = [ctypes.c_int]
+        im, jm, km = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.ref_dims(ctypes.byref(im), ctypes.byref(jm), ctypes.byref(km))
+        self.shape = (im.value, jm.value, km.value)
+        L.ref_quiet(1 if quiet else 0)
+        if threads:
+            L.ref_set_threads(threads)
+        self.h = L.ref_new(None)   # compiled-in defaults = cli/config_cond.xml
+
+    def close(self):
+        if self.h:
+            self.lib.ref_delete(self.h)
+            self.h = None
+
+    def init_state(self):
+        self.lib.ref_init_state(self.h)
+
+    def get(self, name):
+        out = np.empty(self.shape)
+        assert self.lib.ref_get3(self.h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0, name
+        return out
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == self.shape
+        assert self.lib.ref_set3(self.h, name.encode(), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0, name
+
+    def get2(self, name):
+        out = np.empty(self.shape[1:])
+        assert self.lib.ref_get2(self.h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0, name
+        return out
+
+    def set2(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert self.lib.ref_set2(self.h, name.encode(), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0, name
+
+    def getp(self, name):
+        out = np.empty(self.shape[0])
+        r = self.lib.ref_getp(self.h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out if r == 0 else None
+
+    def setp(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert self.lib.ref_setp(self.h, name.encode(), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0
+
+    def constants(self):
+        out = (ctypes.c_double * 8)()
+        self.lib.ref_constants(self.h, out)
+        keys = ["re_turb", "metric_r0", "shell_len", "M_bg", "R_bg", "R_mix", "dt_visc"]
+        return dict(zip(keys, list(out)[:7]))
+
+    def set_scalars(self, dt, diffusion_ramp, buoyancy_ramp, total_iter_count, iter_n):
+        self.lib.ref_set_scalars(self.h, dt, diffusion_ramp, buoyancy_ramp, total_iter_count, iter_n)
+
+    def rhs_cell(self, i, j, k):
+        out = (ctypes.c_double * 17)()
+        self.lib.ref_rhs_cell(self.h, int(i), int(j), int(k), out)
+        return np.array(list(out))

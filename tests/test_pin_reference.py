@@ -1,0 +1,128 @@
+"""Pin of the oracle against the reference itself.
+
+The reference is built from its own sources (oracle/ref/Makefile -> oracle/_ref/pin, an
+IEEE build) and driven through its own functions on its own initial state at its only
+grid, 61 x 181 x 361 (cAtmosphereModel.h:162).  The oracle, in its reference-compatible
+semantics, must reproduce every hot-path function bit for bit:
+
+  * RHS_Atmosphere_Turb at sampled cells;
+  * solveRungeKutta_Atmosphere_Turb, the in-place sweep run with T OpenMP threads;
+  * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes).
+
+Skipped where the reference was not built (a machine without the reference sources).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ref_binding
+from athad_cond_b200._abi import FIELD_NAMES, config_params, Wall
+from oracle_binding import OracleState
+
+pytestmark = pytest.mark.skipif(not ref_binding.available("pin"),
+                                reason="reference not built (oracle/_ref/pin)")
+
+THREADS = max(1, min(8, os.cpu_count() or 1))
+DT = 4e-5
+
+
+@pytest.fixture(scope="module")
+def ref():
+    cwd = os.getcwd()
+    os.chdir(os.environ.get("TMPDIR", "/tmp"))
+    try:
+        R = ref_binding.Reference("pin", threads=THREADS)
+        R.init_state()
+        snap = {n: R.get(n) for n in FIELD_NAMES}
+        snap2 = {n: R.get2(n) for n in ("t_top_init", "p_stat_landscape")}
+        yield R, snap, snap2
+        R.close()
+    finally:
+        os.chdir(cwd)
+
+
+def fresh(ref):
+    R, snap, snap2 = ref
+    for n, a in snap.items():
+        R.set(n, a)
+    for n, a in snap2.items():
+        R.set2(n, a)
+    p = config_params()
+    p.wall_mode = Wall.REFERENCE
+    st = dict(snap)
+    st.update(snap2)
+    return R, OracleState(st, p)
+
+
+def assert_identical(R, o, names):
+    for n in names:
+        a, b = R.get(n), o.f[n]
+        assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))), int(np.count_nonzero(a != b)))
+
+
+def test_derived_constants(ref):
+    R, _, _ = ref
+    c = R.constants()
+    p = config_params()
+    assert c["re_turb"] == p.re_turb
+    assert c["M_bg"] == p.M_bg and c["R_bg"] == p.R_bg and c["R_mix"] == p.R_mix
+    assert c["dt_visc"] == DT
+
+
+def test_rhs_cells_bit_exact(ref):
+    R, o = fresh(ref)
+    R.lib.ref_level_mean(R.h)
+    o.prof["t_ref_level"][:] = R.getp("t_ref_level")
+    R.set_scalars(DT, 1.0, 0.3, 90, 90)
+    im, jm, km = R.shape
+    rng = np.random.default_rng(2026)
+    cells = [(1 + rng.integers(im - 2), 1 + rng.integers(jm - 2), 1 + rng.integers(km - 2)) for _ in range(400)]
+    cells += [(1, 1, 1), (im - 2, jm - 2, km - 2), (1, jm // 2, km // 2), (im // 2, 1, 1)]
+    for (i, j, k) in cells:
+        a = R.rhs_cell(i, j, k)
+        b = o.rhs_cell(i, j, k, dt=DT, buoyancy_ramp=0.3, compat=1)
+        assert np.array_equal(a, b), ((i, j, k), a - b)
+
+
+def test_rk4_step_bit_exact(ref):
+    R, o = fresh(ref)
+    R.set_scalars(DT, 1.0, 0.3, 90, 90)
+    R.lib.ref_rk4(R.h)
+    o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS)
+    assert_identical(R, o, ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
+                            "aux_u", "aux_v", "aux_w"])
+    assert np.array_equal(R.getp("t_ref_level"), o.prof["t_ref_level"])
+
+
+def test_pressure_sweep_bit_exact(ref):
+    R, o = fresh(ref)
+    rng = np.random.default_rng(5)
+    for n in ("aux_u", "aux_v", "aux_w"):
+        a = 1e-2 * rng.standard_normal(R.shape)
+        R.set(n, a)
+        o.f[n][:] = a
+    for it in (4, 400):
+        R.set_scalars(DT, 1.0, 1.0, it, it)
+        R.lib.ref_pressure(R.h)
+        o.pressure_sweep(1, it, compat=1)
+    assert_identical(R, o, ["p_dyn", "aux_u", "aux_v", "aux_w"])
+
+
+def test_saturation_adjustment_bit_exact(ref):
+    R, o = fresh(ref)
+    R.lib.ref_satadj(R.h)
+    o.saturation_adjust(compat=1)
+    assert_identical(R, o, ["t", "c", "cloud", "ice", "gr", "S_c_c", "P_rain", "P_snow", "S_v", "S_c"])
+
+
+@pytest.mark.parametrize("set_water", [0, 1])
+def test_densities_bit_exact(ref, set_water):
+    R, o = fresh(ref)
+    R.lib.ref_densities(R.h, set_water)
+    o.densities(set_water_profile=bool(set_water), compat=1)
+    assert_identical(R, o, ["t", "p_stat", "r_humid", "r_dry", "c"])
+    for n in ("t_top_init", "p_stat_landscape"):
+        assert np.array_equal(R.get2(n), o.f2[n]), n
+    for n in ("rho_base", "dlnrho_dr"):
+        assert np.array_equal(R.getp(n), o.prof[n]), n
