@@ -217,7 +217,15 @@ def run_ours(args, rank, world, device):
         ms = float(t.item())
 
     # ---- end to end through the C ABI with host buffers ----
-    host_up = {n: torch.from_numpy(st[n]).pin_memory() for n in E2E_UP}
+    if args.no_e2e:
+        g.close()
+        peak, peak_kind = measured_peaks()
+        rk_avg = sum(rk_ms) / len(rk_ms)
+        achieved = RK4_FIELDS_PER_POINT * 8.0 * pts / (rk_avg * 1e-3) / 1e9
+        return {"value": pts * args.steps * world / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                "e2e_value": None, "h2d": 0, "d2h": 0, "rk4_ms": rk_avg, "achieved": achieved,
+                "peak": peak, "peak_kind": peak_kind, "clocks": clk.summary(), "finite": True}
+    host_up = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in E2E_UP}
     host_down = {n: torch.empty(GRID, dtype=torch.float64).pin_memory() for n in E2E_DOWN}
     lib = g.lib
     from athad_cond_b200._abi import FIELD
@@ -268,7 +276,13 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", default=None, help="IMxJMxKM (default: the 41x181x361 workload)")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
+    global GRID
+    if args.grid:
+        GRID = tuple(int(x) for x in args.grid.lower().split("x"))
     if args.warmup < 3:
         args.warmup = 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -292,7 +306,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                  device_id=device)
     r = run_ours(args, rank, world, device)
-    base = cpu_baseline() if (rank == 0 and world == 1) else None
+    base = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     if world > 1:
         import torch.distributed as tdist
         tdist.barrier()

@@ -126,3 +126,21 @@ def test_densities_bit_exact(ref, set_water):
         assert np.array_equal(R.get2(n), o.f2[n]), n
     for n in ("rho_base", "dlnrho_dr"):
         assert np.array_equal(R.getp(n), o.prof[n]), n
+
+
+MC_FIELDS = ["s", "s_u", "s_d", "M_u", "M_d", "q_v_u", "q_c_u", "q_v_d", "u_u", "v_u", "w_u",
+             "u_d", "v_d", "w_d", "E_u", "D_u", "E_d", "D_d", "c_u", "e_l", "e_d", "e_p", "g_p",
+             "P_conv", "CloudBase", "LevelFreeSinking", "Deep_beg", "Deep_end",
+             "MC_t", "MC_q", "MC_v", "MC_w"]
+
+
+def test_moist_convection_bit_exact_two_calls(ref):
+    """Two consecutive calls: the second reads the first's leftovers (E_u, D_u, w_u, ...
+    are not reset between calls, MoistConvection.h:339-376)."""
+    R, o = fresh(ref)
+    for n in ("Evaporation", "Q_sensible_2D"):
+        o.f2[n][:] = R.get2(n)
+    for it in (2, 4):
+        R.lib.ref_moist(R.h, it)
+        o.moist_convection(it, compat=1)
+        assert_identical(R, o, MC_FIELDS)
