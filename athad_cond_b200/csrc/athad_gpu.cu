@@ -47,7 +47,7 @@ Layout make_layout(const athad_grid& g)
     b += ATHAD_NPROFILES * round_up((size_t)g.im, 64) * sizeof(double);
     b += round_up((size_t)g.im * g.jm * sizeof(GeoIJ), 256);
     b += round_up((size_t)g.im * g.jm * sizeof(PoiIJ), 256);
-    b += 4 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat
+    b += 6 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose
     b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
     b += 256;                                                                         // counters
     L.bytes = b;
@@ -76,6 +76,8 @@ struct athad_ctx {
     double* height = nullptr;
     double* step_f = nullptr;
     double* coslat = nullptr;
+    double* step_mc = nullptr;
+    double* cose = nullptr;
     double* row_sum = nullptr;
     double* row_cnt = nullptr;
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
@@ -201,6 +203,8 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     c->height = (double*)take(nmax);
     c->step_f = (double*)take(nmax);
     c->coslat = (double*)take(nmax);
+    c->step_mc = (double*)take(nmax);
+    c->cose = (double*)take(nmax);
     c->row_sum = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->counters = (unsigned long long*)take(256);
@@ -252,6 +256,16 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
         const float h0 = (float)height[i];
         step[i] = (double)(float)(h1 - h0);
     }
+    // MoistConvection::precompute (MoistConvection.h:300-309): double differences of the
+    // layer heights; and cos(theta_equator - theta_j) of entrainmentGradients (:239) with
+    // the equator row (jm-1)/2, mirror-symmetric
+    std::vector<double> step_mc(im), cose(jm);
+    for (int i = 0; i < im - 1; i++) step_mc[i] = height[i + 1] - height[i];
+    step_mc[im - 1] = step_mc[im - 2];
+    for (int j = 0; j < jm; j++) {
+        const int jj = (j < jm - 1 - j) ? j : jm - 1 - j;
+        cose[j] = std::cos(the[(jm - 1) / 2] - the[jj]);
+    }
     std::vector<GeoIJ> geo((size_t)im * jm);
     std::vector<PoiIJ> poi((size_t)im * jm);
     const double inv_dr2 = 1.0 / (c->dr * c->dr), inv_dthe2 = 1.0 / (c->dthe * c->dthe),
@@ -273,6 +287,9 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
             G.inv_rm2sinthe = G.inv_rm2 / G.sinthe;
             G.inv_rm2sinthe2 = G.inv_rm2 / G.sinthe2;
             G.costhe_inv_rm2sinthe = G.costhe * G.inv_rm2sinthe;
+            G.two_over_rm_exp = 2.0 * G.inv_rm * G.exp_rm;
+            G.v_metric = (1.0 + G.costhe * G.costhe / G.sinthe2) * G.inv_rm2;
+            G.cos4lat = G.sinthe2 * G.sinthe2;
             PoiIJ& P = poi[(size_t)i * jm + j];          // PressureSolverAtm.h:236-269
             const double m_the = params->poisson_metric_fix ? G.inv_rm2 : G.inv_rm;
             const double m_phi = params->poisson_metric_fix ? G.inv_rm2sinthe2 : G.inv_rmsinthe;
@@ -291,6 +308,8 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->height, height.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "height");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_f, step.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->coslat, coslat.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "coslat");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_mc, step_mc.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step_mc");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->cose, cose.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "cose");
     if (s == ATHAD_OK) s = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
     if (s != ATHAD_OK) {
         cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
@@ -462,6 +481,13 @@ athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
     a.coeff_MC_t = p.L_atm / (p.u_0 * p.t_0);
     a.lv = p.lv; a.ls = p.ls; a.g = p.g; a.u_0 = p.u_0; a.L_atm = p.L_atm; a.re_turb = p.re_turb;
     a.pr_turb = p.pr_turb; a.sc_WaterVapour = p.sc_WaterVapour; a.sc_CO2 = p.sc_CO2;
+    a.inv_re = 1.0 / p.re_turb;
+    a.nue_max = 1000.0 / (p.u_0 * p.L_atm);
+    a.nue_air_nd = 1.5e-5 / (p.u_0 * p.L_atm);
+    a.diff_prec_re_inv = 1.0 / (p.sc_WaterVapour * p.re_turb);
+    a.diff_co2_re_inv = 1.0 / (p.sc_CO2 * p.re_turb);
+    a.buoy_pref = s->buoyancy_ramp * 1.0 * p.g * s->dt / p.u_0;
+    a.drag_pref = 1.0 / 86400.0 * p.L_atm / p.u_0 * s->dt;
     a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
     a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
     a.write_diag = s->write_diagnostics;
@@ -581,8 +607,24 @@ athad_status athad_densities(athad_ctx* ctx, int32_t set_water_profile)
 
 athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n)
 {
-    (void)iter_n;
-    return fail(ctx, ATHAD_ERR_UNSUPPORTED, "moist_convection: not built yet");
+    (void)iter_n;   // MoistConvection::run keeps it (m.iter_n) but no phase reads it
+    if (!ctx) return ATHAD_ERR_INVALID;
+    const athad_params& p = ctx->p;
+    MoistArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    for (int f = 0; f < ATHAD_NFIELDS; f++) a.F[f] = ctx->field[f];
+    a.evaporation = ctx->f2d[ATHAD_2D_EVAPORATION];
+    a.q_sensible = ctx->f2d[ATHAD_2D_Q_SENSIBLE];
+    a.height = ctx->height; a.step = ctx->step_mc; a.cose = ctx->cose;
+    a.t_0 = p.t_0; a.cp_l = p.cp_l; a.s_0 = p.s_0; a.lv = p.lv; a.ls = p.ls; a.g = p.g; a.u_0 = p.u_0;
+    a.r_Earth = p.r_Earth; a.p_0 = p.p_0; a.co2_0 = p.co2_0; a.c_0 = p.c_0; a.M_bg = p.M_bg; a.R_bg = p.R_bg;
+    a.convection_perturbation = p.convection_perturbation;
+    a.convection_mode = p.convection_mode;
+    a.iter_prec = p.iter_prec;
+    launch_moist_convection(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "moist_convection");
+    return ATHAD_OK;
 }
 
 athad_status athad_get_report(athad_ctx* ctx, athad_report* out)

@@ -42,6 +42,10 @@ ATHAD_HD double safe_clamp(double v, double lo, double hi)
 struct GeoIJ {
     double exp_rm, exp_2_rm, sinthe, sinthe2, costhe;
     double inv_rm, inv_rm2, inv_rmsinthe, inv_rm2sinthe, inv_rm2sinthe2, costhe_inv_rm2sinthe;
+    // products the right-hand side forms from the factors above, evaluated once per (i,j)
+    // with the same operations: 2*inv_rm*exp_rm (RHS_Atm_Turb.cpp:858),
+    // (1 + costhe^2/sinthe2)*inv_rm2 (:864), sinthe2^2 (:985)
+    double two_over_rm_exp, v_metric, cos4lat;
 };
 
 // Grid extents and the strides of a pitched field: element (i,j,k) is at

@@ -66,38 +66,32 @@ __device__ __forceinline__ double minmod(double a, double b)
     return (a * b <= 0.0) ? 0.0 : (fabs(a) < fabs(b) ? a : b);
 }
 
-// Central derivatives of one field at one cell (RHS_Atm_Turb.cpp:121-123, 223-225, 327-329).
-struct Der {
-    double c;                       // centre value
-    double d1r, d2r, d1t, d2t, d1p, d2p;
-    double ar, at, ap;              // minmod-limited advective gradients
+// The 7-point star of one field at one cell.
+struct Star {
+    double c, ip, im, jp, jm, kp, km;
 };
-
-template <bool LIMIT>
-__device__ __forceinline__ Der derivs(const double* __restrict__ F, long long c, long long sI,
-                                      long long sJ, const RK4Args& a)
+__device__ __forceinline__ Star load_star(const double* __restrict__ F, long long c, long long sI, long long sJ)
 {
-    const double f0 = __ldg(F + c);
-    const double fip = __ldg(F + c + sI), fim = __ldg(F + c - sI);
-    const double fjp = __ldg(F + c + sJ), fjm = __ldg(F + c - sJ);
-    const double fkp = __ldg(F + c + 1), fkm = __ldg(F + c - 1);
-    Der r;
-    r.c = f0;
-    r.d1r = (fip - fim) * a.inv_2dr;
-    r.d2r = (fip - 2.0 * f0 + fim) * a.inv_dr2;
-    r.d1t = (fjp - fjm) * a.inv_2dthe;
-    r.d2t = ((fjp + fjm) - 2.0 * f0) * a.inv_dthe2;     // mirror-exact form
-    r.d1p = (fkp - fkm) * a.inv_2dphi;
-    r.d2p = (fkp - 2.0 * f0 + fkm) * a.inv_dphi2;
-    if (LIMIT) {   // RHS_Atm_Turb.cpp:788-814; inv_dr = 2 * inv_2dr as in :762-764
-        r.ar = minmod(f0 - fim, fip - f0) * (2.0 * a.inv_2dr);
-        r.at = minmod(f0 - fjm, fjp - f0) * (2.0 * a.inv_2dthe);
-        r.ap = minmod(f0 - fkm, fkp - f0) * (2.0 * a.inv_2dphi);
-    } else {
-        r.ar = r.d1r; r.at = r.d1t; r.ap = r.d1p;
-    }
-    return r;
+    Star s;
+    s.c = __ldg(F + c);
+    s.ip = __ldg(F + c + sI); s.im = __ldg(F + c - sI);
+    s.jp = __ldg(F + c + sJ); s.jm = __ldg(F + c - sJ);
+    s.kp = __ldg(F + c + 1);  s.km = __ldg(F + c - 1);
+    return s;
 }
+// central first differences (RHS_Atm_Turb.cpp:122, 224, 328)
+__device__ __forceinline__ double d1r(const Star& s, const RK4Args& a) { return (s.ip - s.im) * a.inv_2dr; }
+__device__ __forceinline__ double d1t(const Star& s, const RK4Args& a) { return (s.jp - s.jm) * a.inv_2dthe; }
+__device__ __forceinline__ double d1p(const Star& s, const RK4Args& a) { return (s.kp - s.km) * a.inv_2dphi; }
+// second differences (:123, :329); the meridional one sums the two neighbours first, the
+// mirror-exact form of :225
+__device__ __forceinline__ double d2r(const Star& s, const RK4Args& a) { return (s.ip - 2.0 * s.c + s.im) * a.inv_dr2; }
+__device__ __forceinline__ double d2t(const Star& s, const RK4Args& a) { return ((s.jp + s.jm) - 2.0 * s.c) * a.inv_dthe2; }
+__device__ __forceinline__ double d2p(const Star& s, const RK4Args& a) { return (s.kp - 2.0 * s.c + s.km) * a.inv_dphi2; }
+// minmod-limited advective gradients (:788-814), inv_dx = 2 * inv_2dx (:762-764)
+__device__ __forceinline__ double ar(const Star& s, const RK4Args& a) { return minmod(s.c - s.im, s.ip - s.c) * (2.0 * a.inv_2dr); }
+__device__ __forceinline__ double at(const Star& s, const RK4Args& a) { return minmod(s.c - s.jm, s.jp - s.c) * (2.0 * a.inv_2dthe); }
+__device__ __forceinline__ double ap(const Star& s, const RK4Args& a) { return minmod(s.c - s.km, s.kp - s.c) * (2.0 * a.inv_2dphi); }
 
 // Stage update of one field (RungeKutta_Atm_Turb.cpp:167-182, 199-209, 226-236, 253-263).
 // Field n: 0 t, 1 u, 2 v, 3 w, 4 c, 5 cloud, 6 ice, 7 gr, 8 co2, 9 tke, 10 dis.
@@ -125,8 +119,12 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
     a.Yout[n][c] = out;
 }
 
+// One RK4 stage.  The right-hand side is evaluated in the order that keeps the fewest
+// values live (turbulence, momentum, temperature, tracers), each term with the operation
+// order of RHS_Atm_Turb.cpp; stencil values a later phase needs again are re-read, which
+// hits L1.
 template <int STAGE>
-__global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
+__global__ void __launch_bounds__(128, 4) rk4_stage_kernel(const RK4Args a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -149,41 +147,30 @@ __global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
         return;
     }
     const long long sI = d.plane, sJ = d.pitch;
-    const GeoIJ G = a.geo[i * d.jm + j];
-    const double exp_rm = G.exp_rm, exp_2_rm = G.exp_2_rm;
-    const double sinthe = G.sinthe, sinthe2 = G.sinthe2, costhe = G.costhe;
-    const double inv_rm = G.inv_rm, inv_rm2 = G.inv_rm2, inv_rmsinthe = G.inv_rmsinthe;
-    const double inv_rm2sinthe = G.inv_rm2sinthe, inv_rm2sinthe2 = G.inv_rm2sinthe2;
-    const double cos_rm2sin = G.costhe_inv_rm2sinthe;
+    const GeoIJ* G = a.geo + (i * d.jm + j);
+    const double exp_rm = G->exp_rm, inv_rm = G->inv_rm, inv_rmsinthe = G->inv_rmsinthe;
 
-    // velocities
-    const Der U = derivs<true>(a.Yin[1], c, sI, sJ, a);
-    const Der V = derivs<true>(a.Yin[2], c, sI, sJ, a);
-    const Der W = derivs<true>(a.Yin[3], c, sI, sJ, a);
-    const double u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
-    // pressure gradient
-    const double* P = a.p_dyn;
-    const double dpdr = (__ldg(P + c + sI) - __ldg(P + c - sI)) * a.inv_2dr;
-    const double dpdthe = (__ldg(P + c + sJ) - __ldg(P + c - sJ)) * a.inv_2dthe;
-    const double dpdphi = (__ldg(P + c + 1) - __ldg(P + c - 1)) * a.inv_2dphi;
+    const double u_ijk = __ldg(a.Yin[1] + c), v_ijk = __ldg(a.Yin[2] + c), w_ijk = __ldg(a.Yin[3] + c);
     const double nue_ijk = __ldg(a.nue + c);
+    const double u_exp = u_ijk * exp_rm, v_invrm = v_ijk * inv_rm, w_invrs = w_ijk * inv_rmsinthe;
+    const double diffusion_vel_re = (a.inv_re + nue_ijk) * a.diffusion_ramp;
 
-    // ---- turbulence: production (RHS_Atm_Turb.cpp:528-561) ----
-    const Der TK = derivs<false>(a.Yin[9], c, sI, sJ, a);
-    const Der DI = derivs<false>(a.Yin[10], c, sI, sJ, a);
-    const double tke_ijk = TK.c, dis_ijk = DI.c;
+    // ---- turbulence: production from the velocity shear (RHS_Atm_Turb.cpp:528-561) ----
     double prod;
     {
-        const double dudr_s = U.d1r * exp_rm, dvdr_s = V.d1r * exp_rm, dwdr_s = W.d1r * exp_rm;
-        const double dudthe_s = U.d1t * inv_rm, dvdthe_s = V.d1t * inv_rm, dwdthe_s = W.d1t * inv_rm;
-        const double dudphi_s = U.d1p * inv_rmsinthe, dvdphi_s = V.d1p * inv_rmsinthe,
-                     dwdphi_s = W.d1p * inv_rmsinthe;
+        const Star U = load_star(a.Yin[1], c, sI, sJ);
+        const Star V = load_star(a.Yin[2], c, sI, sJ);
+        const Star W = load_star(a.Yin[3], c, sI, sJ);
+        const double dudr_s = d1r(U, a) * exp_rm, dvdr_s = d1r(V, a) * exp_rm, dwdr_s = d1r(W, a) * exp_rm;
+        const double dudthe_s = d1t(U, a) * inv_rm, dvdthe_s = d1t(V, a) * inv_rm, dwdthe_s = d1t(W, a) * inv_rm;
+        const double dudphi_s = d1p(U, a) * inv_rmsinthe, dvdphi_s = d1p(V, a) * inv_rmsinthe,
+                     dwdphi_s = d1p(W, a) * inv_rmsinthe;
+        const double tke_ijk = __ldg(a.Yin[9] + c), dis_ijk = __ldg(a.Yin[10] + c);
         const double dis_here = smax(dis_ijk, 1.0e-10);
         const double tke_here = smax(tke_ijk, 0.0);
-        const double nue_max = 1000.0 / (a.u_0 * a.L_atm);
         double cnue = (a.turb_model == ATHAD_TURB_K_EPSILON) ? 0.028 * tke_here * tke_here / dis_here
                                                             : tke_here / dis_here;
-        cnue = smin(cnue, nue_max);
+        cnue = smin(cnue, a.nue_max);
         const double der = 0.66667 * (dudr_s + dvdthe_s + dwdphi_s);
         prod = smax(0.0,
               (cnue * (2.0 * dudr_s - der) - 0.66667 * tke_ijk) * dudr_s
@@ -196,32 +183,37 @@ __global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
             + (cnue * (dwdr_s + dudphi_s)) * dwdr_s
             + (cnue * (dwdthe_s + dvdphi_s)) * dwdthe_s);
     }
-    // ---- closures (RHS_Atm_Turb.cpp:563-721) ----
-    double diffusion_t_re, diffusion_vel_re, diffusion_tke_re, diffusion_dis_re;
-    double tke_source, dis_source;
+
+    // ---- tke and omega/epsilon: closure, sources, transport, diffusion ----
+    //      (RHS_Atm_Turb.cpp:563-721, 835-836, 936-942, 1074-1075)
     {
-        const double inv_re = 1.0 / a.re_turb;
-        diffusion_t_re = (inv_re + nue_ijk) / a.pr_turb;
-        diffusion_vel_re = inv_re + nue_ijk;
+        const double exp_2_rm = G->exp_2_rm, inv_rm2 = G->inv_rm2, inv_rm2sinthe2 = G->inv_rm2sinthe2;
+        const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
+        const Star TK = load_star(a.Yin[9], c, sI, sJ);
+        const Star DI = load_star(a.Yin[10], c, sI, sJ);
+        const double tke_ijk = TK.c, dis_ijk = DI.c;
+        const double dtkedr = d1r(TK, a), dtkedthe = d1t(TK, a), dtkedphi = d1p(TK, a);
+        const double ddisdr = d1r(DI, a), ddisdthe = d1t(DI, a), ddisdphi = d1p(DI, a);
         const double tke_s = smax(tke_ijk, 1.0e-10), dis_s = smax(dis_ijk, 1.0e-10);
         const double dis_src_max = 20.0 * dis_s * dis_s, tke_src_max = 20.0 * tke_s * dis_s;
+        double diffusion_tke_re, diffusion_dis_re, tke_source, dis_source;
         if (a.turb_model == ATHAD_TURB_K_EPSILON) {
-            diffusion_tke_re = inv_re + nue_ijk / 1.0;
-            diffusion_dis_re = inv_re + nue_ijk / 1.3;
+            diffusion_tke_re = a.inv_re + nue_ijk / 1.0;
+            diffusion_dis_re = a.inv_re + nue_ijk / 1.3;
             const double P_k = prod, Y_k = dis_s;
             const double P_w = 1.35 * (dis_s / tke_s) * P_k;
             const double Y_w = 1.80 * dis_s * dis_s / tke_s;
             tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
             dis_source = sclamp(P_w - Y_w, -dis_src_max, dis_src_max);
         } else if (a.turb_model == ATHAD_TURB_K_OMEGA) {
-            diffusion_tke_re = inv_re + 0.6 * nue_ijk;
-            diffusion_dis_re = inv_re + 0.5 * nue_ijk;
+            diffusion_tke_re = a.inv_re + 0.6 * nue_ijk;
+            diffusion_dis_re = a.inv_re + 0.5 * nue_ijk;
             const double P_k = smin(prod, 20.0 * 0.09 * tke_s * dis_s);
             const double Y_k = 0.09 * tke_s * dis_s;
             const double P_w = 0.52 * (dis_s / tke_s) * P_k;
             const double Y_w = 0.0708 * dis_s * dis_s;
-            const double cross = TK.d1r * DI.d1r + TK.d1t * inv_rm * DI.d1t * inv_rm
-                               + TK.d1p * inv_rmsinthe * DI.d1p * inv_rmsinthe;
+            const double cross = dtkedr * ddisdr + dtkedthe * inv_rm * ddisdthe * inv_rm
+                               + dtkedphi * inv_rmsinthe * ddisdphi * inv_rmsinthe;
             const double sig_d = (cross <= 0.0) ? 0.0 : 0.125;
             const double D_w = sig_d * cross / dis_s;
             tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
@@ -232,23 +224,23 @@ __global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
             // ATHAD_WALL_MIRROR measures the meridional distance to the nearer pole
             double d_j = (double)j;
             if (a.wall_mode == ATHAD_WALL_MIRROR) { const int jr = d.jm - 1 - j; if (jr < j) d_j = (double)jr; }
-            const double d_k = (double)k;
             double d_close = (double)i;
             if (d_j <= d_close) d_close = d_j;
-            if (d_k <= d_close) d_close = d_k;
-            const double cross = TK.d1r * DI.d1r + TK.d1t * inv_rm * DI.d1t * inv_rm
-                               + TK.d1p * inv_rmsinthe * DI.d1p * inv_rmsinthe;
+            if ((double)k <= d_close) d_close = (double)k;
+            const double cross = dtkedr * ddisdr + dtkedthe * inv_rm * ddisdthe * inv_rm
+                               + dtkedphi * inv_rmsinthe * ddisdphi * inv_rmsinthe;
             const double CD_kw = smax((2.0 * sig_w2) / dis_ijk * cross, 1.0e-20);
-            const double nue_air_nd = 1.5e-5 / (a.u_0 * a.L_atm);
             const double arg1 = smin(smax(
                 sqrt(tke_ijk) / (bet_star * dis_ijk * d_close),
-                (500.0 * nue_air_nd) / (d_close * d_close * dis_ijk)),
+                (500.0 * a.nue_air_nd) / (d_close * d_close * dis_ijk)),
                 (4.0 * sig_w2 * tke_ijk) / (CD_kw * d_close * d_close));
-            const double F1 = tanh(pow(arg1, 4.0));
+            // pow(arg1, 4) as two squarings: both within two ulp of the exact value
+            const double a2 = arg1 * arg1;
+            const double F1 = tanh(a2 * a2);
             const double bk = F1 * 1.176 + (1.0 - F1) * 1.0;
             const double bw = F1 * 2.0 + (1.0 - F1) * sig_w2;
-            diffusion_tke_re = inv_re + nue_ijk / bk;
-            diffusion_dis_re = inv_re + nue_ijk / bw;
+            diffusion_tke_re = a.inv_re + nue_ijk / bk;
+            diffusion_dis_re = a.inv_re + nue_ijk / bw;
             const double P_k = smin(prod, 20.0 * bet_star * tke_s * dis_s);
             const double Y_k = bet_star * tke_s * dis_s;
             const double P_w = (F1 * 0.413 + (1.0 - F1) * 0.2) * P_k * dis_s / tke_s;
@@ -257,127 +249,145 @@ __global__ void __launch_bounds__(128) rk4_stage_kernel(const RK4Args a)
             tke_source = sclamp(P_k - Y_k, -tke_src_max, tke_src_max);
             dis_source = sclamp(P_w - Y_w + D_w, -dis_src_max, dis_src_max);
         }
-        diffusion_t_re *= a.diffusion_ramp;
-        diffusion_vel_re *= a.diffusion_ramp;
         diffusion_tke_re *= a.diffusion_ramp;
         diffusion_dis_re *= a.diffusion_ramp;
-    }
-
-    // ---- transport / diffusion / assembly (RHS_Atm_Turb.cpp:748-1079) ----
-    const double u_exp = u_ijk * exp_rm, v_invrm = v_ijk * inv_rm, w_invrs = w_ijk * inv_rmsinthe;
-    const double two_over_rm_exp = 2.0 * inv_rm * exp_rm;
-    const double v_metric = (1.0 + costhe * costhe / sinthe2) * inv_rm2;
-    const double dpdr_exp = dpdr * exp_rm, dpdthe_invrm = dpdthe * inv_rm, dpdphi_invrs = dpdphi * inv_rmsinthe;
-    const double nontrad = a.nontrad ? 1.0 : 0.0;
-    const double coriolis_rad = nontrad * 2.0 * sinthe * w_ijk;
-    const double coriolis_the = 2.0 * costhe * w_ijk;
-    const double coriolis_phi = -2.0 * (costhe * v_ijk + nontrad * sinthe * u_ijk);
-    double tr_u = u_exp * U.ar + v_invrm * U.at + w_invrs * U.ap;
-    double tr_v = u_exp * V.ar + v_invrm * V.at + w_invrs * V.ap;
-    double tr_w = u_exp * W.ar + v_invrm * W.at + w_invrs * W.ap;
-    if (a.curvature) {
-        const double cotanthe = costhe / sinthe;
-        tr_u += -(v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
-        tr_v += (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
-        tr_w += (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
-    }
-    const double diffusion_u = (U.d2r * exp_2_rm + 2.0 * u_ijk * inv_rm2
-        + U.d2t * inv_rm2 + 4.0 * U.d1r * inv_rm * exp_rm
-        + U.d1t * cos_rm2sin + U.d2p * inv_rm2sinthe2) * diffusion_vel_re;
-    const double diffusion_v = (V.d2r * exp_2_rm + V.d1r * two_over_rm_exp
-        + V.d2t * inv_rm2 + V.d1t * cos_rm2sin
-        - v_metric * v_ijk + V.d2p * inv_rm2sinthe2
-        + 2.0 * U.d1t * inv_rm2
-        - W.d1p * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
-    const double diffusion_w = (W.d2r * exp_2_rm + W.d1r * two_over_rm_exp
-        + W.d2t * inv_rm2 + W.d1t * cos_rm2sin
-        - v_metric * w_ijk + W.d2p * inv_rm2sinthe2
-        + 2.0 * U.d1p * inv_rm2sinthe
-        + V.d1p * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
-
-    // temperature
-    const Der T = derivs<true>(a.Yin[0], c, sI, sJ, a);
-    const double t_ijk = T.c;
-    const double r_h = __ldg(a.r_humid + c);
-    const double rhs_u = -dpdr_exp - tr_u + diffusion_u
-        + a.buoyancy_ramp * 1.0 * a.g * a.dt / a.u_0 * (t_ijk - __ldg(a.t_ref + i))
-        + 1.0 * a.force_nd * coriolis_rad;
-    double drag_profile = 1.0 - (double)(i - 0) / 5.0;
-    if (drag_profile < 0.0) drag_profile = 0.0;
-    if (drag_profile > 1.0) drag_profile = 1.0;
-    const double surf_drag = (1.0 / 86400.0 * a.L_atm / a.u_0 * a.dt) * drag_profile;
-    const double rhs_v = -dpdthe_invrm - tr_v + diffusion_v
-        + 1.0 * a.force_nd * coriolis_the
-        + a.coeff_MC_vel * __ldg(a.MC_v + c)
-        - surf_drag * v_ijk;
-    const double rhs_w = -dpdphi_invrs - tr_w + diffusion_w
-        + 1.0 * a.force_nd * coriolis_phi
-        + a.coeff_MC_vel * __ldg(a.MC_w + c)
-        - surf_drag * w_ijk;
-    stage_update<STAGE>(a, 1, c, rhs_u);
-    stage_update<STAGE>(a, 2, c, rhs_v);
-    stage_update<STAGE>(a, 3, c, rhs_w);
-    if (STAGE == 4) {
-        a.aux_u[c] = rhs_u + dpdr_exp;
-        a.aux_v[c] = rhs_v + dpdthe_invrm;
-        a.aux_w[c] = rhs_w + dpdphi_invrs;
-        if (a.write_diag) {
+        const double tr_tke = u_exp * dtkedr + v_invrm * dtkedthe + w_invrs * dtkedphi;
+        const double tr_dis = u_exp * ddisdr + v_invrm * ddisdthe + w_invrs * ddisdphi;
+        const double diffusion_tke = (d2r(TK, a) * exp_2_rm + dtkedr * two_over_rm_exp
+            + d2t(TK, a) * inv_rm2 + dtkedthe * cos_rm2sin + d2p(TK, a) * inv_rm2sinthe2) * diffusion_tke_re;
+        const double diffusion_dis = (d2r(DI, a) * exp_2_rm + ddisdr * two_over_rm_exp
+            + d2t(DI, a) * inv_rm2 + ddisdthe * cos_rm2sin + d2p(DI, a) * inv_rm2sinthe2) * diffusion_dis_re;
+        stage_update<STAGE>(a, 9, c, -tr_tke + diffusion_tke + tke_source);
+        stage_update<STAGE>(a, 10, c, -tr_dis + diffusion_dis + dis_source);
+        if (STAGE == 4 && a.write_diag) {
             a.prod[c] = prod;
             a.tke_source[c] = tke_source;
             a.dis_source[c] = dis_source;
         }
     }
+
+    // ---- momentum (RHS_Atm_Turb.cpp:816-828, 870-884, 1001-1057, 1077-1079) ----
     {
-        const double pressure_t = a.coeff_energy_p * (u_exp * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
-        const double tr_t = u_exp * T.ar + v_invrm * T.at + w_invrs * T.ap;
-        const double diffusion_t = (T.d2r * exp_2_rm + T.d1r * two_over_rm_exp
-            + T.d2t * inv_rm2 + T.d1t * cos_rm2sin + T.d2p * inv_rm2sinthe2) * diffusion_t_re;
-        double rhs_t = pressure_t - tr_t + diffusion_t
-            + a.coeff_MC_t * __ldg(a.MC_t + c)
-            + a.coeff_energy * (__ldg(a.S_c + c) + __ldg(a.S_r + c)) * a.lv * r_h
-            + a.coeff_energy * (__ldg(a.S_i + c) + __ldg(a.S_s + c) + __ldg(a.S_g + c)) * a.ls * r_h;
-        // Held-Suarez relaxation, RHS_Atm_Turb.cpp:977-992
-        const double k_a = 1.0 / (4.0 * 86400.0), k_s = 1.0 / (0.4 * 86400.0), sigma_b = 0.7;
-        const double p_surf = __ldg(a.p_stat + idx3(d, 0, j, k));
-        const double sigma = (p_surf > 0.0) ? __ldg(a.p_stat + c) / p_surf : 0.0;
-        double bl = (sigma - sigma_b) / (1.0 - sigma_b);
-        if (bl < 0.0) bl = 0.0;
-        const double cos4lat = sinthe2 * sinthe2;
-        const double k_T = k_a + (k_s - k_a) * bl * cos4lat;
-        rhs_t -= (k_T * a.L_atm / a.u_0) * (t_ijk - __ldg(a.t_eq + c));
-        stage_update<STAGE>(a, 0, c, rhs_t);
+        const double exp_2_rm = G->exp_2_rm, inv_rm2 = G->inv_rm2, inv_rm2sinthe2 = G->inv_rm2sinthe2;
+        const double inv_rm2sinthe = G->inv_rm2sinthe;
+        const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
+        const double sinthe = G->sinthe, costhe = G->costhe, v_metric = G->v_metric;
+        const double* P = a.p_dyn;
+        const double dpdr = (__ldg(P + c + sI) - __ldg(P + c - sI)) * a.inv_2dr;
+        const double dpdthe = (__ldg(P + c + sJ) - __ldg(P + c - sJ)) * a.inv_2dthe;
+        const double dpdphi = (__ldg(P + c + 1) - __ldg(P + c - 1)) * a.inv_2dphi;
+        const double dpdr_exp = dpdr * exp_rm, dpdthe_invrm = dpdthe * inv_rm, dpdphi_invrs = dpdphi * inv_rmsinthe;
+        const double nontrad = a.nontrad ? 1.0 : 0.0;
+        const double cotanthe = a.curvature ? costhe / sinthe : 0.0;
+        double drag_profile = 1.0 - (double)(i - 0) / 5.0;
+        if (drag_profile < 0.0) drag_profile = 0.0;
+        if (drag_profile > 1.0) drag_profile = 1.0;
+        const double surf_drag = a.drag_pref * drag_profile;
+        double dudthe, dudphi, dvdphi, part_v;
+        {   // u
+            const Star U = load_star(a.Yin[1], c, sI, sJ);
+            dudthe = d1t(U, a);
+            dudphi = d1p(U, a);
+            double tr_u = u_exp * ar(U, a) + v_invrm * at(U, a) + w_invrs * ap(U, a);
+            if (a.curvature) tr_u += -(v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
+            const double diffusion_u = (d2r(U, a) * exp_2_rm + 2.0 * u_ijk * inv_rm2
+                + d2t(U, a) * inv_rm2 + 4.0 * d1r(U, a) * inv_rm * exp_rm
+                + dudthe * cos_rm2sin + d2p(U, a) * inv_rm2sinthe2) * diffusion_vel_re;
+            const double t_ijk = __ldg(a.Yin[0] + c);
+            const double coriolis_rad = nontrad * 2.0 * sinthe * w_ijk;
+            const double rhs_u = -dpdr_exp - tr_u + diffusion_u
+                + a.buoy_pref * (t_ijk - __ldg(a.t_ref + i))
+                + 1.0 * a.force_nd * coriolis_rad;
+            stage_update<STAGE>(a, 1, c, rhs_u);
+            if (STAGE == 4) a.aux_u[c] = rhs_u + dpdr_exp;
+        }
+        {   // v: every term but the w-shear one, which closes the sum below
+            const Star V = load_star(a.Yin[2], c, sI, sJ);
+            dvdphi = d1p(V, a);
+            part_v = V.c;   // placeholder for register reuse
+            double tr_v = u_exp * ar(V, a) + v_invrm * at(V, a) + w_invrs * ap(V, a);
+            if (a.curvature) tr_v += (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
+            part_v = d2r(V, a) * exp_2_rm + d1r(V, a) * two_over_rm_exp
+                + d2t(V, a) * inv_rm2 + d1t(V, a) * cos_rm2sin
+                - v_metric * v_ijk + d2p(V, a) * inv_rm2sinthe2
+                + 2.0 * dudthe * inv_rm2;
+            // w shear term of diffusion_v needs dw/dphi: only the zonal neighbours of w
+            const double dwdphi = (__ldg(a.Yin[3] + c + 1) - __ldg(a.Yin[3] + c - 1)) * a.inv_2dphi;
+            const double diffusion_v = (part_v - dwdphi * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
+            const double coriolis_the = 2.0 * costhe * w_ijk;
+            const double rhs_v = -dpdthe_invrm - tr_v + diffusion_v
+                + 1.0 * a.force_nd * coriolis_the
+                + a.coeff_MC_vel * __ldg(a.MC_v + c)
+                - surf_drag * v_ijk;
+            stage_update<STAGE>(a, 2, c, rhs_v);
+            if (STAGE == 4) a.aux_v[c] = rhs_v + dpdthe_invrm;
+        }
+        {   // w
+            const Star W = load_star(a.Yin[3], c, sI, sJ);
+            double tr_w = u_exp * ar(W, a) + v_invrm * at(W, a) + w_invrs * ap(W, a);
+            if (a.curvature) tr_w += (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
+            const double diffusion_w = (d2r(W, a) * exp_2_rm + d1r(W, a) * two_over_rm_exp
+                + d2t(W, a) * inv_rm2 + d1t(W, a) * cos_rm2sin
+                - v_metric * w_ijk + d2p(W, a) * inv_rm2sinthe2
+                + 2.0 * dudphi * inv_rm2sinthe
+                + dvdphi * 2.0 * costhe * inv_rm2sinthe2) * diffusion_vel_re;
+            const double coriolis_phi = -2.0 * (costhe * v_ijk + nontrad * sinthe * u_ijk);
+            const double rhs_w = -dpdphi_invrs - tr_w + diffusion_w
+                + 1.0 * a.force_nd * coriolis_phi
+                + a.coeff_MC_vel * __ldg(a.MC_w + c)
+                - surf_drag * w_ijk;
+            stage_update<STAGE>(a, 3, c, rhs_w);
+            if (STAGE == 4) a.aux_w[c] = rhs_w + dpdphi_invrs;
+        }
+        // ---- temperature (RHS_Atm_Turb.cpp:752, 829, 866-868, 963-992) ----
+        {
+            const Star T = load_star(a.Yin[0], c, sI, sJ);
+            const double t_ijk = T.c;
+            const double r_h = __ldg(a.r_humid + c);
+            const double pressure_t = a.coeff_energy_p * (u_exp * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
+            const double tr_t = u_exp * ar(T, a) + v_invrm * at(T, a) + w_invrs * ap(T, a);
+            const double diffusion_t_re = (a.inv_re + nue_ijk) / a.pr_turb * a.diffusion_ramp;
+            const double diffusion_t = (d2r(T, a) * exp_2_rm + d1r(T, a) * two_over_rm_exp
+                + d2t(T, a) * inv_rm2 + d1t(T, a) * cos_rm2sin + d2p(T, a) * inv_rm2sinthe2) * diffusion_t_re;
+            double rhs_t = pressure_t - tr_t + diffusion_t
+                + a.coeff_MC_t * __ldg(a.MC_t + c)
+                + a.coeff_energy * (__ldg(a.S_c + c) + __ldg(a.S_r + c)) * a.lv * r_h
+                + a.coeff_energy * (__ldg(a.S_i + c) + __ldg(a.S_s + c) + __ldg(a.S_g + c)) * a.ls * r_h;
+            const double k_a = 1.0 / (4.0 * 86400.0), k_s = 1.0 / (0.4 * 86400.0), sigma_b = 0.7;
+            const double p_surf = __ldg(a.p_stat + idx3(d, 0, j, k));
+            const double sigma = (p_surf > 0.0) ? __ldg(a.p_stat + c) / p_surf : 0.0;
+            double bl = (sigma - sigma_b) / (1.0 - sigma_b);
+            if (bl < 0.0) bl = 0.0;
+            const double k_T = k_a + (k_s - k_a) * bl * G->cos4lat;
+            rhs_t -= (k_T * a.L_atm / a.u_0) * (t_ijk - __ldg(a.t_eq + c));
+            stage_update<STAGE>(a, 0, c, rhs_t);
+        }
     }
-    // moisture and tracers (RHS_Atm_Turb.cpp:911-934, 1059-1072)
-    const double dlnrho_dr_i = a.tracer_diff_flux ? __ldg(a.dlnrho + i) * exp_2_rm : 0.0;
-    const double diff_prec_re_inv = 1.0 / (a.sc_WaterVapour * a.re_turb);
-    const double diff_co2_re_inv = 1.0 / (a.sc_CO2 * a.re_turb);
+    // ---- moisture and tracers (RHS_Atm_Turb.cpp:830-834, 911-934, 1059-1072) ----
+    {
+        const double exp_2_rm = G->exp_2_rm, inv_rm2 = G->inv_rm2, inv_rm2sinthe2 = G->inv_rm2sinthe2;
+        const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
+        const double dlnrho_dr_i = a.tracer_diff_flux ? __ldg(a.dlnrho + i) * exp_2_rm : 0.0;
+        const double r_h = __ldg(a.r_humid + c);
 #pragma unroll 1
-    for (int n = 4; n <= 8; n++) {
-        const Der Q = (n <= 6) ? derivs<true>(a.Yin[n], c, sI, sJ, a) : derivs<false>(a.Yin[n], c, sI, sJ, a);
-        const double coef = (n == 8) ? diff_co2_re_inv : diff_prec_re_inv;
-        const double tr = u_exp * Q.ar + v_invrm * Q.at + w_invrs * Q.ap;
-        const double dif = (Q.d2r * exp_2_rm + Q.d1r * two_over_rm_exp
-            + Q.d2t * inv_rm2 + Q.d1t * cos_rm2sin
-            + Q.d2p * inv_rm2sinthe2
-            + Q.d1r * dlnrho_dr_i) * coef;
-        double rhs;
-        if (n == 4)      rhs = -tr + dif + 1.0 * __ldg(a.S_v + c) * r_h + a.coeff_MC_q * __ldg(a.MC_q + c);
-        else if (n == 5) rhs = -tr + dif + 1.0 * __ldg(a.S_c + c) * r_h;
-        else if (n == 6) rhs = -tr + dif + 1.0 * __ldg(a.S_i + c) * r_h;
-        else if (n == 7) rhs = -tr + dif + 1.0 * __ldg(a.S_g + c) * r_h;
-        else             rhs = -tr + dif;
-        stage_update<STAGE>(a, n, c, rhs);
-    }
-    // tke and omega/epsilon (RHS_Atm_Turb.cpp:936-942, 1074-1075)
-    {
-        const double tr_tke = u_exp * TK.d1r + v_invrm * TK.d1t + w_invrs * TK.d1p;
-        const double tr_dis = u_exp * DI.d1r + v_invrm * DI.d1t + w_invrs * DI.d1p;
-        const double diffusion_tke = (TK.d2r * exp_2_rm + TK.d1r * two_over_rm_exp
-            + TK.d2t * inv_rm2 + TK.d1t * cos_rm2sin + TK.d2p * inv_rm2sinthe2) * diffusion_tke_re;
-        const double diffusion_dis = (DI.d2r * exp_2_rm + DI.d1r * two_over_rm_exp
-            + DI.d2t * inv_rm2 + DI.d1t * cos_rm2sin + DI.d2p * inv_rm2sinthe2) * diffusion_dis_re;
-        stage_update<STAGE>(a, 9, c, -tr_tke + diffusion_tke + tke_source);
-        stage_update<STAGE>(a, 10, c, -tr_dis + diffusion_dis + dis_source);
+        for (int n = 4; n <= 8; n++) {
+            const Star Q = load_star(a.Yin[n], c, sI, sJ);
+            const double coef = (n == 8) ? a.diff_co2_re_inv : a.diff_prec_re_inv;
+            const double tr = (n <= 6) ? (u_exp * ar(Q, a) + v_invrm * at(Q, a) + w_invrs * ap(Q, a))
+                                       : (u_exp * d1r(Q, a) + v_invrm * d1t(Q, a) + w_invrs * d1p(Q, a));
+            const double q1r = d1r(Q, a);
+            const double dif = (d2r(Q, a) * exp_2_rm + q1r * two_over_rm_exp
+                + d2t(Q, a) * inv_rm2 + d1t(Q, a) * cos_rm2sin
+                + d2p(Q, a) * inv_rm2sinthe2
+                + q1r * dlnrho_dr_i) * coef;
+            double rhs;
+            if (n == 4)      rhs = -tr + dif + 1.0 * __ldg(a.S_v + c) * r_h + a.coeff_MC_q * __ldg(a.MC_q + c);
+            else if (n == 5) rhs = -tr + dif + 1.0 * __ldg(a.S_c + c) * r_h;
+            else if (n == 6) rhs = -tr + dif + 1.0 * __ldg(a.S_i + c) * r_h;
+            else if (n == 7) rhs = -tr + dif + 1.0 * __ldg(a.S_g + c) * r_h;
+            else             rhs = -tr + dif;
+            stage_update<STAGE>(a, n, c, rhs);
+        }
     }
 }
 

@@ -32,6 +32,11 @@ struct RK4Args {
     double dt, half_dt, dt_sixth, diffusion_ramp, buoyancy_ramp, tke_max_nd, force_nd;
     double coeff_energy_p, coeff_energy, coeff_MC_vel, coeff_MC_q, coeff_MC_t;
     double lv, ls, g, u_0, L_atm, re_turb, pr_turb, sc_WaterVapour, sc_CO2;
+    // launch constants the reference evaluates per cell from the same operands (hoisted,
+    // values identical): 1/re_turb, 1000/(u_0 L_atm), 1.5e-5/(u_0 L_atm), the tracer
+    // diffusivities, the buoyancy prefactor buoyancy_ramp*1*g*dt/u_0 and the drag
+    // prefactor (1/86400)*L_atm/u_0*dt
+    double inv_re, nue_max, nue_air_nd, diff_prec_re_inv, diff_co2_re_inv, buoy_pref, drag_pref;
     int turb_model, wall_mode, nontrad, curvature, tracer_diff_flux, write_diag;
 };
 
@@ -82,6 +87,20 @@ struct ColumnArgs {
 };
 void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st);
 void launch_densities(const ColumnArgs& a, cudaStream_t st);
+
+// Moist convection: every 3-D field by athad_field id, 2-D inputs, column tables, constants.
+struct MoistArgs {
+    Dims d;
+    double* F[ATHAD_NFIELDS];
+    const double* evaporation;   // 2-D [jm][pitch]
+    const double* q_sensible;    // 2-D [jm][pitch]
+    const double* height;        // [im] layer heights (float-rounded)
+    const double* step;          // [im] height differences, step[im-1] = step[im-2]
+    const double* cose;          // [jm] cos(theta_equator - theta_j), mirror-symmetric
+    double t_0, cp_l, s_0, lv, ls, g, u_0, r_Earth, p_0, co2_0, c_0, M_bg, R_bg;
+    int convection_perturbation, convection_mode, iter_prec;
+};
+void launch_moist_convection(const MoistArgs& a, cudaStream_t st);
 
 void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st);
 

@@ -99,6 +99,11 @@ ATHAD_HD double dqsat_dT_from(double E, double L, double T, double p, double M_o
     return sat_deriv_factor_at(E, p, M_other) * L / (R_H2O * T * T);
 }
 
+ATHAD_HD double dqsat_dT(double T, double p, double M_other)   // :257-260
+{
+    return dqsat_dT_from(saturation_pressure_auto(T), latent_heat_auto(T), T, p, M_other);
+}
+
 // full moist lapse rate (SaturationH2O.h:280-293)
 ATHAD_HD double moist_lapse(double T, double p, double M_other, double cp, double R_mix, double g)
 {

@@ -180,8 +180,8 @@ def test_densities_matches_oracle(grid, set_water):
 
 def test_cadence_loop_matches_oracle():
     """Ten model iterations at the reference cadence: RK4 every iteration, one pressure
-    sweep every 4th, saturation adjustment + densities every 2nd (run_3D_loop,
-    cAtmosphereModel.cpp:1156-1509)."""
+    sweep every 4th, saturation adjustment + moist convection + densities every 2nd
+    (run_3D_loop, cAtmosphereModel.cpp:1156-1509)."""
     p = config_params()
     grid = (11, 21, 41)
     st = make_state(*grid, seed=31)
@@ -195,6 +195,8 @@ def test_cadence_loop_matches_oracle():
             if it % 2 == 0:
                 o.saturation_adjust()
                 g.SaturationAdjustment_run()
+                o.moist_convection(it)
+                g.MoistConvection_run(it)
                 o.densities()
                 g.densities()
             o.rk4(dt=4e-5, buoyancy_ramp=br)
