@@ -82,6 +82,14 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
                     double q_v_b = q_v_old, q_c_b = q_c_old, q_i_b = q_i_old;
                     double q_v_hyp = q_v_b;
                     const double T_original = T_nd * a.t_0;
+                    // The Newton step of SaturationAdjustment.h:177-254 with the same values,
+                    // fewer transcendentals: L(T) of the latent-heat update is the L(T) the
+                    // previous pass computed for its gain (T has not changed in between),
+                    // the sublimation latent heat is L(T) + 3.337e5 (SaturationH2O.h:150-154),
+                    // and the ice curve is evaluated only where a term uses it — where the
+                    // deposition weight DEP is 0 and there is no ice its terms are exactly
+                    // zero, so skipping them changes no bit.
+                    double L_T = latent_heat(T);
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
                         const double DEP = 1.0 - CND;
@@ -95,19 +103,21 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
                         q_c_b = smax(0.0, q_c_b - d_cnd);
                         q_i_b = smax(0.0, q_i_b - d_dep);
                         const double cp_loc = cp_of(q_v_b, co2, T, a.M_bg);
-                        T -= (latent_heat(T) * d_cnd + latent_heat_sublimation(T) * d_dep) / cp_loc;
+                        T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
                         const double E_sat = saturation_pressure(T);
-                        const double E_Ice = sublimation_pressure(T);
                         const double q_sat = saturation_mass_fraction(E_sat, p_local, M_other);
-                        const double q_Ice = saturation_mass_fraction(E_Ice, p_local, M_other);
                         const double q_sum = q_c_b + q_i_b;
+                        const bool need_ice = (DEP != 0.0) || (q_i_b > 0.0) || (!(q_sum > 1e-12) && !(T >= a.t_0));
+                        const double E_Ice = need_ice ? sublimation_pressure(T) : 0.0;
+                        const double q_Ice = need_ice ? saturation_mass_fraction(E_Ice, p_local, M_other) : 0.0;
                         const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
                                                                   : ((T >= a.t_0) ? q_sat : q_Ice);
                         const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
                         const double L_cnd = latent_heat(T);
-                        const double L_dep = latent_heat_sublimation(T);
-                        const double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other)
-                                          + DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
+                        const double L_dep = L_cnd + 3.337e5;
+                        double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other);
+                        if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
+                        L_T = L_cnd;
                         const double omega = 1.0 / (1.0 + Gain);
                         q_v_hyp = q_v_b + omega * (q_v_target - q_v_b);
                         if (fabs(q_v_b / q_v_hyp - 1.0) <= 1.0e-6) break;

@@ -123,8 +123,12 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 // values live (turbulence, momentum, temperature, tracers), each term with the operation
 // order of RHS_Atm_Turb.cpp; stencil values a later phase needs again are re-read, which
 // hits L1.
+#ifndef ATHAD_RK4_MIN_BLOCKS
+#define ATHAD_RK4_MIN_BLOCKS 4   // 128 registers per thread, 4 CTAs of 128 threads per SM
+#endif
+
 template <int STAGE>
-__global__ void __launch_bounds__(128, 4) rk4_stage_kernel(const RK4Args a)
+__global__ void __launch_bounds__(128, ATHAD_RK4_MIN_BLOCKS) rk4_stage_kernel(const RK4Args a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;

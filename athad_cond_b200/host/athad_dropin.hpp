@@ -1,0 +1,230 @@
+// athad_dropin.hpp - C++ host side of the drop-in: the five hot-path call sites of
+// cAtmosphereModel::run_3D_loop (atmosphere/cAtmosphereModel.cpp:1158, 1218, 1247, 1418,
+// 1509) routed to the device through the C ABI of include/athad_gpu.h.
+//
+// Header-only and templated on the model type, so it compiles against the reference's
+// cAtmosphereModel without this library depending on the reference's headers.  Each
+// member mirrors one reference call, with the same name and the same in-place effect on
+// the model's Array members:
+//
+//     SolveRungeKutta(m)        m.solveRungeKutta_Atmosphere_Turb()          :1509
+//     PressureSolverRun(m)      PressureSolverAtm(m).run()                   :1158
+//     SaturationAdjustmentRun(m) SaturationAdjustment(m).run()               :1218
+//     MoistConvectionRun(m, it) MoistConvection(m).run(it)                   :1247
+//     Densities(m, water)       ThermoAtm(m).densities(water)                :567, 634, 1418
+//
+// The model's fields stay resident on the device.  While the reference's other modules
+// (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
+// every call uploads the fields it reads and downloads the fields it writes; a caller that
+// keeps those modules off the loop can use the Device() handle and the C ABI directly.
+// Errors surface as std::runtime_error carrying the library's message, which is what the
+// reference's own physics code throws (and cli/cond.cpp:27-29 catches).
+#pragma once
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/athad_gpu.h"
+
+namespace athad_dropin {
+
+inline void check(athad_ctx* ctx, athad_status s, const char* what)
+{
+    if (s != ATHAD_OK)
+        throw std::runtime_error(std::string("athad: ") + what + ": " +
+                                 (ctx ? athad_last_error(ctx) : "no context") + " (status " +
+                                 std::to_string((int)s) + ")");
+}
+
+// Fills athad_params from the model's own members (AtmosphereParams.h.inc and m_comp).
+template <class Model>
+athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRROR)
+{
+    athad_params p;
+    athad_default_params(&p);
+    const std::string& tm = m.turb_model;
+    p.turb_model = (tm == "k_epsilon") ? ATHAD_TURB_K_EPSILON
+                 : (tm == "k_omega") ? ATHAD_TURB_K_OMEGA : ATHAD_TURB_K_OMEGA_SST;
+    p.wall_mode = wall;   // MIRROR: mirror-symmetric SST wall distance; REFERENCE: as the reference
+    p.metric_r0 = m.m_metric_r0;            // as initMetricRadius resolved it
+    p.re_turb = m.re_turb;
+    p.convection_perturbation = m.convection_perturbation;
+    p.convection_mode = m.convection_mode;
+    p.iter_prec = m.iter_prec;
+    p.r_air = m.r_air; p.g = m.g; p.u_0 = m.u_0; p.cp_l = m.cp_l; p.t_0 = m.t_0; p.c_0 = m.c_0;
+    p.L_atm = m.L_atm; p.zeta = m.zeta; p.omega = m.omega; p.lamda = m.lamda; p.lv = m.lv;
+    p.ls = m.ls; p.pr_turb = m.pr_turb; p.sc_WaterVapour = m.sc_WaterVapour; p.sc_CO2 = m.sc_CO2;
+    p.r_Earth = m.r_Earth; p.p_0 = m.p_0; p.t_00 = m.t_00; p.t_max_phys = m.t_max_phys;
+    p.cloud_cap = m.cloud_cap; p.t_skin = m.t_skin; p.c_h2o_dry_top = m.c_h2o_dry_top;
+    p.co2_0 = m.co2_0; p.s_0 = m.s_0; p.R_Air = m.R_Air; p.R_WaterVapour = m.R_WaterVapour;
+    p.M_bg = m.m_comp.M_bg; p.R_bg = m.m_comp.R_bg; p.R_mix = m.m_comp.R_mix;
+    return p;
+}
+
+template <class Model>
+class Device {
+public:
+    explicit Device(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRROR)
+        : im_(m.im), jm_(m.jm), km_(m.km), buf_((size_t)m.im * m.jm * m.km)
+    {
+        const athad_grid g{m.im, m.jm, m.km};
+        const athad_params p = params_from(m, wall);
+        check(nullptr, athad_create(&g, &p, &ctx_), "create");
+    }
+    ~Device() { if (ctx_) athad_destroy(ctx_); }
+    Device(const Device&) = delete;
+    Device& operator=(const Device&) = delete;
+
+    athad_ctx* handle() { return ctx_; }
+
+    // Pack a jagged Array (one new[] row of km doubles per (i, j), lib/Array.cpp:62-71).
+    template <class Arr>
+    void up(athad_field f, const Arr& a)
+    {
+        size_t q = 0;
+        for (int i = 0; i < im_; i++)
+            for (int j = 0; j < jm_; j++)
+                for (int k = 0; k < km_; k++) buf_[q++] = a.x[i][j][k];
+        check(ctx_, athad_upload(ctx_, f, buf_.data(), buf_.size()), "upload");
+        check(ctx_, athad_synchronize(ctx_), "upload sync");
+    }
+    template <class Arr>
+    void down(athad_field f, Arr& a)
+    {
+        check(ctx_, athad_download(ctx_, f, buf_.data(), buf_.size()), "download");
+        size_t q = 0;
+        for (int i = 0; i < im_; i++)
+            for (int j = 0; j < jm_; j++)
+                for (int k = 0; k < km_; k++) a.x[i][j][k] = buf_[q++];
+    }
+    template <class Arr2>
+    void up2(athad_field2d f, const Arr2& a)
+    {
+        std::vector<double> b((size_t)jm_ * km_);
+        for (int j = 0; j < jm_; j++)
+            for (int k = 0; k < km_; k++) b[(size_t)j * km_ + k] = a.y[j][k];
+        check(ctx_, athad_upload_2d(ctx_, f, b.data(), b.size()), "upload_2d");
+        check(ctx_, athad_synchronize(ctx_), "upload sync");
+    }
+    void down_profile(athad_profile f, std::vector<double>& v)
+    {
+        v.resize(im_);
+        check(ctx_, athad_download_profile(ctx_, f, v.data(), v.size()), "download_profile");
+    }
+    void up_profile(athad_profile f, const std::vector<double>& v)
+    {
+        if ((int)v.size() != im_) return;
+        check(ctx_, athad_upload_profile(ctx_, f, v.data(), v.size()), "upload_profile");
+    }
+
+    // cAtmosphereModel::solveRungeKutta_Atmosphere_Turb (RungeKutta_Atm_Turb.cpp:44-273)
+    void SolveRungeKutta(Model& m)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w); up(ATHAD_C, m.c);
+        up(ATHAD_CLOUD, m.cloud); up(ATHAD_ICE, m.ice); up(ATHAD_GR, m.gr); up(ATHAD_CO2, m.co2);
+        up(ATHAD_TKE, m.tke); up(ATHAD_DIS, m.dis);
+        up(ATHAD_TN, m.tn); up(ATHAD_UN, m.un); up(ATHAD_VN, m.vn); up(ATHAD_WN, m.wn);
+        up(ATHAD_CN, m.cn); up(ATHAD_CLOUDN, m.cloudn); up(ATHAD_ICEN, m.icen); up(ATHAD_GRN, m.grn);
+        up(ATHAD_CO2N, m.co2n); up(ATHAD_TKEN, m.tken); up(ATHAD_DISN, m.disn);
+        up(ATHAD_P_DYN, m.p_dyn); up(ATHAD_NUE, m.nue); up(ATHAD_T_EQ, m.t_eq);
+        up(ATHAD_P_STAT, m.p_stat); up(ATHAD_R_HUMID, m.r_humid);
+        up(ATHAD_S_C, m.S_c); up(ATHAD_S_R, m.S_r); up(ATHAD_S_I, m.S_i); up(ATHAD_S_S, m.S_s);
+        up(ATHAD_S_G, m.S_g); up(ATHAD_S_V, m.S_v);
+        up(ATHAD_MC_T, m.MC_t); up(ATHAD_MC_Q, m.MC_q); up(ATHAD_MC_V, m.MC_v); up(ATHAD_MC_W, m.MC_w);
+        up_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+        athad_step_scalars s{m.dt, m.diffusion_ramp, m.buoyancy_ramp, 1, 0};
+        check(ctx_, athad_rk4_step(ctx_, &s), "rk4_step");
+        down(ATHAD_T, m.t); down(ATHAD_U, m.u); down(ATHAD_V, m.v); down(ATHAD_W, m.w);
+        down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud); down(ATHAD_ICE, m.ice); down(ATHAD_GR, m.gr);
+        down(ATHAD_CO2, m.co2); down(ATHAD_TKE, m.tke); down(ATHAD_DIS, m.dis);
+        down(ATHAD_AUX_U, m.aux_u); down(ATHAD_AUX_V, m.aux_v); down(ATHAD_AUX_W, m.aux_w);
+        down(ATHAD_PROD, m.prod); down(ATHAD_TKE_SOURCE, m.tke_source); down(ATHAD_DIS_SOURCE, m.dis_source);
+        down_profile(ATHAD_PROF_T_REF_LEVEL, m.t_ref_level);
+    }
+
+    // PressureSolverAtm::run (PressureSolverAtm.h:27-669)
+    void PressureSolverRun(Model& m, int n_sweeps = 1)
+    {
+        up(ATHAD_AUX_U, m.aux_u); up(ATHAD_AUX_V, m.aux_v); up(ATHAD_AUX_W, m.aux_w);
+        up(ATHAD_P_DYN, m.p_dyn);
+        up_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+        check(ctx_, athad_pressure_sweep(ctx_, n_sweeps, m.total_iter_count), "pressure_sweep");
+        down(ATHAD_P_DYN, m.p_dyn);
+        down(ATHAD_AUX_U, m.aux_u); down(ATHAD_AUX_V, m.aux_v); down(ATHAD_AUX_W, m.aux_w);
+    }
+
+    // SaturationAdjustment::run (SaturationAdjustment.h:25-45)
+    void SaturationAdjustmentRun(Model& m)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_C, m.c); up(ATHAD_CLOUD, m.cloud); up(ATHAD_ICE, m.ice);
+        up(ATHAD_GR, m.gr); up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat); up(ATHAD_R_HUMID, m.r_humid);
+        up(ATHAD_S_C_C, m.S_c_c); up(ATHAD_P_RAIN, m.P_rain); up(ATHAD_P_SNOW, m.P_snow);
+        up(ATHAD_P_GRAUPEL, m.P_graupel); up(ATHAD_PRECIPITATION, m.Precipitation);
+        up(ATHAD_S_V, m.S_v); up(ATHAD_S_C, m.S_c); up(ATHAD_S_I, m.S_i); up(ATHAD_S_R, m.S_r);
+        up(ATHAD_S_S, m.S_s); up(ATHAD_S_G, m.S_g);
+        check(ctx_, athad_saturation_adjust(ctx_), "saturation_adjust");
+        down(ATHAD_T, m.t); down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud); down(ATHAD_ICE, m.ice);
+        down(ATHAD_GR, m.gr); down(ATHAD_S_C_C, m.S_c_c); down(ATHAD_P_RAIN, m.P_rain);
+        down(ATHAD_P_SNOW, m.P_snow); down(ATHAD_P_GRAUPEL, m.P_graupel);
+        down(ATHAD_PRECIPITATION, m.Precipitation); down(ATHAD_S_V, m.S_v); down(ATHAD_S_C, m.S_c);
+        down(ATHAD_S_I, m.S_i); down(ATHAD_S_R, m.S_r); down(ATHAD_S_S, m.S_s); down(ATHAD_S_G, m.S_g);
+    }
+
+    // MoistConvection::run (MoistConvection.h:106-140)
+    void MoistConvectionRun(Model& m, int iter_n)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w); up(ATHAD_C, m.c);
+        up(ATHAD_CLOUD, m.cloud); up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat);
+        up(ATHAD_R_HUMID, m.r_humid);
+        up2(ATHAD_2D_EVAPORATION, m.Evaporation); up2(ATHAD_2D_Q_SENSIBLE, m.Q_sensible_2D);
+        // fields the scheme carries from one call to the next (not reset by precompute)
+        up(ATHAD_E_U, m.E_u); up(ATHAD_D_U, m.D_u); up(ATHAD_E_D, m.E_d); up(ATHAD_D_D, m.D_d);
+        up(ATHAD_U_U, m.u_u); up(ATHAD_V_U, m.v_u); up(ATHAD_W_U, m.w_u);
+        up(ATHAD_U_D, m.u_d); up(ATHAD_V_D, m.v_d); up(ATHAD_W_D, m.w_d);
+        up(ATHAD_CLOUD_BASE, m.CloudBase); up(ATHAD_LEVEL_FREE_SINKING, m.LevelFreeSinking);
+        up(ATHAD_DEEP_BEG, m.Deep_beg); up(ATHAD_DEEP_END, m.Deep_end);
+        up(ATHAD_MC_T, m.MC_t); up(ATHAD_MC_Q, m.MC_q); up(ATHAD_MC_V, m.MC_v); up(ATHAD_MC_W, m.MC_w);
+        check(ctx_, athad_moist_convection(ctx_, iter_n), "moist_convection");
+        down(ATHAD_MC_S, m.s); down(ATHAD_MC_S_U, m.s_u); down(ATHAD_MC_S_D, m.s_d);
+        down(ATHAD_M_U, m.M_u); down(ATHAD_M_D, m.M_d); down(ATHAD_Q_V_U, m.q_v_u);
+        down(ATHAD_Q_C_U, m.q_c_u); down(ATHAD_Q_V_D, m.q_v_d);
+        down(ATHAD_U_U, m.u_u); down(ATHAD_V_U, m.v_u); down(ATHAD_W_U, m.w_u);
+        down(ATHAD_U_D, m.u_d); down(ATHAD_V_D, m.v_d); down(ATHAD_W_D, m.w_d);
+        down(ATHAD_E_U, m.E_u); down(ATHAD_D_U, m.D_u); down(ATHAD_E_D, m.E_d); down(ATHAD_D_D, m.D_d);
+        down(ATHAD_C_U, m.c_u); down(ATHAD_E_L, m.e_l); down(ATHAD_E_DD, m.e_d); down(ATHAD_E_P, m.e_p);
+        down(ATHAD_G_P, m.g_p); down(ATHAD_P_CONV, m.P_conv);
+        down(ATHAD_CLOUD_BASE, m.CloudBase); down(ATHAD_LEVEL_FREE_SINKING, m.LevelFreeSinking);
+        down(ATHAD_DEEP_BEG, m.Deep_beg); down(ATHAD_DEEP_END, m.Deep_end);
+        down(ATHAD_MC_T, m.MC_t); down(ATHAD_MC_Q, m.MC_q); down(ATHAD_MC_V, m.MC_v); down(ATHAD_MC_W, m.MC_w);
+    }
+
+    // ThermoAtm::densities (ThermoAtm.h:1436-1666)
+    void Densities(Model& m, bool set_water_profile = false)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_C, m.c); up(ATHAD_CO2, m.co2); up(ATHAD_CLOUD, m.cloud);
+        up(ATHAD_ICE, m.ice);
+        check(ctx_, athad_densities(ctx_, set_water_profile ? 1 : 0), "densities");
+        down(ATHAD_T, m.t); down(ATHAD_P_STAT, m.p_stat); down(ATHAD_R_HUMID, m.r_humid);
+        down(ATHAD_R_DRY, m.r_dry);
+        if (set_water_profile) down(ATHAD_C, m.c);
+        std::vector<double> tt((size_t)jm_ * km_), ps((size_t)jm_ * km_);
+        check(ctx_, athad_download_2d(ctx_, ATHAD_2D_T_TOP_INIT, tt.data(), tt.size()), "t_top_init");
+        check(ctx_, athad_download_2d(ctx_, ATHAD_2D_P_STAT_LANDSCAPE, ps.data(), ps.size()), "p_stat_landscape");
+        if ((int)m.t_top_init.size() == jm_)
+            for (int j = 0; j < jm_; j++)
+                for (int k = 0; k < km_; k++) m.t_top_init[j][k] = tt[(size_t)j * km_ + k];
+        for (int j = 0; j < jm_; j++)
+            for (int k = 0; k < km_; k++) m.p_stat_landscape.y[j][k] = ps[(size_t)j * km_ + k];
+        down_profile(ATHAD_PROF_RHO_BASE, m.m_rho_base);
+        down_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+    }
+
+private:
+    int im_, jm_, km_;
+    std::vector<double> buf_;
+    athad_ctx* ctx_ = nullptr;
+};
+
+}  // namespace athad_dropin

@@ -147,17 +147,73 @@ def cpu_baseline(seconds_budget: float = 20.0):
 
 
 def reference_arm(args):
-    """The reference's CPU path for the same metric and grid.  Until the reference itself
-    is built (it supports only its compiled-in 61x181x361 grid), this times the C
-    restatement of it (the oracle) on a bounded sample of each step."""
-    b = cpu_baseline(seconds_budget=20.0)
-    im, jm, km = GRID
-    return {"impl": "reference", "metric": "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)",
-            "value": b["value"], "unit": b["unit"], "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"plain FP64 model iteration, {im}x{jm}x{km} grid", "grid": [im, jm, km]},
-            "cpu_baseline": b,
-            "e2e": {"value": b["value"], "unit": b["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    """The reference's own CPU implementation of the path, timed on this host's cores.
+
+    The reference is built from its sources into oracle/_ref/stock with its own Makefile
+    flags (-ffast-math, no -O level) and driven through its own functions: its initial
+    state (not timed), then whole model iterations at its cadence (pressure sweep every
+    4th, saturation adjustment + moist convection + densities every 2nd, RK4 and the
+    time-level copy every iteration), with all host threads.  It supports only its
+    compiled-in 61 x 181 x 361 grid, so the sample runs there; the metric is per grid point.
+    A bounded sample of iterations (at least two, so one moist iteration is included) keeps
+    the run within a few minutes.  Without the built reference it times the oracle instead."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ref_binding
+    metric = "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)"
+    if not ref_binding.available("stock"):
+        b = cpu_baseline(seconds_budget=20.0)
+        val, cores, sample, kind, grid = b["value"], 1, b["sample"], "port", list(GRID)
+    else:
+        threads = len(os.sched_getaffinity(0))
+        cwd = os.getcwd()
+        os.chdir(os.environ.get("TMPDIR", "/tmp"))
+        # the reference prints its progress with printf; keep stdout for the JSON line
+        sys.stdout.flush()
+        saved_fd = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        try:
+            R = ref_binding.Reference("stock", threads=threads)
+            t0 = time.perf_counter()
+            R.init_state()
+            t_init = time.perf_counter() - t0
+            im, jm, km = R.shape
+            it, el = 0, 0.0
+            budget = float(os.environ.get("ATHAD_REF_BUDGET_S", "90"))
+            t0 = time.perf_counter()
+            while True:
+                it += 1
+                R.set_scalars(4e-5, 1.0, min(1.0, it / 300.0), it, it)
+                if it % 4 == 0:
+                    R.lib.ref_pressure(R.h)
+                if it % 2 == 0:
+                    R.lib.ref_satadj(R.h)
+                    R.lib.ref_moist(R.h, it)
+                    R.lib.ref_densities(R.h, 0)
+                R.lib.ref_rk4(R.h)
+                R.lib.ref_store(R.h)
+                el = time.perf_counter() - t0
+                if it >= 2 and (el >= budget or it >= 4):
+                    break
+            R.close()
+        finally:
+            os.dup2(saved_fd, 1)
+            os.close(saved_fd)
+            os.close(devnull)
+            os.chdir(cwd)
+        val = im * jm * km * it / el
+        cores, kind, grid = threads, "reference", [im, jm, km]
+        sample = (f"{it} model iterations of the reference's own {im}x{jm}x{km} grid through its own "
+                  f"functions, built with its Makefile flags (-ffast-math, no -O), OMP_NUM_THREADS={threads}, "
+                  f"{el:.1f} s (initial state {t_init:.1f} s, not timed)")
+    line = {"impl": "reference", "metric": metric, "value": val, "unit": "grid-point steps/s",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic" if kind == "port" else "reference initial state",
+            "config": {"workload": f"plain FP64 model iteration, {grid[0]}x{grid[1]}x{grid[2]} grid", "grid": grid},
+            "cpu_baseline": {"value": val, "unit": "grid-point steps/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": val, "unit": "grid-point steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
 
 
 def run_ours(args, rank, world, device):

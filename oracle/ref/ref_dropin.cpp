@@ -1,0 +1,58 @@
+// ref_dropin.cpp - the drop-in demonstrated on the reference itself (test infrastructure).
+//
+// Compiles the product's C++ adapter (athad_cond_b200/host/athad_dropin.hpp) against the
+// reference's own cAtmosphereModel and exposes it to the tests: the reference's hot-path
+// calls and their drop-in replacements run on the same model object, so the tests compare
+// the reference's CPU results with the device results the reference's call sites would get.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "tinyxml2.h"
+
+#define private public
+#define protected public
+#include "cAtmosphereModel.h"
+#undef private
+#undef protected
+
+#include "../../athad_cond_b200/host/athad_dropin.hpp"
+
+using Dev = athad_dropin::Device<cAtmosphereModel>;
+
+extern "C" {
+
+// what: 0 RK4, 1 pressure sweep, 2 saturation adjustment, 3 moist convection,
+// 4 densities, 5 densities(set_water_profile).  wall: 0 mirror, 1 reference.
+// Returns 0, or -1 with the message in err.
+int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)model;
+    try {
+        Dev d(*m, wall ? ATHAD_WALL_REFERENCE : ATHAD_WALL_MIRROR);
+        switch (what) {
+            case 0: d.SolveRungeKutta(*m); break;
+            case 1: d.PressureSolverRun(*m); break;
+            case 2: d.SaturationAdjustmentRun(*m); break;
+            case 3: d.MoistConvectionRun(*m, arg); break;
+            case 4: d.Densities(*m, false); break;
+            case 5: d.Densities(*m, true); break;
+            default: return -1;
+        }
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return -1;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -12,6 +12,10 @@ REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
 def lib_path(variant: str = "pin") -> str:
+    """pin: the reference (IEEE build); stock: its own Makefile flags; dropin: the IEEE build
+    plus the product's C++ drop-in adapter (needs the product library)."""
+    if variant == "dropin":
+        return os.path.join(REF_DIR, "pin", "libathad_dropin.so")
     return os.path.join(REF_DIR, variant, "libathad_ref.so")
 
 
@@ -95,6 +99,16 @@ class Reference:
 
     def set_scalars(self, dt, diffusion_ramp, buoyancy_ramp, total_iter_count, iter_n):
         self.lib.ref_set_scalars(self.h, dt, diffusion_ramp, buoyancy_ramp, total_iter_count, iter_n)
+
+    def dropin(self, what: int, arg: int = 0, wall: int = 0):
+        """Run one hot-path call through the product's C++ drop-in on this model."""
+        f = self.lib.dropin_run
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        f.restype = ctypes.c_int
+        err = ctypes.create_string_buffer(512)
+        r = f(self.h, what, arg, wall, err, 512)
+        if r != 0:
+            raise RuntimeError(err.value.decode())
 
     def rhs_cell(self, i, j, k):
         out = (ctypes.c_double * 17)()
