@@ -133,7 +133,11 @@ SIGNATURES = {
     "athad_densities": (ctypes.c_int, [_P, ctypes.c_int32]),
     "athad_moist_convection": (ctypes.c_int, [_P, ctypes.c_int32]),
     "athad_get_report": (ctypes.c_int, [_P, ctypes.POINTER(Report)]),
+    "athad_density_profile_noalloc": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_size_t, _P, _P, _P]),
 }
+NOALLOC_MAX_ROWS = 131072
+NOALLOC_MAX_IM = 1024
 
 _lib = None
 

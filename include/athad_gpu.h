@@ -244,6 +244,31 @@ athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n);
 /* Counters of the last calls. */
 athad_status athad_get_report(athad_ctx* ctx, athad_report* out);
 
+/* ---- allocation-free entry point --------------------------------------------- */
+
+/* Largest grid athad_density_profile_noalloc accepts: im*jm (i, j) rows, im levels. */
+#define ATHAD_NOALLOC_MAX_ROWS 131072
+#define ATHAD_NOALLOC_MAX_IM   1024
+
+/* No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory when they need this result (a host that reserved its whole HBM budget up front,
+ * a real-time loop that cannot afford cudaMalloc's implicit synchronisation, a caller
+ * whose device buffers come from another runtime).  It computes what athad_densities
+ * leaves in ATHAD_PROF_RHO_BASE and ATHAD_PROF_DLNRHO_DR - the cos-latitude horizontal
+ * mean of the density and d ln(rho_bar)/d rad.z - from a density field the caller holds on
+ * the device (element (i,j,k) at r_humid[(i*jm + j)*pitch + k]) into two caller-provided
+ * device arrays of im doubles, on the given stream (a cudaStream_t, NULL = default
+ * stream), without a context and without allocating: its scratch is a fixed device array
+ * of 2 * ATHAD_NOALLOC_MAX_ROWS doubles (2 MiB) that every GPU loading the library keeps
+ * until exit.  Grids beyond im*jm > ATHAD_NOALLOC_MAX_ROWS or im > ATHAD_NOALLOC_MAX_IM are
+ * rejected with ATHAD_ERR_INVALID.  The first call on a device looks up the scratch
+ * address (make it before any stream capture).  All calls share the scratch, so calls that
+ * overlap on the GPU race; calls ordered on one stream do not.  Asynchronous: the outputs
+ * are ready when the stream is. */
+athad_status athad_density_profile_noalloc(const double* r_humid, int32_t im, int32_t jm,
+                                           int32_t km, size_t pitch, double* rho_base,
+                                           double* dlnrho_dr, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
