@@ -35,6 +35,11 @@ class Wall(IntEnum):
     REFERENCE = 1
 
 
+class Precision(IntEnum):
+    FP64 = 0
+    MIXED = 1
+
+
 FIELD_NAMES = [
     "t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
     "tn", "un", "vn", "wn", "cn", "cloudn", "icen", "grn", "co2n", "tken", "disn",
@@ -70,7 +75,7 @@ class Grid(ctypes.Structure):
 _PARAM_INTS = [
     "turb_model", "wall_mode", "poisson_metric_fix", "anelastic", "tracer_diff_flux",
     "coriolis_nontrad", "metric_curvature", "metric_divergence",
-    "convection_perturbation", "convection_mode", "iter_prec", "pad0",
+    "convection_perturbation", "convection_mode", "iter_prec", "precision",
 ]
 _PARAM_DOUBLES = [
     "metric_r0", "re_turb",

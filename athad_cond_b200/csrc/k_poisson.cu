@@ -209,4 +209,24 @@ void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st)
     fill_kernel<<<148 * 4, 256, 0, st>>>(d, dst, v);
 }
 
+// Packed (i,j,k) rows of km values -> pitched rows.  One warp-row of 32 threads per 32
+// longitudes, 8 rows per CTA; reads and writes are both coalesced.
+__global__ void __launch_bounds__(256) repitch_kernel(Dims d, const double* __restrict__ packed,
+                                                      double* __restrict__ dst)
+{
+    const int rows = d.im * d.jm;
+    for (int row = blockIdx.y * 8 + threadIdx.y; row < rows; row += gridDim.y * 8) {
+        const double* s = packed + (long long)row * d.km;
+        double* o = dst + (long long)row * d.pitch;
+        for (int k = blockIdx.x * 32 + threadIdx.x; k < d.km; k += gridDim.x * 32) o[k] = s[k];
+    }
+}
+
+void launch_repitch(const Dims& d, const double* packed, double* dst, cudaStream_t st)
+{
+    const int rows = d.im * d.jm;
+    const int gy = (rows + 7) / 8 < 65535 ? (rows + 7) / 8 : 65535;
+    repitch_kernel<<<dim3((d.km + 31) / 32, gy), dim3(32, 8), 0, st>>>(d, packed, dst);
+}
+
 }  // namespace athad

@@ -124,7 +124,7 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 // order of RHS_Atm_Turb.cpp; stencil values a later phase needs again are re-read, which
 // hits L1.
 #ifndef ATHAD_RK4_MIN_BLOCKS
-#define ATHAD_RK4_MIN_BLOCKS 4   // 128 registers per thread, 4 CTAs of 128 threads per SM
+#define ATHAD_RK4_MIN_BLOCKS 7   // 72 registers per thread, 7 CTAs of 128 threads per SM
 #endif
 
 template <int STAGE>

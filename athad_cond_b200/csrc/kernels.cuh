@@ -103,5 +103,6 @@ struct MoistArgs {
 void launch_moist_convection(const MoistArgs& a, cudaStream_t st);
 
 void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st);
+void launch_repitch(const Dims& d, const double* packed, double* dst, cudaStream_t st);
 
 }  // namespace athad

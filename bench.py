@@ -116,6 +116,29 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """The largest of a per-rank time over all ranks of the process group (the value
+    itself without one).  NCCL ranks pass their CUDA device; gloo ranks pass None."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()) or tdist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(points: int, steps: int, world: int, ms: float) -> float:
+    """Grid-point steps per second of all replicas together: every rank advances its own
+    copy of the grid by `steps` iterations; the job takes the slowest rank's time."""
+    return points * steps * world / (ms * 1e-3)
+
+
+def replica_seed(rank: int) -> int:
+    """Each replica integrates its own seeded state."""
+    return 20261203 + rank
+
+
 def cpu_baseline(seconds_budget: float = 20.0):
     """The oracle (single-threaded C restatement of the reference path) on a bounded
     sample: whole model iterations of the same grid until the budget is used."""
@@ -225,7 +248,7 @@ def run_ours(args, rank, world, device):
     im, jm, km = GRID
     pts = im * jm * km
     p = config_params()
-    st = make_state(im, jm, km, seed=20261203 + rank)
+    st = make_state(im, jm, km, seed=replica_seed(rank))
     st["Evaporation"] = np.full((jm, km), 20.0)
     g = GpuAtmosphere(im, jm, km, p)
     g.upload_state(st)
@@ -272,9 +295,7 @@ def run_ours(args, rank, world, device):
     rk_ms = [a.elapsed_time(b) for a, b in rk_ev]
     if dist:
         tdist.barrier()
-        t = torch.tensor([ms], device=device)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, device)
 
     # ---- end to end through the C ABI with host buffers ----
     if args.no_e2e:
@@ -282,7 +303,7 @@ def run_ours(args, rank, world, device):
         peak, peak_kind = measured_peaks()
         rk_avg = sum(rk_ms) / len(rk_ms)
         achieved = RK4_FIELDS_PER_POINT * 8.0 * pts / (rk_avg * 1e-3) / 1e9
-        return {"value": pts * args.steps * world / (ms * 1e-3), "ms_per_step": ms / args.steps,
+        return {"value": whole_job_value(pts, args.steps, world, ms), "ms_per_step": ms / args.steps,
                 "e2e_value": None, "h2d": 0, "d2h": 0, "rk4_ms": rk_avg, "achieved": achieved,
                 "peak": peak, "peak_kind": peak_kind, "clocks": clk.summary(), "finite": True}
     host_up = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in E2E_UP}
@@ -307,11 +328,7 @@ def run_ours(args, rank, world, device):
             lib.athad_download(g._h, FIELD[n], ctypes.cast(h.data_ptr(), ctypes.POINTER(ctypes.c_double)), h.numel())
     e1.record(stream)
     stream.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=device)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), device)
     ok = all(np.isfinite(host_down[n].numpy()).all() for n in ("t", "u", "p_dyn"))
     g.close()
     peak, peak_kind = measured_peaks()
@@ -319,9 +336,9 @@ def run_ours(args, rank, world, device):
     alg_bytes = RK4_FIELDS_PER_POINT * 8.0 * pts
     achieved = alg_bytes / (rk_avg * 1e-3) / 1e9
     res = {
-        "value": pts * args.steps * world / (ms * 1e-3),
+        "value": whole_job_value(pts, args.steps, world, ms),
         "ms_per_step": ms / args.steps,
-        "e2e_value": pts * e2e_steps * world / (e2e_ms * 1e-3),
+        "e2e_value": whole_job_value(pts, e2e_steps, world, e2e_ms),
         "h2d": 8 * pts * len(E2E_UP), "d2h": 8 * pts * len(E2E_DOWN),
         "rk4_ms": rk_avg, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
         "clocks": clk.summary(), "finite": ok,

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 1
+#define ATHAD_ABI_VERSION 2
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -68,6 +68,16 @@ typedef enum athad_wall_mode {
     ATHAD_WALL_REFERENCE = 1
 } athad_wall_mode;
 
+/* Arithmetic of the RK4 step.  FP64 is the reference's arithmetic.  MIXED evaluates the
+ * right-hand side and stores the stage states and the RK4 accumulator in FP32, keeps the
+ * time level n and the final combination y_n + dt/6 (k1 + 2k2 + 2k3 + k4) in FP64 and
+ * leaves the other entry points (Poisson, saturation adjustment, moist convection,
+ * densities) in FP64.  A context's precision is fixed at creation. */
+typedef enum athad_precision {
+    ATHAD_PRECISION_FP64  = 0,
+    ATHAD_PRECISION_MIXED = 1
+} athad_precision;
+
 /* Model constants and switches.  Every double is the cAtmosphereModel member of the
  * same name (atmosphere/AtmosphereParams.h.inc, values from cli/config_cond.xml) unless
  * noted.  athad_default_params() fills the values of cli/config_cond.xml. */
@@ -84,7 +94,8 @@ typedef struct athad_params {
     int32_t  convection_perturbation; /* XML, 1 */
     int32_t  convection_mode;    /* XML, 1 */
     int32_t  iter_prec;          /* XML, 3 */
-    int32_t  pad0;
+    int32_t  precision;          /* athad_precision of the RK4 step (no counterpart in
+                                  * the reference, which is FP64 only); default FP64 */
     /* metric radius in rad.z units; 0 = off.  The reference default (ATM_METRIC_RADIUS
      * unset) is r_Earth*1e3/metricShellLength() (cAtmosphereModel.cpp:382-399); the
      * value 0 reproduces ATM_METRIC_RADIUS=0. */

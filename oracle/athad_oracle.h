@@ -35,7 +35,7 @@ typedef struct or_params {
     uint32_t struct_size;
     int32_t  turb_model, wall_mode, poisson_metric_fix, anelastic, tracer_diff_flux;
     int32_t  coriolis_nontrad, metric_curvature, metric_divergence;
-    int32_t  convection_perturbation, convection_mode, iter_prec, pad0;
+    int32_t  convection_perturbation, convection_mode, iter_prec, precision;   /* precision: unused by the oracle (FP64) */
     double metric_r0, re_turb;
     double r_air, g, u_0, cp_l, t_0, c_0, L_atm, zeta, omega, lamda, lv, ls;
     double pr_turb, sc_WaterVapour, sc_CO2;
