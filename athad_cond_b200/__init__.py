@@ -7,9 +7,9 @@ GpuAtmosphere does, and fails loudly without one or without the built library.
 """
 from ._abi import (FIELD, FIELD_NAMES, FIELD2D, PROFILE, Params, Precision, Status, Turb, Wall,  # noqa: F401
                    default_params, load_library, LIB_PATH)
-from .context import AthadError, GpuAtmosphere  # noqa: F401
+from .context import AthadError, GpuAtmosphere, GpuBatch  # noqa: F401
 from .synthetic import make_state, mirror, layer_heights  # noqa: F401
 
-__all__ = ["GpuAtmosphere", "AthadError", "make_state", "mirror", "layer_heights",
+__all__ = ["GpuAtmosphere", "GpuBatch", "AthadError", "make_state", "mirror", "layer_heights",
            "default_params", "load_library", "Params", "FIELD", "FIELD_NAMES", "Turb", "Wall",
            "Precision"]

@@ -102,6 +102,12 @@ class StepScalars(ctypes.Structure):
                 ("pad0", ctypes.c_int32)]
 
 
+class BatchStepParams(ctypes.Structure):
+    """athad_batch_step"""
+    _fields_ = [("dt", ctypes.c_double), ("diffusion_ramp", ctypes.c_double),
+                ("buoyancy_ramp_iters", ctypes.c_int32), ("pad0", ctypes.c_int32)]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -121,6 +127,7 @@ SIGNATURES = {
     "athad_set_stream": (ctypes.c_int, [_P, _P]),
     "athad_synchronize": (ctypes.c_int, [_P]),
     "athad_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(Grid)]),
+    "athad_footprint_bytes_params": (ctypes.c_size_t, [ctypes.POINTER(Grid), ctypes.POINTER(Params)]),
     "athad_upload": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_download": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_upload_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
@@ -138,6 +145,20 @@ SIGNATURES = {
     "athad_densities": (ctypes.c_int, [_P, ctypes.c_int32]),
     "athad_moist_convection": (ctypes.c_int, [_P, ctypes.c_int32]),
     "athad_get_report": (ctypes.c_int, [_P, ctypes.POINTER(Report)]),
+    "athad_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.POINTER(BatchStepParams),
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_P)]),
+    "athad_batch_destroy": (ctypes.c_int, [_P]),
+    "athad_batch_last_error": (ctypes.c_char_p, [_P]),
+    "athad_batch_set_stream": (ctypes.c_int, [_P, _P]),
+    "athad_batch_synchronize": (ctypes.c_int, [_P]),
+    "athad_batch_member_iter": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "athad_batch_set_active": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "athad_batch_iteration": (ctypes.c_int, [_P]),
+    "athad_batch_iteration_graph": (ctypes.c_int, [_P]),
+    "athad_batch_shape_count": (ctypes.c_int32, []),
+    "athad_batch_set_shape": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "athad_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_float)]),
     "athad_density_profile_noalloc": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                      ctypes.c_size_t, _P, _P, _P]),
 }

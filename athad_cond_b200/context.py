@@ -164,3 +164,73 @@ class GpuAtmosphere:
         r = _abi.Report()
         self._check(self.lib.athad_get_report(self._h, ctypes.byref(r)))
         return {n: getattr(r, n) for n, _ in r._fields_}
+
+
+class GpuBatch:
+    """An ensemble of mixed-precision GpuAtmosphere members advanced together
+    (athad_batch_* of include/athad_gpu.h): per iteration, each member's column physics at
+    its own cadence and every RK4 stage of all members in one persistent launch."""
+
+    def __init__(self, members: list, dt: float = 4e-5, diffusion_ramp: float = 1.0,
+                 buoyancy_ramp_iters: int = 300, first_iter: list | None = None):
+        self.lib = _abi.load_library()
+        self.members = list(members)
+        n = len(self.members)
+        handles = (ctypes.c_void_p * n)(*[m._h.value for m in self.members])
+        step = _abi.BatchStepParams(dt, diffusion_ramp, buoyancy_ramp_iters, 0)
+        fi = (ctypes.c_int32 * n)(*(first_iter or [1] * n))
+        h = ctypes.c_void_p()
+        st = self.lib.athad_batch_create(ctypes.cast(handles, ctypes.POINTER(ctypes.c_void_p)), n,
+                                         ctypes.byref(step), fi, ctypes.byref(h))
+        if st != 0:
+            raise AthadError(st, "athad_batch_create failed")
+        self._h = h
+
+    def _check(self, st: int):
+        if st != 0:
+            raise AthadError(st, self.lib.athad_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.athad_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, cuda_stream_handle: int | None):
+        self._check(self.lib.athad_batch_set_stream(self._h, ctypes.c_void_p(cuda_stream_handle or 0)))
+
+    def synchronize(self):
+        self._check(self.lib.athad_batch_synchronize(self._h))
+
+    def iteration(self, graph: bool = False):
+        fn = self.lib.athad_batch_iteration_graph if graph else self.lib.athad_batch_iteration
+        self._check(fn(self._h))
+
+    def member_iter(self, m: int) -> int:
+        v = ctypes.c_int32()
+        self._check(self.lib.athad_batch_member_iter(self._h, m, ctypes.byref(v)))
+        return int(v.value)
+
+    def set_active(self, m: int, active: bool):
+        self._check(self.lib.athad_batch_set_active(self._h, m, 1 if active else 0))
+
+    def set_shape(self, shape: int):
+        self._check(self.lib.athad_batch_set_shape(self._h, shape))
+
+    def autotune(self, reps: int = 3):
+        n = int(self.lib.athad_batch_shape_count())
+        ms = (ctypes.c_float * n)()
+        best = ctypes.c_int32()
+        self._check(self.lib.athad_batch_autotune(self._h, reps, ctypes.byref(best), ms))
+        return int(best.value), [float(x) for x in ms]

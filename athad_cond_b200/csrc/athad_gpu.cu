@@ -11,102 +11,8 @@
 #include <vector>
 #include <new>
 
-#include "kernels.cuh"
+#include "ctx.cuh"
 #include "thermo.cuh"
-
-using namespace athad;
-
-namespace {
-
-constexpr int kNY = 11;   // prognostic fields t..dis
-
-struct Layout {
-    Dims d;
-    size_t field_elems;   // im*jm*pitch
-    size_t f2d_elems;     // jm*pitch
-    size_t n_fields;      // ATHAD_NFIELDS + internal 3-D buffers
-    size_t bytes;
-};
-
-// stage A, stage B, accumulator K, Poisson source, upload staging (packed rows)
-constexpr int kInternal3D = 3 * kNY + 2;
-
-size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
-Layout make_layout(const athad_grid& g)
-{
-    Layout L;
-    L.d.im = g.im; L.d.jm = g.jm; L.d.km = g.km;
-    L.d.pitch = (int)round_up((size_t)g.km, 32);
-    L.d.plane = (long long)g.jm * L.d.pitch;
-    L.field_elems = round_up((size_t)g.im * L.d.plane, 64);
-    L.d.fstride = (long long)L.field_elems;
-    L.f2d_elems = round_up((size_t)g.jm * L.d.pitch, 64);
-    L.n_fields = ATHAD_NFIELDS + kInternal3D;
-    size_t b = L.n_fields * L.field_elems * sizeof(double);
-    b += ATHAD_NFIELDS2D * L.f2d_elems * sizeof(double);
-    b += ATHAD_NPROFILES * round_up((size_t)g.im, 64) * sizeof(double);
-    b += round_up((size_t)g.im * g.jm * sizeof(GeoIJ), 256);
-    b += round_up((size_t)g.im * g.jm * sizeof(PoiIJ), 256);
-    b += 6 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose
-    b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
-    b += 256;                                                                         // counters
-    L.bytes = b;
-    return L;
-}
-
-}  // namespace
-
-struct athad_ctx {
-    athad_grid grid{};
-    athad_params p{};
-    Layout L{};
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    char* slab = nullptr;
-    double* field[ATHAD_NFIELDS] = {};
-    double* stA[kNY] = {};
-    double* stB[kNY] = {};
-    double* stK[kNY] = {};
-    double* src = nullptr;
-    double* upload_stage = nullptr;   // im*jm*km packed doubles
-    double* f2d[ATHAD_NFIELDS2D] = {};
-    double* prof[ATHAD_NPROFILES] = {};
-    GeoIJ* geo = nullptr;
-    PoiIJ* poi = nullptr;
-    double* sin_w = nullptr;
-    double* height = nullptr;
-    double* step_f = nullptr;
-    double* coslat = nullptr;
-    double* step_mc = nullptr;
-    double* cose = nullptr;
-    double* row_sum = nullptr;
-    double* row_cnt = nullptr;
-    unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
-    double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
-    std::vector<double> rad;
-    int64_t poisson_sweeps_since_reset = 0;
-    std::string err;
-};
-
-static athad_status fail(athad_ctx* c, athad_status s, const char* msg)
-{
-    if (c) c->err = msg;
-    return s;
-}
-
-static athad_status cuda_check(athad_ctx* c, cudaError_t e, const char* what)
-{
-    if (e == cudaSuccess) return ATHAD_OK;
-    if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
-    return (e == cudaErrorMemoryAllocation) ? ATHAD_ERR_OOM : ATHAD_ERR_CUDA;
-}
-
-#define ATHAD_CHECK_LAUNCH(ctx, what)                                         \
-    do {                                                                      \
-        athad_status _s = cuda_check((ctx), cudaGetLastError(), (what));      \
-        if (_s != ATHAD_OK) return _s;                                        \
-    } while (0)
 
 extern "C" {
 
@@ -147,7 +53,14 @@ void athad_default_params(athad_params* p)
 size_t athad_footprint_bytes(const athad_grid* grid)
 {
     if (!grid || grid->im < 4 || grid->jm < 5 || grid->km < 5) return 0;
-    return make_layout(*grid).bytes;
+    return make_layout(*grid, ATHAD_PRECISION_FP64).bytes;
+}
+
+size_t athad_footprint_bytes_params(const athad_grid* grid, const athad_params* params)
+{
+    if (!grid || !params || grid->im < 4 || grid->jm < 5 || grid->km < 5) return 0;
+    if (params->precision != ATHAD_PRECISION_FP64 && params->precision != ATHAD_PRECISION_MIXED) return 0;
+    return make_layout(*grid, params->precision).bytes;
 }
 
 const char* athad_last_error(const athad_ctx* ctx)
@@ -164,7 +77,8 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (grid->im < 4 || grid->jm < 5 || grid->km < 5 || grid->im > 1024) return ATHAD_ERR_INVALID;
     if (params->turb_model < ATHAD_TURB_K_EPSILON || params->turb_model > ATHAD_TURB_K_OMEGA_SST)
         return ATHAD_ERR_UNSUPPORTED;
-    if (params->precision != ATHAD_PRECISION_FP64) return ATHAD_ERR_UNSUPPORTED;
+    if (params->precision != ATHAD_PRECISION_FP64 && params->precision != ATHAD_PRECISION_MIXED)
+        return ATHAD_ERR_UNSUPPORTED;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return ATHAD_ERR_NO_DEVICE; }
     cudaDeviceProp prop;
@@ -175,7 +89,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (!c) return ATHAD_ERR_OOM;
     c->grid = *grid;
     c->p = *params;
-    c->L = make_layout(*grid);
+    c->L = make_layout(*grid, params->precision);
     const Layout& L = c->L;
     const int im = grid->im, jm = grid->jm, km = grid->km;
 
@@ -212,6 +126,15 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     c->row_sum = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->counters = (unsigned long long*)take(256);
+    if (params->precision == ATHAD_PRECISION_MIXED) {
+        const size_t fb = L.field_elems * sizeof(float);
+        for (int n = 0; n < kNY; n++) c->mA[n] = (float*)take(fb);
+        for (int n = 0; n < kNY; n++) c->mB[n] = (float*)take(fb);
+        for (int n = 0; n < kNY; n++) c->mK[n] = (float*)take(fb);
+        for (int n = 0; n < kNY; n++) c->mYn[n] = (float*)take(fb);
+        for (int f = 0; f < ATHAD_MF_COUNT; f++) c->mF[f] = (float*)take(fb);
+        c->geof = (GeoF*)take((size_t)im * jm * sizeof(GeoF));
+    }
     if ((size_t)(q - c->slab) > L.bytes) {
         cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
         return ATHAD_ERR_INVALID;
@@ -314,6 +237,21 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->coslat, coslat.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "coslat");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_mc, step_mc.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step_mc");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->cose, cose.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "cose");
+    std::vector<GeoF> geof;
+    if (s == ATHAD_OK && c->geof) {   // FP32 factors rounded from the FP64 ones (mirror-exact)
+        geof.resize(geo.size());
+        for (size_t q2 = 0; q2 < geo.size(); q2++) {
+            const GeoIJ& G = geo[q2];
+            GeoF& F = geof[q2];
+            F.exp_rm = (float)G.exp_rm; F.exp_2_rm = (float)G.exp_2_rm; F.sinthe = (float)G.sinthe;
+            F.costhe = (float)G.costhe; F.inv_rm = (float)G.inv_rm; F.inv_rm2 = (float)G.inv_rm2;
+            F.inv_rmsinthe = (float)G.inv_rmsinthe; F.inv_rm2sinthe = (float)G.inv_rm2sinthe;
+            F.inv_rm2sinthe2 = (float)G.inv_rm2sinthe2; F.costhe_inv_rm2sinthe = (float)G.costhe_inv_rm2sinthe;
+            F.two_over_rm_exp = (float)G.two_over_rm_exp; F.v_metric = (float)G.v_metric;
+            F.cos4lat = (float)G.cos4lat; F.pad = 0.0f;
+        }
+        s = cuda_check(c, cudaMemcpyAsync(c->geof, geof.data(), geof.size() * sizeof(GeoF), cudaMemcpyHostToDevice, c->stream), "geof");
+    }
     if (s == ATHAD_OK) s = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
     if (s != ATHAD_OK) {
         cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
@@ -453,9 +391,12 @@ athad_status athad_level_mean(athad_ctx* ctx)
     return ATHAD_OK;
 }
 
+static athad_status rk4_step_mixed(athad_ctx* ctx, const athad_step_scalars* s);
+
 athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
 {
     if (!ctx || !s) return fail(ctx, ATHAD_ERR_INVALID, "rk4_step: bad argument");
+    if (ctx->p.precision == ATHAD_PRECISION_MIXED) return rk4_step_mixed(ctx, s);
     const athad_params& p = ctx->p;
     athad_status st = athad_level_mean(ctx);
     if (st != ATHAD_OK) return st;
@@ -509,6 +450,83 @@ athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
         }
         launch_rk4_stage(stage, a, ctx->stream);
         ATHAD_CHECK_LAUNCH(ctx, "rk4 stage");
+    }
+    return ATHAD_OK;
+}
+
+}  // extern "C"
+
+// Arguments of the mixed-precision stage kernels for one context and step (the stage
+// buffers are set per stage by the caller).
+void athad::mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a)
+{
+    const athad_params& p = ctx->p;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    a.geo = ctx->geof;
+    a.t_ref = ctx->prof[ATHAD_PROF_T_REF_LEVEL];
+    a.dlnrho = ctx->prof[ATHAD_PROF_DLNRHO_DR];
+    for (int n = 0; n < kNY; n++) {
+        a.Y[n] = ctx->field[ATHAD_T + n];
+        a.Yn[n] = ctx->field[ATHAD_TN + n];
+        a.Yn32[n] = ctx->mYn[n];
+        a.K[n] = ctx->mK[n];
+    }
+    for (int f = 0; f < ATHAD_MF_COUNT; f++) a.F[f] = ctx->mF[f];
+    double** F = ctx->field;
+    a.p_dyn = F[ATHAD_P_DYN]; a.nue = F[ATHAD_NUE]; a.t_eq = F[ATHAD_T_EQ]; a.p_stat = F[ATHAD_P_STAT];
+    a.r_humid = F[ATHAD_R_HUMID];
+    a.S_c = F[ATHAD_S_C]; a.S_r = F[ATHAD_S_R]; a.S_i = F[ATHAD_S_I]; a.S_s = F[ATHAD_S_S];
+    a.S_g = F[ATHAD_S_G]; a.S_v = F[ATHAD_S_V];
+    a.MC_t = F[ATHAD_MC_T]; a.MC_q = F[ATHAD_MC_Q]; a.MC_v = F[ATHAD_MC_V]; a.MC_w = F[ATHAD_MC_W];
+    a.aux_u = F[ATHAD_AUX_U]; a.aux_v = F[ATHAD_AUX_V]; a.aux_w = F[ATHAD_AUX_W];
+    a.prod = F[ATHAD_PROD]; a.tke_source = F[ATHAD_TKE_SOURCE]; a.dis_source = F[ATHAD_DIS_SOURCE];
+    const double inv_2dr = 1.0 / (2.0 * ctx->dr), inv_2dthe = 1.0 / (2.0 * ctx->dthe), inv_2dphi = 1.0 / (2.0 * ctx->dphi);
+    a.inv_2dr = (float)inv_2dr; a.inv_2dthe = (float)inv_2dthe; a.inv_2dphi = (float)inv_2dphi;
+    a.inv_dr = (float)(2.0 * inv_2dr); a.inv_dthe = (float)(2.0 * inv_2dthe); a.inv_dphi = (float)(2.0 * inv_2dphi);
+    a.inv_dr2 = (float)(1.0 / (ctx->dr * ctx->dr)); a.inv_dthe2 = (float)(1.0 / (ctx->dthe * ctx->dthe));
+    a.inv_dphi2 = (float)(1.0 / (ctx->dphi * ctx->dphi));
+    a.half_dt = 0.5 * s->dt; a.dt_sixth = s->dt / 6.0;
+    a.half_dt_f = (float)(0.5 * s->dt); a.dt_f = (float)s->dt;
+    a.diffusion_ramp = (float)s->diffusion_ramp;
+    a.tke_max_nd = (float)(1000.0 / (p.u_0 * p.u_0));
+    a.force_nd = (float)(p.omega * ctx->shell_len / p.u_0);
+    a.coeff_energy_p = (float)(p.u_0 * p.u_0 / (p.cp_l * p.t_0));
+    a.coeff_energy = 1.0 / (p.c_0 * p.cp_l * p.t_0);
+    a.coeff_MC_vel = p.L_atm / (p.u_0 * p.u_0);
+    a.coeff_MC_q = p.L_atm / (p.u_0 * p.c_0);
+    a.coeff_MC_t = p.L_atm / (p.u_0 * p.t_0);
+    a.lv = p.lv; a.ls = p.ls; a.L_atm_over_u0 = p.L_atm / p.u_0;
+    a.inv_re = (float)(1.0 / p.re_turb);
+    a.inv_pr_turb = (float)(1.0 / p.pr_turb);
+    a.nue_max = (float)(1000.0 / (p.u_0 * p.L_atm));
+    a.nue_air_nd = (float)(1.5e-5 / (p.u_0 * p.L_atm));
+    a.diff_prec_re_inv = (float)(1.0 / (p.sc_WaterVapour * p.re_turb));
+    a.diff_co2_re_inv = (float)(1.0 / (p.sc_CO2 * p.re_turb));
+    a.buoy_pref = (float)(s->buoyancy_ramp * p.g * s->dt / p.u_0);
+    a.drag_pref = (float)(1.0 / 86400.0 * p.L_atm / p.u_0 * s->dt);
+    a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
+    a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
+    a.write_diag = s->write_diagnostics;
+}
+
+extern "C" {
+
+// The mixed-precision step (k_rk4m.cu): same launches, FP32 private buffers.
+static athad_status rk4_step_mixed(athad_ctx* ctx, const athad_step_scalars* s)
+{
+    athad_status st = athad_level_mean(ctx);
+    if (st != ATHAD_OK) return st;
+    RK4MArgs a;
+    mixed_args(ctx, s, a);
+    for (int stage = 1; stage <= 4; stage++) {
+        for (int n = 0; n < kNY; n++) {
+            a.Yin[n] = (stage == 3) ? ctx->mB[n] : ctx->mA[n];
+            a.Yout[n] = (stage == 1 || stage == 3) ? ctx->mA[n] : ctx->mB[n];
+            a.Ybnd[n] = ctx->mB[n];
+        }
+        launch_rk4m_stage(stage, a, ctx->stream);
+        ATHAD_CHECK_LAUNCH(ctx, "rk4 mixed stage");
     }
     return ATHAD_OK;
 }

@@ -1,0 +1,121 @@
+// ctx.cuh - the context object behind the opaque athad_ctx handle of include/athad_gpu.h,
+// shared by the C ABI translation units (athad_gpu.cu, batch.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace athad {
+
+constexpr int kNY = 11;   // prognostic fields t..dis
+
+struct Layout {
+    Dims d;
+    size_t field_elems;   // im*jm*pitch
+    size_t f2d_elems;     // jm*pitch
+    size_t n_fields;      // ATHAD_NFIELDS + internal 3-D buffers
+    size_t bytes;
+};
+
+// stage A, stage B, accumulator K, Poisson source, upload staging (packed rows)
+constexpr int kInternal3D = 3 * kNY + 2;
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// FP32 buffers of the mixed-precision RK4 step: stage A, stage B, accumulator K, level n
+// (11 each) and the packed forcing
+constexpr int kMixed32 = 4 * kNY + ATHAD_MF_COUNT;
+
+inline Layout make_layout(const athad_grid& g, int precision)
+{
+    Layout L;
+    L.d.im = g.im; L.d.jm = g.jm; L.d.km = g.km;
+    L.d.pitch = (int)round_up((size_t)g.km, 32);
+    L.d.plane = (long long)g.jm * L.d.pitch;
+    L.field_elems = round_up((size_t)g.im * L.d.plane, 64);
+    L.d.fstride = (long long)L.field_elems;
+    L.f2d_elems = round_up((size_t)g.jm * L.d.pitch, 64);
+    L.n_fields = ATHAD_NFIELDS + kInternal3D;
+    size_t b = L.n_fields * L.field_elems * sizeof(double);
+    b += ATHAD_NFIELDS2D * L.f2d_elems * sizeof(double);
+    b += ATHAD_NPROFILES * round_up((size_t)g.im, 64) * sizeof(double);
+    b += round_up((size_t)g.im * g.jm * sizeof(GeoIJ), 256);
+    b += round_up((size_t)g.im * g.jm * sizeof(PoiIJ), 256);
+    b += 6 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose
+    b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
+    b += 256;                                                                         // counters
+    if (precision == ATHAD_PRECISION_MIXED) {
+        b += (size_t)kMixed32 * round_up(L.field_elems * sizeof(float), 256);
+        b += round_up((size_t)g.im * g.jm * sizeof(GeoF), 256);
+    }
+    L.bytes = b;
+    return L;
+}
+
+
+}  // namespace athad
+
+using namespace athad;
+
+struct athad_ctx {
+    athad_grid grid{};
+    athad_params p{};
+    Layout L{};
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    char* slab = nullptr;
+    double* field[ATHAD_NFIELDS] = {};
+    double* stA[kNY] = {};
+    double* stB[kNY] = {};
+    double* stK[kNY] = {};
+    double* src = nullptr;
+    double* upload_stage = nullptr;   // im*jm*km packed doubles
+    float* mA[kNY] = {};              // mixed precision: FP32 stage buffers, accumulator,
+    float* mB[kNY] = {};              // level n and packed forcing; FP32 geometry
+    float* mK[kNY] = {};
+    float* mYn[kNY] = {};
+    float* mF[ATHAD_MF_COUNT] = {};
+    GeoF* geof = nullptr;
+    double* f2d[ATHAD_NFIELDS2D] = {};
+    double* prof[ATHAD_NPROFILES] = {};
+    GeoIJ* geo = nullptr;
+    PoiIJ* poi = nullptr;
+    double* sin_w = nullptr;
+    double* height = nullptr;
+    double* step_f = nullptr;
+    double* coslat = nullptr;
+    double* step_mc = nullptr;
+    double* cose = nullptr;
+    double* row_sum = nullptr;
+    double* row_cnt = nullptr;
+    unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
+    double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
+    std::vector<double> rad;
+    int64_t poisson_sweeps_since_reset = 0;
+    std::string err;
+};
+
+inline athad_status fail(athad_ctx* c, athad_status s, const char* msg)
+{
+    if (c) c->err = msg;
+    return s;
+}
+
+inline athad_status cuda_check(athad_ctx* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return ATHAD_OK;
+    if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? ATHAD_ERR_OOM : ATHAD_ERR_CUDA;
+}
+
+#define ATHAD_CHECK_LAUNCH(ctx, what)                                         \
+    do {                                                                      \
+        athad_status _s = cuda_check((ctx), cudaGetLastError(), (what));      \
+        if (_s != ATHAD_OK) return _s;                                        \
+    } while (0)
+
+namespace athad {
+void mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a);
+}

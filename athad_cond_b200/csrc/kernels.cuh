@@ -44,6 +44,83 @@ void launch_level_mean(const Dims& d, const double* t, const double* sin_w, doub
                        cudaStream_t st);
 void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st);
 
+// Mixed-precision RK4 step (k_rk4m.cu).  FP32 geometry factors (rounded from GeoIJ, so
+// still mirror-exact) and the packed FP32 forcing fields stage 1 writes.
+struct GeoF {
+    float exp_rm, exp_2_rm, sinthe, costhe, inv_rm, inv_rm2, inv_rmsinthe, inv_rm2sinthe,
+          inv_rm2sinthe2, costhe_inv_rm2sinthe, two_over_rm_exp, v_metric, cos4lat, pad;
+};
+enum {
+    ATHAD_MF_P = 0,   // p_dyn (read as a stencil)
+    ATHAD_MF_NUE,     // nue
+    ATHAD_MF_QT,      // moist-convective and latent heating of t
+    ATHAD_MF_KT,      // Held-Suarez rate k_T * L_atm / u_0
+    ATHAD_MF_TEQ,     // t_eq
+    ATHAD_MF_QC,      // sources of c, cloud, ice, gr (consecutive)
+    ATHAD_MF_QCL,
+    ATHAD_MF_QI,
+    ATHAD_MF_QG,
+    ATHAD_MF_MV,      // moist-convective momentum sources of v and w
+    ATHAD_MF_MW,
+    ATHAD_MF_COUNT
+};
+struct RK4MArgs {
+    Dims d;
+    const GeoF* geo;
+    const double* t_ref;
+    const double* dlnrho;
+    double* Y[11];              // FP64 current level: stage-1 stencil input, stage-4 output
+    const double* Yn[11];       // FP64 time level n
+    const double* p_dyn; const double* nue; const double* t_eq; const double* p_stat; const double* r_humid;
+    const double* S_c; const double* S_r; const double* S_i; const double* S_s; const double* S_g; const double* S_v;
+    const double* MC_t; const double* MC_q; const double* MC_v; const double* MC_w;
+    const float* Yin[11];       // FP32 stage state read (stages 2-4)
+    float* Yout[11];            // FP32 stage state written (stages 1-3)
+    float* Ybnd[11];            // stage 1: second stage buffer that receives the boundary
+    float* Yn32[11];            // FP32 time level n (written by stage 1, read by 2-3)
+    float* K[11];               // FP32 accumulator
+    float* F[ATHAD_MF_COUNT];   // packed forcing
+    double* Yn_store[11];       // store_n: stage 4 also writes the new time level n here
+    double* aux_u; double* aux_v; double* aux_w;
+    double* prod; double* tke_source; double* dis_source;
+    float inv_2dr, inv_2dthe, inv_2dphi, inv_dr, inv_dthe, inv_dphi, inv_dr2, inv_dthe2, inv_dphi2;
+    float half_dt_f, dt_f, diffusion_ramp, tke_max_nd, force_nd, coeff_energy_p;
+    float inv_re, inv_pr_turb, nue_max, nue_air_nd, diff_prec_re_inv, diff_co2_re_inv, buoy_pref, drag_pref;
+    double half_dt, dt_sixth, coeff_energy, coeff_MC_t, coeff_MC_q, coeff_MC_vel, lv, ls, L_atm_over_u0;
+    int turb_model, wall_mode, nontrad, curvature, tracer_diff_flux, write_diag;
+    int store_n;                // fuse storeIntermediateData3D into stage 4
+};
+void launch_rk4m_stage(int stage, const RK4MArgs& a, cudaStream_t st);
+
+// Batched mixed-precision step (k_rk4m.cu): per-member step scalars, the device tables the
+// persistent stage kernel reads, and the batched level mean.
+struct BatchStep {
+    float half_dt_f, dt_f, diffusion_ramp, drag_pref;
+    double half_dt, dt_sixth;
+    double g, dt, u_0;         // buoyancy prefactor ramp * g * dt / u_0, formed per stage
+    int iter;                  // the member's current iteration number (1-based)
+    int ramp_iters;            // buoyancy ramp = min(1, iter / ramp_iters)
+    int write_diag, active;
+};
+struct BatchTables {
+    const RK4MArgs* args;      // [n] per member; stage buffer A in Yout, B in Ybnd
+    const BatchStep* step;     // [n]
+    const int* tile_start;     // [n+1] first tile of each member (for the launch's shape)
+    int n, total_tiles;
+};
+struct BatchShape { int bx, by, min_blocks; };
+int batch_shape_count();
+BatchShape batch_shape_info(int shape);
+int batch_shape_grid(int shape);   // persistent grid: SMs x resident CTAs of that shape
+void launch_rk4m_batch_stage(int stage, int shape, const BatchTables& T, int grid, cudaStream_t st);
+struct LevelMeanMember {
+    Dims d;
+    const double* t; const double* sin_w; double* out;
+    int level0;                // first global level index of this member
+};
+void launch_batch_level_mean(const LevelMeanMember* M, int n, int total_levels, int max_jm,
+                             const BatchStep* step, cudaStream_t st);
+
 // Per-(i,j) coefficients of the 7-point Poisson operator, PressureSolverAtm.h:236-269,
 // computed on the host once per context.
 struct PoiIJ {

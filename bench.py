@@ -7,9 +7,13 @@ pressure-Poisson sweep every 4th, saturation adjustment, moist convection and th
 densities every 2nd, and the time-level copy (storeIntermediateData3D) that closes it.
 Metric: grid-point RK4 steps per second = im*jm*km * steps / time.
 
-Workload: the 41 x 181 x 361 grid of the reference's second configuration (plain FP64), a
-seeded synthetic state with the reference's shapes and value ranges.  The inputs (about
-40 fields of 21 MB) are far larger than the 126 MB L2, so no flush is needed between steps.
+Workload: the 41 x 181 x 361 grid, 1000 iterations, run twice from the same seeded
+synthetic state (the reference's shapes and value ranges): the plain FP64 form and the
+mixed-precision form (athad_params.precision = MIXED: FP32 RK4 stencil arithmetic and stage
+storage, FP64 time level and column physics).  The headline value is the mixed form; both
+forms' rates, their RK4 rooflines and the mixed form's per-field error against the FP64
+form after the same iterations are in the line.  The inputs (about 40 fields of 21 MB) are
+far larger than the 126 MB L2, so no flush is needed between steps.
 
 --gpus N > 1 (under torchrun): independent replicas, one per GPU (the path has no
 cross-replica exchange), weak scaling; value = all ranks' grid-point steps / max time.
@@ -37,9 +41,18 @@ GRID = (41, 181, 361)
 E2E_UP = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "nue",
           "S_c", "S_r", "S_i", "S_s", "S_g", "S_v", "t_eq"]
 E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "p_dyn"]
-# algorithmic FP64 fields moved per grid point by one RK4 step (level mean: 1 read; stage 1:
-# 37 reads + 22 writes; stages 2-3: 48 + 22; stage 4: 48 + 14)
-RK4_FIELDS_PER_POINT = 1 + 59 + 70 + 70 + 62
+# algorithmic bytes moved per grid point by one RK4 step.  FP64 form: 262 fields of 8 B
+# (level mean 1 read; stage 1: 37 reads + 22 writes; stages 2-3: 48 + 22; stage 4: 48 + 14).
+# Mixed form: level mean 8 B, stage 1 296 B read + 176 B written, stages 2-3 176 + 88 B,
+# stage 4 220 + 112 B (the field lists of k_rk4m.cu) = 1340 B.
+RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62), 1: 8 + 472 + 264 + 264 + 332}
+# fields compared between the two forms after the timed iterations: the 11 prognostics and
+# the diagnosed pressure and densities
+# DRAM bytes (read + write) of one RK4 step measured by ncu, per form and grid: None until
+# a capture of all four stages exists for that build
+RK4_TRAFFIC = {}
+ERR_FIELDS = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
+              "p_dyn", "p_stat", "r_humid"]
 
 
 def iteration(g, it: int, dt: float):
@@ -239,15 +252,19 @@ def reference_arm(args):
     return line
 
 
-def run_ours(args, rank, world, device):
+def run_form(args, rank, world, device, precision):
+    """One form (FP64 or mixed) of the model iteration: warm-up, the device-timed region
+    of args.steps iterations, then the end-to-end leg through the C ABI with host buffers.
+    Returns the timings and the final fields of ERR_FIELDS (for the error report)."""
     import numpy as np
     import torch
     from athad_cond_b200 import GpuAtmosphere, make_state
-    from athad_cond_b200._abi import config_params
+    from athad_cond_b200._abi import config_params, Precision
 
     im, jm, km = GRID
     pts = im * jm * km
     p = config_params()
+    p.precision = int(precision)
     st = make_state(im, jm, km, seed=replica_seed(rank))
     st["Evaporation"] = np.full((jm, km), 20.0)
     g = GpuAtmosphere(im, jm, km, p)
@@ -296,16 +313,18 @@ def run_ours(args, rank, world, device):
     if dist:
         tdist.barrier()
     ms = max_over_ranks(ms, device)
-
-    # ---- end to end through the C ABI with host buffers ----
+    final = {n: g.download(n) for n in ERR_FIELDS}
+    fields_per_point = RK4_BYTES_PER_POINT[int(precision)]
+    rk_avg = sum(rk_ms) / len(rk_ms)
+    res = {"value": whole_job_value(pts, args.steps, world, ms), "ms_per_step": ms / args.steps,
+           "rk4_ms": rk_avg, "achieved": fields_per_point * pts / (rk_avg * 1e-3) / 1e9,
+           "rk4_bytes_per_point": fields_per_point, "clocks": clk.summary(), "final": final,
+           "e2e_value": None, "h2d": 0, "d2h": 0, "finite": True}
     if args.no_e2e:
         g.close()
-        peak, peak_kind = measured_peaks()
-        rk_avg = sum(rk_ms) / len(rk_ms)
-        achieved = RK4_FIELDS_PER_POINT * 8.0 * pts / (rk_avg * 1e-3) / 1e9
-        return {"value": whole_job_value(pts, args.steps, world, ms), "ms_per_step": ms / args.steps,
-                "e2e_value": None, "h2d": 0, "d2h": 0, "rk4_ms": rk_avg, "achieved": achieved,
-                "peak": peak, "peak_kind": peak_kind, "clocks": clk.summary(), "finite": True}
+        return res
+
+    # ---- end to end through the C ABI with host buffers ----
     host_up = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in E2E_UP}
     host_down = {n: torch.empty(GRID, dtype=torch.float64).pin_memory() for n in E2E_DOWN}
     lib = g.lib
@@ -329,33 +348,34 @@ def run_ours(args, rank, world, device):
     e1.record(stream)
     stream.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), device)
-    ok = all(np.isfinite(host_down[n].numpy()).all() for n in ("t", "u", "p_dyn"))
+    res["finite"] = all(np.isfinite(host_down[n].numpy()).all() for n in ("t", "u", "p_dyn"))
     g.close()
-    peak, peak_kind = measured_peaks()
-    rk_avg = sum(rk_ms) / len(rk_ms)
-    alg_bytes = RK4_FIELDS_PER_POINT * 8.0 * pts
-    achieved = alg_bytes / (rk_avg * 1e-3) / 1e9
-    res = {
-        "value": whole_job_value(pts, args.steps, world, ms),
-        "ms_per_step": ms / args.steps,
-        "e2e_value": whole_job_value(pts, e2e_steps, world, e2e_ms),
-        "h2d": 8 * pts * len(E2E_UP), "d2h": 8 * pts * len(E2E_DOWN),
-        "rk4_ms": rk_avg, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-        "clocks": clk.summary(), "finite": ok,
-        "launches_per_step": None,
-    }
+    res.update({"e2e_value": whole_job_value(pts, e2e_steps, world, e2e_ms),
+                "h2d": 8 * pts * len(E2E_UP), "d2h": 8 * pts * len(E2E_DOWN)})
     return res
+
+
+def field_errors(a: dict, b: dict) -> dict:
+    """max |a - b| / max |b| per field (b the FP64 form)."""
+    import numpy as np
+    out = {}
+    for n in ERR_FIELDS:
+        den = float(np.max(np.abs(b[n])))
+        out[n] = float(np.max(np.abs(a[n] - b[n]))) / den if den > 0 else float(np.max(np.abs(a[n])))
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", default=None, help="IMxJMxKM (default: the 41x181x361 workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="forms to run; the headline value is the mixed form when it runs")
     args = ap.parse_args()
     global GRID
     if args.grid:
@@ -382,7 +402,10 @@ def main():
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                  device_id=device)
-    r = run_ours(args, rank, world, device)
+    from athad_cond_b200._abi import Precision
+    forms = {"fp64": Precision.FP64, "mixed": Precision.MIXED}
+    wanted = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    runs = {f: run_form(args, rank, world, device, forms[f]) for f in wanted}
     base = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     if world > 1:
         import torch.distributed as tdist
@@ -390,16 +413,34 @@ def main():
         tdist.destroy_process_group()
     if rank != 0:
         return
+    head_name = "mixed" if "mixed" in runs else "fp64"
+    r = runs[head_name]
+    peak, peak_kind = measured_peaks()
     # kernel launches per step of our own kernels, averaged over the cadence cycle:
     # RK4 = level mean + 4 stages; pressure = aux BC + source + 2 colours + 3 BCs + ceiling;
     # saturation adjustment 1; moist convection 1; densities 3
     launches = args.steps * 5 + (args.steps // 4) * 8 + (args.steps // 2) * 5
+    summary = {}
+    for f, rr in runs.items():
+        summary[f] = {"value": rr["value"], "ms_per_step": rr["ms_per_step"], "rk4_ms": rr["rk4_ms"],
+                      "rk4_gbs": rr["achieved"], "rk4_roofline_frac": rr["achieved"] / peak,
+                      "rk4_bytes_per_point": rr["rk4_bytes_per_point"], "e2e": rr["e2e_value"],
+                      "finite": rr["finite"]}
+    errors = None
+    if "fp64" in runs and "mixed" in runs:
+        errors = {"after_iterations": args.warmup + args.steps, "fields": field_errors(
+            runs["mixed"]["final"], runs["fp64"]["final"]), "measure": "max|mixed-fp64| / max|fp64|"}
+        summary["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
+    form_text = {"mixed": "mixed-precision (FP32 RK4 stencil arithmetic and stage storage, FP64 time "
+                          "level, final combination and column physics)",
+                 "fp64": "plain FP64"}[head_name]
     line = {
         "metric": "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)",
         "value": r["value"], "unit": "grid-point steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"plain FP64 model iteration, {im}x{jm}x{km} grid "
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if head_name == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"{form_text} model iteration, {im}x{jm}x{km} grid "
                                "(RK4 every step, pressure sweep every 4th, saturation adjustment, "
                                "moist convection and densities every 2nd)",
                    "grid": [im, jm, km], "points": im * jm * km,
@@ -407,10 +448,13 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": r["e2e_value"], "unit": "grid-point steps/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
-        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
-                     "frac": r["achieved"] / r["peak"], "traffic": None,
-                     "kernel": "rk4 step (level mean + 4 stage launches)",
-                     "peak_source": r["peak_kind"]},
+        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": peak, "unit": "GB/s",
+                     "frac": r["achieved"] / peak, "traffic": RK4_TRAFFIC.get((head_name, GRID)),
+                     "kernel": f"{head_name} rk4 step (level mean + 4 stage launches), "
+                               f"{r['rk4_bytes_per_point']} algorithmic B per grid point",
+                     "peak_source": peak_kind},
+        "forms": summary,
+        "error_vs_fp64": errors,
         "cpu_baseline": base,
         "gpu_launches": launches,
         "clocks": r["clocks"],

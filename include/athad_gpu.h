@@ -195,6 +195,10 @@ athad_status athad_set_stream(athad_ctx* ctx, void* cuda_stream);
 athad_status athad_synchronize(athad_ctx* ctx);
 /* Device bytes held by a context of this grid (admission by HBM footprint). */
 size_t athad_footprint_bytes(const athad_grid* grid);
+/* The same for a context created with these params (the mixed-precision step holds its
+ * FP32 buffers in addition); 0 for an invalid grid or precision.  No counterpart in the
+ * reference. */
+size_t athad_footprint_bytes_params(const athad_grid* grid, const athad_params* params);
 
 /* ---- state transfer --------------------------------------------------------- */
 
@@ -258,6 +262,52 @@ athad_status athad_get_report(athad_ctx* ctx, athad_report* out);
 /* ---- allocation-free entry point --------------------------------------------- */
 
 /* Largest grid athad_density_profile_noalloc accepts: im*jm (i, j) rows, im levels. */
+/* ---- ensembles: batched iteration of many contexts ----------------------------
+ * No counterpart in the reference, which runs one grid per process.  A batch advances
+ * mixed-precision contexts (members, each with its own grid and parameters) together on
+ * one stream: every member's column physics at its own cadence, the level mean of all
+ * members in one launch, each RK4 stage of all members in one persistent launch, the
+ * time-level copy (storeIntermediateData3D) fused into the last stage.  The members stay
+ * ordinary contexts: upload/download work on them between batch calls (on the batch's
+ * stream order: call athad_batch_synchronize first).  A member's result is bit-for-bit
+ * the result of the same iterations run on it alone through athad_rk4_step and friends
+ * with the same scalars. */
+typedef struct athad_batch athad_batch;
+
+typedef struct athad_batch_step {
+    double  dt;                   /* non-dimensional time step (dt_visc, cli/config_cond.xml: 4e-5) */
+    double  diffusion_ramp;       /* 1 */
+    int32_t buoyancy_ramp_iters;  /* buoyancy ramp of iteration n = min(1, n / this); 300 */
+    int32_t pad0;
+} athad_batch_step;
+
+/* members: n_members distinct MIXED contexts on the current device; first_iter: each
+ * member's next iteration number (NULL = all 1).  The batch holds small device tables
+ * only. */
+athad_status athad_batch_create(athad_ctx* const* members, int32_t n_members,
+                                const athad_batch_step* step, const int32_t* first_iter,
+                                athad_batch** out);
+athad_status athad_batch_destroy(athad_batch* b);
+const char*  athad_batch_last_error(const athad_batch* b);
+athad_status athad_batch_set_stream(athad_batch* b, void* cuda_stream);
+athad_status athad_batch_synchronize(athad_batch* b);
+/* A member's next iteration number. */
+athad_status athad_batch_member_iter(const athad_batch* b, int32_t member, int32_t* next_iter);
+/* An inactive member is skipped by every launch (its state and counter stay). */
+athad_status athad_batch_set_active(athad_batch* b, int32_t member, int32_t active);
+/* One model iteration of every active member (cadence of cAtmosphereModel.cpp:1156-1509). */
+athad_status athad_batch_iteration(athad_batch* b);
+/* The same iteration replayed from a CUDA graph, captured on first use for the current
+ * cadence pattern of the members (at most a few per batch). */
+athad_status athad_batch_iteration_graph(athad_batch* b);
+/* Tile shapes of the persistent RK4 kernel; athad_batch_autotune times RK4 stages 1-3 of
+ * the whole batch once per shape (reps repetitions, model state unchanged), keeps the
+ * fastest and reports each shape's milliseconds per stage triple. */
+int32_t      athad_batch_shape_count(void);
+athad_status athad_batch_set_shape(athad_batch* b, int32_t shape);
+athad_status athad_batch_autotune(athad_batch* b, int32_t reps, int32_t* best_shape,
+                                  float* ms_per_shape);
+
 #define ATHAD_NOALLOC_MAX_ROWS 131072
 #define ATHAD_NOALLOC_MAX_IM   1024
 

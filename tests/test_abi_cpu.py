@@ -67,3 +67,20 @@ def test_no_device_is_reported_not_faked():
     p = _abi.config_params()
     h = ctypes.c_void_p()
     assert lib.athad_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == _abi.Status.ERR_NO_DEVICE
+
+
+def test_footprint_of_mixed_context_includes_fp32_buffers():
+    """athad_footprint_bytes_params: the mixed form holds 55 FP32 fields and an FP32
+    geometry table on top of the FP64 context; invalid precision gives 0."""
+    from athad_cond_b200._abi import Grid, Precision, config_params
+    lib = _abi.load_library()
+    g = Grid(21, 91, 181)
+    p = config_params()
+    f64 = lib.athad_footprint_bytes_params(ctypes.byref(g), ctypes.byref(p))
+    assert f64 == lib.athad_footprint_bytes(ctypes.byref(g))
+    p.precision = int(Precision.MIXED)
+    fm = lib.athad_footprint_bytes_params(ctypes.byref(g), ctypes.byref(p))
+    field32 = 21 * 91 * 192 * 4
+    assert fm - f64 >= 55 * field32
+    p.precision = 7
+    assert lib.athad_footprint_bytes_params(ctypes.byref(g), ctypes.byref(p)) == 0
