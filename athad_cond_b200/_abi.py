@@ -129,6 +129,7 @@ SIGNATURES = {
     "athad_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(Grid)]),
     "athad_footprint_bytes_params": (ctypes.c_size_t, [ctypes.POINTER(Grid), ctypes.POINTER(Params)]),
     "athad_upload": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_upload_device": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_size_t]),
     "athad_download": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_upload_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_download_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),

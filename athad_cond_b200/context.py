@@ -82,6 +82,14 @@ class GpuAtmosphere:
         # keep the buffer alive until the (possibly asynchronous) copy has been issued
         self.synchronize()
 
+    def upload_tensor(self, name: str, t):
+        """A packed (im, jm, km) float64 CUDA tensor on this device (a state built on the
+        device), copied on the context's stream."""
+        if tuple(t.shape) != self.shape or not t.is_contiguous() or not t.is_cuda:
+            raise ValueError(f"{name}: need a contiguous CUDA tensor of shape {self.shape}")
+        self._check(self.lib.athad_upload_device(self._h, FIELD[name], ctypes.c_void_p(t.data_ptr()),
+                                                 t.numel()))
+
     def download(self, name: str) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)
         self._check(self.lib.athad_download(self._h, FIELD[name], _dptr(out), out.size))

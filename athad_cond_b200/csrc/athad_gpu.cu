@@ -301,6 +301,17 @@ athad_status athad_upload(athad_ctx* ctx, athad_field f, const double* host, siz
     return ATHAD_OK;
 }
 
+athad_status athad_upload_device(athad_ctx* ctx, athad_field f, const double* device_src, size_t n)
+{
+    if (!ctx || !device_src || (int)f < 0 || (int)f >= ATHAD_NFIELDS)
+        return fail(ctx, ATHAD_ERR_INVALID, "upload_device: bad argument");
+    const Dims& d = ctx->L.d;
+    if (n != (size_t)d.im * d.jm * d.km) return fail(ctx, ATHAD_ERR_INVALID, "upload_device: size mismatch");
+    launch_repitch(d, device_src, ctx->field[f], ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "upload_device repitch");
+    return ATHAD_OK;
+}
+
 athad_status athad_download(athad_ctx* ctx, athad_field f, double* host, size_t n)
 {
     if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "download: bad argument");
@@ -608,6 +619,7 @@ static ColumnArgs column_args(athad_ctx* ctx)
     a.M_bg = p.M_bg; a.R_bg = p.R_bg; a.R_mix = p.R_mix; a.r_air = p.r_air; a.g = p.g; a.t_skin = p.t_skin;
     a.c_h2o_dry_top = p.c_h2o_dry_top;
     a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_dr = 1.0 / ctx->dr;
+    a.mixed = (p.precision == ATHAD_PRECISION_MIXED) ? 1 : 0;
     return a;
 }
 

@@ -52,7 +52,14 @@ __device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, dou
 
 // adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
 // Neither reads a neighbour, so the two passes of the reference fuse into one.
-__global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs a)
+#ifndef ATHAD_SATADJ_MIN_BLOCKS
+#define ATHAD_SATADJ_MIN_BLOCKS 6   // 80 registers, 6 CTAs of 128 threads per SM
+#endif
+// MIXED: the Newton step's latent heats, heat capacities, derivative factors, gain and
+// damping in FP32; the saturation curves and mass fractions, the state it updates and the
+// clamp-and-fade pass in FP64.
+template <bool MIXED>
+__global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS) saturation_adjust_kernel(const ColumnArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,7 +96,8 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
                     // and the ice curve is evaluated only where a term uses it — where the
                     // deposition weight DEP is 0 and there is no ice its terms are exactly
                     // zero, so skipping them changes no bit.
-                    double L_T = latent_heat(T);
+                    double L_T = MIXED ? (double)thermo_f::latent_heat((float)T) : latent_heat(T);
+                    const float M_bg_f = (float)a.M_bg, co2_f = (float)co2, M_other_f = (float)M_other;
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
                         const double DEP = 1.0 - CND;
@@ -102,7 +110,8 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
                         q_v_b += d_q_v;
                         q_c_b = smax(0.0, q_c_b - d_cnd);
                         q_i_b = smax(0.0, q_i_b - d_dep);
-                        const double cp_loc = cp_of(q_v_b, co2, T, a.M_bg);
+                        const double cp_loc = MIXED ? (double)thermo_f::cp_of((float)q_v_b, co2_f, (float)T, M_bg_f)
+                                                    : cp_of(q_v_b, co2, T, a.M_bg);
                         T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
                         const double E_sat = saturation_pressure(T);
                         const double q_sat = saturation_mass_fraction(E_sat, p_local, M_other);
@@ -112,13 +121,25 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
                         const double q_Ice = need_ice ? saturation_mass_fraction(E_Ice, p_local, M_other) : 0.0;
                         const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
                                                                   : ((T >= a.t_0) ? q_sat : q_Ice);
-                        const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
-                        const double L_cnd = latent_heat(T);
-                        const double L_dep = L_cnd + 3.337e5;
-                        double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other);
-                        if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
-                        L_T = L_cnd;
-                        const double omega = 1.0 / (1.0 + Gain);
+                        double omega;
+                        if (MIXED) {
+                            const float Tf = (float)T;
+                            const float cp_g = thermo_f::cp_of((float)q_v_b, co2_f, Tf, M_bg_f);
+                            const float L_cnd = thermo_f::latent_heat(Tf);
+                            const float L_dep = L_cnd + 3.337e5f;
+                            float Gain = (float)CND * (L_cnd / cp_g) * thermo_f::dqsat_dT_from(E_sat, L_cnd, Tf, p_local, M_other_f);
+                            if (need_ice) Gain += (float)DEP * (L_dep / cp_g) * thermo_f::dqsat_dT_from(E_Ice, L_dep, Tf, p_local, M_other_f);
+                            L_T = (double)L_cnd;
+                            omega = (double)(1.0f / (1.0f + Gain));
+                        } else {
+                            const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
+                            const double L_cnd = latent_heat(T);
+                            const double L_dep = L_cnd + 3.337e5;
+                            double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other);
+                            if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
+                            L_T = L_cnd;
+                            omega = 1.0 / (1.0 + Gain);
+                        }
                         q_v_hyp = q_v_b + omega * (q_v_target - q_v_b);
                         if (fabs(q_v_b / q_v_hyp - 1.0) <= 1.0e-6) break;
                     }
@@ -178,7 +199,8 @@ __global__ void __launch_bounds__(128) saturation_adjust_kernel(const ColumnArgs
 void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st)
 {
     const dim3 block(128), grid((a.d.km + 127) / 128, a.d.jm, a.d.im);
-    saturation_adjust_kernel<<<grid, block, 0, st>>>(a);
+    if (a.mixed) saturation_adjust_kernel<true><<<grid, block, 0, st>>>(a);
+    else saturation_adjust_kernel<false><<<grid, block, 0, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -442,6 +442,7 @@ __device__ __forceinline__ void load_member_args(RK4MArgs& sa, const BatchTables
     long long* dst = reinterpret_cast<long long*>(&sa);
     const int nthreads = blockDim.x * blockDim.y;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    __syncthreads();   // every warp is done with the previous member's arguments
     for (int w = tid; w < (int)(sizeof(RK4MArgs) / sizeof(long long)); w += nthreads) dst[w] = src[w];
     __syncthreads();
     if (tid < 11) {   // the table holds buffer A in Yout and buffer B in Ybnd

@@ -4,7 +4,7 @@
 // Pruss, IAPWS-2011 sublimation curve, Watson latent heat, the exact non-dilute saturation
 // mass fraction, the exact derivative factor and the full moist-lapse expression) and
 // atmosphere/MixtureAtm.h:33-227 (Shomate heat capacities, mass-weighted R and cp).  FP64
-// throughout; the transcendentals are CUDA's own exp/pow/sqrt.  Host+device so the host
+// throughout; the transcendentals are CUDA's own exp/log/sqrt.  Host+device so the host
 // can build tables with the same code.
 #pragma once
 
@@ -40,14 +40,17 @@ ATHAD_HD double saturation_pressure(double T)
     return 220640.0 * exp((T_CRIT / T) * sum);
 }
 
-// IAPWS (2011) sublimation curve (SaturationH2O.h:105-120)
+// IAPWS (2011) sublimation curve (SaturationH2O.h:105-120).  The three powers of theta
+// share one logarithm: theta^a = exp(a ln theta), within two ulp of pow(theta, a) for the
+// theta of the atmosphere (0.5..2.4), at a third of the cost of three pow calls.
 ATHAD_HD double sublimation_pressure(double T)
 {
     if (T <= 0.0) return 0.0;
     const double theta = T / T_TRIPLE;
-    const double sum = -0.212144006e2 * pow(theta, 0.333333333e-2)
-                     + 0.273203819e2 * pow(theta, 0.120666667e1)
-                     + -0.610598130e1 * pow(theta, 0.170333333e1);
+    const double lt = log(theta);
+    const double sum = -0.212144006e2 * exp(0.333333333e-2 * lt)
+                     + 0.273203819e2 * exp(0.120666667e1 * lt)
+                     + -0.610598130e1 * exp(0.170333333e1 * lt);
     return 6.11657 * exp(sum / theta);
 }
 
@@ -57,10 +60,12 @@ ATHAD_HD double saturation_pressure_auto(double T)   // SaturationH2O.h:123-127
     return (T >= T_TRIPLE) ? saturation_pressure(T) : sublimation_pressure(T);
 }
 
-ATHAD_HD double latent_heat(double T)                // Watson, SaturationH2O.h:138-147
+// Watson, SaturationH2O.h:138-147; x^0.38 as exp(0.38 ln x) (within two ulp of pow)
+ATHAD_HD double latent_heat(double T)
 {
     if (T >= T_CRIT) return 0.0;
-    return 2.501e6 * pow((T_CRIT - T) / (T_CRIT - 273.15), 0.38);
+    const double x = (T_CRIT - T) / (T_CRIT - 273.15);
+    return (x > 0.0) ? 2.501e6 * exp(0.38 * log(x)) : 0.0;
 }
 ATHAD_HD double latent_heat_sublimation(double T) { return latent_heat(T) + 3.337e5; }
 ATHAD_HD double latent_heat_auto(double T)
@@ -161,4 +166,51 @@ ATHAD_HD double M_nonwater(double c, double co2, double M_b)   // MixtureAtm.h:2
 }
 
 }  // namespace thermo
+
+// FP32 versions of the parts of the saturation adjustment's Newton step that are not the
+// saturation curve itself (latent heat, heat capacity, the derivative factor), used by the
+// mixed-precision form; p_sat, p_subl and q_sat stay FP64.
+namespace thermo_f {
+
+ATHAD_HD float latent_heat(float T)
+{
+    const float Tc = (float)thermo::T_CRIT;
+    if (T >= Tc) return 0.0f;
+    const float x = (Tc - T) / (Tc - 273.15f);
+    return (x > 0.0f) ? 2.501e6f * expf(0.38f * logf(x)) : 0.0f;
+}
+
+ATHAD_HD float shomate(float T, float A, float B, float Cc, float D, float E)
+{
+    float t = (T < 298.0f) ? 298.0f : T;
+    t = (t > 2000.0f) ? 2000.0f : t;
+    t *= 1.0e-3f;
+    const float t2 = t * t;
+    return A + B * t + Cc * t2 + D * t2 * t + E / t2;
+}
+
+ATHAD_HD float cp_of(float c, float co2, float T, float M_b)
+{
+    float q_v = fminf(fmaxf(c, 0.0f), 1.0f), q_c = fminf(fmaxf(co2, 0.0f), 1.0f);
+    const float sum = q_v + q_c;
+    if (sum > 1.0f) { q_v /= sum; q_c /= sum; }
+    const float q_b = fmaxf(0.0f, 1.0f - q_v - q_c);
+    return q_v * (shomate(T, 30.09200f, 6.832514f, 6.793435f, -2.534480f, 0.082139f) / (float)thermo::M_H2O)
+         + q_c * (shomate(T, 24.99735f, 55.18696f, -33.69137f, 7.948387f, -0.136638f) / (float)thermo::M_CO2)
+         + q_b * (shomate(T, 28.98641f, 1.853978f, -9.647459f, 16.63537f, 0.000117f) / M_b);
+}
+
+// dq_sat/dT from a FP64 saturation pressure (SaturationH2O.h:230-255)
+ATHAD_HD float dqsat_dT_from(double E, float L, float T, double p, float M_other)
+{
+    if (E == thermo::NO_SATURATION || !(p > 0.0) || E >= p || !(T > 0.0f)) return 0.0f;
+    const float x = (float)(E / p);
+    const float mh = (float)thermo::M_H2O;
+    const float den = x * mh + (1.0f - x) * M_other;
+    if (!(den > 0.0f)) return 0.0f;
+    const float A = x * mh * M_other / (den * den);
+    return A * L / ((float)thermo::R_H2O * T * T);
+}
+
+}  // namespace thermo_f
 }  // namespace athad

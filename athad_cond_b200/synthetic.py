@@ -131,3 +131,82 @@ def mirror(a: np.ndarray, antisymmetric: bool = False) -> np.ndarray:
     """field(i, jm-1-j, k) (negated for the meridional components)."""
     m = a[:, ::-1, :]
     return -m if antisymmetric else m
+
+
+def make_state_device(im: int, jm: int, km: int, seed: int = 20261203, params: dict | None = None,
+                      device=None, amp: float = 1.0) -> dict:
+    """make_state's fields built with torch on a CUDA device (a serving loop admits runs
+    faster than numpy builds their states).  Same formulas and magnitudes; the noise comes
+    from torch's seeded generator, so the values differ from make_state's.  Returns packed
+    (im, jm, km) float64 tensors for GpuAtmosphere.upload_tensor; 2-D fields as (jm, km)."""
+    import torch
+    p = {"t_0": 273.15, "t_surf_equator": 513.15, "t_surf_pole": 503.15, "t_skin": 254.0,
+         "u_0": 8.0, "L_atm": 6287.5, "zeta": 3.0, "c_0": 0.3464, "co2_0": 0.6233,
+         "c_h2o_dry_top": 0.00423, "r_air": 40.8}
+    if params:
+        p.update({k: v for k, v in params.items() if k in p})
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    f64 = dict(dtype=torch.float64, device=dev)
+    shape = (im, jm, km)
+    z = torch.tensor(layer_heights(im, p["L_atm"], p["zeta"]), **f64)
+    lat = torch.linspace(90.0, -90.0, jm, **f64)
+    phi = torch.linspace(0.0, 2 * math.pi, km, **f64)
+    Z = z[:, None, None]
+    LAT = torch.deg2rad(lat)[None, :, None]
+    PHI = phi[None, None, :]
+
+    def noise(scale):
+        return scale * torch.randn(shape, generator=gen, **f64)
+
+    def full(a):
+        return torch.broadcast_to(a, shape).contiguous()
+
+    Ts = p["t_surf_pole"] + (p["t_surf_equator"] - p["t_surf_pole"]) * (1.0 - (LAT / (math.pi / 2)) ** 2)
+    T = torch.clamp(Ts - 5.0e-3 * Z, min=p["t_skin"]) + amp * 0.05 * torch.cos(2 * PHI) * torch.exp(-Z / 30e3)
+    T = full(T)
+    t = T / p["t_0"] + noise(1e-6 * amp)
+    Rm = 386.0
+    H = Rm * T / 9.8066
+    p_surf = 1e-2 * p["r_air"] * Rm * full(Ts)[0]
+    dz = (Z[1:] - Z[:-1])
+    steps = dz / (0.5 * (H[1:] + H[:-1]))
+    cum = torch.cat([torch.zeros((1, jm, km), **f64), torch.cumsum(steps, dim=0)], dim=0)
+    p_stat = p_surf[None] * torch.exp(-cum)
+    c = full(torch.clamp(p["c_0"] * torch.exp(-Z / 12e3), min=p["c_h2o_dry_top"]) * (1.0 + 0.02 * torch.cos(PHI) * amp))
+    c = c + torch.abs(noise(1e-7 * amp))
+    co2 = p["co2_0"] * (1.0 - c) / (1.0 - p["c_0"])
+    band = torch.exp(-((Z - 25e3) / 8e3) ** 2)
+    cloud = full(1e-4 * band * (1 + 0.5 * torch.sin(3 * PHI))) + torch.abs(noise(1e-8))
+    ice = full(5e-5 * torch.exp(-((Z - 60e3) / 10e3) ** 2)) + torch.abs(noise(1e-8))
+    gr = full(1e-6 * band) + torch.abs(noise(1e-9))
+    cell = torch.sin(math.pi * Z / Z.max())
+    u = full(amp * 1e-3 * cell * torch.cos(3 * LAT) * (1 + 0.3 * torch.cos(PHI))) + noise(1e-6 * amp)
+    v = full(-amp * 0.2 * cell * torch.sin(2 * LAT) * (1 + 0.2 * torch.sin(2 * PHI))) + noise(1e-5 * amp)
+    w = full(amp * (0.8 * torch.cos(LAT) ** 2 * (1 - torch.exp(-Z / 5e3)) + 0.05 * torch.sin(PHI))) + noise(1e-5 * amp)
+    tke = full(1e-3 * torch.exp(-Z / 10e3) + 1e-5) + torch.abs(noise(1e-7))
+    dis = full(0.5 * torch.exp(-Z / 20e3) + 0.05) + torch.abs(noise(1e-4))
+    nue = full(1e-3 * torch.exp(-Z / 8e3) + 1e-5) + torch.abs(noise(1e-7))
+    p_dyn = full(amp * 1e-3 * torch.cos(2 * LAT) * torch.sin(math.pi * Z / Z.max()) * (1 + 0.5 * torch.cos(PHI))) + noise(1e-6 * amp)
+    t_eq = t + 0.01 * full(torch.cos(LAT) * torch.exp(-Z / 40e3))
+    r_humid = 1e2 * p_stat / (Rm * T)
+    st = {"t": t, "u": u, "v": v, "w": w, "c": c, "cloud": cloud, "ice": ice, "gr": gr,
+          "co2": co2, "tke": tke, "dis": dis, "p_dyn": p_dyn, "nue": nue, "t_eq": t_eq,
+          "p_stat": p_stat.contiguous(), "r_humid": r_humid}
+    for k_, n in enumerate(["S_c", "S_r", "S_i", "S_s", "S_g", "S_v"]):
+        st[n] = full(1e-8 * band * torch.cos(PHI + k_)) + noise(1e-10)
+    st["MC_t"] = full(1e-7 * band) + noise(1e-9)
+    st["MC_q"] = full(-1e-8 * band) + noise(1e-10)
+    st["MC_v"] = full(1e-8 * torch.sin(2 * LAT) * band) + noise(1e-10)
+    st["MC_w"] = full(1e-8 * band * torch.cos(PHI)) + noise(1e-10)
+    for n_ in ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis"]:
+        a = st[n_]
+        b = a + 1e-6 * torch.randn(shape, generator=gen, **f64) * (torch.abs(a) + 1e-6)
+        if n_ in ("c", "cloud", "ice", "gr", "tke"):
+            b = torch.abs(b)
+        if n_ == "dis":
+            b = torch.clamp(b, min=1e-10)
+        st[n_ + "n"] = b
+    st["Evaporation"] = torch.full((jm, km), 20.0, **f64)
+    return {k: (v.contiguous() if v.dim() == 3 else v) for k, v in st.items()}

@@ -365,6 +365,129 @@ def field_errors(a: dict, b: dict) -> dict:
     return out
 
 
+def _iteration_fp64(g, it: int, dt: float = 4e-5):
+    iteration(g, it, dt)
+
+
+def run_ensemble(args, device) -> dict:
+    """Batched ensemble of seeded members with uneven grids and condition points
+    (athad_cond_b200.ensemble.draw_ensemble): the mixed-precision batch, autotuned, one
+    CUDA graph per iteration, against the same members advanced one after another in the
+    plain FP64 form.  States are built on the device (synthetic.make_state_device)."""
+    import numpy as np
+    import torch
+    from athad_cond_b200 import GpuAtmosphere, GpuBatch
+    from athad_cond_b200._abi import Precision
+    from athad_cond_b200.ensemble import draw_ensemble, condition_params, state_params
+    from athad_cond_b200.synthetic import make_state_device
+    specs = draw_ensemble(args.members)
+    pts = sum(s.grid[0] * s.grid[1] * s.grid[2] for s in specs)
+    stream = torch.cuda.Stream(device=device)
+
+    def build(prec):
+        gs = []
+        with torch.cuda.stream(stream):
+            for s in specs:
+                g = GpuAtmosphere(*s.grid, condition_params(s.cond, prec))
+                g.set_stream(stream.cuda_stream)
+                st = make_state_device(*s.grid, seed=s.seed, params=state_params(s.cond), device=device)
+                for n, t in st.items():
+                    if t.dim() == 3:
+                        g.upload_tensor(n, t)
+                g.upload_2d("Evaporation", st["Evaporation"].cpu().numpy())
+                gs.append(g)
+        stream.synchronize()
+        return gs
+
+    out = {"members": len(specs), "points": pts}
+    gs = build(Precision.MIXED)
+    b = GpuBatch(gs)
+    b.set_stream(stream.cuda_stream)
+    best, times = b.autotune(reps=3)
+    for _ in range(args.warmup):
+        b.iteration(graph=True)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device.index or 0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.iteration(graph=True)
+        e1.record(stream)
+        stream.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    finite = all(bool(np.isfinite(g.download("t")).all()) for g in gs[:4])
+    b.close()
+    for g in gs:
+        g.close()
+    torch.cuda.empty_cache()
+    out.update({"batched_mixed": {"ms_per_iteration": ms, "value": pts / (ms * 1e-3), "shape": best,
+                                  "autotune_ms": times, "finite": finite}, "clocks": clk.summary()})
+    gs = build(Precision.FP64)
+    k64 = max(4, min(args.steps, 20))
+    for it in range(1, 4):
+        for g in gs:
+            _iteration_fp64(g, it)
+    stream.synchronize()
+    e0.record(stream)
+    for it in range(4, 4 + k64):
+        for g in gs:
+            _iteration_fp64(g, it)
+    e1.record(stream)
+    stream.synchronize()
+    ms64 = e0.elapsed_time(e1) / k64
+    for g in gs:
+        g.close()
+    torch.cuda.empty_cache()
+    out["sequential_fp64"] = {"ms_per_iteration": ms64, "value": pts / (ms64 * 1e-3), "iterations": k64}
+    out["batched_mixed_over_fp64"] = out["batched_mixed"]["value"] / out["sequential_fp64"]["value"]
+    return out
+
+
+def run_serving(args, device) -> dict:
+    """Serving loop (athad_cond_b200.serving): Poisson arrivals, continuous batching,
+    admission by HBM footprint; plus the plain FP64 per-grid iteration times that give the
+    'each request alone in the FP64 form' baseline."""
+    import torch
+    from athad_cond_b200 import GpuAtmosphere
+    from athad_cond_b200.serving import GRIDS, Server, poisson_requests
+    from athad_cond_b200.synthetic import make_state_device
+    from athad_cond_b200._abi import config_params
+    reqs = poisson_requests(rate=args.rate, duration=args.duration, steps=(args.min_steps, args.max_steps))
+    srv = Server(max_slots=args.slots)
+    rep = srv.run(reqs)
+    # FP64 alone: iteration time per grid
+    t64 = {}
+    stream = torch.cuda.Stream(device=device)
+    for grid in GRIDS:
+        g = GpuAtmosphere(*grid, config_params())
+        g.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            st = make_state_device(*grid, device=device)
+            for n, t in st.items():
+                if t.dim() == 3:
+                    g.upload_tensor(n, t)
+        for it in range(1, 5):
+            _iteration_fp64(g, it)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for it in range(5, 21):
+            _iteration_fp64(g, it)
+        e1.record(stream)
+        stream.synchronize()
+        t64[grid] = e0.elapsed_time(e1) / 16 * 1e-3
+        g.close()
+    done = [r for r in reqs if r.finished >= 0]
+    alone_s = sum(r.steps * t64[tuple(r.grid)] for r in done)
+    rep["fp64_alone"] = {"seconds": alone_s, "gp_steps_per_s": rep["gp_steps"] / alone_s,
+                         "iteration_s": {f"{g[0]}x{g[1]}x{g[2]}": v for g, v in t64.items()}}
+    rep["offered"] = {"rate_per_s": args.rate, "duration_s": args.duration,
+                      "steps": [args.min_steps, args.max_steps], "requests": len(reqs)}
+    rep["batch_rebuilds"] = srv.rebuilds
+    rep["batched_iterations"] = srv.iterations
+    return rep
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -376,6 +499,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="forms to run; the headline value is the mixed form when it runs")
+    ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving"],
+                    help="iteration: the 41x181x361 model iteration (default); ensemble: the "
+                         "batched ensemble; serving: the serving loop")
+    ap.add_argument("--members", type=int, default=64, help="ensemble members")
+    ap.add_argument("--rate", type=float, default=2.0, help="serving: arrivals per second")
+    ap.add_argument("--duration", type=float, default=30.0, help="serving: seconds of arrivals")
+    ap.add_argument("--min-steps", type=int, default=20, help="serving: fewest iterations of a run")
+    ap.add_argument("--max-steps", type=int, default=200, help="serving: most iterations of a run")
+    ap.add_argument("--slots", type=int, default=64, help="serving: most resident runs")
     args = ap.parse_args()
     global GRID
     if args.grid:
@@ -397,6 +529,27 @@ def main():
     import torch
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.workload != "iteration":
+        if world > 1 and rank != 0:
+            return
+        fn = run_ensemble if args.workload == "ensemble" else run_serving
+        r = fn(args, device)
+        if args.workload == "ensemble":
+            line = {"metric": "ensemble grid-point steps/s (batched mixed-precision model iterations)",
+                    "value": r["batched_mixed"]["value"], "unit": "grid-point steps/s", "n_gpus": 1,
+                    "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": r["batched_mixed"]["ms_per_iteration"], "higher_is_better": True,
+                    "dtype": "f32+f64", "data": "synthetic",
+                    "config": {"workload": f"{r['members']} members, uneven grids, seeded condition points",
+                               "points": r["points"]}, "detail": r}
+        else:
+            line = {"metric": "serving: grid-point steps/s and latency per simulated day",
+                    "value": r.get("gp_steps_per_s"), "unit": "grid-point steps/s", "n_gpus": 1,
+                    "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+                    "config": {"workload": "Poisson arrivals, continuous batching", **r.get("offered", {})},
+                    "detail": r}
+        print(json.dumps(line))
+        return
     if world > 1:
         import datetime
         import torch.distributed as tdist

@@ -203,6 +203,9 @@ size_t athad_footprint_bytes_params(const athad_grid* grid, const athad_params* 
 /* ---- state transfer --------------------------------------------------------- */
 
 athad_status athad_upload(athad_ctx* ctx, athad_field f, const double* host, size_t n);
+/* The same from a packed (i,j,k) buffer already in this device's memory (a state built on
+ * the device); ordered on the context's stream.  No counterpart in the reference. */
+athad_status athad_upload_device(athad_ctx* ctx, athad_field f, const double* device_src, size_t n);
 athad_status athad_download(athad_ctx* ctx, athad_field f, double* host, size_t n);
 athad_status athad_upload_2d(athad_ctx* ctx, athad_field2d f, const double* host, size_t n);
 athad_status athad_download_2d(athad_ctx* ctx, athad_field2d f, double* host, size_t n);

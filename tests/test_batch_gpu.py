@@ -2,8 +2,9 @@
 
 The batched kernels run the per-cell code of the single-grid mixed-precision step on every
 member, so each member's result must be bit-for-bit what the same iterations give on that
-member alone: through a batch of one, and through the single-context entry points with the
-same scalars.  Covered: uneven grids, members at different iteration numbers (different
+member alone: through a batch of one (the serving path of a request run alone), and
+through the single-context entry points with the same scalars (the mixed-precision kernels
+are compiled without fused multiply-add, so both kernels round every operation alike).  Covered: uneven grids, members at different iteration numbers (different
 cadence phases), the CUDA-graph replay, every tile shape of the autotuner, inactive members.
 """
 import numpy as np
