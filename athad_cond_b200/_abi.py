@@ -108,6 +108,13 @@ class BatchStepParams(ctypes.Structure):
                 ("buoyancy_ramp_iters", ctypes.c_int32), ("pad0", ctypes.c_int32)]
 
 
+class SolveReport(ctypes.Structure):
+    """athad_solve_report"""
+    _fields_ = [("iterations", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("rel_residual", ctypes.c_double), ("history", ctypes.c_double * 64),
+                ("precond_levels", ctypes.c_int32), ("pad0", ctypes.c_int32), ("seconds", ctypes.c_double)]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -141,6 +148,7 @@ SIGNATURES = {
     "athad_level_mean": (ctypes.c_int, [_P]),
     "athad_rk4_step": (ctypes.c_int, [_P, ctypes.POINTER(StepScalars)]),
     "athad_pressure_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),
     "athad_densities": (ctypes.c_int, [_P, ctypes.c_int32]),

@@ -152,6 +152,14 @@ class GpuAtmosphere:
         """PressureSolverAtm::run (PressureSolverAtm.h:27-669; call site cAtmosphereModel.cpp:1158)."""
         self._check(self.lib.athad_pressure_sweep(self._h, n_sweeps, total_iter_count))
 
+    def pressure_solve(self, rel_tol: float = 1e-10, max_iter: int = 200) -> dict:
+        """The sweep's pressure equation solved to a relative residual (athad_pressure_solve)."""
+        r = _abi.SolveReport()
+        self._check(self.lib.athad_pressure_solve(self._h, float(rel_tol), int(max_iter), ctypes.byref(r)))
+        return {"iterations": r.iterations, "converged": bool(r.converged), "rel_residual": r.rel_residual,
+                "history": list(r.history)[:max(0, min(r.iterations, 64))], "levels": r.precond_levels,
+                "seconds": r.seconds}
+
     def project_initial_velocity(self, n_sweeps: int = 200, total_iter_count: int = 0):
         """PressureSolverAtm::project_initial_velocity (PressureSolverAtm.h:686-767)."""
         self._check(self.lib.athad_project_initial_velocity(self._h, n_sweeps, total_iter_count))

@@ -265,6 +265,7 @@ athad_status athad_destroy(athad_ctx* ctx)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
     cudaStreamSynchronize(ctx->stream);
+    mg_free(ctx->mg);
     cudaFree(ctx->slab);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;

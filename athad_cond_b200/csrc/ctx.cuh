@@ -9,6 +9,9 @@
 
 namespace athad {
 
+struct MGSolver;                 // pressure_solve hierarchy (k_mg.cu), built on first use
+void mg_free(MGSolver* s);
+
 constexpr int kNY = 11;   // prognostic fields t..dis
 
 struct Layout {
@@ -94,6 +97,7 @@ struct athad_ctx {
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
     std::vector<double> rad;
     int64_t poisson_sweeps_since_reset = 0;
+    MGSolver* mg = nullptr;
     std::string err;
 };
 

@@ -168,6 +168,15 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     poisson_ceiling_kernel<<<grid, block, 0, st>>>(a);
 }
 
+// the boundary conditions of a sweep alone (radial, pole, seam), PressureSolverAtm.h:504-552
+void launch_poisson_bcs(const PoissonArgs& a, cudaStream_t st)
+{
+    const Dims& d = a.d;
+    poisson_bc_radial_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
+    poisson_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
+    poisson_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
+}
+
 // gradient correction of project_initial_velocity, PressureSolverAtm.h:728-749
 __global__ void __launch_bounds__(256) project_correct_kernel(PoissonArgs a, double* u, double* v, double* w)
 {

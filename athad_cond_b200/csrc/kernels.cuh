@@ -142,6 +142,7 @@ struct PoissonArgs {
 };
 void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st);   // aux BC + source
 void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st);     // colours + BCs + ceiling
+void launch_poisson_bcs(const PoissonArgs& a, cudaStream_t st);       // BCs only
 void launch_project_correct(const PoissonArgs& a, double* u, double* v, double* w, cudaStream_t st);
 
 // Column physics

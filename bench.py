@@ -488,6 +488,53 @@ def run_serving(args, device) -> dict:
     return rep
 
 
+def run_poisson(args, device) -> dict:
+    """Pressure-Poisson stress solve: a 61 x 361 x 721 grid, the source the divergence of
+    a seeded mirror-symmetric Gaussian velocity perturbation of 0.5 m/s (u, w symmetric,
+    v antisymmetric; torch's Philox generator, seed 20261203) on the nominal state, solved
+    to a 1e-10 relative residual (athad_pressure_solve)."""
+    import torch
+    from athad_cond_b200 import GpuAtmosphere
+    from athad_cond_b200._abi import config_params
+    from athad_cond_b200.synthetic import make_state_device
+    im, jm, km = args.poisson_grid
+    stream = torch.cuda.Stream(device=device)
+    g = GpuAtmosphere(im, jm, km, config_params())
+    g.set_stream(stream.cuda_stream)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(20261203)
+    jh = (jm + 1) // 2
+    with torch.cuda.stream(stream):
+        st = make_state_device(im, jm, km, device=device)
+        for n, t in st.items():
+            if t.dim() == 3 and n != "p_dyn":
+                g.upload_tensor(n, t)
+        amp = 0.5 / 8.0                                   # 0.5 m/s in units of u_0
+        for n, anti in (("aux_u", False), ("aux_v", True), ("aux_w", False)):
+            half = amp * torch.randn((im, jh, km), generator=gen, dtype=torch.float64, device=device)
+            full = torch.empty((im, jm, km), dtype=torch.float64, device=device)
+            full[:, :jh] = half
+            full[:, jh:] = (-1.0 if anti else 1.0) * torch.flip(half[:, :jm - jh], dims=[1])
+            if anti:
+                full[:, jm // 2] = 0.0
+            g.upload_tensor(n, full.contiguous())
+        g.upload_tensor("p_dyn", torch.zeros((im, jm, km), dtype=torch.float64, device=device))
+    stream.synchronize()
+    reps = []
+    with ClockSampler(device.index or 0) as clk:
+        for _ in range(max(1, args.steps)):
+            g.upload_tensor("p_dyn", torch.zeros((im, jm, km), dtype=torch.float64, device=device))
+            g.synchronize()
+            reps.append(g.pressure_solve(1e-10, 500))
+    best = min(reps, key=lambda r: r["seconds"])
+    pts = im * jm * km
+    g.close()
+    return {"grid": [im, jm, km], "points": pts, "iterations": best["iterations"],
+            "converged": best["converged"], "rel_residual": best["rel_residual"],
+            "seconds": best["seconds"], "all_seconds": [r["seconds"] for r in reps],
+            "levels": best["levels"], "history": best["history"], "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,7 +546,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="forms to run; the headline value is the mixed form when it runs")
-    ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving"],
+    ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving", "poisson"],
                     help="iteration: the 41x181x361 model iteration (default); ensemble: the "
                          "batched ensemble; serving: the serving loop")
     ap.add_argument("--members", type=int, default=64, help="ensemble members")
@@ -508,12 +555,14 @@ def main():
     ap.add_argument("--min-steps", type=int, default=20, help="serving: fewest iterations of a run")
     ap.add_argument("--max-steps", type=int, default=200, help="serving: most iterations of a run")
     ap.add_argument("--slots", type=int, default=64, help="serving: most resident runs")
+    ap.add_argument("--poisson-grid", default="61x361x721", help="poisson: IMxJMxKM")
     args = ap.parse_args()
     global GRID
     if args.grid:
         GRID = tuple(int(x) for x in args.grid.lower().split("x"))
     if args.warmup < 3:
         args.warmup = 3
+    args.poisson_grid = tuple(int(x) for x in args.poisson_grid.lower().split("x"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -532,9 +581,16 @@ def main():
     if args.workload != "iteration":
         if world > 1 and rank != 0:
             return
-        fn = run_ensemble if args.workload == "ensemble" else run_serving
+        fn = {"ensemble": run_ensemble, "serving": run_serving, "poisson": run_poisson}[args.workload]
         r = fn(args, device)
-        if args.workload == "ensemble":
+        if args.workload == "poisson":
+            line = {"metric": "pressure-Poisson solve to 1e-10 relative residual: seconds",
+                    "value": r["seconds"], "unit": "s", "n_gpus": 1, "higher_is_better": False,
+                    "dtype": "f64+f32", "data": "synthetic",
+                    "config": {"workload": "61x361x721 stress solve, mirror-symmetric Gaussian "
+                                           "velocity perturbation 0.5 m/s", "grid": r["grid"]},
+                    "detail": r}
+        elif args.workload == "ensemble":
             line = {"metric": "ensemble grid-point steps/s (batched mixed-precision model iterations)",
                     "value": r["batched_mixed"]["value"], "unit": "grid-point steps/s", "n_gpus": 1,
                     "steps": args.steps, "warmup": args.warmup,

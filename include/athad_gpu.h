@@ -244,6 +244,29 @@ athad_status athad_pressure_sweep(athad_ctx* ctx, int32_t n_sweeps, int32_t tota
 
 /* PressureSolverAtm::project_initial_velocity (PressureSolverAtm.h:686-767); call site
  * cAtmosphereModel.cpp:665. */
+/* Result of athad_pressure_solve. */
+typedef struct athad_solve_report {
+    int32_t iterations;        /* conjugate-gradient iterations                              */
+    int32_t converged;         /* rel_residual <= rel_tol                                    */
+    double  rel_residual;      /* ||b - A p||_2 / ||b||_2 at the end: b the projected source,
+                                * A the sweep's operator with its boundary conditions (FP64) */
+    double  history[64];       /* relative residual after iteration n (n <= 64)              */
+    int32_t precond_levels;    /* multigrid levels of the FP32 preconditioner                */
+    int32_t pad0;
+    double  seconds;           /* device time of the solve                                   */
+} athad_solve_report;
+
+/* Solve the pressure-Poisson equation of the sweep to a relative residual: the fixed point
+ * of PressureSolverAtm::run's red-black relaxation (PressureSolverAtm.h:225-552) for the
+ * current aux_u/v/w, with the same clamped divergence source and boundary conditions,
+ * without the |p| ceiling.  FP64 conjugate gradients preconditioned by an FP32 multigrid
+ * V-cycle; the source is projected onto the operator's range (the operator has the
+ * constants as its null space) and p_dyn is returned with zero interior mean.  The
+ * multigrid hierarchy is allocated on the first call and kept by the context.  Not
+ * supported with the anelastic term (ATHAD_ERR_UNSUPPORTED).  The reference has no such
+ * call: it relaxes one sweep per call (athad_pressure_sweep). */
+athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int32_t max_iter,
+                                  athad_solve_report* report);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 
