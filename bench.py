@@ -552,8 +552,8 @@ def main():
     ap.add_argument("--members", type=int, default=64, help="ensemble members")
     ap.add_argument("--rate", type=float, default=2.0, help="serving: arrivals per second")
     ap.add_argument("--duration", type=float, default=30.0, help="serving: seconds of arrivals")
-    ap.add_argument("--min-steps", type=int, default=20, help="serving: fewest iterations of a run")
-    ap.add_argument("--max-steps", type=int, default=200, help="serving: most iterations of a run")
+    ap.add_argument("--min-steps", type=int, default=200, help="serving: fewest iterations of a run")
+    ap.add_argument("--max-steps", type=int, default=2000, help="serving: most iterations of a run")
     ap.add_argument("--slots", type=int, default=64, help="serving: most resident runs")
     ap.add_argument("--poisson-grid", default="61x361x721", help="poisson: IMxJMxKM")
     args = ap.parse_args()
