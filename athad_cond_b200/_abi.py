@@ -62,7 +62,7 @@ NFIELDS = len(FIELD_NAMES)
 PROGNOSTIC = FIELD_NAMES[0:11]
 N_LEVEL = FIELD_NAMES[11:22]
 
-FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D"]
+FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star"]
 FIELD2D = {n: i for i, n in enumerate(FIELD2D_NAMES)}
 PROFILE_NAMES = ["t_ref_level", "rho_base", "dlnrho_dr"]
 PROFILE = {n: i for i, n in enumerate(PROFILE_NAMES)}
@@ -148,6 +148,7 @@ SIGNATURES = {
     "athad_level_mean": (ctypes.c_int, [_P]),
     "athad_rk4_step": (ctypes.c_int, [_P, ctypes.POINTER(StepScalars)]),
     "athad_pressure_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "athad_boundary_conditions": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),

@@ -152,6 +152,11 @@ class GpuAtmosphere:
         """PressureSolverAtm::run (PressureSolverAtm.h:27-669; call site cAtmosphereModel.cpp:1158)."""
         self._check(self.lib.athad_pressure_sweep(self._h, n_sweeps, total_iter_count))
 
+    def boundary_conditions(self):
+        """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi
+        (call site cAtmosphereModel.cpp:1439-1442)."""
+        self._check(self.lib.athad_boundary_conditions(self._h))
+
     def pressure_solve(self, rel_tol: float = 1e-10, max_iter: int = 200) -> dict:
         """The sweep's pressure equation solved to a relative residual (athad_pressure_solve)."""
         r = _abi.SolveReport()

@@ -178,6 +178,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     const float hL = (float)params->L_atm;
     for (int i = 0; i < im; i++)
         height[i] = (double)(float)((std::exp(params->zeta * (rad[i] - rad[0])) - 1) * (double)hL);
+    c->layer_height1 = height[1];
     for (int i = 0; i < im; i++) {   // SaturationAdjustment::computeSteps: float difference
         const float h1 = (i + 1 <= im - 1) ? (float)height[i + 1] : -1.0f;
         const float h0 = (float)height[i];
@@ -678,6 +679,33 @@ athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
     out->poisson_src_cells = (int64_t)h[0] * ctx->poisson_sweeps_since_reset;
     out->poisson_src_clamped = (int64_t)h[1] * ctx->poisson_sweeps_since_reset;
     out->satadj_ceiling_hits = (int64_t)h[2];
+    return ATHAD_OK;
+}
+
+athad_status athad_boundary_conditions(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    const athad_params& p = ctx->p;
+    BcArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    for (int f = 0; f < ATHAD_NFIELDS; f++) a.F[f] = ctx->field[f];
+    a.t_top_init = ctx->f2d[ATHAD_2D_T_TOP_INIT];
+    a.vel_star = ctx->f2d[ATHAD_2D_VEL_STAR];
+    // TurbulenceAtm::apply_wall_bc (TurbulenceAtm.h:109-147): C_nue = 0.028, the
+    // constructor's nue_air = 1.5e-5, y1 = get_layer_height(1)
+    a.tke_wall_den = std::sqrt(0.028) * p.u_0 * p.u_0;
+    const double y1_safe = (ctx->layer_height1 < 1.0e-6) ? 1.0e-6 : ctx->layer_height1;
+    const double nd_omega = p.L_atm / p.u_0, nue_air = 1.5e-5;
+    if (p.turb_model == ATHAD_TURB_K_EPSILON) {
+        a.dis_wall = 0.0; a.set_dis_wall = 1;
+    } else if (p.turb_model == ATHAD_TURB_K_OMEGA) {
+        a.dis_wall = 6.0 * nue_air / (0.075 * y1_safe * y1_safe) * nd_omega; a.set_dis_wall = 1;
+    } else {
+        a.dis_wall = 60.0 * nue_air / (0.0333 * y1_safe * y1_safe) * nd_omega; a.set_dis_wall = 1;
+    }
+    launch_boundary_conditions(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "boundary_conditions");
     return ATHAD_OK;
 }
 

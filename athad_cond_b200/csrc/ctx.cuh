@@ -95,6 +95,7 @@ struct athad_ctx {
     double* row_cnt = nullptr;
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
+    double layer_height1 = 0;   // get_layer_height(1): the first layer's height, float-rounded
     std::vector<double> rad;
     int64_t poisson_sweeps_since_reset = 0;
     MGSolver* mg = nullptr;

@@ -127,8 +127,16 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 #define ATHAD_RK4_MIN_BLOCKS 7   // 72 registers per thread, 7 CTAs of 128 threads per SM
 #endif
 
+#ifndef ATHAD_RK4_BX
+#define ATHAD_RK4_BX 32          // CTA: BX longitudes x BY rows of one level
+#endif
+#ifndef ATHAD_RK4_BY
+#define ATHAD_RK4_BY 4
+#endif
+
 template <int STAGE>
-__global__ void __launch_bounds__(128, ATHAD_RK4_MIN_BLOCKS) rk4_stage_kernel(const RK4Args a)
+__global__ void __launch_bounds__(ATHAD_RK4_BX * ATHAD_RK4_BY, ATHAD_RK4_MIN_BLOCKS * 128 / (ATHAD_RK4_BX * ATHAD_RK4_BY))
+rk4_stage_kernel(const RK4Args a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -397,8 +405,8 @@ __global__ void __launch_bounds__(128, ATHAD_RK4_MIN_BLOCKS) rk4_stage_kernel(co
 
 void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((a.d.km + 31) / 32, (a.d.jm + 3) / 4, a.d.im);
+    const dim3 block(ATHAD_RK4_BX, ATHAD_RK4_BY, 1);
+    const dim3 grid((a.d.km + ATHAD_RK4_BX - 1) / ATHAD_RK4_BX, (a.d.jm + ATHAD_RK4_BY - 1) / ATHAD_RK4_BY, a.d.im);
     switch (stage) {
         case 1: rk4_stage_kernel<1><<<grid, block, 0, st>>>(a); break;
         case 2: rk4_stage_kernel<2><<<grid, block, 0, st>>>(a); break;

@@ -406,8 +406,16 @@ __device__ __forceinline__ void rk4m_cell(const RK4MArgs& a, int i, int j, int k
 #define ATHAD_RK4M_MIN_BLOCKS 12   // 40 registers per thread, 12 CTAs of 128 threads per SM
 #endif
 
+#ifndef ATHAD_RK4M_BX
+#define ATHAD_RK4M_BX 32         // CTA: BX longitudes x BY rows of one level
+#endif
+#ifndef ATHAD_RK4M_BY
+#define ATHAD_RK4M_BY 4
+#endif
+
 template <int STAGE>
-__global__ void __launch_bounds__(128, ATHAD_RK4M_MIN_BLOCKS) rk4m_stage_kernel(const RK4MArgs a)
+__global__ void __launch_bounds__(ATHAD_RK4M_BX * ATHAD_RK4M_BY, ATHAD_RK4M_MIN_BLOCKS * 128 / (ATHAD_RK4M_BX * ATHAD_RK4M_BY))
+rk4m_stage_kernel(const RK4MArgs a)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -417,8 +425,8 @@ __global__ void __launch_bounds__(128, ATHAD_RK4M_MIN_BLOCKS) rk4m_stage_kernel(
 
 void launch_rk4m_stage(int stage, const RK4MArgs& a, cudaStream_t st)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((a.d.km + 31) / 32, (a.d.jm + 3) / 4, a.d.im);
+    const dim3 block(ATHAD_RK4M_BX, ATHAD_RK4M_BY, 1);
+    const dim3 grid((a.d.km + ATHAD_RK4M_BX - 1) / ATHAD_RK4M_BX, (a.d.jm + ATHAD_RK4M_BY - 1) / ATHAD_RK4M_BY, a.d.im);
     switch (stage) {
         case 1: rk4m_stage_kernel<1><<<grid, block, 0, st>>>(a); break;
         case 2: rk4m_stage_kernel<2><<<grid, block, 0, st>>>(a); break;

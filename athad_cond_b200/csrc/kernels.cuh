@@ -182,6 +182,18 @@ struct MoistArgs {
 void launch_moist_convection(const MoistArgs& a, cudaStream_t st);
 
 void launch_fill(const Dims& d, double* dst, double v, cudaStream_t st);
+
+// Per-iteration boundary conditions (k_bc.cu)
+struct BcArgs {
+    Dims d;
+    double* F[ATHAD_NFIELDS];
+    const double* t_top_init;   // 2-D, pitched rows [jm][pitch]
+    const double* vel_star;     // 2-D, pitched rows [jm][pitch]
+    double tke_wall_den;        // sqrt(C_nue) * u_0 * u_0
+    double dis_wall;            // omega (or epsilon) at the wall, non-dimensional
+    int set_dis_wall;
+};
+void launch_boundary_conditions(const BcArgs& a, cudaStream_t st);
 void launch_repitch(const Dims& d, const double* packed, double* dst, cudaStream_t st);
 
 }  // namespace athad

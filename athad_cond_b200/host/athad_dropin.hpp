@@ -12,6 +12,8 @@
 //     SaturationAdjustmentRun(m) SaturationAdjustment(m).run()               :1218
 //     MoistConvectionRun(m, it) MoistConvection(m).run(it)                   :1247
 //     Densities(m, water)       ThermoAtm(m).densities(water)                :567, 634, 1418
+//     BoundaryConditions(m)     BC_Atm(m).bcRadius(); TurbulenceAtm(m).apply_wall_bc();
+//                               BC_Atm(m).bcTheta(); BC_Atm(m).bcPhi()       :1439-1442
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -219,6 +221,39 @@ public:
             for (int k = 0; k < km_; k++) m.p_stat_landscape.y[j][k] = ps[(size_t)j * km_ + k];
         down_profile(ATHAD_PROF_RHO_BASE, m.m_rho_base);
         down_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+    }
+
+    // the per-iteration boundary conditions (cAtmosphereModel.cpp:1439-1442), flat terrain
+    void BoundaryConditions(Model& m)
+    {
+#define ATHAD_BC_FIELDS(X) X(ATHAD_T, t) X(ATHAD_U, u) X(ATHAD_V, v) X(ATHAD_W, w) X(ATHAD_C, c) \
+        X(ATHAD_CLOUD, cloud) X(ATHAD_ICE, ice) X(ATHAD_GR, gr) X(ATHAD_CO2, co2) X(ATHAD_TKE, tke) \
+        X(ATHAD_DIS, dis) X(ATHAD_NUE, nue) X(ATHAD_PROD, prod) X(ATHAD_TKE_SOURCE, tke_source) \
+        X(ATHAD_DIS_SOURCE, dis_source) X(ATHAD_UN, un) X(ATHAD_VN, vn) X(ATHAD_WN, wn) \
+        X(ATHAD_P_STAT, p_stat) X(ATHAD_R_HUMID, r_humid) X(ATHAD_R_DRY, r_dry) X(ATHAD_S_C_C, S_c_c) \
+        X(ATHAD_S_V, S_v) X(ATHAD_S_C, S_c) X(ATHAD_S_I, S_i) X(ATHAD_S_R, S_r) X(ATHAD_S_S, S_s) \
+        X(ATHAD_S_G, S_g) X(ATHAD_Q_V_U, q_v_u) X(ATHAD_Q_C_U, q_c_u) X(ATHAD_U_U, u_u) \
+        X(ATHAD_V_U, v_u) X(ATHAD_W_U, w_u) X(ATHAD_MC_S, s) X(ATHAD_MC_S_U, s_u) X(ATHAD_MC_S_D, s_d) \
+        X(ATHAD_M_U, M_u) X(ATHAD_M_D, M_d) X(ATHAD_C_U, c_u) X(ATHAD_E_DD, e_d) X(ATHAD_E_L, e_l) \
+        X(ATHAD_E_P, e_p) X(ATHAD_G_P, g_p) X(ATHAD_P_CONV, P_conv)
+#define ATHAD_BC_UP(F, N) up(F, m.N);
+#define ATHAD_BC_DOWN(F, N) down(F, m.N);
+        ATHAD_BC_FIELDS(ATHAD_BC_UP)
+        std::vector<double> tt((size_t)jm_ * km_, 0.0);
+        if ((int)m.t_top_init.size() == jm_) {
+            for (int j = 0; j < jm_; j++)
+                for (int k = 0; k < km_; k++) tt[(size_t)j * km_ + k] = m.t_top_init[j][k];
+        } else {   // BC_Atm.h:613-614: without the snapshot the lid is a zero-gradient copy
+            for (int j = 0; j < jm_; j++)
+                for (int k = 0; k < km_; k++) tt[(size_t)j * km_ + k] = m.t.x[im_ - 2][j][k];
+        }
+        check(ctx_, athad_upload_2d(ctx_, ATHAD_2D_T_TOP_INIT, tt.data(), tt.size()), "t_top_init");
+        up2(ATHAD_2D_VEL_STAR, m.vel_star);
+        check(ctx_, athad_boundary_conditions(ctx_), "boundary_conditions");
+        ATHAD_BC_FIELDS(ATHAD_BC_DOWN)
+#undef ATHAD_BC_UP
+#undef ATHAD_BC_DOWN
+#undef ATHAD_BC_FIELDS
     }
 
 private:

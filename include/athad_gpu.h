@@ -147,6 +147,8 @@ typedef enum athad_field2d {
     ATHAD_2D_P_STAT_LANDSCAPE,      /* Array_2D p_stat_landscape                      */
     ATHAD_2D_EVAPORATION,           /* Array_2D Evaporation (MoistConvection input)   */
     ATHAD_2D_Q_SENSIBLE,            /* Array_2D Q_sensible_2D (MoistConvection input) */
+    ATHAD_2D_VEL_STAR,              /* Array_2D vel_star, friction velocity [m/s]
+                                     * (TurbulenceAtm::compute_vel_star; wall BC input) */
     ATHAD_NFIELDS2D
 } athad_field2d;
 
@@ -267,6 +269,11 @@ typedef struct athad_solve_report {
  * call: it relaxes one sweep per call (athad_pressure_sweep). */
 athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int32_t max_iter,
                                   athad_solve_report* report);
+/* The per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1442 for flat
+ * terrain: BC_Atm::bcRadius (BC_Atm.h:556-746), TurbulenceAtm::apply_wall_bc
+ * (TurbulenceAtm.h:109-147; reads the 2-D field ATHAD_2D_VEL_STAR), BC_Atm::bcTheta
+ * (:750-796) and BC_Atm::bcPhi (:803-918), on the fields the context holds. */
+athad_status athad_boundary_conditions(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

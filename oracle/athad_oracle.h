@@ -68,7 +68,7 @@ enum {
     OF_P_CONV, OF_CLOUD_BASE, OF_LEVEL_FREE_SINKING, OF_DEEP_BEG, OF_DEEP_END,
     OF_NFIELDS
 };
-enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_N };
+enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR, OF2_N };
 enum { OFP_T_REF_LEVEL = 0, OFP_RHO_BASE, OFP_DLNRHO_DR, OFP_N };
 
 size_t or_params_size(void);
@@ -110,6 +110,11 @@ void or_densities(int im, int jm, int km, const or_params* p, int compat,
 /* MoistConvection::run, MoistConvection.h:106-140 */
 int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, int iter_n,
                         double* const* f, double* const* f2);
+
+/* the per-iteration boundary conditions, cAtmosphereModel.cpp:1439-1442: BC_Atm::bcRadius,
+ * TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta, BC_Atm::bcPhi (flat terrain) */
+void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* const* f,
+                            double* const* f2);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

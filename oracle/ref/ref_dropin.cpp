@@ -46,6 +46,7 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 3: d.MoistConvectionRun(*m, arg); break;
             case 4: d.Densities(*m, false); break;
             case 5: d.Densities(*m, true); break;
+            case 6: d.BoundaryConditions(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

@@ -98,6 +98,7 @@ Array_2D* field2(cAtmosphereModel* m, const std::string& n)
     if (n == "p_stat_landscape") return &m->p_stat_landscape;
     if (n == "Evaporation") return &m->Evaporation;
     if (n == "Q_sensible_2D") return &m->Q_sensible_2D;
+    if (n == "vel_star") return &m->vel_star;
     return nullptr;
 }
 
@@ -337,6 +338,16 @@ void ref_moist(void* p, int iter_n)
     MoistConvection(*m).run(iter_n);
 }
 void ref_store(void* p) { UtilsAtm(*(cAtmosphereModel*)p).storeIntermediateData3D(1.0); }
+// the per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1442 (flat terrain:
+// bcScalarSurfSur and bcSolidGround change nothing and are left out)
+void ref_bc(void* p)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    BC_Atm(*m).bcRadius();
+    if (m->turb_model != "laminar") TurbulenceAtm(*m).apply_wall_bc();
+    BC_Atm(*m).bcTheta();
+    BC_Atm(*m).bcPhi();
+}
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
 
 // RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4

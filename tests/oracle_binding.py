@@ -148,3 +148,9 @@ class OracleState:
         F, _, _ = self._args()
         im, jm, km = self.shape
         lib().or_store_n_level(im, jm, km, F)
+
+    def boundary_conditions(self):
+        """or_boundary_conditions: bcRadius, apply_wall_bc, bcTheta, bcPhi."""
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_boundary_conditions(im, jm, km, ctypes.byref(self.params), F, F2)

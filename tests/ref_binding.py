@@ -110,6 +110,10 @@ class Reference:
         if r != 0:
             raise RuntimeError(err.value.decode())
 
+    def bc(self):
+        """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi."""
+        self.lib.ref_bc(self.h)
+
     def rhs_cell(self, i, j, k):
         out = (ctypes.c_double * 17)()
         self.lib.ref_rhs_cell(self.h, int(i), int(j), int(k), out)

@@ -5,6 +5,7 @@ results must match what the reference's own CPU call produces on the same state:
 
   * saturation adjustment, densities, moist convection, pressure sweep: 1e-10 relative
     (CUDA vs glibc transcendentals, mirror-symmetric trig tables);
+  * the boundary conditions: bit-identical (copies and short sums in the same order);
   * the RK4 step: the device integrates the four stages Jacobi-style where the reference
     updates cells in place, so the difference is bounded by a small fraction of the step's
     own change, with the reference's SST wall distance selected.
@@ -98,3 +99,16 @@ def test_dropin_rk4(model):
     for n, (a, b) in out.items():
         step = np.max(np.abs(b - snap[n]))
         assert np.max(np.abs(a - b)) <= 1e-2 * step, n
+
+
+def test_dropin_boundary_conditions(model):
+    """BC_Atm::bcRadius + TurbulenceAtm::apply_wall_bc + bcTheta + bcPhi through the adapter,
+    on the reference's state with every field moved off its boundary values: bit-identical."""
+    R, snap = model
+    im, jm, km = R.shape
+    pattern = 1.0 + 1e-3 * np.sin(np.arange(im * jm * km, dtype=np.float64) * 0.37).reshape(im, jm, km)
+    moved = {n: a * pattern for n, a in snap.items()}
+    out = run_both(R, moved, lambda: R.bc(), lambda: R.dropin(6), FIELD_NAMES)
+    reset(R, snap)
+    for n, (a, b) in out.items():
+        assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))

@@ -7,7 +7,8 @@ semantics, must reproduce every hot-path function bit for bit:
 
   * RHS_Atmosphere_Turb at sampled cells;
   * solveRungeKutta_Atmosphere_Turb, the in-place sweep run with T OpenMP threads;
-  * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes).
+  * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes);
+  * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi).
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -35,7 +36,7 @@ def ref():
         R = ref_binding.Reference("pin", threads=THREADS)
         R.init_state()
         snap = {n: R.get(n) for n in FIELD_NAMES}
-        snap2 = {n: R.get2(n) for n in ("t_top_init", "p_stat_landscape")}
+        snap2 = {n: R.get2(n) for n in ("t_top_init", "p_stat_landscape", "vel_star")}
         yield R, snap, snap2
         R.close()
     finally:
@@ -144,3 +145,18 @@ def test_moist_convection_bit_exact_two_calls(ref):
         R.lib.ref_moist(R.h, it)
         o.moist_convection(it, compat=1)
         assert_identical(R, o, MC_FIELDS)
+
+
+def test_boundary_conditions_bit_exact(ref):
+    """bcRadius + apply_wall_bc + bcTheta + bcPhi on a state whose every field was moved off
+    its boundary-consistent values (so every boundary formula writes something new)."""
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    pattern = 1.0 + 1e-3 * np.sin(np.arange(im * jm * km, dtype=np.float64) * 0.37).reshape(im, jm, km)
+    for n in FIELD_NAMES:
+        a = R.get(n) * pattern
+        R.set(n, a)
+        o.f[n][...] = a
+    R.bc()
+    o.boundary_conditions()
+    assert_identical(R, o, FIELD_NAMES)
