@@ -149,6 +149,8 @@ SIGNATURES = {
     "athad_rk4_step": (ctypes.c_int, [_P, ctypes.POINTER(StepScalars)]),
     "athad_pressure_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_boundary_conditions": (ctypes.c_int, [_P]),
+    "athad_post_rk4_filters": (ctypes.c_int, [_P]),
+    "athad_damp_wiggles": (ctypes.c_int, [_P, ctypes.c_int]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),

@@ -157,6 +157,14 @@ class GpuAtmosphere:
         (call site cAtmosphereModel.cpp:1439-1442)."""
         self._check(self.lib.athad_boundary_conditions(self._h))
 
+    def post_rk4_filters(self):
+        """Polar zonal and radial Shapiro filters of u, v, w (cAtmosphereModel.cpp:1507-1520)."""
+        self._check(self.lib.athad_post_rk4_filters(self._h))
+
+    def damp_wiggles(self, name: str):
+        """AtomUtils::damp_wiggles(field, i, j, k) (lib/Utils.cpp:429-531)."""
+        self._check(self.lib.athad_damp_wiggles(self._h, FIELD[name]))
+
     def pressure_solve(self, rel_tol: float = 1e-10, max_iter: int = 200) -> dict:
         """The sweep's pressure equation solved to a relative residual (athad_pressure_solve)."""
         r = _abi.SolveReport()

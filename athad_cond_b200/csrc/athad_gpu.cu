@@ -126,6 +126,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     c->row_sum = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->counters = (unsigned long long*)take(256);
+    c->polar_passes = (int*)take((size_t)jm * sizeof(int));
     if (params->precision == ATHAD_PRECISION_MIXED) {
         const size_t fb = L.field_elems * sizeof(float);
         for (int n = 0; n < kNY; n++) c->mA[n] = (float*)take(fb);
@@ -194,6 +195,17 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
         const int jj = (j < jm - 1 - j) ? j : jm - 1 - j;
         cose[j] = std::cos(the[(jm - 1) / 2] - the[jj]);
     }
+    // AtomUtils::polar_zonal_filter's passes per row (lib/Utils.cpp:559-571), from the
+    // mirror-exact sin table: clamp(lround(3 (sin30/sin_j)^2 - 3), 0, 12) poleward of 30 deg
+    std::vector<int> polar(jm, 0);
+    for (int j = 0; j < jm; j++) {
+        const double sin_ref = std::cos(30.0 * (M_PI / 180.0));
+        const double sin_j = (sin_w[j] < 1.0e-6) ? 1.0e-6 : sin_w[j];
+        if (sin_j >= sin_ref) continue;
+        const double ratio = sin_ref / sin_j;
+        long pp = std::lround(3.0 * (ratio * ratio - 1.0));
+        polar[j] = (int)(pp < 0 ? 0 : pp > 12 ? 12 : pp);
+    }
     std::vector<GeoIJ> geo((size_t)im * jm);
     std::vector<PoiIJ> poi((size_t)im * jm);
     const double inv_dr2 = 1.0 / (c->dr * c->dr), inv_dthe2 = 1.0 / (c->dthe * c->dthe),
@@ -238,6 +250,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->coslat, coslat.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "coslat");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_mc, step_mc.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step_mc");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->cose, cose.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "cose");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->polar_passes, polar.data(), jm * sizeof(int), cudaMemcpyHostToDevice, c->stream), "polar passes");
     std::vector<GeoF> geof;
     if (s == ATHAD_OK && c->geof) {   // FP32 factors rounded from the FP64 ones (mirror-exact)
         geof.resize(geo.size());
@@ -706,6 +719,30 @@ athad_status athad_boundary_conditions(athad_ctx* ctx)
     }
     launch_boundary_conditions(a, ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "boundary_conditions");
+    return ATHAD_OK;
+}
+
+athad_status athad_post_rk4_filters(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (ctx->L.d.km > 3072) return fail(ctx, ATHAD_ERR_UNSUPPORTED, "post_rk4_filters: km > 3072");
+    FilterArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    a.field[0] = ctx->field[ATHAD_U]; a.field[1] = ctx->field[ATHAD_V]; a.field[2] = ctx->field[ATHAD_W];
+    a.polar_passes = ctx->polar_passes;
+    launch_post_rk4_filters(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "post_rk4_filters");
+    return ATHAD_OK;
+}
+
+athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field f)
+{
+    if (!ctx || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "damp_wiggles: bad argument");
+    if (ctx->L.d.km > 3072) return fail(ctx, ATHAD_ERR_UNSUPPORTED, "damp_wiggles: km > 3072");
+    // the RK4 stage buffer A is free between RK4 steps
+    launch_damp_wiggles(ctx->L.d, ctx->field[f], ctx->stA[0], ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "damp_wiggles");
     return ATHAD_OK;
 }
 

@@ -49,6 +49,7 @@ inline Layout make_layout(const athad_grid& g, int precision)
     b += 6 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose
     b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
     b += 256;                                                                         // counters
+    b += round_up((size_t)g.jm * sizeof(int), 256);                                   // polar passes
     if (precision == ATHAD_PRECISION_MIXED) {
         b += (size_t)kMixed32 * round_up(L.field_elems * sizeof(float), 256);
         b += round_up((size_t)g.im * g.jm * sizeof(GeoF), 256);
@@ -94,6 +95,7 @@ struct athad_ctx {
     double* row_sum = nullptr;
     double* row_cnt = nullptr;
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
+    int* polar_passes = nullptr;              // [jm] zonal filter passes per row
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
     double layer_height1 = 0;   // get_layer_height(1): the first layer's height, float-rounded
     std::vector<double> rad;

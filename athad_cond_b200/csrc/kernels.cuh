@@ -194,6 +194,15 @@ struct BcArgs {
     int set_dis_wall;
 };
 void launch_boundary_conditions(const BcArgs& a, cudaStream_t st);
+
+// Smoothing filters (k_filters.cu)
+struct FilterArgs {
+    Dims d;
+    double* field[3];           // u, v, w for the post-RK4 filters
+    const int* polar_passes;    // [jm] zonal passes per row
+};
+void launch_post_rk4_filters(const FilterArgs& a, cudaStream_t st);
+void launch_damp_wiggles(const Dims& d, double* f, double* scratch, cudaStream_t st);
 void launch_repitch(const Dims& d, const double* packed, double* dst, cudaStream_t st);
 
 }  // namespace athad

@@ -14,6 +14,8 @@
 //     Densities(m, water)       ThermoAtm(m).densities(water)                :567, 634, 1418
 //     BoundaryConditions(m)     BC_Atm(m).bcRadius(); TurbulenceAtm(m).apply_wall_bc();
 //                               BC_Atm(m).bcTheta(); BC_Atm(m).bcPhi()       :1439-1442
+//     PostRK4Filters(m)         the polar zonal and radial Shapiro filters   :1507-1520
+//     DampMoistWiggles(m)       AtomUtils::damp_wiggles of t, ice, c, cloud  :1225-1228
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -254,6 +256,23 @@ public:
 #undef ATHAD_BC_UP
 #undef ATHAD_BC_DOWN
 #undef ATHAD_BC_FIELDS
+    }
+
+    // the filters after the RK4 step (cAtmosphereModel.cpp:1507-1520), flat terrain
+    void PostRK4Filters(Model& m)
+    {
+        up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w);
+        check(ctx_, athad_post_rk4_filters(ctx_), "post_rk4_filters");
+        down(ATHAD_U, m.u); down(ATHAD_V, m.v); down(ATHAD_W, m.w);
+    }
+
+    // AtomUtils::damp_wiggles of t, ice, c, cloud (cAtmosphereModel.cpp:1225-1228)
+    void DampMoistWiggles(Model& m)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_ICE, m.ice); up(ATHAD_C, m.c); up(ATHAD_CLOUD, m.cloud);
+        const athad_field f[4] = {ATHAD_T, ATHAD_ICE, ATHAD_C, ATHAD_CLOUD};
+        for (int q = 0; q < 4; q++) check(ctx_, athad_damp_wiggles(ctx_, f[q]), "damp_wiggles");
+        down(ATHAD_T, m.t); down(ATHAD_ICE, m.ice); down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud);
     }
 
 private:

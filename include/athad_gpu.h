@@ -274,6 +274,16 @@ athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int32_t max_it
  * (TurbulenceAtm.h:109-147; reads the 2-D field ATHAD_2D_VEL_STAR), BC_Atm::bcTheta
  * (:750-796) and BC_Atm::bcPhi (:803-918), on the fields the context holds. */
 athad_status athad_boundary_conditions(athad_ctx* ctx);
+/* The filters after the RK4 step (cAtmosphereModel.cpp:1507-1520), flat terrain:
+ * AtomUtils::polar_zonal_filter of u, v, w (lib/Utils.cpp:542-611), radial_shapiro_filter
+ * of u (:831-873), radial_shapiro_filter_ho of v, w (:884-940); the orographic,
+ * steep-massif and coastal filters change nothing without land.  Grids with km > 3072 are
+ * rejected. */
+athad_status athad_post_rk4_filters(athad_ctx* ctx);
+/* AtomUtils::damp_wiggles(field, along i, j and k; strength 1, one pass), lib/Utils.cpp:
+ * 429-531: what the moist iteration applies to t, ice, c and cloud after the saturation
+ * adjustment (cAtmosphereModel.cpp:1225-1228).  Uses the RK4 stage buffers as scratch. */
+athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field field);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

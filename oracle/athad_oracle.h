@@ -116,6 +116,14 @@ int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, 
 void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* const* f,
                             double* const* f2);
 
+/* the filters after the RK4 step (cAtmosphereModel.cpp:1507-1520): polar zonal filter of
+ * u, v, w; radial Shapiro filter of u; 4th-order radial Shapiro filter of v, w (flat
+ * terrain) */
+void or_post_rk4_filters(int im, int jm, int km, const or_params* p, double* const* f);
+/* AtomUtils::damp_wiggles(field, along i, j, k), lib/Utils.cpp:429-531 */
+void or_damp_wiggles(int im, int jm, int km, double* field);
+int  or_polar_passes(int jm, int j, const double* sin_w);
+
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);
 

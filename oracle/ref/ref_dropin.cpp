@@ -47,6 +47,8 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 4: d.Densities(*m, false); break;
             case 5: d.Densities(*m, true); break;
             case 6: d.BoundaryConditions(*m); break;
+            case 7: d.PostRK4Filters(*m); break;
+            case 8: d.DampMoistWiggles(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

@@ -338,6 +338,40 @@ void ref_moist(void* p, int iter_n)
     MoistConvection(*m).run(iter_n);
 }
 void ref_store(void* p) { UtilsAtm(*(cAtmosphereModel*)p).storeIntermediateData3D(1.0); }
+// the filters after the RK4 step, cAtmosphereModel.cpp:1507-1520, in their order
+void ref_post_rk4_filters(void* p)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    AtomUtils::polar_zonal_filter(m->u, m->the.z, &m->i_topography, 30.0, 12, 3.0);
+    AtomUtils::polar_zonal_filter(m->v, m->the.z, &m->i_topography, 30.0, 12, 3.0);
+    AtomUtils::polar_zonal_filter(m->w, m->the.z, &m->i_topography, 30.0, 12, 3.0);
+    AtomUtils::orographic_shapiro_filter(m->u, m->i_topography, 2, 3, 3);
+    AtomUtils::orographic_shapiro_filter(m->v, m->i_topography, 2, 3, 3);
+    AtomUtils::orographic_shapiro_filter(m->w, m->i_topography, 2, 3, 3);
+    AtomUtils::radial_shapiro_filter(m->u, m->i_topography, 2, 1.0);
+    AtomUtils::radial_shapiro_filter_ho(m->v, m->i_topography, 2, 1.0);
+    AtomUtils::radial_shapiro_filter_ho(m->w, m->i_topography, 2, 1.0);
+    AtomUtils::orographic_radial_shapiro_filter(m->t, m->i_topography, 2, 10, 2);
+    AtomUtils::orographic_radial_shapiro_filter(m->c, m->i_topography, 2, 10, 2);
+    AtomUtils::orographic_radial_shapiro_filter(m->cloud, m->i_topography, 2, 10, 2);
+    AtomUtils::orographic_radial_shapiro_filter(m->ice, m->i_topography, 2, 10, 2);
+    AtomUtils::steep_massif_field_smoothing(m->u, m->i_topography, 6, 3, 30, 1);
+    AtomUtils::steep_massif_field_smoothing(m->v, m->i_topography, 6, 3, 30, 1);
+    AtomUtils::steep_massif_field_smoothing(m->w, m->i_topography, 6, 3, 30, 1);
+    AtomUtils::steep_massif_field_smoothing(m->p_dyn, m->i_topography, 6, 3, 30, 1);
+    AtomUtils::coastal_velocity_sponge(m->u, m->i_topography, 3.0, 1.0, 12);
+    AtomUtils::coastal_velocity_sponge(m->v, m->i_topography, 3.0, 1.0, 12);
+    AtomUtils::coastal_velocity_sponge(m->w, m->i_topography, 3.0, 1.0, 12);
+}
+// the moist iteration's damp_wiggles of one field (cAtmosphereModel.cpp:1225-1228)
+int ref_damp_wiggles(void* p, const char* name)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    Array* a = field3(m, name);
+    if (!a) return -1;
+    AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
+    return 0;
+}
 // the per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1442 (flat terrain:
 // bcScalarSurfSur and bcSolidGround change nothing and are left out)
 void ref_bc(void* p)

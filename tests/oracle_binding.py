@@ -154,3 +154,14 @@ class OracleState:
         F, F2, _ = self._args()
         im, jm, km = self.shape
         lib().or_boundary_conditions(im, jm, km, ctypes.byref(self.params), F, F2)
+
+    def post_rk4_filters(self):
+        """polar zonal filter of u, v, w; radial Shapiro filters (flat terrain)."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_post_rk4_filters(im, jm, km, ctypes.byref(self.params), F)
+
+    def damp_wiggles(self, name):
+        im, jm, km = self.shape
+        a = self.f[name]
+        lib().or_damp_wiggles(im, jm, km, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))

@@ -110,6 +110,12 @@ class Reference:
         if r != 0:
             raise RuntimeError(err.value.decode())
 
+    def post_rk4_filters(self):
+        self.lib.ref_post_rk4_filters(self.h)
+
+    def damp_wiggles(self, name):
+        assert self.lib.ref_damp_wiggles(self.h, name.encode()) == 0, name
+
     def bc(self):
         """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi."""
         self.lib.ref_bc(self.h)

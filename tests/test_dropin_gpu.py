@@ -5,7 +5,8 @@ results must match what the reference's own CPU call produces on the same state:
 
   * saturation adjustment, densities, moist convection, pressure sweep: 1e-10 relative
     (CUDA vs glibc transcendentals, mirror-symmetric trig tables);
-  * the boundary conditions: bit-identical (copies and short sums in the same order);
+  * the boundary conditions and the smoothing filters: bit-identical (copies and short
+    sums in the same order);
   * the RK4 step: the device integrates the four stages Jacobi-style where the reference
     updates cells in place, so the difference is bounded by a small fraction of the step's
     own change, with the reference's SST wall distance selected.
@@ -109,6 +110,32 @@ def test_dropin_boundary_conditions(model):
     pattern = 1.0 + 1e-3 * np.sin(np.arange(im * jm * km, dtype=np.float64) * 0.37).reshape(im, jm, km)
     moved = {n: a * pattern for n, a in snap.items()}
     out = run_both(R, moved, lambda: R.bc(), lambda: R.dropin(6), FIELD_NAMES)
+    reset(R, snap)
+    for n, (a, b) in out.items():
+        assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))
+
+
+def test_dropin_filters(model):
+    """The post-RK4 filters and the moist iteration's damp_wiggles through the adapter, on
+    the reference's state with grid-scale noise added: bit-identical to the reference's own
+    AtomUtils calls."""
+    R, snap = model
+    im, jm, km = R.shape
+    rng = np.random.default_rng(7)
+    noisy = dict(snap)
+    for n in ("u", "v", "w", "t", "c", "cloud", "ice"):
+        noisy[n] = snap[n] + 1e-3 * np.abs(snap[n]).max() * rng.standard_normal((im, jm, km))
+
+    def cpu():
+        R.post_rk4_filters()
+        for n in ("t", "ice", "c", "cloud"):
+            R.damp_wiggles(n)
+
+    def gpu():
+        R.dropin(7)
+        R.dropin(8)
+
+    out = run_both(R, noisy, cpu, gpu, ["u", "v", "w", "t", "c", "cloud", "ice"])
     reset(R, snap)
     for n, (a, b) in out.items():
         assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))

@@ -8,7 +8,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * RHS_Atmosphere_Turb at sampled cells;
   * solveRungeKutta_Atmosphere_Turb, the in-place sweep run with T OpenMP threads;
   * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes);
-  * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi).
+  * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
+  * the filters after the RK4 step and the moist iteration's damp_wiggles.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -160,3 +161,27 @@ def test_boundary_conditions_bit_exact(ref):
     R.bc()
     o.boundary_conditions()
     assert_identical(R, o, FIELD_NAMES)
+
+
+def test_post_rk4_filters_bit_exact(ref):
+    """The post-RK4 filter sequence of the reference (its orographic, steep-massif and
+    coastal filters included, which flat terrain leaves without effect) against the
+    oracle's polar zonal and radial Shapiro filters."""
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    rng = np.random.default_rng(31)
+    for n in ("u", "v", "w"):
+        a = R.get(n) + 1e-3 * rng.standard_normal((im, jm, km))
+        R.set(n, a)
+        o.f[n][...] = a
+    R.post_rk4_filters()
+    o.post_rk4_filters()
+    assert_identical(R, o, FIELD_NAMES)
+
+
+def test_damp_wiggles_bit_exact(ref):
+    R, o = fresh(ref)
+    for n in ("t", "ice", "c", "cloud"):
+        R.damp_wiggles(n)
+        o.damp_wiggles(n)
+    assert_identical(R, o, ["t", "ice", "c", "cloud"])
