@@ -203,8 +203,10 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
         const double sin_j = (sin_w[j] < 1.0e-6) ? 1.0e-6 : sin_w[j];
         if (sin_j >= sin_ref) continue;
         const double ratio = sin_ref / sin_j;
-        long pp = std::lround(3.0 * (ratio * ratio - 1.0));
-        polar[j] = (int)(pp < 0 ? 0 : pp > 12 ? 12 : pp);
+        // (int) of the long, as lib/Utils.cpp:566 converts it: on the pole rows (sin
+        // guarded to 1e-6) the count does not fit an int and wraps before the clamp
+        int pp = (int)std::lround(3.0 * (ratio * ratio - 1.0));
+        polar[j] = (pp < 0) ? 0 : (pp > 12) ? 12 : pp;
     }
     std::vector<GeoIJ> geo((size_t)im * jm);
     std::vector<PoiIJ> poi((size_t)im * jm);

@@ -33,13 +33,14 @@ namespace {
 
 constexpr int kMaxLevels = 16;
 #ifndef ATHAD_MG_NU
-#define ATHAD_MG_NU 1            // symmetric zebra sweeps before and after the coarse correction
+#define ATHAD_MG_NU 2            // symmetric zebra sweeps before and after the coarse correction
 #endif
 #ifndef ATHAD_MG_COARSE_SWEEPS
 #define ATHAD_MG_COARSE_SWEEPS 4 // symmetric sweeps on the coarsest level
 #endif
 #ifndef ATHAD_MG_CSCALE
-#define ATHAD_MG_CSCALE 1.0f     // scale of the prolongated coarse correction
+#define ATHAD_MG_CSCALE 1.7f     // scale of the prolongated coarse correction (61x361x721:
+                                 // 1.0 -> 86 CG iterations, 1.7 -> 44; with NU 2, 27)
 #endif
 
 template <typename T>
@@ -220,19 +221,26 @@ __global__ void __launch_bounds__(128) mg_sub_mean_kernel(int nk, int pitch, lon
 // column solved exactly with the horizontal neighbours fixed.  The seam neighbour of the
 // columns k = 0 and k = nk-1 is read from `seam` (the two seam planes before the
 // half-sweep), because with an odd nk both ends have the same colour.
+template <bool SMEM>
 __global__ void __launch_bounds__(128) mg_smooth_kernel(OpView<float> o, const float* __restrict__ tm,
                                                         const float* __restrict__ tc, const float* __restrict__ f,
                                                         float* __restrict__ e, const float* __restrict__ seam,
                                                         float* __restrict__ w, int colour)
 {
+    // SMEM: the thread's column (rhs, then the forward-elimination values) lives in shared
+    // memory, so the two sequential recurrences wait on shared-memory latency instead of
+    // global memory; column element i of thread t is col[i * blockDim.x + t]
+    extern __shared__ float col_smem[];
     const int j = blockIdx.y;
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((colour + j) & 1);
     if (k >= o.nk) return;
     const int kc = kclass(k, o.nk);
     const long long c0 = (long long)j * o.pitch + k;
+    float* col = col_smem + threadIdx.x;
+    const int cs = blockDim.x;
     // the column's right-hand side with the horizontal neighbours fixed: independent loads,
-    // stored in the scratch field w (a separate array, so the loads of e are not ordered
-    // behind these stores)
+    // stored in shared memory or the scratch field w (a separate array, so the loads of e
+    // are not ordered behind these stores)
 #pragma unroll 4
     for (int i = 0; i < o.ni; i++) {
         const long long c = i * o.plane + c0;
@@ -245,23 +253,26 @@ __global__ void __launch_bounds__(128) mg_smooth_kernel(OpView<float> o, const f
         if (k < o.nk - 1) s -= ckv * e[c + 1];
         if (k == 0) s -= o.cs[ij] * seam[(long long)(o.ni * o.nj) + ij];        // plane k = nk-1
         else if (k == o.nk - 1) s -= o.cs[ij] * seam[ij];                       // plane k = 0
-        w[c] = s;
+        if (SMEM) col[i * cs] = s;
+        else w[c] = s;
     }
     // forward elimination: y_i = (rhs_i - ci_{i-1} y_{i-1}) m_i
     float y_prev = 0.0f;
     for (int i = 0; i < o.ni; i++) {
         const long long c = i * o.plane + c0;
         const int ij = i * o.nj + j;
-        float s = w[c];
+        float s = SMEM ? col[i * cs] : w[c];
         if (i > 0) s -= o.ci[(ij - o.nj) * 3 + kc] * y_prev;
         y_prev = s * tm[ij * 3 + kc];
-        e[c] = y_prev;
+        if (SMEM) col[i * cs] = y_prev;
+        else e[c] = y_prev;
     }
     // back substitution: x_i = y_i - c'_i x_{i+1}
     float x_next = y_prev;
+    if (SMEM) e[(o.ni - 1) * o.plane + c0] = x_next;
     for (int i = o.ni - 2; i >= 0; i--) {
         const long long c = i * o.plane + c0;
-        x_next = e[c] - tc[(i * o.nj + j) * 3 + kc] * x_next;
+        x_next = (SMEM ? col[i * cs] : e[c]) - tc[(i * o.nj + j) * 3 + kc] * x_next;
         e[c] = x_next;
     }
 }
@@ -578,7 +589,13 @@ void smooth(const MGLevel& L, float* seam, int colour, cudaStream_t st)
 {
     mg_seam_copy_kernel<<<(L.ni * L.nj + 255) / 256, 256, 0, st>>>(L.ni, L.nj, L.nk, L.pitch, L.plane, L.e, seam);
     const int half = (L.nk + 1) / 2;
-    mg_smooth_kernel<<<dim3((half + 127) / 128, L.nj), 128, 0, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam, L.r, colour);
+    const size_t smem = (size_t)128 * L.ni * sizeof(float);
+    if (smem <= 48 * 1024)   // columns of up to 96 levels in shared memory
+        mg_smooth_kernel<true><<<dim3((half + 127) / 128, L.nj), 128, smem, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
+                                                                              L.r, colour);
+    else
+        mg_smooth_kernel<false><<<dim3((half + 127) / 128, L.nj), 128, 0, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
+                                                                             L.r, colour);
 }
 
 // one V-cycle on level l: L[l].e ~= S_l^-1 L[l].f, starting from zero

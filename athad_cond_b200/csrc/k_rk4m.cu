@@ -407,10 +407,10 @@ __device__ __forceinline__ void rk4m_cell(const RK4MArgs& a, int i, int j, int k
 #endif
 
 #ifndef ATHAD_RK4M_BX
-#define ATHAD_RK4M_BX 32         // CTA: BX longitudes x BY rows of one level
-#endif
+#define ATHAD_RK4M_BX 128        // CTA: BX longitudes x BY rows of one level (128 x 1 was 1 %
+#endif                           // faster than 32 x 4, 64 x 2, 64 x 4, 32 x 8 at 41x181x361)
 #ifndef ATHAD_RK4M_BY
-#define ATHAD_RK4M_BY 4
+#define ATHAD_RK4M_BY 1
 #endif
 
 template <int STAGE>

@@ -48,9 +48,9 @@ E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", 
 RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62), 1: 8 + 472 + 264 + 264 + 332}
 # fields compared between the two forms after the timed iterations: the 11 prognostics and
 # the diagnosed pressure and densities
-# DRAM bytes (read + write) of one RK4 step measured by ncu, per form and grid: None until
-# a capture of all four stages exists for that build
-RK4_TRAFFIC = {}
+# DRAM bytes (read + write) of one RK4 step (its four stage launches) measured by ncu
+# (profiles/rk4_stage_41x181x361.md): per form and grid
+RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.510e9, ("mixed", (41, 181, 361)): 4.260e9}
 ERR_FIELDS = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
               "p_dyn", "p_stat", "r_humid"]
 

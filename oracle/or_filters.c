@@ -33,6 +33,8 @@ int or_polar_passes(int jm, int j, const double* sin_w)
     const double sin_j = or_max(sin_w[j], 1.0e-6);
     if (sin_j >= sin_ref) return 0;
     const double ratio = sin_ref / sin_j;
+    /* (int) of the long, as the reference converts it: on the pole rows (sin guarded to
+     * 1e-6) the count overflows an int and wraps before the clamp */
     int p = (int)lround(3.0 * (ratio * ratio - 1.0));
     if (p < 0) p = 0;
     if (p > 12) p = 12;
