@@ -143,9 +143,12 @@ class GpuAtmosphere:
         self._check(self.lib.athad_level_mean(self._h))
 
     def solveRungeKutta_Atmosphere_Turb(self, dt: float, diffusion_ramp: float = 1.0,
-                                        buoyancy_ramp: float = 1.0, write_diagnostics: bool = False):
-        """RungeKutta_Atm_Turb.cpp:44-273 (call site cAtmosphereModel.cpp:1509)."""
-        s = _abi.StepScalars(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0, 0)
+                                        buoyancy_ramp: float = 1.0, write_diagnostics: bool = False,
+                                        store_n_level: bool = False):
+        """RungeKutta_Atm_Turb.cpp:44-273 (call site cAtmosphereModel.cpp:1509); with
+        store_n_level the following storeIntermediateData3D is fused into the last stage."""
+        s = _abi.StepScalars(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0,
+                             1 if store_n_level else 0)
         self._check(self.lib.athad_rk4_step(self._h, ctypes.byref(s)))
 
     def PressureSolverAtm_run(self, total_iter_count: int, n_sweeps: int = 1):
@@ -164,6 +167,10 @@ class GpuAtmosphere:
     def damp_wiggles(self, name: str):
         """AtomUtils::damp_wiggles(field, i, j, k) (lib/Utils.cpp:429-531)."""
         self._check(self.lib.athad_damp_wiggles(self._h, FIELD[name]))
+
+    def turbulence_run(self):
+        """TurbulenceAtm::run (TurbulenceAtm.h:62-79; call site cAtmosphereModel.cpp:1426)."""
+        self._check(self.lib.athad_turbulence_run(self._h))
 
     def pressure_solve(self, rel_tol: float = 1e-10, max_iter: int = 200) -> dict:
         """The sweep's pressure equation solved to a relative residual (athad_pressure_solve)."""

@@ -4,6 +4,7 @@
 // All device memory of a context is one allocation made at creation (fields, RK4 stage
 // buffers, the Poisson source, geometry tables, counters), so the hot path allocates
 // nothing and a context's HBM footprint is known before it is created.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -39,6 +40,7 @@ void athad_default_params(athad_params* p)
     p->sc_CO2 = 0.96; p->r_Earth = 6370.001; p->p_0 = 60000.0; p->t_00 = 236.15;
     p->t_max_phys = 2000.0; p->cloud_cap = 0.05; p->t_skin = 254.0; p->c_h2o_dry_top = 0.00423;
     p->co2_0 = 0.6233; p->s_0 = 274515.75; p->R_Air = 296.8; p->R_WaterVapour = 461.5;
+    p->abl_height = 10000.0;
     const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
     const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
     const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
@@ -74,7 +76,10 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     *out = nullptr;
     if (!grid || !params) return ATHAD_ERR_INVALID;
     if (params->struct_size != sizeof(athad_params)) return ATHAD_ERR_INVALID;
-    if (grid->im < 4 || grid->jm < 5 || grid->km < 5 || grid->im > 1024) return ATHAD_ERR_INVALID;
+    // im <= 1024 (per-level profiles), jm <= 6144 (the level mean stages a level's row sums
+    // in shared memory)
+    if (grid->im < 4 || grid->jm < 5 || grid->km < 5 || grid->im > 1024 || grid->jm > 6144)
+        return ATHAD_ERR_INVALID;
     if (params->turb_model < ATHAD_TURB_K_EPSILON || params->turb_model > ATHAD_TURB_K_OMEGA_SST)
         return ATHAD_ERR_UNSUPPORTED;
     if (params->precision != ATHAD_PRECISION_FP64 && params->precision != ATHAD_PRECISION_MIXED)
@@ -127,6 +132,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->counters = (unsigned long long*)take(256);
     c->polar_passes = (int*)take((size_t)jm * sizeof(int));
+    c->turb_lev = (TurbLevel*)take((size_t)im * sizeof(TurbLevel));
     if (params->precision == ATHAD_PRECISION_MIXED) {
         const size_t fb = L.field_elems * sizeof(float);
         for (int n = 0; n < kNY; n++) c->mA[n] = (float*)take(fb);
@@ -208,6 +214,23 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
         int pp = (int)std::lround(3.0 * (ratio * ratio - 1.0));
         polar[j] = (pp < 0) ? 0 : (pp > 12) ? 12 : pp;
     }
+    // TurbulenceAtm's per-level constants; clamp_nue's taper (TurbulenceAtm.h:271-295): the
+    // eddy viscosity fades to zero over the grid layer that straddles abl_height
+    std::vector<TurbLevel> tlev(im);
+    {
+        int i_abl = 0;
+        while (i_abl < im - 1 && height[i_abl] <= params->abl_height) i_abl++;
+        const double taper_dz = std::max(1.0, height[std::min(i_abl, im - 1)] - height[std::max(i_abl - 1, 0)]);
+        for (int i = 0; i < im; i++) {
+            TurbLevel& T = tlev[i];
+            T.rm = rad[i];
+            T.exp_rm = 1.0 / (rad[i] + 1.0);
+            T.rmet = rmet_of(rad[i]);
+            T.height = height[i];
+            const double z_agl = height[i] - height[0];
+            T.nue_fac = std::clamp((params->abl_height + taper_dz - z_agl) / taper_dz, 0.0, 1.0);
+        }
+    }
     std::vector<GeoIJ> geo((size_t)im * jm);
     std::vector<PoiIJ> poi((size_t)im * jm);
     const double inv_dr2 = 1.0 / (c->dr * c->dr), inv_dthe2 = 1.0 / (c->dthe * c->dthe),
@@ -253,6 +276,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->step_mc, step_mc.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "step_mc");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->cose, cose.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "cose");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->polar_passes, polar.data(), jm * sizeof(int), cudaMemcpyHostToDevice, c->stream), "polar passes");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->turb_lev, tlev.data(), im * sizeof(TurbLevel), cudaMemcpyHostToDevice, c->stream), "turbulence levels");
     std::vector<GeoF> geof;
     if (s == ATHAD_OK && c->geof) {   // FP32 factors rounded from the FP64 ones (mirror-exact)
         geof.resize(geo.size());
@@ -414,7 +438,8 @@ athad_status athad_store_n_level(athad_ctx* ctx)
 athad_status athad_level_mean(athad_ctx* ctx)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
-    launch_level_mean(ctx->L.d, ctx->field[ATHAD_T], ctx->sin_w, ctx->prof[ATHAD_PROF_T_REF_LEVEL], ctx->stream);
+    launch_level_mean(ctx->L.d, ctx->field[ATHAD_T], ctx->sin_w, ctx->prof[ATHAD_PROF_T_REF_LEVEL], ctx->row_sum,
+                      ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "level_mean");
     return ATHAD_OK;
 }
@@ -469,6 +494,8 @@ athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
     a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
     a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
     a.write_diag = s->write_diagnostics;
+    a.store_n = s->store_n_level ? 1 : 0;
+    for (int n = 0; n < kNY; n++) a.Yn_store[n] = ctx->field[ATHAD_TN + n];
     for (int stage = 1; stage <= 4; stage++) {
         for (int n = 0; n < kNY; n++) {
             double* cur = ctx->field[ATHAD_T + n];
@@ -536,6 +563,8 @@ void athad::mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a)
     a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
     a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
     a.write_diag = s->write_diagnostics;
+    a.store_n = s->store_n_level ? 1 : 0;
+    for (int n = 0; n < kNY; n++) a.Yn_store[n] = ctx->field[ATHAD_TN + n];
 }
 
 extern "C" {
@@ -745,6 +774,31 @@ athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field f)
     // the RK4 stage buffer A is free between RK4 steps
     launch_damp_wiggles(ctx->L.d, ctx->field[f], ctx->stA[0], ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "damp_wiggles");
+    return ATHAD_OK;
+}
+
+athad_status athad_turbulence_run(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    const athad_params& p = ctx->p;
+    TurbArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    double** F = ctx->field;
+    a.u = F[ATHAD_U]; a.v = F[ATHAD_V]; a.w = F[ATHAD_W];
+    a.tke = F[ATHAD_TKE]; a.dis = F[ATHAD_DIS]; a.prod = F[ATHAD_PROD]; a.nue = F[ATHAD_NUE];
+    a.tke_source = F[ATHAD_TKE_SOURCE]; a.dis_source = F[ATHAD_DIS_SOURCE];
+    a.vel_star = ctx->f2d[ATHAD_2D_VEL_STAR];
+    a.sin_w = ctx->sin_w;
+    a.lev = ctx->turb_lev;
+    a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_2dthe = 1.0 / (2.0 * ctx->dthe); a.inv_2dphi = 1.0 / (2.0 * ctx->dphi);
+    a.dr = ctx->dr; a.dthe = ctx->dthe; a.dphi = ctx->dphi;
+    a.u_0 = p.u_0; a.L_atm = p.L_atm; a.re_turb = p.re_turb;
+    a.nue_max = 1000.0 / (p.u_0 * p.L_atm);    // TurbulenceAtm.h:272, :454
+    a.y_mount = 0.0;                             // get_layer_height(0) of flat terrain
+    a.turb_model = p.turb_model;
+    launch_turbulence_run(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "turbulence_run");
     return ATHAD_OK;
 }
 

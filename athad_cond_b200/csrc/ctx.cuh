@@ -50,6 +50,7 @@ inline Layout make_layout(const athad_grid& g, int precision)
     b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
     b += 256;                                                                         // counters
     b += round_up((size_t)g.jm * sizeof(int), 256);                                   // polar passes
+    b += round_up((size_t)g.im * sizeof(TurbLevel), 256);                             // turbulence levels
     if (precision == ATHAD_PRECISION_MIXED) {
         b += (size_t)kMixed32 * round_up(L.field_elems * sizeof(float), 256);
         b += round_up((size_t)g.im * g.jm * sizeof(GeoF), 256);
@@ -96,6 +97,7 @@ struct athad_ctx {
     double* row_cnt = nullptr;
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
     int* polar_passes = nullptr;              // [jm] zonal filter passes per row
+    TurbLevel* turb_lev = nullptr;            // [im] TurbulenceAtm per-level constants
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
     double layer_height1 = 0;   // get_layer_height(1): the first layer's height, float-rounded
     std::vector<double> rad;

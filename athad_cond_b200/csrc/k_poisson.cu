@@ -62,12 +62,22 @@ __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
         else if (div_src < -src_max) { div_src = -src_max; clamped = true; }
         a.src[c] = div_src;
     }
-    // warp-aggregated counters
+    // counters aggregated per CTA: one global atomic per counter and CTA instead of one
+    // per warp, which would serialise on the two addresses
+    __shared__ unsigned cnt[2];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid < 2) cnt[tid] = 0u;
+    __syncthreads();
     const unsigned nf = __popc(__ballot_sync(0xffffffffu, fluid));
     const unsigned nc = __popc(__ballot_sync(0xffffffffu, clamped));
-    if ((threadIdx.x & 31) == 0 && a.counters) {
-        if (nf) atomicAdd(a.counters + 0, (unsigned long long)nf);
-        if (nc) atomicAdd(a.counters + 1, (unsigned long long)nc);
+    if ((tid & 31) == 0) {
+        if (nf) atomicAdd(&cnt[0], nf);
+        if (nc) atomicAdd(&cnt[1], nc);
+    }
+    __syncthreads();
+    if (tid == 0 && a.counters) {
+        if (cnt[0]) atomicAdd(a.counters + 0, (unsigned long long)cnt[0]);
+        if (cnt[1]) atomicAdd(a.counters + 1, (unsigned long long)cnt[1]);
     }
 }
 

@@ -20,43 +20,52 @@
 namespace athad {
 
 // ---------------------------------------------------------------------------------------
-// computeLevelMeanTemperature (RungeKutta_Atm_Turb.cpp:24-41).  One CTA per level i.  Each
-// row sum is a 32-lane strided partial sum reduced by xor butterfly; rows j and jm-1-j are
-// added before weighting, so the mean of a mirrored field is identical.
-__global__ void __launch_bounds__(256) level_mean_kernel(Dims d, const double* __restrict__ t,
-                                                         const double* __restrict__ sin_w,
-                                                         double* __restrict__ out)
+// computeLevelMeanTemperature (RungeKutta_Atm_Turb.cpp:24-41).  Row sums first, one warp
+// per (i, j) row over all SMs: a 32-lane strided partial sum reduced by xor butterfly; then
+// one CTA per level stages its row sums in shared memory (jm <= 6144) and one thread adds
+// rows j and jm-1-j before weighting, so the mean of a mirrored field is identical.
+__global__ void __launch_bounds__(256) level_rows_kernel(Dims d, const double* __restrict__ t,
+                                                         double* __restrict__ rows)
 {
-    extern __shared__ double rows[];   // [jm]
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= d.im * d.jm) return;
+    const double* r = t + (long long)row * d.pitch;
+    double s = 0.0;
+    for (int k = lane; k < d.km; k += 32) s += __ldg(r + k);
+    for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) rows[row] = s;
+}
+
+__global__ void __launch_bounds__(128) level_combine_kernel(Dims d, const double* __restrict__ rows,
+                                                            const double* __restrict__ sin_w,
+                                                            double* __restrict__ out)
+{
+    extern __shared__ double r[];   // [jm] row sums of level i
     const int i = blockIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int j = warp; j < d.jm; j += nwarp) {
-        const double* row = t + idx3(d, i, j, 0);
-        double s = 0.0;
-        for (int k = lane; k < d.km; k += 32) s += __ldg(row + k);
-        for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
-        if (lane == 0) rows[j] = s;
-    }
+    for (int j = threadIdx.x; j < d.jm; j += blockDim.x) r[j] = rows[(long long)i * d.jm + j];
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double sum = 0.0, wsum = 0.0;
-        const int half = d.jm / 2;
-        for (int j = 0; j < half; j++) {
-            sum += sin_w[j] * (rows[j] + rows[d.jm - 1 - j]);
-            wsum += 2.0 * sin_w[j] * (double)d.km;
-        }
-        if (d.jm & 1) {
-            sum += sin_w[half] * rows[half];
-            wsum += sin_w[half] * (double)d.km;
-        }
-        out[i] = (wsum > 0.0) ? sum / wsum : 1.0;
+    if (threadIdx.x != 0) return;
+    const double* __restrict__ sin_w_s = sin_w;
+    double sum = 0.0, wsum = 0.0;
+    const int half = d.jm / 2;
+    for (int j = 0; j < half; j++) {
+        sum += sin_w_s[j] * (r[j] + r[d.jm - 1 - j]);
+        wsum += 2.0 * sin_w_s[j] * (double)d.km;
     }
+    if (d.jm & 1) {
+        sum += sin_w_s[half] * r[half];
+        wsum += sin_w_s[half] * (double)d.km;
+    }
+    out[i] = (wsum > 0.0) ? sum / wsum : 1.0;
 }
 
 void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
-                       cudaStream_t st)
+                       double* row_sum, cudaStream_t st)
 {
-    level_mean_kernel<<<d.im, 256, sizeof(double) * d.jm, st>>>(d, t, sin_w, out);
+    const int rows = d.im * d.jm;
+    level_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(d, t, row_sum);
+    level_combine_kernel<<<d.im, 128, d.jm * sizeof(double), st>>>(d, row_sum, sin_w, out);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -117,6 +126,7 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
     else if (n == 10) out = smax(1.0e-10, y);
     else out = y;
     a.Yout[n][c] = out;
+    if (STAGE == 4 && a.store_n) a.Yn_store[n][c] = out;   // storeIntermediateData3D fused
 }
 
 // One RK4 stage.  The right-hand side is evaluated in the order that keeps the fewest
@@ -155,6 +165,10 @@ rk4_stage_kernel(const RK4Args a)
                 a.Yout[n][c] = v;
                 a.Ybnd[n][c] = v;
             }
+        }
+        if (STAGE == 4 && a.store_n) {   // the time-level copy of the cells RK4 leaves alone
+#pragma unroll
+            for (int n = 0; n < 11; n++) a.Yn_store[n][c] = a.Yout[n][c];
         }
         return;
     }

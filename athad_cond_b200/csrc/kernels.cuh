@@ -17,6 +17,7 @@ struct RK4Args {
     const double* Yn[11];      // time level n
     double*       K[11];       // RK4 accumulator k1 + 2 k2 + 2 k3
     double*       Ybnd[11];    // stage 1 only: second stage buffer that receives the boundary
+    double*       Yn_store[11];    // store_n: stage 4 also writes the new time level n here
     const double* p_dyn;
     const double* nue;
     const double* t_eq;
@@ -38,10 +39,11 @@ struct RK4Args {
     // prefactor (1/86400)*L_atm/u_0*dt
     double inv_re, nue_max, nue_air_nd, diff_prec_re_inv, diff_co2_re_inv, buoy_pref, drag_pref;
     int turb_model, wall_mode, nontrad, curvature, tracer_diff_flux, write_diag;
+    int store_n;               // fuse storeIntermediateData3D into stage 4
 };
 
 void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
-                       cudaStream_t st);
+                       double* row_sum, cudaStream_t st);
 void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st);
 
 // Mixed-precision RK4 step (k_rk4m.cu).  FP32 geometry factors (rounded from GeoIJ, so
@@ -204,5 +206,24 @@ struct FilterArgs {
 void launch_post_rk4_filters(const FilterArgs& a, cudaStream_t st);
 void launch_damp_wiggles(const Dims& d, double* f, double* scratch, cudaStream_t st);
 void launch_repitch(const Dims& d, const double* packed, double* dst, cudaStream_t st);
+
+// TurbulenceAtm::run (k_turb.cu).  Per-level constants built on the host as the reference
+// forms them: rad.z, 1/(rm+1), metricRadius(rm), get_layer_height(i), and clamp_nue's
+// taper factor of the eddy viscosity above abl_height.
+struct TurbLevel {
+    double rm, exp_rm, rmet, height, nue_fac;
+};
+struct TurbArgs {
+    Dims d;
+    const double* u; const double* v; const double* w;
+    double* tke; double* dis; double* prod; double* nue; double* tke_source; double* dis_source;
+    double* vel_star;           // 2-D, jm rows of pitch
+    const double* sin_w;        // sin(theta), mirror-exact
+    const TurbLevel* lev;       // [im]
+    double inv_2dr, inv_2dthe, inv_2dphi, dr, dthe, dphi;
+    double u_0, L_atm, re_turb, nue_max, y_mount;
+    int turb_model;
+};
+void launch_turbulence_run(const TurbArgs& a, cudaStream_t st);
 
 }  // namespace athad

@@ -16,6 +16,7 @@
 //                               BC_Atm(m).bcTheta(); BC_Atm(m).bcPhi()       :1439-1442
 //     PostRK4Filters(m)         the polar zonal and radial Shapiro filters   :1507-1520
 //     DampMoistWiggles(m)       AtomUtils::damp_wiggles of t, ice, c, cloud  :1225-1228
+//     TurbulenceRun(m)          TurbulenceAtm(m).run()                       :614, 1426
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -64,6 +65,7 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.cloud_cap = m.cloud_cap; p.t_skin = m.t_skin; p.c_h2o_dry_top = m.c_h2o_dry_top;
     p.co2_0 = m.co2_0; p.s_0 = m.s_0; p.R_Air = m.R_Air; p.R_WaterVapour = m.R_WaterVapour;
     p.M_bg = m.m_comp.M_bg; p.R_bg = m.m_comp.R_bg; p.R_mix = m.m_comp.R_mix;
+    p.abl_height = m.abl_height;
     return p;
 }
 
@@ -111,6 +113,14 @@ public:
             for (int k = 0; k < km_; k++) b[(size_t)j * km_ + k] = a.y[j][k];
         check(ctx_, athad_upload_2d(ctx_, f, b.data(), b.size()), "upload_2d");
         check(ctx_, athad_synchronize(ctx_), "upload sync");
+    }
+    template <class Arr2>
+    void down2(athad_field2d f, Arr2& a)
+    {
+        std::vector<double> b((size_t)jm_ * km_);
+        check(ctx_, athad_download_2d(ctx_, f, b.data(), b.size()), "download_2d");
+        for (int j = 0; j < jm_; j++)
+            for (int k = 0; k < km_; k++) a.y[j][k] = b[(size_t)j * km_ + k];
     }
     void down_profile(athad_profile f, std::vector<double>& v)
     {
@@ -273,6 +283,19 @@ public:
         const athad_field f[4] = {ATHAD_T, ATHAD_ICE, ATHAD_C, ATHAD_CLOUD};
         for (int q = 0; q < 4; q++) check(ctx_, athad_damp_wiggles(ctx_, f[q]), "damp_wiggles");
         down(ATHAD_T, m.t); down(ATHAD_ICE, m.ice); down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud);
+    }
+
+    // TurbulenceAtm(m).run() (cAtmosphereModel.cpp:614, 1426), flat terrain.  The closure is
+    // the one the context was created with (athad_params.turb_model from m.turb_model).
+    void TurbulenceRun(Model& m)
+    {
+        up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w);
+        up(ATHAD_TKE, m.tke); up(ATHAD_DIS, m.dis); up(ATHAD_NUE, m.nue);
+        check(ctx_, athad_turbulence_run(ctx_), "turbulence_run");
+        down(ATHAD_TKE, m.tke); down(ATHAD_DIS, m.dis); down(ATHAD_NUE, m.nue);
+        down(ATHAD_PROD, m.prod); down(ATHAD_TKE_SOURCE, m.tke_source);
+        down(ATHAD_DIS_SOURCE, m.dis_source);
+        down2(ATHAD_2D_VEL_STAR, m.vel_star);
     }
 
 private:

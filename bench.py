@@ -4,7 +4,8 @@
 One step = one model iteration of cAtmosphereModel::run_3D_loop restricted to the hot path,
 at the reference cadence (cAtmosphereModel.cpp:1156-1509): the RK4 step every iteration, one
 pressure-Poisson sweep every 4th, saturation adjustment, moist convection and the column
-densities every 2nd, and the time-level copy (storeIntermediateData3D) that closes it.
+densities every 2nd, and the time-level copy (storeIntermediateData3D) that closes it,
+written by the last RK4 stage (athad_step_scalars.store_n_level: nothing runs in between).
 Metric: grid-point RK4 steps per second = im*jm*km * steps / time.
 
 Workload: the 41 x 181 x 361 grid, 1000 iterations, run twice from the same seeded
@@ -41,16 +42,17 @@ GRID = (41, 181, 361)
 E2E_UP = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "nue",
           "S_c", "S_r", "S_i", "S_s", "S_g", "S_v", "t_eq"]
 E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", "p_dyn"]
-# algorithmic bytes moved per grid point by one RK4 step.  FP64 form: 262 fields of 8 B
-# (level mean 1 read; stage 1: 37 reads + 22 writes; stages 2-3: 48 + 22; stage 4: 48 + 14).
-# Mixed form: level mean 8 B, stage 1 296 B read + 176 B written, stages 2-3 176 + 88 B,
-# stage 4 220 + 112 B (the field lists of k_rk4m.cu) = 1340 B.
-RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62), 1: 8 + 472 + 264 + 264 + 332}
+# algorithmic bytes moved per grid point by one RK4 step with the time-level copy fused into
+# stage 4.  FP64 form: 273 fields of 8 B (level mean 1 read; stage 1: 37 reads + 22 writes;
+# stages 2-3: 48 + 22; stage 4: 48 + 14 + the 11 time-level writes).  Mixed form: level mean
+# 8 B, stage 1 296 B read + 176 B written, stages 2-3 176 + 88 B, stage 4 220 + 200 B (the
+# field lists of k_rk4m.cu) = 1428 B.
+RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62 + 11), 1: 8 + 472 + 264 + 264 + 332 + 88}
+# DRAM bytes (read + write) of one RK4 step (level mean and the four stage launches, the
+# time-level copy fused) measured by ncu (profiles/rk4_stage_41x181x361.md): per form, grid
+RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.883e9, ("mixed", (41, 181, 361)): 4.566e9}
 # fields compared between the two forms after the timed iterations: the 11 prognostics and
 # the diagnosed pressure and densities
-# DRAM bytes (read + write) of one RK4 step (its four stage launches) measured by ncu
-# (profiles/rk4_stage_41x181x361.md): per form and grid
-RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.510e9, ("mixed", (41, 181, 361)): 4.260e9}
 ERR_FIELDS = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
               "p_dyn", "p_stat", "r_humid"]
 
@@ -63,8 +65,7 @@ def iteration(g, it: int, dt: float):
         g.SaturationAdjustment_run()
         g.MoistConvection_run(it)
         g.densities()
-    g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0))
-    g.storeIntermediateData3D()
+    g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0), store_n_level=True)
 
 
 class ClockSampler:
@@ -301,10 +302,9 @@ def run_form(args, rank, world, device, precision):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0))
+            g.solveRungeKutta_Atmosphere_Turb(dt, 1.0, min(1.0, it / 300.0), store_n_level=True)
             b.record(stream)
             rk_ev.append((a, b))
-            g.storeIntermediateData3D()
         ev1.record(stream)
         stream.synchronize()
     torch.cuda.synchronize(device)
@@ -626,9 +626,9 @@ def main():
     r = runs[head_name]
     peak, peak_kind = measured_peaks()
     # kernel launches per step of our own kernels, averaged over the cadence cycle:
-    # RK4 = level mean + 4 stages; pressure = aux BC + source + 2 colours + 3 BCs + ceiling;
-    # saturation adjustment 1; moist convection 1; densities 3
-    launches = args.steps * 5 + (args.steps // 4) * 8 + (args.steps // 2) * 5
+    # RK4 = level mean (row sums + combine) + 4 stages; pressure = aux BC + source + 2 colours
+    # + 3 BCs + ceiling; saturation adjustment 1; moist convection 1; densities 3
+    launches = args.steps * 6 + (args.steps // 4) * 8 + (args.steps // 2) * 5
     summary = {}
     for f, rr in runs.items():
         summary[f] = {"value": rr["value"], "ms_per_step": rr["ms_per_step"], "rk4_ms": rr["rk4_ms"],
@@ -659,7 +659,8 @@ def main():
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": peak, "unit": "GB/s",
                      "frac": r["achieved"] / peak, "traffic": RK4_TRAFFIC.get((head_name, GRID)),
-                     "kernel": f"{head_name} rk4 step (level mean + 4 stage launches), "
+                     "kernel": f"{head_name} rk4 step (level mean + 4 stage launches, the "
+                               "time-level copy fused into stage 4), "
                                f"{r['rk4_bytes_per_point']} algorithmic B per grid point",
                      "peak_source": peak_kind},
         "forms": summary,

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 2
+#define ATHAD_ABI_VERSION 3
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -108,6 +108,8 @@ typedef struct athad_params {
     /* composition resolved from the configured mole fractions, AtmMixture::resolve
      * (MixtureAtm.h:82-109), i.e. cAtmosphereModel::m_comp */
     double M_bg, R_bg, R_mix;
+    double abl_height;           /* XML abl_height [m], 10000 (cli/config_cond.xml:76):
+                                  * the eddy-viscosity ceiling of TurbulenceAtm::clamp_nue */
 } athad_params;
 
 /* 3-D fields, one per cAtmosphereModel Array member of the same name. */
@@ -166,7 +168,10 @@ typedef struct athad_step_scalars {
     double diffusion_ramp;   /* diffusion_ramp in [0,1]                                */
     double buoyancy_ramp;    /* min(1, total_iter_count / 300)                         */
     int32_t write_diagnostics; /* 1: store prod/tke_source/dis_source of stage 4       */
-    int32_t pad0;
+    int32_t store_n_level;   /* 1: storeIntermediateData3D (UtilsAtm.h:25-49) fused into
+                              * the last stage: the caller runs nothing between the RK4
+                              * step and the time-level copy (no counterpart in the
+                              * reference, which copies in a separate pass) */
 } athad_step_scalars;
 
 /* Counters a call leaves behind (read with athad_get_report). */
@@ -187,7 +192,8 @@ void athad_default_params(athad_params* p);
 int32_t athad_abi_version(void);
 size_t athad_params_size(void);
 
-/* Create a context on the current CUDA device; allocates every field once. */
+/* Create a context on the current CUDA device; allocates every field once.  Grids:
+ * 4 <= im <= 1024, 5 <= jm <= 6144, km >= 5 (ATHAD_ERR_INVALID otherwise). */
 athad_status athad_create(const athad_grid* grid, const athad_params* params, athad_ctx** out);
 athad_status athad_destroy(athad_ctx* ctx);
 const char*  athad_last_error(const athad_ctx* ctx);
@@ -284,6 +290,13 @@ athad_status athad_post_rk4_filters(athad_ctx* ctx);
  * 429-531: what the moist iteration applies to t, ice, c and cloud after the saturation
  * adjustment (cAtmosphereModel.cpp:1225-1228).  Uses the RK4 stage buffers as scratch. */
 athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field field);
+/* TurbulenceAtm(*this).run() (TurbulenceAtm.h:62-79; call sites cAtmosphereModel.cpp:614, 1426),
+ * flat terrain: compute_vel_star into ATHAD_2D_VEL_STAR, compute_sources with the
+ * configured closure (prod, nue, tke_source, dis_source; the floors of tke and dis) and
+ * clamp_nue (the eddy-viscosity ceiling athad_params.abl_height).  Every cell reads the
+ * state before the call: the reference's in-place sweep lets a cell see the floored tke/dis
+ * of the neighbours visited before it, which differs only where a floor binds there. */
+athad_status athad_turbulence_run(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

@@ -42,6 +42,7 @@ typedef struct or_params {
     double r_Earth, p_0, t_00, t_max_phys, cloud_cap, t_skin, c_h2o_dry_top, co2_0, s_0;
     double R_Air, R_WaterVapour;
     double M_bg, R_bg, R_mix;
+    double abl_height;
 } or_params;
 
 typedef struct or_step {
@@ -123,6 +124,14 @@ void or_post_rk4_filters(int im, int jm, int km, const or_params* p, double* con
 /* AtomUtils::damp_wiggles(field, along i, j, k), lib/Utils.cpp:429-531 */
 void or_damp_wiggles(int im, int jm, int km, double* field);
 int  or_polar_passes(int jm, int j, const double* sin_w);
+
+/* TurbulenceAtm::run, TurbulenceAtm.h:62-79 (compute_vel_star, compute_sources with the
+ * k-epsilon, k-omega or k-omega SST closure, clamp_nue), flat terrain.  compat = 1: the
+ * reference's serial in-place sweep (j, k, i loops; a cell reads the floored tke/dis of the
+ * neighbours processed before it); compat = 0: every cell reads the values before the call
+ * (the device form). */
+void or_turbulence_run(int im, int jm, int km, const or_params* p, int compat,
+                       double* const* f, double* const* f2);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

@@ -382,6 +382,10 @@ void ref_bc(void* p)
     BC_Atm(*m).bcTheta();
     BC_Atm(*m).bcPhi();
 }
+// TurbulenceAtm::run, the moist iteration's call (cAtmosphereModel.cpp:1426); the closure
+// is the model's turb_model string, which TurbulenceAtm parses on construction
+void ref_turbulence_run(void* p) { TurbulenceAtm(*(cAtmosphereModel*)p).run(); }
+void ref_set_turb_model(void* p, const char* s) { ((cAtmosphereModel*)p)->turb_model = s; }
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
 
 // RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4

@@ -161,6 +161,12 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_post_rk4_filters(im, jm, km, ctypes.byref(self.params), F)
 
+    def turbulence_run(self, compat=0):
+        """or_turbulence_run: TurbulenceAtm::run; compat=1 the reference's serial sweep."""
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_turbulence_run(im, jm, km, ctypes.byref(self.params), int(compat), F, F2)
+
     def damp_wiggles(self, name):
         im, jm, km = self.shape
         a = self.f[name]

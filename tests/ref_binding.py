@@ -32,7 +32,8 @@ class Reference:
         L.ref_new.restype = ctypes.c_void_p
         L.ref_new.argtypes = [ctypes.c_char_p]
         for n in ["ref_init_state", "ref_rk4", "ref_pressure", "ref_satadj", "ref_store",
-                  "ref_level_mean", "ref_delete"]:
+                  "ref_level_mean", "ref_delete", "ref_bc", "ref_post_rk4_filters",
+                  "ref_turbulence_run"]:
             getattr(L, n).argtypes = [ctypes.c_void_p]
         for n in ["ref_get3", "ref_set3", "ref_get2", "ref_set2", "ref_getp", "ref_setp"]:
             getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
@@ -46,6 +47,9 @@ class Reference:
                                    ctypes.POINTER(ctypes.c_double)]
         L.ref_constants.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_damp_wiggles.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.ref_damp_wiggles.restype = ctypes.c_int
+        self.threads = threads
         L.ref_quiet.argtypes = [ctypes.c_int]
         im, jm, km = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         L.ref_dims(ctypes.byref(im), ctypes.byref(jm), ctypes.byref(km))
@@ -115,6 +119,21 @@ class Reference:
 
     def damp_wiggles(self, name):
         assert self.lib.ref_damp_wiggles(self.h, name.encode()) == 0, name
+
+    def set_turb_model(self, name: str):
+        f = self.lib.ref_set_turb_model
+        f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        f(self.h, name.encode())
+
+    def turbulence_run(self, threads=None):
+        """TurbulenceAtm::run; threads=1 for the serial sweep order."""
+        if threads:
+            self.lib.ref_set_threads(threads)
+        try:
+            self.lib.ref_turbulence_run(self.h)
+        finally:
+            if threads and self.threads:
+                self.lib.ref_set_threads(self.threads)
 
     def bc(self):
         """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi."""

@@ -9,7 +9,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * solveRungeKutta_Atmosphere_Turb, the in-place sweep run with T OpenMP threads;
   * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes);
   * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
-  * the filters after the RK4 step and the moist iteration's damp_wiggles.
+  * the filters after the RK4 step and the moist iteration's damp_wiggles;
+  * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -185,3 +186,33 @@ def test_damp_wiggles_bit_exact(ref):
         R.damp_wiggles(n)
         o.damp_wiggles(n)
     assert_identical(R, o, ["t", "ice", "c", "cloud"])
+
+
+@pytest.mark.parametrize("model", ["k_epsilon", "k_omega", "k_omega_SST"])
+def test_turbulence_run_bit_exact(ref, model):
+    """TurbulenceAtm::run on one thread (its serial in-place sweep) against the oracle's
+    compat mode, on the initial state with tke pulled below its background floor in a band
+    of cells, so the floors bind at neighbours visited before and after."""
+    from athad_cond_b200._abi import Turb
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    R.set_turb_model(model)
+    o.params.turb_model = {"k_epsilon": Turb.K_EPSILON, "k_omega": Turb.K_OMEGA,
+                           "k_omega_SST": Turb.K_OMEGA_SST}[model]
+    rng = np.random.default_rng(47)
+    tke = R.get("tke")
+    tke[:, jm // 3: jm // 3 + 20, :] *= rng.uniform(0.0, 1.0, (im, 20, km))
+    tke[2:6, :, 100:110] = -1e-4
+    R.set("tke", tke)
+    o.f["tke"][...] = tke
+    for n in ("u", "v", "w"):
+        a = R.get(n) * (1.0 + 0.1 * rng.standard_normal((im, jm, km)))
+        R.set(n, a)
+        o.f[n][...] = a
+    try:
+        R.turbulence_run(threads=1)
+    finally:
+        R.set_turb_model("k_omega_SST")
+    o.turbulence_run(compat=1)
+    assert_identical(R, o, ["tke", "dis", "nue", "prod", "tke_source", "dis_source"])
+    assert np.array_equal(R.get2("vel_star"), o.f2["vel_star"])
