@@ -56,6 +56,7 @@ FIELD_NAMES = [
     "E_u", "D_u", "E_d", "D_d",
     "c_u", "e_l", "e_d", "e_p", "g_p",
     "P_conv", "CloudBase", "LevelFreeSinking", "Deep_beg", "Deep_end",
+    "P_rainn", "P_snown",
 ]
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 NFIELDS = len(FIELD_NAMES)
@@ -84,7 +85,7 @@ _PARAM_DOUBLES = [
     "r_Earth", "p_0", "t_00", "t_max_phys", "cloud_cap", "t_skin", "c_h2o_dry_top", "co2_0", "s_0",
     "R_Air", "R_WaterVapour",
     "M_bg", "R_bg", "R_mix",
-    "abl_height",
+    "abl_height", "t_000",
 ]
 
 
@@ -153,6 +154,7 @@ SIGNATURES = {
     "athad_post_rk4_filters": (ctypes.c_int, [_P]),
     "athad_damp_wiggles": (ctypes.c_int, [_P, ctypes.c_int]),
     "athad_turbulence_run": (ctypes.c_int, [_P]),
+    "athad_two_cat_ice_scheme": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),
@@ -226,7 +228,8 @@ def config_params() -> Params:
                 zeta=3.0, omega=0.000317, lamda=0.0262, lv=2520000.0, ls=2830000.0, pr_turb=0.9,
                 sc_WaterVapour=0.61, sc_CO2=0.96, r_Earth=6370.001, p_0=60000.0, t_00=236.15,
                 t_max_phys=2000.0, cloud_cap=0.05, t_skin=254.0, c_h2o_dry_top=0.00423,
-                co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5, abl_height=10000.0)
+                co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5, abl_height=10000.0,
+                t_000=253.15)
     for k, v in vals.items():
         setattr(p, k, v)
     R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010

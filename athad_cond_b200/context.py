@@ -168,6 +168,10 @@ class GpuAtmosphere:
         """AtomUtils::damp_wiggles(field, i, j, k) (lib/Utils.cpp:429-531)."""
         self._check(self.lib.athad_damp_wiggles(self._h, FIELD[name]))
 
+    def two_cat_ice_scheme(self):
+        """TwoCatIceScheme::run (TwoCatIceScheme.h:89-109; call site cAtmosphereModel.cpp:1238)."""
+        self._check(self.lib.athad_two_cat_ice_scheme(self._h))
+
     def turbulence_run(self):
         """TurbulenceAtm::run (TurbulenceAtm.h:62-79; call site cAtmosphereModel.cpp:1426)."""
         self._check(self.lib.athad_turbulence_run(self._h))

@@ -41,6 +41,7 @@ void athad_default_params(athad_params* p)
     p->t_max_phys = 2000.0; p->cloud_cap = 0.05; p->t_skin = 254.0; p->c_h2o_dry_top = 0.00423;
     p->co2_0 = 0.6233; p->s_0 = 274515.75; p->R_Air = 296.8; p->R_WaterVapour = 461.5;
     p->abl_height = 10000.0;
+    p->t_000 = 253.15;
     const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
     const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
     const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
@@ -423,16 +424,23 @@ athad_status athad_fill(athad_ctx* ctx, athad_field f, double value)
 
 // ---- hot path -----------------------------------------------------------------------------
 
+// P_rain, P_snow -> P_rainn, P_snown (UtilsAtm.h:41-42): consecutive fields, one copy
+static athad_status store_precip_n_level(athad_ctx* ctx, cudaStream_t st)
+{
+    const size_t bytes = ctx->L.field_elems * sizeof(double);
+    return cuda_check(ctx, cudaMemcpyAsync(ctx->field[ATHAD_P_RAINN], ctx->field[ATHAD_P_RAIN], 2 * bytes,
+                                           cudaMemcpyDeviceToDevice, st), "store_n_level precipitation");
+}
+
 athad_status athad_store_n_level(athad_ctx* ctx)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
+    // the fields are consecutive in the slab: t..dis -> tn..disn is one copy
     const size_t bytes = ctx->L.field_elems * sizeof(double);
-    for (int n = 0; n < kNY; n++) {
-        athad_status s = cuda_check(ctx, cudaMemcpyAsync(ctx->field[ATHAD_TN + n], ctx->field[ATHAD_T + n], bytes,
-                                                         cudaMemcpyDeviceToDevice, ctx->stream), "store_n_level");
-        if (s != ATHAD_OK) return s;
-    }
-    return ATHAD_OK;
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(ctx->field[ATHAD_TN], ctx->field[ATHAD_T], kNY * bytes,
+                                                     cudaMemcpyDeviceToDevice, ctx->stream), "store_n_level");
+    if (s != ATHAD_OK) return s;
+    return store_precip_n_level(ctx, ctx->stream);
 }
 
 athad_status athad_level_mean(athad_ctx* ctx)
@@ -506,7 +514,7 @@ athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
         launch_rk4_stage(stage, a, ctx->stream);
         ATHAD_CHECK_LAUNCH(ctx, "rk4 stage");
     }
-    return ATHAD_OK;
+    return s->store_n_level ? store_precip_n_level(ctx, ctx->stream) : ATHAD_OK;
 }
 
 }  // extern "C"
@@ -585,7 +593,7 @@ static athad_status rk4_step_mixed(athad_ctx* ctx, const athad_step_scalars* s)
         launch_rk4m_stage(stage, a, ctx->stream);
         ATHAD_CHECK_LAUNCH(ctx, "rk4 mixed stage");
     }
-    return ATHAD_OK;
+    return s->store_n_level ? store_precip_n_level(ctx, ctx->stream) : ATHAD_OK;
 }
 
 static PoissonArgs poisson_args(athad_ctx* ctx, int total_iter_count)
@@ -774,6 +782,28 @@ athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field f)
     // the RK4 stage buffer A is free between RK4 steps
     launch_damp_wiggles(ctx->L.d, ctx->field[f], ctx->stA[0], ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "damp_wiggles");
+    return ATHAD_OK;
+}
+
+athad_status athad_two_cat_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (ctx->L.d.im < 3 || ctx->L.d.jm < 3 || ctx->L.d.km < 3)
+        return fail(ctx, ATHAD_ERR_UNSUPPORTED, "two_cat_ice_scheme: grid too small");
+    IceArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    double** F = ctx->field;
+    a.t = F[ATHAD_T]; a.c = F[ATHAD_C]; a.cloud = F[ATHAD_CLOUD]; a.ice = F[ATHAD_ICE]; a.gr = F[ATHAD_GR];
+    a.co2 = F[ATHAD_CO2]; a.p_stat = F[ATHAD_P_STAT]; a.r_humid = F[ATHAD_R_HUMID];
+    a.P_rain = F[ATHAD_P_RAIN]; a.P_snow = F[ATHAD_P_SNOW]; a.P_graupel = F[ATHAD_P_GRAUPEL];
+    a.Precipitation = F[ATHAD_PRECIPITATION]; a.P_rainn = F[ATHAD_P_RAINN]; a.P_snown = F[ATHAD_P_SNOWN];
+    a.S_v = F[ATHAD_S_V]; a.S_c = F[ATHAD_S_C]; a.S_i = F[ATHAD_S_I]; a.S_r = F[ATHAD_S_R];
+    a.S_s = F[ATHAD_S_S]; a.S_g = F[ATHAD_S_G]; a.S_c_c = F[ATHAD_S_C_C];
+    a.step_f = ctx->step_f;
+    a.t_0 = ctx->p.t_0; a.t_000 = ctx->p.t_000; a.M_bg = ctx->p.M_bg;
+    launch_two_cat_ice(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "two_cat_ice_scheme");
     return ATHAD_OK;
 }
 

@@ -117,6 +117,16 @@ static athad_status enqueue_iteration(athad_batch* b)
         s = bcuda(b, cudaGetLastError(), "batch rk4 stage");
         if (s != ATHAD_OK) return s;
     }
+    // the time-level copy's precipitation fluxes (UtilsAtm.h:41-42); the stage kernel wrote
+    // the eleven prognostic fields' level n
+    for (int q = 0; q < n; q++) {
+        if (!b->active[q]) continue;
+        athad_ctx* c = b->m[q];
+        s = bcuda(b, cudaMemcpyAsync(c->field[ATHAD_P_RAINN], c->field[ATHAD_P_RAIN],
+                                     2 * c->L.field_elems * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     b->stream), "batch precipitation level n");
+        if (s != ATHAD_OK) return s;
+    }
     batch_advance_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_step, n);
     return bcuda(b, cudaGetLastError(), "batch advance");
 }

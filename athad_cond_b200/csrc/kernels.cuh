@@ -226,4 +226,17 @@ struct TurbArgs {
 };
 void launch_turbulence_run(const TurbArgs& a, cudaStream_t st);
 
+// TwoCatIceScheme::run (k_ice.cu)
+struct IceArgs {
+    Dims d;
+    double* t; double* c; double* cloud; double* ice; double* gr;
+    const double* co2; const double* p_stat; const double* r_humid;
+    double* P_rain; double* P_snow; double* P_graupel; double* Precipitation;
+    double* P_rainn; double* P_snown;
+    double* S_v; double* S_c; double* S_i; double* S_r; double* S_s; double* S_g; double* S_c_c;
+    const double* step_f;       // [im] float layer thickness, get_layer_height(i+1) - (i)
+    double t_0, t_000, M_bg;
+};
+void launch_two_cat_ice(const IceArgs& a, cudaStream_t st);
+
 }  // namespace athad

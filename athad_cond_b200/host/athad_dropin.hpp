@@ -17,6 +17,7 @@
 //     PostRK4Filters(m)         the polar zonal and radial Shapiro filters   :1507-1520
 //     DampMoistWiggles(m)       AtomUtils::damp_wiggles of t, ice, c, cloud  :1225-1228
 //     TurbulenceRun(m)          TurbulenceAtm(m).run()                       :614, 1426
+//     TwoCatIceSchemeRun(m)     TwoCatIceScheme(m).run()                     :589, 1238
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -65,7 +66,7 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.cloud_cap = m.cloud_cap; p.t_skin = m.t_skin; p.c_h2o_dry_top = m.c_h2o_dry_top;
     p.co2_0 = m.co2_0; p.s_0 = m.s_0; p.R_Air = m.R_Air; p.R_WaterVapour = m.R_WaterVapour;
     p.M_bg = m.m_comp.M_bg; p.R_bg = m.m_comp.R_bg; p.R_mix = m.m_comp.R_mix;
-    p.abl_height = m.abl_height;
+    p.abl_height = m.abl_height; p.t_000 = m.t_000;
     return p;
 }
 
@@ -285,12 +286,33 @@ public:
         down(ATHAD_T, m.t); down(ATHAD_ICE, m.ice); down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud);
     }
 
+    // TwoCatIceScheme(m).run() (cAtmosphereModel.cpp:589, 1238), flat terrain
+    void TwoCatIceSchemeRun(Model& m)
+    {
+#define ATHAD_ICE_FIELDS(X) X(ATHAD_T, t) X(ATHAD_C, c) X(ATHAD_CLOUD, cloud) X(ATHAD_ICE, ice) \
+        X(ATHAD_GR, gr) X(ATHAD_P_RAIN, P_rain) X(ATHAD_P_SNOW, P_snow) X(ATHAD_P_GRAUPEL, P_graupel) \
+        X(ATHAD_PRECIPITATION, Precipitation) X(ATHAD_P_RAINN, P_rainn) X(ATHAD_P_SNOWN, P_snown) \
+        X(ATHAD_S_V, S_v) X(ATHAD_S_C, S_c) X(ATHAD_S_I, S_i) X(ATHAD_S_R, S_r) X(ATHAD_S_S, S_s) \
+        X(ATHAD_S_G, S_g) X(ATHAD_S_C_C, S_c_c)
+#define ATHAD_ICE_UP(F, N) up(F, m.N);
+#define ATHAD_ICE_DOWN(F, N) down(F, m.N);
+        ATHAD_ICE_FIELDS(ATHAD_ICE_UP)
+        up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat); up(ATHAD_R_HUMID, m.r_humid);
+        check(ctx_, athad_two_cat_ice_scheme(ctx_), "two_cat_ice_scheme");
+        ATHAD_ICE_FIELDS(ATHAD_ICE_DOWN)
+#undef ATHAD_ICE_UP
+#undef ATHAD_ICE_DOWN
+#undef ATHAD_ICE_FIELDS
+    }
+
     // TurbulenceAtm(m).run() (cAtmosphereModel.cpp:614, 1426), flat terrain.  The closure is
     // the one the context was created with (athad_params.turb_model from m.turb_model).
     void TurbulenceRun(Model& m)
     {
         up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w);
         up(ATHAD_TKE, m.tke); up(ATHAD_DIS, m.dis); up(ATHAD_NUE, m.nue);
+        // the sources are written in the interior only; the rest keeps the model's values
+        up(ATHAD_PROD, m.prod); up(ATHAD_TKE_SOURCE, m.tke_source); up(ATHAD_DIS_SOURCE, m.dis_source);
         check(ctx_, athad_turbulence_run(ctx_), "turbulence_run");
         down(ATHAD_TKE, m.tke); down(ATHAD_DIS, m.dis); down(ATHAD_NUE, m.nue);
         down(ATHAD_PROD, m.prod); down(ATHAD_TKE_SOURCE, m.tke_source);

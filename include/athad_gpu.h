@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 3
+#define ATHAD_ABI_VERSION 4
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -110,6 +110,8 @@ typedef struct athad_params {
     double M_bg, R_bg, R_mix;
     double abl_height;           /* XML abl_height [m], 10000 (cli/config_cond.xml:76):
                                   * the eddy-viscosity ceiling of TurbulenceAtm::clamp_nue */
+    double t_000;                /* XML t_000 [K], 253.15 (cli/config_cond.xml:102): the
+                                  * snow-flux floor temperature of TwoCatIceScheme */
 } athad_params;
 
 /* 3-D fields, one per cAtmosphereModel Array member of the same name. */
@@ -140,6 +142,9 @@ typedef enum athad_field {
     ATHAD_E_U, ATHAD_D_U, ATHAD_E_D, ATHAD_D_D,
     ATHAD_C_U, ATHAD_E_L, ATHAD_E_DD, ATHAD_E_P, ATHAD_G_P,
     ATHAD_P_CONV, ATHAD_CLOUD_BASE, ATHAD_LEVEL_FREE_SINKING, ATHAD_DEEP_BEG, ATHAD_DEEP_END,
+    /* precipitation fluxes of the time level n (storeIntermediateData3D, UtilsAtm.h:41-42),
+     * the ice scheme's starting fluxes (TwoCatIceScheme.h:149-153) */
+    ATHAD_P_RAINN, ATHAD_P_SNOWN,
     ATHAD_NFIELDS
 } athad_field;
 
@@ -169,9 +174,10 @@ typedef struct athad_step_scalars {
     double buoyancy_ramp;    /* min(1, total_iter_count / 300)                         */
     int32_t write_diagnostics; /* 1: store prod/tke_source/dis_source of stage 4       */
     int32_t store_n_level;   /* 1: storeIntermediateData3D (UtilsAtm.h:25-49) fused into
-                              * the last stage: the caller runs nothing between the RK4
-                              * step and the time-level copy (no counterpart in the
-                              * reference, which copies in a separate pass) */
+                              * the last stage (the precipitation fluxes copied right
+                              * after it): the caller runs nothing between the RK4 step
+                              * and the time-level copy (no counterpart in the reference,
+                              * which copies in a separate pass) */
 } athad_step_scalars;
 
 /* Counters a call leaves behind (read with athad_get_report). */
@@ -228,7 +234,7 @@ athad_status athad_fill(athad_ctx* ctx, athad_field f, double value);
 /* ---- the hot path ----------------------------------------------------------- */
 
 /* storeIntermediateData3D(1.0) (UtilsAtm.h:25-49; call sites cAtmosphereModel.cpp:667,
- * 1647): the n-level fields := the current ones. */
+ * 1647): tn..disn := t..dis and P_rainn, P_snown := P_rain, P_snow. */
 athad_status athad_store_n_level(athad_ctx* ctx);
 
 /* cAtmosphereModel::computeLevelMeanTemperature (RungeKutta_Atm_Turb.cpp:24-41):
@@ -297,6 +303,13 @@ athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field field);
  * state before the call: the reference's in-place sweep lets a cell see the floored tke/dis
  * of the neighbours visited before it, which differs only where a floor binds there. */
 athad_status athad_turbulence_run(athad_ctx* ctx);
+/* TwoCatIceScheme(*this).run() (TwoCatIceScheme.h:89-109; the configuration's
+ * CategoryIceScheme = 2, call sites cAtmosphereModel.cpp:589, 1238), flat terrain: the
+ * falling rain and snow restarted from ATHAD_P_RAINN/ATHAD_P_SNOWN, the COSMO sources and
+ * sinks S_v, S_c, S_i, S_r, S_s (reading S_c_c), the capped fluxes P_rain, P_snow and
+ * Precipitation, and their boundary extrapolation; cells where no condensed phase can exist
+ * evaporate their condensate (IceSchemeCommon.h:121-190). */
+athad_status athad_two_cat_ice_scheme(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

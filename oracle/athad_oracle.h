@@ -42,7 +42,7 @@ typedef struct or_params {
     double r_Earth, p_0, t_00, t_max_phys, cloud_cap, t_skin, c_h2o_dry_top, co2_0, s_0;
     double R_Air, R_WaterVapour;
     double M_bg, R_bg, R_mix;
-    double abl_height;
+    double abl_height, t_000;
 } or_params;
 
 typedef struct or_step {
@@ -67,6 +67,7 @@ enum {
     OF_E_U, OF_D_U, OF_E_D, OF_D_D,
     OF_C_U, OF_E_L, OF_E_DD, OF_E_P, OF_G_P,
     OF_P_CONV, OF_CLOUD_BASE, OF_LEVEL_FREE_SINKING, OF_DEEP_BEG, OF_DEEP_END,
+    OF_P_RAINN, OF_P_SNOWN,
     OF_NFIELDS
 };
 enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR, OF2_N };
@@ -132,6 +133,10 @@ int  or_polar_passes(int jm, int j, const double* sin_w);
  * (the device form). */
 void or_turbulence_run(int im, int jm, int km, const or_params* p, int compat,
                        double* const* f, double* const* f2);
+
+/* TwoCatIceScheme::run, TwoCatIceScheme.h:89-109 (initArrays, computeColumns,
+ * applyBoundaryConditions; applyTopography does nothing without land), flat terrain */
+void or_two_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

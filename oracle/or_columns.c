@@ -6,7 +6,7 @@
 #include "or_internal.h"
 
 /* IceSchemeCommon::evaporateWhereImpossible, IceSchemeCommon.h:121-190 */
-static void evaporate_where_impossible(const or_params* p, double* const* f, size_t c, double t_u)
+void or_evaporate_where_impossible(const or_params* p, double* const* f, size_t c, double t_u)
 {
     const double q_cond = or_max(0.0, f[OF_CLOUD][c]) + or_max(0.0, f[OF_ICE][c])
                         + or_max(0.0, f[OF_GR][c]);
@@ -156,7 +156,7 @@ void or_saturation_adjust(int im, int jm, int km, const or_params* p, int compat
             const double M_o = or_M_nonwater(f[OF_C][c], f[OF_CO2][c], p->M_bg);
             const double q_s = or_saturation_mass_fraction_at(T_dim, f[OF_P_STAT][c], M_o);
             if (T_dim >= OR_T_CRIT || q_s >= 1.0) {
-                evaporate_where_impossible(p, f, c, T_dim);
+                or_evaporate_where_impossible(p, f, c, T_dim);
                 continue;
             }
         }

@@ -766,6 +766,8 @@ void or_store_n_level(int im, int jm, int km, double* const* f)
 {
     const size_t n = (size_t)im * jm * km;
     for (int q = 0; q < 11; q++) memcpy(f[OF_TN + q], f[OF_T + q], n * sizeof(double));
+    memcpy(f[OF_P_RAINN], f[OF_P_RAIN], n * sizeof(double));    /* UtilsAtm.h:41-42 */
+    memcpy(f[OF_P_SNOWN], f[OF_P_SNOW], n * sizeof(double));
 }
 
 /* RHS_Atmosphere_Turb at one interior cell of the current state (t_ref_level taken from

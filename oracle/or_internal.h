@@ -65,6 +65,9 @@ double or_latent_heat_auto(double T);
 double or_sat_deriv_factor_at(double E, double p, double M_other);
 double or_dqsat_dT_from(double E, double L, double T, double p, double M_other);
 
+/* IceSchemeCommon::evaporateWhereImpossible at cell c (or_columns.c) */
+void or_evaporate_where_impossible(const or_params* p, double* const* f, size_t c, double t_u);
+
 #define OR_IDX(i, j, k) (((size_t)(i) * (size_t)jm + (size_t)(j)) * (size_t)km + (size_t)(k))
 
 #endif

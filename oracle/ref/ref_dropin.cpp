@@ -50,6 +50,7 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 7: d.PostRK4Filters(*m); break;
             case 8: d.DampMoistWiggles(*m); break;
             case 9: d.TurbulenceRun(*m); break;
+            case 10: d.TwoCatIceSchemeRun(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

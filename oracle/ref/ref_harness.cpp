@@ -87,6 +87,7 @@ Array* field3(cAtmosphereModel* m, const std::string& n)
     F(E_u) F(D_u) F(E_d) F(D_d)
     F(c_u) F(e_l) F(e_d) F(e_p) F(g_p)
     F(P_conv) F(CloudBase) F(LevelFreeSinking) F(Deep_beg) F(Deep_end)
+    F(P_rainn) F(P_snown)
     F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
     F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
 #undef F
@@ -386,6 +387,9 @@ void ref_bc(void* p)
 // is the model's turb_model string, which TurbulenceAtm parses on construction
 void ref_turbulence_run(void* p) { TurbulenceAtm(*(cAtmosphereModel*)p).run(); }
 void ref_set_turb_model(void* p, const char* s) { ((cAtmosphereModel*)p)->turb_model = s; }
+// the moist iteration's ice scheme of the configuration (CategoryIceScheme = 2,
+// cAtmosphereModel.cpp:1238)
+void ref_two_cat_ice(void* p) { TwoCatIceScheme(*(cAtmosphereModel*)p).run(); }
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
 
 // RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4

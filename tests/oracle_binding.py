@@ -167,6 +167,12 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_turbulence_run(im, jm, km, ctypes.byref(self.params), int(compat), F, F2)
 
+    def two_cat_ice_scheme(self):
+        """or_two_cat_ice_scheme: TwoCatIceScheme::run."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_two_cat_ice_scheme(im, jm, km, ctypes.byref(self.params), F)
+
     def damp_wiggles(self, name):
         im, jm, km = self.shape
         a = self.f[name]

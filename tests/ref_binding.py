@@ -120,6 +120,11 @@ class Reference:
     def damp_wiggles(self, name):
         assert self.lib.ref_damp_wiggles(self.h, name.encode()) == 0, name
 
+    def two_cat_ice(self):
+        f = self.lib.ref_two_cat_ice
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
     def set_turb_model(self, name: str):
         f = self.lib.ref_set_turb_model
         f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]

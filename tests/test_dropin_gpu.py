@@ -167,3 +167,25 @@ def test_dropin_turbulence(model):
     scale = max(np.max(np.abs(b)), 1e-300)
     assert np.max(np.abs(a - b)[~near]) / scale <= 1e-10
     assert relerr(a, b) <= 1e-2
+
+
+def test_dropin_two_cat_ice_scheme(model):
+    """TwoCatIceScheme::run through the adapter against the reference's own call, on the
+    reference's state after its saturation adjustment with rain and snow seeded: within
+    1e-10 (CUDA vs glibc pow/exp and the saturation curves)."""
+    R, snap = model
+    im, jm, km = R.shape
+    rng = np.random.default_rng(59)
+    seeded = dict(snap)
+    seeded["P_rainn"] = 2e-4 * rng.random((im, jm, km))
+    seeded["P_snown"] = 2e-4 * rng.random((im, jm, km))
+    names = ["t", "c", "cloud", "ice", "P_rain", "P_snow", "Precipitation", "S_v", "S_c", "S_i",
+             "S_r", "S_s"]
+
+    def prep():
+        R.lib.ref_satadj(R.h)
+
+    out = run_both(R, seeded, lambda: (prep(), R.two_cat_ice()), lambda: (prep(), R.dropin(10)), names)
+    reset(R, snap)
+    for n, (a, b) in out.items():
+        assert relerr(a, b) <= 1e-10, (n, relerr(a, b))

@@ -210,15 +210,19 @@ def test_cadence_loop_matches_oracle():
 @pytest.mark.parametrize("precision", [0, 1])
 def test_fused_time_level_copy_equals_separate_copy(precision):
     """athad_step_scalars.store_n_level: the time-level copy written by the last RK4 stage
-    is bit-identical to the RK4 step followed by storeIntermediateData3D, boundary cells
-    included, and the following step starts from it."""
+    (and the precipitation fluxes copied after it) is bit-identical to the RK4 step followed
+    by storeIntermediateData3D, boundary cells included, and the following step starts
+    from it."""
     p = config_params()
     p.precision = precision
     st = make_state(11, 21, 41, seed=29)
+    rng = np.random.default_rng(29)
+    st["P_rain"] = 1e-5 * rng.random(st["t"].shape)
+    st["P_snow"] = 1e-5 * rng.random(st["t"].shape)
     with gpu_with(st, p) as a, gpu_with(st, p) as b:
         for it in range(3):
             a.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5)
             a.storeIntermediateData3D()
             b.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5, store_n_level=True)
-        for n in PROG + [x + "n" for x in PROG]:
+        for n in PROG + [x + "n" for x in PROG] + ["P_rainn", "P_snown"]:
             assert np.array_equal(a.download(n), b.download(n)), n

@@ -10,7 +10,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * PressureSolverAtm::run; SaturationAdjustment::run; ThermoAtm::densities (both modes);
   * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
   * the filters after the RK4 step and the moist iteration's damp_wiggles;
-  * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures.
+  * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
+  * TwoCatIceScheme::run.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -216,3 +217,24 @@ def test_turbulence_run_bit_exact(ref, model):
     o.turbulence_run(compat=1)
     assert_identical(R, o, ["tke", "dis", "nue", "prod", "tke_source", "dis_source"])
     assert np.array_equal(R.get2("vel_star"), o.f2["vel_star"])
+
+
+ICE_FIELDS = ["t", "c", "cloud", "ice", "gr", "P_rain", "P_snow", "P_graupel", "Precipitation",
+              "P_rainn", "P_snown", "S_v", "S_c", "S_i", "S_r", "S_s", "S_g", "S_c_c"]
+
+
+def test_two_cat_ice_scheme_bit_exact(ref):
+    """TwoCatIceScheme::run (the configuration's CategoryIceScheme 2) on the reference's state
+    after a saturation adjustment, with falling rain and snow seeded from above."""
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    R.lib.ref_satadj(R.h)
+    o.saturation_adjust(compat=1)
+    rng = np.random.default_rng(53)
+    for n in ("P_rainn", "P_snown"):
+        a = 2e-4 * rng.random((im, jm, km))
+        R.set(n, a)
+        o.f[n][...] = a
+    R.two_cat_ice()
+    o.two_cat_ice_scheme()
+    assert_identical(R, o, ICE_FIELDS)
