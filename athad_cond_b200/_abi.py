@@ -57,13 +57,15 @@ FIELD_NAMES = [
     "c_u", "e_l", "e_d", "e_p", "g_p",
     "P_conv", "CloudBase", "LevelFreeSinking", "Deep_beg", "Deep_end",
     "P_rainn", "P_snown",
+    "radiation", "epsilon",
 ]
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 NFIELDS = len(FIELD_NAMES)
 PROGNOSTIC = FIELD_NAMES[0:11]
 N_LEVEL = FIELD_NAMES[11:22]
 
-FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star"]
+FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star",
+                 "epsilon_2D", "albedo"]
 FIELD2D = {n: i for i, n in enumerate(FIELD2D_NAMES)}
 PROFILE_NAMES = ["t_ref_level", "rho_base", "dlnrho_dr"]
 PROFILE = {n: i for i, n in enumerate(PROFILE_NAMES)}
@@ -86,6 +88,8 @@ _PARAM_DOUBLES = [
     "R_Air", "R_WaterVapour",
     "M_bg", "R_bg", "R_mix",
     "abl_height", "t_000",
+    "sigma", "kappa_H2O", "kappa_CO2", "kappa_bg", "geothermal_flux", "albedo_surface",
+    "albedo_cloud", "rad_equator_short", "rad_pole_short",
 ]
 
 
@@ -155,6 +159,8 @@ SIGNATURES = {
     "athad_damp_wiggles": (ctypes.c_int, [_P, ctypes.c_int]),
     "athad_turbulence_run": (ctypes.c_int, [_P]),
     "athad_two_cat_ice_scheme": (ctypes.c_int, [_P]),
+    "athad_multilayer_radiation": (ctypes.c_int, [_P]),
+    "athad_radiative_heating": (ctypes.c_int, [_P, ctypes.c_double]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),
@@ -229,7 +235,9 @@ def config_params() -> Params:
                 sc_WaterVapour=0.61, sc_CO2=0.96, r_Earth=6370.001, p_0=60000.0, t_00=236.15,
                 t_max_phys=2000.0, cloud_cap=0.05, t_skin=254.0, c_h2o_dry_top=0.00423,
                 co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5, abl_height=10000.0,
-                t_000=253.15)
+                t_000=253.15, sigma=5.67028e-08, kappa_H2O=0.01, kappa_CO2=0.001, kappa_bg=1e-06,
+                geothermal_flux=150.0, albedo_surface=0.08, albedo_cloud=0.5,
+                rad_equator_short=298.0, rad_pole_short=0.0)
     for k, v in vals.items():
         setattr(p, k, v)
     R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010

@@ -168,6 +168,14 @@ class GpuAtmosphere:
         """AtomUtils::damp_wiggles(field, i, j, k) (lib/Utils.cpp:429-531)."""
         self._check(self.lib.athad_damp_wiggles(self._h, FIELD[name]))
 
+    def multilayer_radiation(self):
+        """MultiLayerRadiation::run (MultiLayerRadiation.h:56-388): t := radiative equilibrium."""
+        self._check(self.lib.athad_multilayer_radiation(self._h))
+
+    def radiative_heating(self, omega_rad: float = 0.05):
+        """Radiation mode 2's apply_radiative_heating (cAtmosphereModel.cpp:864-879)."""
+        self._check(self.lib.athad_radiative_heating(self._h, float(omega_rad)))
+
     def two_cat_ice_scheme(self):
         """TwoCatIceScheme::run (TwoCatIceScheme.h:89-109; call site cAtmosphereModel.cpp:1238)."""
         self._check(self.lib.athad_two_cat_ice_scheme(self._h))

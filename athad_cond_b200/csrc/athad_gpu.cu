@@ -42,6 +42,9 @@ void athad_default_params(athad_params* p)
     p->co2_0 = 0.6233; p->s_0 = 274515.75; p->R_Air = 296.8; p->R_WaterVapour = 461.5;
     p->abl_height = 10000.0;
     p->t_000 = 253.15;
+    p->sigma = 5.67028e-08; p->kappa_H2O = 0.01; p->kappa_CO2 = 0.001; p->kappa_bg = 1e-06;
+    p->geothermal_flux = 150.0; p->albedo_surface = 0.08; p->albedo_cloud = 0.5;
+    p->rad_equator_short = 298.0; p->rad_pole_short = 0.0;
     const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
     const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
     const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
@@ -782,6 +785,49 @@ athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field f)
     // the RK4 stage buffer A is free between RK4 steps
     launch_damp_wiggles(ctx->L.d, ctx->field[f], ctx->stA[0], ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "damp_wiggles");
+    return ATHAD_OK;
+}
+
+static athad_status multilayer_radiation(athad_ctx* ctx)
+{
+    const athad_params& p = ctx->p;
+    RadArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    double** F = ctx->field;
+    a.t = F[ATHAD_T]; a.c = F[ATHAD_C]; a.co2 = F[ATHAD_CO2]; a.p_stat = F[ATHAD_P_STAT];
+    a.cloud = F[ATHAD_CLOUD]; a.ice = F[ATHAD_ICE];
+    a.radiation = F[ATHAD_RADIATION]; a.epsilon = F[ATHAD_EPSILON];
+    a.epsilon_2D = ctx->f2d[ATHAD_2D_EPSILON]; a.albedo = ctx->f2d[ATHAD_2D_ALBEDO];
+    a.T = ctx->stA[1]; a.dn = ctx->stA[2];   // RK4 stage buffers, free between RK4 steps
+    a.step_f = ctx->step_f;
+    a.t_0 = p.t_0; a.g = p.g; a.R_bg = p.R_bg; a.sigma = p.sigma;
+    a.kappa_H2O = p.kappa_H2O; a.kappa_CO2 = p.kappa_CO2; a.kappa_bg = p.kappa_bg;
+    a.geothermal_flux = p.geothermal_flux; a.albedo_surface = p.albedo_surface;
+    a.albedo_cloud = p.albedo_cloud; a.rad_equator_short = p.rad_equator_short;
+    a.rad_pole_short = p.rad_pole_short;
+    launch_multilayer_radiation(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "multilayer_radiation");
+    return ATHAD_OK;
+}
+
+athad_status athad_multilayer_radiation(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    return multilayer_radiation(ctx);
+}
+
+athad_status athad_radiative_heating(athad_ctx* ctx, double omega_rad)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    double* t = ctx->field[ATHAD_T];
+    double* t_before = ctx->stA[0];
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(t_before, t, ctx->L.field_elems * sizeof(double),
+                                                     cudaMemcpyDeviceToDevice, ctx->stream), "radiative_heating");
+    if (s == ATHAD_OK) s = multilayer_radiation(ctx);
+    if (s != ATHAD_OK) return s;
+    launch_rad_blend(ctx->L.d, t_before, t, omega_rad, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "radiative_heating blend");
     return ATHAD_OK;
 }
 

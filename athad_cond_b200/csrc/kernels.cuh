@@ -239,4 +239,19 @@ struct IceArgs {
 };
 void launch_two_cat_ice(const IceArgs& a, cudaStream_t st);
 
+// MultiLayerRadiation::run (k_rad.cu)
+struct RadArgs {
+    Dims d;
+    double* t;
+    const double* c; const double* co2; const double* p_stat; const double* cloud; const double* ice;
+    double* radiation; double* epsilon;
+    double* epsilon_2D; double* albedo;   // 2-D, jm rows of pitch
+    double* T; double* dn;                // scratch fields: layer temperature [K], downward flux
+    const double* step_f;                 // [im] float layer thickness
+    double t_0, g, R_bg, sigma, kappa_H2O, kappa_CO2, kappa_bg, geothermal_flux;
+    double albedo_surface, albedo_cloud, rad_equator_short, rad_pole_short;
+};
+void launch_multilayer_radiation(const RadArgs& a, cudaStream_t st);
+void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
+
 }  // namespace athad

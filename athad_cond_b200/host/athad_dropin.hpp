@@ -18,6 +18,8 @@
 //     DampMoistWiggles(m)       AtomUtils::damp_wiggles of t, ice, c, cloud  :1225-1228
 //     TurbulenceRun(m)          TurbulenceAtm(m).run()                       :614, 1426
 //     TwoCatIceSchemeRun(m)     TwoCatIceScheme(m).run()                     :589, 1238
+//     MultiLayerRadiationRun(m) MultiLayerRadiation(m).run()                 :831-1007
+//     RadiativeHeating(m, w)    radiation mode 2's apply_radiative_heating   :864-879, 1656
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -67,6 +69,10 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.co2_0 = m.co2_0; p.s_0 = m.s_0; p.R_Air = m.R_Air; p.R_WaterVapour = m.R_WaterVapour;
     p.M_bg = m.m_comp.M_bg; p.R_bg = m.m_comp.R_bg; p.R_mix = m.m_comp.R_mix;
     p.abl_height = m.abl_height; p.t_000 = m.t_000;
+    p.sigma = m.sigma; p.kappa_H2O = m.kappa_H2O; p.kappa_CO2 = m.kappa_CO2; p.kappa_bg = m.kappa_bg;
+    p.geothermal_flux = m.geothermal_flux; p.albedo_surface = m.albedo_surface;
+    p.albedo_cloud = m.albedo_cloud; p.rad_equator_short = m.rad_equator_short;
+    p.rad_pole_short = m.rad_pole_short;
     return p;
 }
 
@@ -305,6 +311,11 @@ public:
 #undef ATHAD_ICE_FIELDS
     }
 
+    // MultiLayerRadiation(m).run() (cAtmosphereModel.cpp:831-1007), and radiation mode 2's
+    // heating t := t (1 - omega) + MLR(t) omega (:864-879; omega_rad = 0.05, :801)
+    void MultiLayerRadiationRun(Model& m) { radiation(m, false, 0.0); }
+    void RadiativeHeating(Model& m, double omega_rad) { radiation(m, true, omega_rad); }
+
     // TurbulenceAtm(m).run() (cAtmosphereModel.cpp:614, 1426), flat terrain.  The closure is
     // the one the context was created with (athad_params.turb_model from m.turb_model).
     void TurbulenceRun(Model& m)
@@ -321,6 +332,16 @@ public:
     }
 
 private:
+    void radiation(Model& m, bool heating, double omega_rad)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_C, m.c); up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat);
+        up(ATHAD_CLOUD, m.cloud); up(ATHAD_ICE, m.ice);
+        if (heating) check(ctx_, athad_radiative_heating(ctx_, omega_rad), "radiative_heating");
+        else check(ctx_, athad_multilayer_radiation(ctx_), "multilayer_radiation");
+        down(ATHAD_T, m.t); down(ATHAD_RADIATION, m.radiation); down(ATHAD_EPSILON, m.epsilon);
+        down2(ATHAD_2D_EPSILON, m.epsilon_2D); down2(ATHAD_2D_ALBEDO, m.albedo);
+    }
+
     int im_, jm_, km_;
     std::vector<double> buf_;
     athad_ctx* ctx_ = nullptr;

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 4
+#define ATHAD_ABI_VERSION 5
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -112,6 +112,12 @@ typedef struct athad_params {
                                   * the eddy-viscosity ceiling of TurbulenceAtm::clamp_nue */
     double t_000;                /* XML t_000 [K], 253.15 (cli/config_cond.xml:102): the
                                   * snow-flux floor temperature of TwoCatIceScheme */
+    /* MultiLayerRadiation (cli/config_cond.xml:29-37, 66-67; cAtmosphereDefaults.cpp.inc) */
+    double sigma;                /* Stefan-Boltzmann constant, 5.67028e-8              */
+    double kappa_H2O, kappa_CO2, kappa_bg;  /* grey LW mass absorption [m2/kg]          */
+    double geothermal_flux;      /* [W/m2], 150                                          */
+    double albedo_surface, albedo_cloud;
+    double rad_equator_short, rad_pole_short;   /* TOA short-wave insolation [W/m2]     */
 } athad_params;
 
 /* 3-D fields, one per cAtmosphereModel Array member of the same name. */
@@ -145,6 +151,9 @@ typedef enum athad_field {
     /* precipitation fluxes of the time level n (storeIntermediateData3D, UtilsAtm.h:41-42),
      * the ice scheme's starting fluxes (TwoCatIceScheme.h:149-153) */
     ATHAD_P_RAINN, ATHAD_P_SNOWN,
+    /* MultiLayerRadiation outputs (MultiLayerRadiation.h): upward long-wave flux per layer
+     * [W/m2] and the layer emissivity */
+    ATHAD_RADIATION, ATHAD_EPSILON,
     ATHAD_NFIELDS
 } athad_field;
 
@@ -156,6 +165,8 @@ typedef enum athad_field2d {
     ATHAD_2D_Q_SENSIBLE,            /* Array_2D Q_sensible_2D (MoistConvection input) */
     ATHAD_2D_VEL_STAR,              /* Array_2D vel_star, friction velocity [m/s]
                                      * (TurbulenceAtm::compute_vel_star; wall BC input) */
+    ATHAD_2D_EPSILON,               /* Array_2D epsilon_2D, surface-layer emissivity     */
+    ATHAD_2D_ALBEDO,                /* Array_2D albedo (MultiLayerRadiation)             */
     ATHAD_NFIELDS2D
 } athad_field2d;
 
@@ -310,6 +321,16 @@ athad_status athad_turbulence_run(athad_ctx* ctx);
  * Precipitation, and their boundary extrapolation; cells where no condensed phase can exist
  * evaporate their condensate (IceSchemeCommon.h:121-190). */
 athad_status athad_two_cat_ice_scheme(athad_ctx* ctx);
+/* MultiLayerRadiation(*this).run() (MultiLayerRadiation.h:56-388; call sites
+ * cAtmosphereModel.cpp:831-1007), flat terrain: per (j, k) column the grey long-wave
+ * emissivities, four radiative-equilibrium sweeps and the surface energy balance.  Writes t
+ * (the radiative equilibrium), ATHAD_RADIATION, ATHAD_EPSILON, ATHAD_2D_EPSILON and
+ * ATHAD_2D_ALBEDO.  Uses RK4 stage buffers as scratch. */
+athad_status athad_multilayer_radiation(athad_ctx* ctx);
+/* Radiation mode 2 (cAtmosphereModel.cpp:799, 1655-1656): apply_radiative_heating
+ * (:864-879), t := t (1 - omega_rad) + MultiLayerRadiation(t) omega_rad; the reference's
+ * omega_rad is 0.05 (:801). */
+athad_status athad_radiative_heating(athad_ctx* ctx, double omega_rad);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

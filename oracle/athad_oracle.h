@@ -43,6 +43,8 @@ typedef struct or_params {
     double R_Air, R_WaterVapour;
     double M_bg, R_bg, R_mix;
     double abl_height, t_000;
+    double sigma, kappa_H2O, kappa_CO2, kappa_bg, geothermal_flux, albedo_surface, albedo_cloud;
+    double rad_equator_short, rad_pole_short;
 } or_params;
 
 typedef struct or_step {
@@ -68,9 +70,11 @@ enum {
     OF_C_U, OF_E_L, OF_E_DD, OF_E_P, OF_G_P,
     OF_P_CONV, OF_CLOUD_BASE, OF_LEVEL_FREE_SINKING, OF_DEEP_BEG, OF_DEEP_END,
     OF_P_RAINN, OF_P_SNOWN,
+    OF_RADIATION, OF_EPSILON,
     OF_NFIELDS
 };
-enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR, OF2_N };
+enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR,
+       OF2_EPSILON, OF2_ALBEDO, OF2_N };
 enum { OFP_T_REF_LEVEL = 0, OFP_RHO_BASE, OFP_DLNRHO_DR, OFP_N };
 
 size_t or_params_size(void);
@@ -137,6 +141,14 @@ void or_turbulence_run(int im, int jm, int km, const or_params* p, int compat,
 /* TwoCatIceScheme::run, TwoCatIceScheme.h:89-109 (initArrays, computeColumns,
  * applyBoundaryConditions; applyTopography does nothing without land), flat terrain */
 void or_two_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
+
+/* MultiLayerRadiation::run (MultiLayerRadiation.h:56-388): t := the radiative equilibrium;
+ * radiation, epsilon, epsilon_2D, albedo.  or_radiative_heating: radiation mode 2's
+ * apply_radiative_heating (cAtmosphereModel.cpp:864-879), t := t (1 - omega) + RE omega. */
+void or_multilayer_radiation(int im, int jm, int km, const or_params* p, double* const* f,
+                             double* const* f2);
+void or_radiative_heating(int im, int jm, int km, const or_params* p, double omega_rad,
+                          double* const* f, double* const* f2);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

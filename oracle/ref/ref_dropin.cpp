@@ -51,6 +51,8 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 8: d.DampMoistWiggles(*m); break;
             case 9: d.TurbulenceRun(*m); break;
             case 10: d.TwoCatIceSchemeRun(*m); break;
+            case 11: d.MultiLayerRadiationRun(*m); break;
+            case 12: d.RadiativeHeating(*m, 0.05); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

@@ -59,6 +59,7 @@
 #include "UtilsAtm.h"
 #include "BC_Atm.h"
 #include "TurbulenceAtm.h"
+#include "MultiLayerRadiation.h"
 #undef private
 #undef protected
 
@@ -87,7 +88,7 @@ Array* field3(cAtmosphereModel* m, const std::string& n)
     F(E_u) F(D_u) F(E_d) F(D_d)
     F(c_u) F(e_l) F(e_d) F(e_p) F(g_p)
     F(P_conv) F(CloudBase) F(LevelFreeSinking) F(Deep_beg) F(Deep_end)
-    F(P_rainn) F(P_snown)
+    F(P_rainn) F(P_snown) F(radiation) F(epsilon)
     F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
     F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
 #undef F
@@ -100,6 +101,8 @@ Array_2D* field2(cAtmosphereModel* m, const std::string& n)
     if (n == "Evaporation") return &m->Evaporation;
     if (n == "Q_sensible_2D") return &m->Q_sensible_2D;
     if (n == "vel_star") return &m->vel_star;
+    if (n == "epsilon_2D") return &m->epsilon_2D;
+    if (n == "albedo") return &m->albedo;
     return nullptr;
 }
 
@@ -390,6 +393,27 @@ void ref_set_turb_model(void* p, const char* s) { ((cAtmosphereModel*)p)->turb_m
 // the moist iteration's ice scheme of the configuration (CategoryIceScheme = 2,
 // cAtmosphereModel.cpp:1238)
 void ref_two_cat_ice(void* p) { TwoCatIceScheme(*(cAtmosphereModel*)p).run(); }
+// MultiLayerRadiation::run, and radiation mode 2's apply_radiative_heating (the lambda of
+// cAtmosphereModel.cpp:864-879, which saves t, runs the radiation and blends t toward the
+// radiative equilibrium by omega_rad; restated here around the reference's own run())
+void ref_mlr(void* p) { MultiLayerRadiation(*(cAtmosphereModel*)p).run(); }
+void ref_radiative_heating(void* p, double omega_rad)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    std::vector<double> t_backup((size_t)m->im * m->jm * m->km);
+    size_t idx = 0;
+    for (int i = 0; i < m->im; i++)
+        for (int j = 0; j < m->jm; j++)
+            for (int k = 0; k < m->km; k++) t_backup[idx++] = m->t.x[i][j][k];
+    MultiLayerRadiation(*m).run();
+    idx = 0;
+    for (int i = 0; i < m->im; i++)
+        for (int j = 0; j < m->jm; j++)
+            for (int k = 0; k < m->km; k++) {
+                const double re = m->t.x[i][j][k];
+                m->t.x[i][j][k] = t_backup[idx++] * (1.0 - omega_rad) + re * omega_rad;
+            }
+}
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
 
 // RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4

@@ -167,6 +167,18 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_turbulence_run(im, jm, km, ctypes.byref(self.params), int(compat), F, F2)
 
+    def multilayer_radiation(self):
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_multilayer_radiation(im, jm, km, ctypes.byref(self.params), F, F2)
+
+    def radiative_heating(self, omega_rad=0.05):
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        fn = lib().or_radiative_heating
+        fn.argtypes = None
+        fn(im, jm, km, ctypes.byref(self.params), ctypes.c_double(omega_rad), F, F2)
+
     def two_cat_ice_scheme(self):
         """or_two_cat_ice_scheme: TwoCatIceScheme::run."""
         F, _, _ = self._args()

@@ -120,6 +120,16 @@ class Reference:
     def damp_wiggles(self, name):
         assert self.lib.ref_damp_wiggles(self.h, name.encode()) == 0, name
 
+    def mlr(self):
+        f = self.lib.ref_mlr
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
+    def radiative_heating(self, omega_rad=0.05):
+        f = self.lib.ref_radiative_heating
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        f(self.h, omega_rad)
+
     def two_cat_ice(self):
         f = self.lib.ref_two_cat_ice
         f.argtypes = [ctypes.c_void_p]

@@ -189,3 +189,20 @@ def test_dropin_two_cat_ice_scheme(model):
     reset(R, snap)
     for n, (a, b) in out.items():
         assert relerr(a, b) <= 1e-10, (n, relerr(a, b))
+
+
+def test_dropin_radiation(model):
+    """MultiLayerRadiation::run and radiation mode 2's heating through the adapter against the
+    reference's own calls, cloud and ice seeded: within 1e-12 (CUDA vs glibc pow/exp)."""
+    R, snap = model
+    im, jm, km = R.shape
+    rng = np.random.default_rng(61)
+    seeded = dict(snap)
+    seeded["cloud"] = 2e-4 * rng.random((im, jm, km))
+    seeded["ice"] = 2e-4 * rng.random((im, jm, km))
+    names = ["t", "radiation", "epsilon"]
+    for cpu, what in ((R.mlr, 11), (lambda: R.radiative_heating(0.05), 12)):
+        out = run_both(R, seeded, cpu, lambda: R.dropin(what), names)
+        for n, (a, b) in out.items():
+            assert relerr(a, b) <= 1e-12, (what, n, relerr(a, b))
+    reset(R, snap)

@@ -11,7 +11,7 @@ semantics, must reproduce every hot-path function bit for bit:
   * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
   * the filters after the RK4 step and the moist iteration's damp_wiggles;
   * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
-  * TwoCatIceScheme::run.
+  * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -238,3 +238,24 @@ def test_two_cat_ice_scheme_bit_exact(ref):
     R.two_cat_ice()
     o.two_cat_ice_scheme()
     assert_identical(R, o, ICE_FIELDS)
+
+
+def test_multilayer_radiation_bit_exact(ref):
+    """MultiLayerRadiation::run on the reference's state (cloud and ice seeded so the cloud
+    optical depth and the short-wave albedo bump act), then radiation mode 2's heating."""
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    rng = np.random.default_rng(67)
+    for n in ("cloud", "ice"):
+        a = 2e-4 * rng.random((im, jm, km))
+        R.set(n, a)
+        o.f[n][...] = a
+    R.mlr()
+    o.multilayer_radiation()
+    assert_identical(R, o, ["t", "radiation", "epsilon"])
+    for n in ("epsilon_2D", "albedo"):
+        assert np.array_equal(R.get2(n), o.f2[n]), n
+    R, o = fresh(ref)
+    R.radiative_heating(0.05)
+    o.radiative_heating(0.05)
+    assert_identical(R, o, ["t", "radiation", "epsilon"])
