@@ -144,6 +144,11 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 #define ATHAD_RK4_BY 4
 #endif
 
+#ifndef ATHAD_RK4_TRACER_UNROLL
+#define ATHAD_RK4_TRACER_UNROLL 1
+#endif
+constexpr int kTracerUnroll64 = ATHAD_RK4_TRACER_UNROLL;
+
 template <int STAGE>
 __global__ void __launch_bounds__(ATHAD_RK4_BX * ATHAD_RK4_BY, ATHAD_RK4_MIN_BLOCKS * 128 / (ATHAD_RK4_BX * ATHAD_RK4_BY))
 rk4_stage_kernel(const RK4Args a)
@@ -395,7 +400,7 @@ rk4_stage_kernel(const RK4Args a)
         const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
         const double dlnrho_dr_i = a.tracer_diff_flux ? __ldg(a.dlnrho + i) * exp_2_rm : 0.0;
         const double r_h = __ldg(a.r_humid + c);
-#pragma unroll 1
+#pragma unroll kTracerUnroll64
         for (int n = 4; n <= 8; n++) {
             const Star Q = load_star(a.Yin[n], c, sI, sJ);
             const double coef = (n == 8) ? a.diff_co2_re_inv : a.diff_prec_re_inv;

@@ -130,6 +130,13 @@ __device__ __forceinline__ float forcing(const RK4MArgs& a, int f, long long c, 
 
 }  // namespace
 
+// the tracer loop of the right-hand side (c, cloud, ice, gr, co2): unrolled, the five
+// stencil loads of one tracer can be issued before the previous tracer's arithmetic
+#ifndef ATHAD_RK4M_TRACER_UNROLL
+#define ATHAD_RK4M_TRACER_UNROLL 1
+#endif
+constexpr int kTracerUnroll = ATHAD_RK4M_TRACER_UNROLL;
+
 // One cell of one stage.  Shared by the single-grid kernel and the batched persistent
 // kernel (k_batch.cu), which reads each member's arguments from shared memory.
 template <int STAGE>
@@ -375,7 +382,7 @@ __device__ __forceinline__ void rk4m_cell(const RK4MArgs& a, int i, int j, int k
         const float dlnrho_dr_i = a.tracer_diff_flux ? (float)__ldg(a.dlnrho + i) * exp_2_rm : 0.0f;
         double r_h = 0.0;
         if (STAGE == 1) r_h = __ldg(a.r_humid + c);
-#pragma unroll 1
+#pragma unroll kTracerUnroll
         for (int n = 4; n <= 8; n++) {
             const StarF Q = load_star<STAGE>(a, n, c, sI, sJ);
             const float coef = (n == 8) ? a.diff_co2_re_inv : a.diff_prec_re_inv;
