@@ -221,58 +221,101 @@ __global__ void __launch_bounds__(128) mg_sub_mean_kernel(int nk, int pitch, lon
 // column solved exactly with the horizontal neighbours fixed.  The seam neighbour of the
 // columns k = 0 and k = nk-1 is read from `seam` (the two seam planes before the
 // half-sweep), because with an odd nk both ends have the same colour.
-template <bool SMEM>
+//
+// A CTA takes 32 columns of one row j with four warps: warp q forms the right-hand sides
+// (the horizontal neighbours fixed) of levels q, q+4, ... of all 32 columns and stages them
+// in shared memory with the elimination factors, so the independent loads of a column run
+// four ways in parallel; then warp 0 runs the two sequential recurrences of its 32 columns
+// out of shared memory.  Element (i, column t) of an array is at [i * 32 + t].
+__device__ __forceinline__ float smooth_rhs(const OpView<float>& o, const float* __restrict__ f,
+                                            const float* __restrict__ e, const float* __restrict__ seam,
+                                            int i, int j, int k, int kc, long long c)
+{
+    const int ij = i * o.nj + j;
+    float s = f[c];
+    if (j > 0) s -= o.cj[(ij - 1) * 3 + kc] * e[c - o.pitch];
+    if (j < o.nj - 1) s -= o.cj[ij * 3 + kc] * e[c + o.pitch];
+    const float ckv = o.ck[ij];
+    if (k > 0) s -= ckv * e[c - 1];
+    if (k < o.nk - 1) s -= ckv * e[c + 1];
+    if (k == 0) s -= o.cs[ij] * seam[(long long)(o.ni * o.nj) + ij];        // plane k = nk-1
+    else if (k == o.nk - 1) s -= o.cs[ij] * seam[ij];                       // plane k = 0
+    return s;
+}
+
+__global__ void __launch_bounds__(128) mg_smooth_split_kernel(OpView<float> o, const float* __restrict__ tm,
+                                                              const float* __restrict__ tc, const float* __restrict__ f,
+                                                              float* __restrict__ e, const float* __restrict__ seam,
+                                                              int colour)
+{
+    extern __shared__ float sm[];   // rhs, forward factor m_i, coupling c_{i-1}, backward factor: [4][ni][32]
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    const int j = blockIdx.y;
+    const int k = 2 * (blockIdx.x * 32 + lane) + ((colour + j) & 1);
+    const bool valid = k < o.nk;
+    const int ni = o.ni;
+    float* rhs = sm;
+    float* fm = sm + ni * 32;
+    float* fc = sm + 2 * ni * 32;
+    float* bc = sm + 3 * ni * 32;
+    const int kc = valid ? kclass(k, o.nk) : 1;
+    const long long c0 = (long long)j * o.pitch + k;
+    if (valid) {
+#pragma unroll 2
+        for (int i = q; i < ni; i += 4) {
+            const int ij = i * o.nj + j;
+            rhs[i * 32 + lane] = smooth_rhs(o, f, e, seam, i, j, k, kc, i * o.plane + c0);
+            fm[i * 32 + lane] = tm[ij * 3 + kc];
+            fc[i * 32 + lane] = (i > 0) ? o.ci[(ij - o.nj) * 3 + kc] : 0.0f;
+            bc[i * 32 + lane] = tc[ij * 3 + kc];
+        }
+    }
+    __syncthreads();
+    if (q != 0 || !valid) return;
+    // forward elimination: y_i = (rhs_i - c_{i-1} y_{i-1}) m_i
+    float y = 0.0f;
+    for (int i = 0; i < ni; i++) {
+        float s = rhs[i * 32 + lane];
+        if (i > 0) s -= fc[i * 32 + lane] * y;
+        y = s * fm[i * 32 + lane];
+        rhs[i * 32 + lane] = y;
+    }
+    // back substitution: x_i = y_i - c'_i x_{i+1}
+    float x = y;
+    e[(ni - 1) * o.plane + c0] = x;
+    for (int i = ni - 2; i >= 0; i--) {
+        x = rhs[i * 32 + lane] - bc[i * 32 + lane] * x;
+        e[i * o.plane + c0] = x;
+    }
+}
+
+// the same relaxation one thread per column with the right-hand side in the scratch field
+// w, for columns too tall for the shared-memory form
 __global__ void __launch_bounds__(128) mg_smooth_kernel(OpView<float> o, const float* __restrict__ tm,
                                                         const float* __restrict__ tc, const float* __restrict__ f,
                                                         float* __restrict__ e, const float* __restrict__ seam,
                                                         float* __restrict__ w, int colour)
 {
-    // SMEM: the thread's column (rhs, then the forward-elimination values) lives in shared
-    // memory, so the two sequential recurrences wait on shared-memory latency instead of
-    // global memory; column element i of thread t is col[i * blockDim.x + t]
-    extern __shared__ float col_smem[];
     const int j = blockIdx.y;
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((colour + j) & 1);
     if (k >= o.nk) return;
     const int kc = kclass(k, o.nk);
     const long long c0 = (long long)j * o.pitch + k;
-    float* col = col_smem + threadIdx.x;
-    const int cs = blockDim.x;
-    // the column's right-hand side with the horizontal neighbours fixed: independent loads,
-    // stored in shared memory or the scratch field w (a separate array, so the loads of e
-    // are not ordered behind these stores)
 #pragma unroll 4
-    for (int i = 0; i < o.ni; i++) {
-        const long long c = i * o.plane + c0;
-        const int ij = i * o.nj + j;
-        float s = f[c];
-        if (j > 0) s -= o.cj[(ij - 1) * 3 + kc] * e[c - o.pitch];
-        if (j < o.nj - 1) s -= o.cj[ij * 3 + kc] * e[c + o.pitch];
-        const float ckv = o.ck[ij];
-        if (k > 0) s -= ckv * e[c - 1];
-        if (k < o.nk - 1) s -= ckv * e[c + 1];
-        if (k == 0) s -= o.cs[ij] * seam[(long long)(o.ni * o.nj) + ij];        // plane k = nk-1
-        else if (k == o.nk - 1) s -= o.cs[ij] * seam[ij];                       // plane k = 0
-        if (SMEM) col[i * cs] = s;
-        else w[c] = s;
-    }
-    // forward elimination: y_i = (rhs_i - ci_{i-1} y_{i-1}) m_i
+    for (int i = 0; i < o.ni; i++) w[i * o.plane + c0] = smooth_rhs(o, f, e, seam, i, j, k, kc, i * o.plane + c0);
     float y_prev = 0.0f;
     for (int i = 0; i < o.ni; i++) {
         const long long c = i * o.plane + c0;
         const int ij = i * o.nj + j;
-        float s = SMEM ? col[i * cs] : w[c];
+        float s = w[c];
         if (i > 0) s -= o.ci[(ij - o.nj) * 3 + kc] * y_prev;
         y_prev = s * tm[ij * 3 + kc];
-        if (SMEM) col[i * cs] = y_prev;
-        else e[c] = y_prev;
+        e[c] = y_prev;
     }
-    // back substitution: x_i = y_i - c'_i x_{i+1}
     float x_next = y_prev;
-    if (SMEM) e[(o.ni - 1) * o.plane + c0] = x_next;
     for (int i = o.ni - 2; i >= 0; i--) {
         const long long c = i * o.plane + c0;
-        x_next = (SMEM ? col[i * cs] : e[c]) - tc[(i * o.nj + j) * 3 + kc] * x_next;
+        x_next = e[c] - tc[(i * o.nj + j) * 3 + kc] * x_next;
         e[c] = x_next;
     }
 }
@@ -589,13 +632,13 @@ void smooth(const MGLevel& L, float* seam, int colour, cudaStream_t st)
 {
     mg_seam_copy_kernel<<<(L.ni * L.nj + 255) / 256, 256, 0, st>>>(L.ni, L.nj, L.nk, L.pitch, L.plane, L.e, seam);
     const int half = (L.nk + 1) / 2;
-    const size_t smem = (size_t)128 * L.ni * sizeof(float);
+    const size_t smem = (size_t)4 * 32 * L.ni * sizeof(float);
     if (smem <= 48 * 1024)   // columns of up to 96 levels in shared memory
-        mg_smooth_kernel<true><<<dim3((half + 127) / 128, L.nj), 128, smem, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
-                                                                              L.r, colour);
+        mg_smooth_split_kernel<<<dim3((half + 31) / 32, L.nj), 128, smem, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
+                                                                              colour);
     else
-        mg_smooth_kernel<false><<<dim3((half + 127) / 128, L.nj), 128, 0, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
-                                                                             L.r, colour);
+        mg_smooth_kernel<<<dim3((half + 127) / 128, L.nj), 128, 0, st>>>(L.op, L.tm, L.tc, L.f, L.e, seam,
+                                                                       L.r, colour);
 }
 
 // one V-cycle on level l: L[l].e ~= S_l^-1 L[l].f, starting from zero

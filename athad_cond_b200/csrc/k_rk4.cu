@@ -145,7 +145,7 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 #endif
 
 #ifndef ATHAD_RK4_TRACER_UNROLL
-#define ATHAD_RK4_TRACER_UNROLL 1
+#define ATHAD_RK4_TRACER_UNROLL 5    // 41x181x361: 1.92 ms per step with 1, 1.64 ms with 5
 #endif
 constexpr int kTracerUnroll64 = ATHAD_RK4_TRACER_UNROLL;
 
