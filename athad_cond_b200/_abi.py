@@ -121,6 +121,12 @@ class SolveReport(ctypes.Structure):
                 ("precond_levels", ctypes.c_int32), ("pad0", ctypes.c_int32), ("seconds", ctypes.c_double)]
 
 
+class CeilingReport(ctypes.Structure):
+    """athad_ceiling_report"""
+    _fields_ = [("n_ceiling", ctypes.c_int64), ("pad0", ctypes.c_int64),
+                ("q_clipped", ctypes.c_double), ("w_air", ctypes.c_double)]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -161,6 +167,8 @@ SIGNATURES = {
     "athad_two_cat_ice_scheme": (ctypes.c_int, [_P]),
     "athad_multilayer_radiation": (ctypes.c_int, [_P]),
     "athad_radiative_heating": (ctypes.c_int, [_P, ctypes.c_double]),
+    "athad_moist_caps": (ctypes.c_int, [_P]),
+    "athad_vapour_ceiling": (ctypes.c_int, [_P, _P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),

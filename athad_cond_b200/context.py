@@ -168,6 +168,16 @@ class GpuAtmosphere:
         """AtomUtils::damp_wiggles(field, i, j, k) (lib/Utils.cpp:429-531)."""
         self._check(self.lib.athad_damp_wiggles(self._h, FIELD[name]))
 
+    def moist_caps(self):
+        """precipitationSum and the source / condensate caps (cAtmosphereModel.cpp:1265-1334)."""
+        self._check(self.lib.athad_moist_caps(self._h))
+
+    def vapour_ceiling(self) -> dict:
+        """c in [0, 1 - co2] (cAtmosphereModel.cpp:1369-1391); what it removed."""
+        r = _abi.CeilingReport()
+        self._check(self.lib.athad_vapour_ceiling(self._h, ctypes.byref(r)))
+        return {"n_ceiling": r.n_ceiling, "q_clipped": r.q_clipped, "w_air": r.w_air}
+
     def multilayer_radiation(self):
         """MultiLayerRadiation::run (MultiLayerRadiation.h:56-388): t := radiative equilibrium."""
         self._check(self.lib.athad_multilayer_radiation(self._h))

@@ -788,6 +788,55 @@ athad_status athad_damp_wiggles(athad_ctx* ctx, athad_field f)
     return ATHAD_OK;
 }
 
+static CapsArgs caps_args(athad_ctx* ctx)
+{
+    CapsArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.d = ctx->L.d;
+    double** F = ctx->field;
+    a.c = F[ATHAD_C]; a.cloud = F[ATHAD_CLOUD]; a.ice = F[ATHAD_ICE]; a.co2 = F[ATHAD_CO2];
+    a.p_stat = F[ATHAD_P_STAT];
+    a.P_rain = F[ATHAD_P_RAIN]; a.P_snow = F[ATHAD_P_SNOW]; a.P_graupel = F[ATHAD_P_GRAUPEL];
+    a.P_conv = F[ATHAD_P_CONV]; a.Precipitation = F[ATHAD_PRECIPITATION];
+    const athad_field S[7] = {ATHAD_S_V, ATHAD_S_C, ATHAD_S_I, ATHAD_S_R, ATHAD_S_S, ATHAD_S_G, ATHAD_S_C_C};
+    for (int s = 0; s < 7; s++) a.S[s] = F[S[s]];
+    a.cloud_cap = ctx->p.cloud_cap; a.g = ctx->p.g;
+    a.row_q = ctx->row_sum; a.row_w = ctx->row_cnt;
+    a.count = ctx->counters + 3;
+    a.sums = reinterpret_cast<double*>(ctx->counters + 8);
+    return a;
+}
+
+athad_status athad_moist_caps(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    launch_moist_caps(caps_args(ctx), ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "moist_caps");
+    return ATHAD_OK;
+}
+
+athad_status athad_vapour_ceiling(athad_ctx* ctx, athad_ceiling_report* out)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    CapsArgs a = caps_args(ctx);
+    athad_status s = cuda_check(ctx, cudaMemsetAsync(a.count, 0, sizeof(unsigned long long), ctx->stream),
+                                "vapour_ceiling");
+    if (s != ATHAD_OK) return s;
+    launch_vapour_ceiling(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "vapour_ceiling");
+    if (!out) return ATHAD_OK;
+    unsigned long long h[11];
+    s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, ctx->stream),
+                   "vapour_ceiling report");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "vapour_ceiling sync");
+    if (s != ATHAD_OK) return s;
+    std::memset(out, 0, sizeof *out);
+    out->n_ceiling = (int64_t)h[3];
+    std::memcpy(&out->q_clipped, &h[8], sizeof(double));
+    std::memcpy(&out->w_air, &h[9], sizeof(double));
+    return ATHAD_OK;
+}
+
 static athad_status multilayer_radiation(athad_ctx* ctx)
 {
     const athad_params& p = ctx->p;

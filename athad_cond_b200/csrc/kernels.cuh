@@ -252,6 +252,21 @@ struct RadArgs {
     double albedo_surface, albedo_cloud, rad_equator_short, rad_pole_short;
 };
 void launch_multilayer_radiation(const RadArgs& a, cudaStream_t st);
+
+// the moist iteration's caps and the vapour ceiling (k_caps.cu)
+struct CapsArgs {
+    Dims d;
+    double* c; double* cloud; double* ice; const double* co2; const double* p_stat;
+    const double* P_rain; const double* P_snow; const double* P_graupel; const double* P_conv;
+    double* Precipitation;
+    double* S[7];                 // S_v, S_c, S_i, S_r, S_s, S_g, S_c_c
+    double cloud_cap, g;
+    double* row_q; double* row_w; // [im*jm] per-row partial sums
+    unsigned long long* count;    // cells clamped to the ceiling
+    double* sums;                 // [2]: clipped water, air mass
+};
+void launch_moist_caps(const CapsArgs& a, cudaStream_t st);
+void launch_vapour_ceiling(const CapsArgs& a, cudaStream_t st);
 void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
 
 }  // namespace athad

@@ -200,6 +200,14 @@ typedef struct athad_report {
     double  last_kernel_ms;        /* device time of the last timed entry point          */
 } athad_report;
 
+/* What the vapour ceiling removed in one call (cAtmosphereModel.cpp:1369-1391). */
+typedef struct athad_ceiling_report {
+    int64_t n_ceiling;             /* cells where c was lowered to 1 - co2                 */
+    int64_t pad0;
+    double  q_clipped;             /* sum of the removed mass fraction x layer air mass [kg/m2] */
+    double  w_air;                 /* sum of the layer air masses [kg/m2]                  */
+} athad_ceiling_report;
+
 typedef struct athad_ctx athad_ctx;
 
 /* ---- lifetime -------------------------------------------------------------- */
@@ -331,6 +339,17 @@ athad_status athad_multilayer_radiation(athad_ctx* ctx);
  * (:864-879), t := t (1 - omega_rad) + MultiLayerRadiation(t) omega_rad; the reference's
  * omega_rad is 0.05 (:801). */
 athad_status athad_radiative_heating(athad_ctx* ctx, double omega_rad);
+/* The moist iteration's bookkeeping after the moist convection: UtilsAtm::precipitationSum
+ * (UtilsAtm.h:51-65; Precipitation = P_rain + P_snow + P_graupel + P_conv), the caps of the
+ * microphysics sources S_v, S_c, S_i, S_r, S_s, S_g, S_c_c at +-1e-3 with non-finite values
+ * set to 0 (cAtmosphereModel.cpp:1277-1297), and of cloud + ice at cloud_cap with c, cloud,
+ * ice made finite, non-negative and c <= 1 - co2 (:1310-1334). */
+athad_status athad_moist_caps(athad_ctx* ctx);
+/* Water vapour's ceiling (cAtmosphereModel.cpp:1369-1391): c >= 0 and c <= 1 - co2 in every
+ * cell.  With out non-NULL the call waits for the device and reports the clamped cells, the
+ * air-mass-weighted water removed and the air mass (summed in a fixed order; the reference
+ * accumulates m_q_h2o_clipped += q_clipped / w_air). */
+athad_status athad_vapour_ceiling(athad_ctx* ctx, athad_ceiling_report* out);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

@@ -150,6 +150,12 @@ void or_multilayer_radiation(int im, int jm, int km, const or_params* p, double*
 void or_radiative_heating(int im, int jm, int km, const or_params* p, double omega_rad,
                           double* const* f, double* const* f2);
 
+/* the moist iteration's caps (UtilsAtm.h:51-65, cAtmosphereModel.cpp:1277-1334) and the
+ * vapour ceiling (:1369-1391) with its sums in the reference's serial order */
+void or_moist_caps(int im, int jm, int km, const or_params* p, double* const* f);
+void or_vapour_ceiling(int im, int jm, int km, const or_params* p, double* const* f,
+                       int64_t* n_ceiling, double* q_clipped, double* w_air);
+
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);
 

@@ -396,6 +396,8 @@ void ref_two_cat_ice(void* p) { TwoCatIceScheme(*(cAtmosphereModel*)p).run(); }
 // MultiLayerRadiation::run, and radiation mode 2's apply_radiative_heating (the lambda of
 // cAtmosphereModel.cpp:864-879, which saves t, runs the radiation and blends t toward the
 // radiative equilibrium by omega_rad; restated here around the reference's own run())
+// UtilsAtm::precipitationSum (the only callable part of the moist iteration's caps)
+void ref_precipitation_sum(void* p) { UtilsAtm(*(cAtmosphereModel*)p).precipitationSum(); }
 void ref_mlr(void* p) { MultiLayerRadiation(*(cAtmosphereModel*)p).run(); }
 void ref_radiative_heating(void* p, double omega_rad)
 {

@@ -167,6 +167,19 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_turbulence_run(im, jm, km, ctypes.byref(self.params), int(compat), F, F2)
 
+    def moist_caps(self):
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_moist_caps(im, jm, km, ctypes.byref(self.params), F)
+
+    def vapour_ceiling(self) -> dict:
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        n, q, w = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        lib().or_vapour_ceiling(im, jm, km, ctypes.byref(self.params), F, ctypes.byref(n),
+                                ctypes.byref(q), ctypes.byref(w))
+        return {"n_ceiling": n.value, "q_clipped": q.value, "w_air": w.value}
+
     def multilayer_radiation(self):
         F, F2, _ = self._args()
         im, jm, km = self.shape

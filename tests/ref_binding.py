@@ -120,6 +120,11 @@ class Reference:
     def damp_wiggles(self, name):
         assert self.lib.ref_damp_wiggles(self.h, name.encode()) == 0, name
 
+    def precipitation_sum(self):
+        f = self.lib.ref_precipitation_sum
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
     def mlr(self):
         f = self.lib.ref_mlr
         f.argtypes = [ctypes.c_void_p]

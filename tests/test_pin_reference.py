@@ -259,3 +259,23 @@ def test_multilayer_radiation_bit_exact(ref):
     R.radiative_heating(0.05)
     o.radiative_heating(0.05)
     assert_identical(R, o, ["t", "radiation", "epsilon"])
+
+
+def test_precipitation_sum_bit_exact(ref):
+    """UtilsAtm::precipitationSum against the oracle's moist caps (the caps themselves are
+    inline code of run_3D_loop; on this state's values within the caps they change nothing
+    but Precipitation)."""
+    R, o = fresh(ref)
+    im, jm, km = R.shape
+    rng = np.random.default_rng(71)
+    for n in ("P_rain", "P_snow", "P_graupel", "P_conv"):
+        a = 1e-4 * rng.random((im, jm, km))
+        R.set(n, a)
+        o.f[n][...] = a
+    for n in ("S_v", "S_c", "S_i", "S_r", "S_s", "S_g", "S_c_c"):
+        z = np.zeros((im, jm, km))
+        R.set(n, z)
+        o.f[n][...] = z
+    R.precipitation_sum()
+    o.moist_caps()
+    assert np.array_equal(R.get("Precipitation"), o.f["Precipitation"])
