@@ -50,7 +50,7 @@ E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", 
 RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62 + 11), 1: 8 + 472 + 264 + 264 + 332 + 88}
 # DRAM bytes (read + write) of one RK4 step (level mean and the four stage launches, the
 # time-level copy fused) measured by ncu (profiles/rk4_stage_41x181x361.md): per form, grid
-RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.883e9, ("mixed", (41, 181, 361)): 4.566e9}
+RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.871e9, ("mixed", (41, 181, 361)): 3.871e9}
 # fields compared between the two forms after the timed iterations: the 11 prognostics and
 # the diagnosed pressure and densities
 ERR_FIELDS = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
