@@ -127,6 +127,12 @@ class CeilingReport(ctypes.Structure):
                 ("q_clipped", ctypes.c_double), ("w_air", ctypes.c_double)]
 
 
+class MinMaxReport(ctypes.Structure):
+    """athad_min_max_report"""
+    _fields_ = [("max", ctypes.c_double), ("min", ctypes.c_double)] + [
+        (n, ctypes.c_int32) for n in ("imax", "jmax", "kmax", "imin", "jmin", "kmin")]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -169,6 +175,9 @@ SIGNATURES = {
     "athad_radiative_heating": (ctypes.c_int, [_P, ctypes.c_double]),
     "athad_moist_caps": (ctypes.c_int, [_P]),
     "athad_vapour_ceiling": (ctypes.c_int, [_P, _P]),
+    "athad_min_max": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "athad_checkpoint_begin": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),
+    "athad_checkpoint_wait": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
     "athad_project_initial_velocity": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "athad_saturation_adjust": (ctypes.c_int, [_P]),

@@ -178,6 +178,27 @@ class GpuAtmosphere:
         self._check(self.lib.athad_vapour_ceiling(self._h, ctypes.byref(r)))
         return {"n_ceiling": r.n_ceiling, "q_clipped": r.q_clipped, "w_air": r.w_air}
 
+    def min_max(self, name: str) -> dict:
+        """searchMinMax_3D (MinMax_Atm.cpp:51-109) of one field."""
+        r = _abi.MinMaxReport()
+        self._check(self.lib.athad_min_max(self._h, FIELD[name], ctypes.byref(r)))
+        return {"max": r.max, "min": r.min, "at_max": (r.imax, r.jmax, r.kmax),
+                "at_min": (r.imin, r.jmin, r.kmin)}
+
+    def checkpoint_begin(self, names):
+        """Snapshot the named fields and copy them to page-locked host arrays on a side
+        stream (athad_checkpoint_begin); the arrays are valid after checkpoint_wait()."""
+        import torch
+        bufs = {n: torch.empty(self.shape, dtype=torch.float64, pin_memory=True) for n in names}
+        ids = (ctypes.c_int32 * len(names))(*[FIELD[n] for n in names])
+        ptrs = (ctypes.c_void_p * len(names))(*[bufs[n].data_ptr() for n in names])
+        self._check(self.lib.athad_checkpoint_begin(self._h, ids, len(names), ptrs))
+        self._ckpt = (ids, ptrs, bufs)       # kept alive until the copies are done
+        return {n: b.numpy() for n, b in bufs.items()}
+
+    def checkpoint_wait(self):
+        self._check(self.lib.athad_checkpoint_wait(self._h))
+
     def multilayer_radiation(self):
         """MultiLayerRadiation::run (MultiLayerRadiation.h:56-388): t := radiative equilibrium."""
         self._check(self.lib.athad_multilayer_radiation(self._h))

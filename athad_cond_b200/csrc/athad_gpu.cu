@@ -309,6 +309,13 @@ athad_status athad_destroy(athad_ctx* ctx)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->ckpt_stream) {
+        cudaStreamSynchronize(ctx->ckpt_stream);
+        cudaStreamDestroy(ctx->ckpt_stream);
+        cudaEventDestroy(ctx->ckpt_ready);
+        cudaEventDestroy(ctx->ckpt_done);
+        cudaFree(ctx->ckpt_buf);
+    }
     mg_free(ctx->mg);
     cudaFree(ctx->slab);
     cudaStreamDestroy(ctx->own_stream);
@@ -835,6 +842,85 @@ athad_status athad_vapour_ceiling(athad_ctx* ctx, athad_ceiling_report* out)
     std::memcpy(&out->q_clipped, &h[8], sizeof(double));
     std::memcpy(&out->w_air, &h[9], sizeof(double));
     return ATHAD_OK;
+}
+
+athad_status athad_min_max(athad_ctx* ctx, athad_field f, athad_min_max_report* out)
+{
+    if (!ctx || !out || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "min_max: bad argument");
+    const Dims& d = ctx->L.d;
+    double* out_v = reinterpret_cast<double*>(ctx->counters + 12);
+    long long* out_a = reinterpret_cast<long long*>(ctx->counters + 14);
+    launch_min_max(d, ctx->field[f], ctx->stB[0], out_v, out_a, ctx->stream);   // stage buffer B: scratch
+    ATHAD_CHECK_LAUNCH(ctx, "min_max");
+    unsigned long long h[4];
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters + 12, sizeof h, cudaMemcpyDeviceToHost,
+                                                     ctx->stream), "min_max report");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "min_max sync");
+    if (s != ATHAD_OK) return s;
+    std::memset(out, 0, sizeof *out);
+    double v[2];
+    long long at[2];
+    std::memcpy(v, h, sizeof v);
+    std::memcpy(at, h + 2, sizeof at);
+    const long long plane = (long long)d.jm * d.km;
+    if (at[0] >= 0) {   // MinMax_Atm.cpp:75-76: no finite value -> 0 at (0, 0, 0)
+        out->max = v[0];
+        out->imax = (int32_t)(at[0] / plane); out->jmax = (int32_t)(at[0] / d.km % d.jm); out->kmax = (int32_t)(at[0] % d.km);
+    }
+    if (at[1] >= 0) {
+        out->min = v[1];
+        out->imin = (int32_t)(at[1] / plane); out->jmin = (int32_t)(at[1] / d.km % d.jm); out->kmin = (int32_t)(at[1] % d.km);
+    }
+    return ATHAD_OK;
+}
+
+athad_status athad_checkpoint_begin(athad_ctx* ctx, const int32_t* fields, int32_t n, double* const* hosts)
+{
+    if (!ctx || n < 0 || (n > 0 && (!fields || !hosts))) return fail(ctx, ATHAD_ERR_INVALID, "checkpoint_begin: bad argument");
+    for (int q = 0; q < n; q++)
+        if (fields[q] < 0 || fields[q] >= ATHAD_NFIELDS || !hosts[q])
+            return fail(ctx, ATHAD_ERR_INVALID, "checkpoint_begin: bad field or host buffer");
+    const Dims& d = ctx->L.d;
+    const size_t fb = ctx->L.field_elems * sizeof(double);
+    athad_status s = ATHAD_OK;
+    if (!ctx->ckpt_stream) {
+        s = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->ckpt_stream, cudaStreamNonBlocking), "checkpoint stream");
+        if (s == ATHAD_OK) s = cuda_check(ctx, cudaEventCreateWithFlags(&ctx->ckpt_ready, cudaEventDisableTiming), "checkpoint event");
+        if (s == ATHAD_OK) s = cuda_check(ctx, cudaEventCreateWithFlags(&ctx->ckpt_done, cudaEventDisableTiming), "checkpoint event");
+        if (s == ATHAD_OK) s = cuda_check(ctx, cudaEventRecord(ctx->ckpt_done, ctx->ckpt_stream), "checkpoint event");
+        if (s != ATHAD_OK) return s;
+    }
+    // the snapshot may still be on its way to the host from the previous checkpoint
+    s = cuda_check(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ckpt_done, 0), "checkpoint wait");
+    if (s != ATHAD_OK) return s;
+    if (n > ctx->ckpt_cap) {
+        s = cuda_check(ctx, cudaStreamSynchronize(ctx->ckpt_stream), "checkpoint sync");
+        if (s != ATHAD_OK) return s;
+        cudaFree(ctx->ckpt_buf);
+        ctx->ckpt_buf = nullptr;
+        ctx->ckpt_cap = 0;
+        s = cuda_check(ctx, cudaMalloc((void**)&ctx->ckpt_buf, (size_t)n * fb), "checkpoint buffer");
+        if (s != ATHAD_OK) return s;
+        ctx->ckpt_cap = n;
+    }
+    for (int q = 0; q < n && s == ATHAD_OK; q++)
+        s = cuda_check(ctx, cudaMemcpyAsync(ctx->ckpt_buf + (size_t)q * ctx->L.field_elems, ctx->field[fields[q]], fb,
+                                            cudaMemcpyDeviceToDevice, ctx->stream), "checkpoint snapshot");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaEventRecord(ctx->ckpt_ready, ctx->stream), "checkpoint event");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamWaitEvent(ctx->ckpt_stream, ctx->ckpt_ready, 0), "checkpoint wait");
+    for (int q = 0; q < n && s == ATHAD_OK; q++)
+        s = cuda_check(ctx, cudaMemcpy2DAsync(hosts[q], d.km * sizeof(double), ctx->ckpt_buf + (size_t)q * ctx->L.field_elems,
+                                              d.pitch * sizeof(double), d.km * sizeof(double), (size_t)d.im * d.jm,
+                                              cudaMemcpyDeviceToHost, ctx->ckpt_stream), "checkpoint download");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaEventRecord(ctx->ckpt_done, ctx->ckpt_stream), "checkpoint event");
+    return s;
+}
+
+athad_status athad_checkpoint_wait(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (!ctx->ckpt_stream) return ATHAD_OK;
+    return cuda_check(ctx, cudaEventSynchronize(ctx->ckpt_done), "checkpoint_wait");
 }
 
 static athad_status multilayer_radiation(athad_ctx* ctx)

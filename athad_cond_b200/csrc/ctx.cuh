@@ -98,6 +98,12 @@ struct athad_ctx {
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
     int* polar_passes = nullptr;              // [jm] zonal filter passes per row
     TurbLevel* turb_lev = nullptr;            // [im] TurbulenceAtm per-level constants
+    // asynchronous checkpoints (athad_checkpoint_begin): a device snapshot of the fields,
+    // copied to the host on a side stream while the compute stream goes on
+    double* ckpt_buf = nullptr;
+    int ckpt_cap = 0;                         // fields the snapshot holds
+    cudaStream_t ckpt_stream = nullptr;
+    cudaEvent_t ckpt_ready = nullptr, ckpt_done = nullptr;
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
     double layer_height1 = 0;   // get_layer_height(1): the first layer's height, float-rounded
     std::vector<double> rad;

@@ -266,6 +266,9 @@ struct CapsArgs {
     double* sums;                 // [2]: clipped water, air mass
 };
 void launch_moist_caps(const CapsArgs& a, cudaStream_t st);
+// searchMinMax_3D (k_diag.cu); scratch holds 32 B per (i, j) row
+void launch_min_max(const Dims& d, const double* x, double* scratch, double* out_v, long long* out_a,
+                    cudaStream_t st);
 void launch_vapour_ceiling(const CapsArgs& a, cudaStream_t st);
 void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
 

@@ -208,6 +208,14 @@ typedef struct athad_ceiling_report {
     double  w_air;                 /* sum of the layer air masses [kg/m2]                  */
 } athad_ceiling_report;
 
+/* cAtmosphereModel::searchMinMax_3D (MinMax_Atm.cpp:51-109): the largest and smallest
+ * finite value of a field and the first cell in (i, j, k) order holding each; 0 at (0, 0, 0)
+ * where the field has none. */
+typedef struct athad_min_max_report {
+    double  max, min;
+    int32_t imax, jmax, kmax, imin, jmin, kmin;
+} athad_min_max_report;
+
 typedef struct athad_ctx athad_ctx;
 
 /* ---- lifetime -------------------------------------------------------------- */
@@ -350,6 +358,21 @@ athad_status athad_moist_caps(athad_ctx* ctx);
  * air-mass-weighted water removed and the air mass (summed in a fixed order; the reference
  * accumulates m_q_h2o_clipped += q_clipped / w_air). */
 athad_status athad_vapour_ceiling(athad_ctx* ctx, athad_ceiling_report* out);
+
+/* ---- diagnostics and checkpoints ----------------------------------------------- */
+
+/* searchMinMax_3D of one field (the values before the reference's unit conversion and
+ * printing, MinMax_Atm.cpp:96-108).  Waits for the device.  Uses an RK4 stage buffer as
+ * scratch. */
+athad_status athad_min_max(athad_ctx* ctx, athad_field f, athad_min_max_report* out);
+/* Checkpoint without stalling the model (the data of save_state, FileIO_Atm.cpp:293-356):
+ * the n fields are snapshot on the device in stream order, then copied into the caller's
+ * host arrays (packed (i, j, k), im*jm*km doubles each; page-locked memory makes the copy
+ * asynchronous) on a side stream while later calls proceed.  The host arrays must stay valid
+ * until athad_checkpoint_wait returns.  The first call, and a call with more fields than
+ * before, allocates the snapshot (n fields of device memory outside the context's slab). */
+athad_status athad_checkpoint_begin(athad_ctx* ctx, const int32_t* fields, int32_t n, double* const* hosts);
+athad_status athad_checkpoint_wait(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
                                             int32_t total_iter_count);
 

@@ -156,6 +156,9 @@ void or_moist_caps(int im, int jm, int km, const or_params* p, double* const* f)
 void or_vapour_ceiling(int im, int jm, int km, const or_params* p, double* const* f,
                        int64_t* n_ceiling, double* q_clipped, double* w_air);
 
+/* searchMinMax_3D, MinMax_Atm.cpp:51-109 */
+void or_min_max(int im, int jm, int km, const double* x, double* out, int* idx);
+
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);
 

@@ -77,3 +77,24 @@ void or_vapour_ceiling(int im, int jm, int km, const or_params* p, double* const
     *q_clipped = qc;
     *w_air = wa;
 }
+
+/* cAtmosphereModel::searchMinMax_3D (MinMax_Atm.cpp:51-109): the largest and smallest finite
+ * value of a field and the first cell, in (i, j, k) order, holding each; 0 where there is
+ * none.  out = max, min; idx = imax, jmax, kmax, imin, jmin, kmin. */
+void or_min_max(int im, int jm, int km, const double* x, double* out, int* idx)
+{
+    double mx = -1.7976931348623157e308, mn = 1.7976931348623157e308;
+    int a[6] = { 0, 0, 0, 0, 0, 0 };
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) {
+                const double v = x[OR_IDX(i, j, k)];
+                if (!isfinite(v)) continue;
+                if (v > mx) { mx = v; a[0] = i; a[1] = j; a[2] = k; }
+                if (v < mn) { mn = v; a[3] = i; a[4] = j; a[5] = k; }
+            }
+    if (mx == -1.7976931348623157e308) mx = 0.0;
+    if (mn == 1.7976931348623157e308) mn = 0.0;
+    out[0] = mx; out[1] = mn;
+    for (int q = 0; q < 6; q++) idx[q] = a[q];
+}

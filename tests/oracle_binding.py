@@ -167,6 +167,14 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_turbulence_run(im, jm, km, ctypes.byref(self.params), int(compat), F, F2)
 
+    def min_max(self, name) -> dict:
+        im, jm, km = self.shape
+        out = (ctypes.c_double * 2)()
+        idx = (ctypes.c_int * 6)()
+        a = np.ascontiguousarray(self.f[name])
+        lib().or_min_max(im, jm, km, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out, idx)
+        return {"max": out[0], "min": out[1], "at_max": tuple(idx[0:3]), "at_min": tuple(idx[3:6])}
+
     def moist_caps(self):
         F, _, _ = self._args()
         im, jm, km = self.shape
