@@ -50,16 +50,79 @@ __device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, dou
     a.S_g[c] = 0.0; a.S_c_c[c] = 0.0;
 }
 
+// The Newton step's saturation curves (thermo.cuh: SaturationH2O.h:68-120, 168-178,
+// 230-255) with the reciprocals they divide by formed once: 1/T per Newton step, shared by
+// the saturation and sublimation curves and the derivative factor, and 1/p per cell.  A
+// product by a reciprocal instead of a quotient moves a result by at most an ulp or two.
+__device__ __forceinline__ double p_sat_r(double T, double invT)
+{
+    if (T >= T_CRIT) return NO_SATURATION;
+    if (T <= 0.0) return 0.0;
+    const double theta = 1.0 - T * (1.0 / T_CRIT);
+    const double sq = sqrt(theta);
+    const double t15 = theta * sq;
+    const double t3 = theta * theta * theta;
+    const double t35 = t3 * sq;
+    const double t4 = t3 * theta;
+    const double t75 = t4 * t3 * sq;
+    const double sum = -7.85951783 * theta + 1.84408259 * t15 + -11.7866497 * t3
+                     + 22.6807411 * t35 + -15.9618719 * t4 + 1.80122502 * t75;
+    return 220640.0 * exp((T_CRIT * invT) * sum);
+}
+__device__ __forceinline__ double p_subl_r(double T, double invT)
+{
+    if (T <= 0.0) return 0.0;
+    const double lt = log(T * (1.0 / T_TRIPLE));
+    const double sum = -0.212144006e2 * exp(0.333333333e-2 * lt)
+                     + 0.273203819e2 * exp(0.120666667e1 * lt)
+                     + -0.610598130e1 * exp(0.170333333e1 * lt);
+    return 6.11657 * exp(sum * (T_TRIPLE * invT));
+}
+__device__ __forceinline__ double q_sat_r(double E, double p, double inv_p, double M_other)
+{
+    if (E == NO_SATURATION) return 1.0;
+    if (!(p > 0.0)) return 0.0;
+    if (E >= p) return 1.0;
+    const double x = E * inv_p;
+    const double num = x * M_H2O;
+    const double den = num + (1.0 - x) * M_other;
+    return (den > 0.0) ? num / den : 1.0;
+}
+__device__ __forceinline__ double dqsat_r(double E, double L, double T, double invT, double p, double inv_p,
+                                          double M_other)
+{
+    if (!(T > 0.0)) return 0.0;
+    if (E == NO_SATURATION || !(p > 0.0) || E >= p) return 0.0;
+    const double x = E * inv_p;
+    const double den = x * M_H2O + (1.0 - x) * M_other;
+    if (!(den > 0.0)) return 0.0;
+    return x * M_H2O * M_other / (den * den) * L * (invT * invT) * (1.0 / R_H2O);
+}
+__device__ __forceinline__ float dqsat_f(double E, float L, float T, double p, double inv_p, float M_other)
+{
+    if (E == NO_SATURATION || !(p > 0.0) || E >= p || !(T > 0.0f)) return 0.0f;
+    const float x = (float)(E * inv_p);
+    const float mh = (float)M_H2O;
+    const float den = x * mh + (1.0f - x) * M_other;
+    if (!(den > 0.0f)) return 0.0f;
+    const float A = x * mh * M_other / (den * den);
+    return A * L / ((float)R_H2O * T * T);
+}
+
 // adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
 // Neither reads a neighbour, so the two passes of the reference fuse into one.
 #ifndef ATHAD_SATADJ_MIN_BLOCKS
-#define ATHAD_SATADJ_MIN_BLOCKS 6   // 80 registers, 6 CTAs of 128 threads per SM
+#define ATHAD_SATADJ_MIN_BLOCKS 7         // FP64 form: 72 registers, 7 CTAs of 128 threads per SM
 #endif
+#ifndef ATHAD_SATADJ_MIN_BLOCKS_MIXED
+#define ATHAD_SATADJ_MIN_BLOCKS_MIXED 8   // mixed form: 64 registers, 8 CTAs (41x181x361 state
+#endif                                    // after 40 iterations: 6 -> 8 CTAs, 1.96 -> 1.89 ms)
 // MIXED: the Newton step's latent heats, heat capacities, derivative factors, gain and
 // damping in FP32; the saturation curves and mass fractions, the state it updates and the
 // clamp-and-fade pass in FP64.
 template <bool MIXED>
-__global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS) saturation_adjust_kernel(const ColumnArgs a)
+__global__ void __launch_bounds__(128, MIXED ? ATHAD_SATADJ_MIN_BLOCKS_MIXED : ATHAD_SATADJ_MIN_BLOCKS)
+saturation_adjust_kernel(const ColumnArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -97,6 +160,7 @@ __global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS) saturation_adjus
                     // deposition weight DEP is 0 and there is no ice its terms are exactly
                     // zero, so skipping them changes no bit.
                     double L_T = MIXED ? (double)thermo_f::latent_heat((float)T) : latent_heat(T);
+                    const double inv_p = 1.0 / p_local;
                     const float M_bg_f = (float)a.M_bg, co2_f = (float)co2, M_other_f = (float)M_other;
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
@@ -113,12 +177,13 @@ __global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS) saturation_adjus
                         const double cp_loc = MIXED ? (double)thermo_f::cp_of((float)q_v_b, co2_f, (float)T, M_bg_f)
                                                     : cp_of(q_v_b, co2, T, a.M_bg);
                         T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
-                        const double E_sat = saturation_pressure(T);
-                        const double q_sat = saturation_mass_fraction(E_sat, p_local, M_other);
+                        const double invT = 1.0 / T;
+                        const double E_sat = p_sat_r(T, invT);
+                        const double q_sat = q_sat_r(E_sat, p_local, inv_p, M_other);
                         const double q_sum = q_c_b + q_i_b;
                         const bool need_ice = (DEP != 0.0) || (q_i_b > 0.0) || (!(q_sum > 1e-12) && !(T >= a.t_0));
-                        const double E_Ice = need_ice ? sublimation_pressure(T) : 0.0;
-                        const double q_Ice = need_ice ? saturation_mass_fraction(E_Ice, p_local, M_other) : 0.0;
+                        const double E_Ice = need_ice ? p_subl_r(T, invT) : 0.0;
+                        const double q_Ice = need_ice ? q_sat_r(E_Ice, p_local, inv_p, M_other) : 0.0;
                         const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
                                                                   : ((T >= a.t_0) ? q_sat : q_Ice);
                         double omega;
@@ -127,16 +192,16 @@ __global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS) saturation_adjus
                             const float cp_g = thermo_f::cp_of((float)q_v_b, co2_f, Tf, M_bg_f);
                             const float L_cnd = thermo_f::latent_heat(Tf);
                             const float L_dep = L_cnd + 3.337e5f;
-                            float Gain = (float)CND * (L_cnd / cp_g) * thermo_f::dqsat_dT_from(E_sat, L_cnd, Tf, p_local, M_other_f);
-                            if (need_ice) Gain += (float)DEP * (L_dep / cp_g) * thermo_f::dqsat_dT_from(E_Ice, L_dep, Tf, p_local, M_other_f);
+                            float Gain = (float)CND * (L_cnd / cp_g) * dqsat_f(E_sat, L_cnd, Tf, p_local, inv_p, M_other_f);
+                            if (need_ice) Gain += (float)DEP * (L_dep / cp_g) * dqsat_f(E_Ice, L_dep, Tf, p_local, inv_p, M_other_f);
                             L_T = (double)L_cnd;
                             omega = (double)(1.0f / (1.0f + Gain));
                         } else {
                             const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
                             const double L_cnd = latent_heat(T);
                             const double L_dep = L_cnd + 3.337e5;
-                            double Gain = CND * (L_cnd / cp_g) * dqsat_dT_from(E_sat, L_cnd, T, p_local, M_other);
-                            if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_dT_from(E_Ice, L_dep, T, p_local, M_other);
+                            double Gain = CND * (L_cnd / cp_g) * dqsat_r(E_sat, L_cnd, T, invT, p_local, inv_p, M_other);
+                            if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_r(E_Ice, L_dep, T, invT, p_local, inv_p, M_other);
                             L_T = L_cnd;
                             omega = 1.0 / (1.0 + Gain);
                         }
@@ -315,13 +380,66 @@ __global__ void densities_profile_kernel(const ColumnArgs a)
     }
 }
 
+// The same rho_bar(i) with one CTA per level: the level's row sums and counts staged in
+// shared memory by the whole CTA, then summed by one thread in the order above (the
+// single-CTA form waits on a global load per row); the log-derivative follows in
+// densities_dlnrho_kernel.
+__global__ void __launch_bounds__(128) densities_level_kernel(const ColumnArgs a)
+{
+    extern __shared__ double rs[];   // [jm] row sums, [jm] counts of level i
+    const Dims& d = a.d;
+    const int i = blockIdx.x;
+    double* rc = rs + d.jm;
+    for (int j = threadIdx.x; j < d.jm; j += blockDim.x) {
+        rs[j] = a.row_sum[i * d.jm + j];
+        rc[j] = a.row_cnt[i * d.jm + j];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double num = 0.0, den = 0.0;
+    for (int j = 0; j <= d.jm / 2; j++) {
+        const int jr = d.jm - 1 - j;
+        if (jr < j) break;
+        const double cl = a.coslat[j];
+        if (jr != j) {
+            num += cl * (rs[j] + rs[jr]);
+            den += cl * (rc[j] + rc[jr]);
+        } else {
+            num += cl * rs[j];
+            den += cl * rc[j];
+        }
+    }
+    const double rb = (den > 0.0) ? num / den : 0.0;
+    a.rho_base[i] = rb;
+    a.row_sum[i * d.jm] = (rb > 0.0) ? log(rb) : 0.0;   // reuse as lnrho store
+}
+
+__global__ void densities_dlnrho_kernel(const ColumnArgs a)
+{
+    const Dims& d = a.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.im) return;
+    const double inv_2dr = a.inv_2dr, inv_dr = a.inv_dr;
+    double v = 0.0;
+    if (i >= 1 && i < d.im - 1) v = (a.row_sum[(i + 1) * d.jm] - a.row_sum[(i - 1) * d.jm]) * inv_2dr;
+    else if (i == 0 && d.im > 1) v = (a.row_sum[1 * d.jm] - a.row_sum[0]) * inv_dr;
+    else if (i == d.im - 1 && d.im > 1) v = (a.row_sum[(d.im - 1) * d.jm] - a.row_sum[(d.im - 2) * d.jm]) * inv_dr;
+    a.dlnrho[i] = v;
+}
+
 void launch_densities(const ColumnArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
     densities_column_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
     const int rows = d.im * d.jm;
     densities_rowsum_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a);
-    densities_profile_kernel<<<1, ((d.im + 31) / 32) * 32, 0, st>>>(a);
+    const size_t smem = 2 * (size_t)d.jm * sizeof(double);
+    if (smem <= 48 * 1024) {
+        densities_level_kernel<<<d.im, 128, smem, st>>>(a);
+        densities_dlnrho_kernel<<<(d.im + 63) / 64, 64, 0, st>>>(a);
+    } else {
+        densities_profile_kernel<<<1, ((d.im + 31) / 32) * 32, 0, st>>>(a);
+    }
 }
 
 }  // namespace athad

@@ -423,8 +423,17 @@ __device__ __forceinline__ void rk4m_cell(const RK4MArgs& a, int i, int j, int k
 #define ATHAD_RK4M_BY 1
 #endif
 
+#ifndef ATHAD_RK4M_MIN_BLOCKS_S1
+#define ATHAD_RK4M_MIN_BLOCKS_S1 ATHAD_RK4M_MIN_BLOCKS   // stage 1 (forcing packing, FP64 reads)
+#endif
+#ifndef ATHAD_RK4M_MIN_BLOCKS_S4
+#define ATHAD_RK4M_MIN_BLOCKS_S4 ATHAD_RK4M_MIN_BLOCKS   // stage 4 (FP64 combination, time level)
+#endif
+
 template <int STAGE>
-__global__ void __launch_bounds__(ATHAD_RK4M_BX * ATHAD_RK4M_BY, ATHAD_RK4M_MIN_BLOCKS * 128 / (ATHAD_RK4M_BX * ATHAD_RK4M_BY))
+__global__ void __launch_bounds__(ATHAD_RK4M_BX * ATHAD_RK4M_BY,
+    (STAGE == 1 ? ATHAD_RK4M_MIN_BLOCKS_S1 : STAGE == 4 ? ATHAD_RK4M_MIN_BLOCKS_S4 : ATHAD_RK4M_MIN_BLOCKS)
+    * 128 / (ATHAD_RK4M_BX * ATHAD_RK4M_BY))
 rk4m_stage_kernel(const RK4MArgs a)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
