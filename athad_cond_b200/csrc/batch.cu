@@ -1,9 +1,12 @@
 // batch.cu - ensembles of contexts advanced together (athad_batch_* of include/athad_gpu.h).
 //
 // A batch owns no field memory: its members are ordinary mixed-precision contexts, each
-// with its own grid and parameters.  One batched model iteration enqueues, on the batch's
-// stream, each member's column physics at that member's own cadence (pressure sweep every
-// 4th iteration, saturation adjustment + moist convection + densities every 2nd), the
+// with its own grid and parameters.  One batched model iteration enqueues each member's
+// column physics at that member's own cadence (pressure sweep every 4th iteration,
+// saturation adjustment + moist convection + densities every 2nd) on a few side streams
+// forked from the batch's stream and joined back to it, so that the small kernels of
+// different members run side by side (a member's column kernels fill only part of the
+// GPU: one thread per column, or latency-bound recurrences), then on the batch's stream the
 // level mean of all members in one launch, the four RK4 stages of all members as one
 // persistent launch each (k_rk4m.cu), with the time-level copy fused into stage 4, and a
 // tiny launch that advances the members' device-side iteration counters.
@@ -42,8 +45,13 @@ struct GraphEntry {
 
 }  // namespace
 
+constexpr int kSideStreams = 8;   // concurrent column-physics lanes of a batched iteration
+
 struct athad_batch {
     std::vector<athad_ctx*> m;
+    std::vector<cudaStream_t> side;     // member q's column physics runs on side[q % size]
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
     std::vector<int32_t> iter;          // host mirror of each member's next iteration number
     std::vector<uint8_t> active;
     athad_batch_step step{};
@@ -87,11 +95,15 @@ static void drop_graphs(athad_batch* b)
 static athad_status enqueue_iteration(athad_batch* b)
 {
     const int n = (int)b->m.size();
+    const int ns = (int)b->side.size();
+    athad_status sf = bcuda(b, cudaEventRecord(b->fork, b->stream), "batch fork");
+    for (int q = 0; q < ns && sf == ATHAD_OK; q++) sf = bcuda(b, cudaStreamWaitEvent(b->side[q], b->fork, 0), "batch fork");
+    if (sf != ATHAD_OK) return sf;
     for (int q = 0; q < n; q++) {
         if (!b->active[q]) continue;
         athad_ctx* c = b->m[q];
         cudaStream_t saved = c->stream;
-        c->stream = b->stream;
+        c->stream = b->side[q % ns];
         const int it = b->iter[q];
         athad_status s = ATHAD_OK;
         if (it % 4 == 0) s = athad_pressure_sweep(c, 1, it);
@@ -102,6 +114,11 @@ static athad_status enqueue_iteration(athad_batch* b)
         }
         c->stream = saved;
         if (s != ATHAD_OK) return bfail(b, s, std::string("member ") + std::to_string(q) + ": " + c->err);
+    }
+    for (int q = 0; q < ns; q++) {   // join: the batched kernels below read every member's state
+        athad_status sj = bcuda(b, cudaEventRecord(b->join[q], b->side[q]), "batch join");
+        if (sj == ATHAD_OK) sj = bcuda(b, cudaStreamWaitEvent(b->stream, b->join[q], 0), "batch join");
+        if (sj != ATHAD_OK) return sj;
     }
     launch_batch_level_mean(b->d_lm, n, b->total_levels, b->max_jm, b->d_step, b->stream);
     athad_status s = bcuda(b, cudaGetLastError(), "batch level mean");
@@ -255,7 +272,21 @@ athad_status athad_batch_create(athad_ctx* const* members, int32_t n_members, co
     if (st == ATHAD_OK) st = bcuda(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, b->stream), "tiles");
     if (st == ATHAD_OK) st = bcuda(b, cudaMemcpyAsync(b->d_lm, lm.data(), sizeof(LevelMeanMember) * n, cudaMemcpyHostToDevice, b->stream), "levels");
     if (st == ATHAD_OK) st = bcuda(b, cudaStreamSynchronize(b->stream), "batch create sync");
+    // the side streams and events of the column-physics fork/join
+    if (st == ATHAD_OK) st = bcuda(b, cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "batch events");
+    const int ns = std::min(n, kSideStreams);
+    for (int q = 0; q < ns && st == ATHAD_OK; q++) {
+        cudaStream_t s = nullptr;
+        cudaEvent_t e = nullptr;
+        st = bcuda(b, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "batch side stream");
+        if (st == ATHAD_OK) b->side.push_back(s);
+        if (st == ATHAD_OK) st = bcuda(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch events");
+        if (st == ATHAD_OK) b->join.push_back(e);
+    }
     if (st != ATHAD_OK) {
+        for (cudaStream_t s : b->side) cudaStreamDestroy(s);
+        for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+        if (b->fork) cudaEventDestroy(b->fork);
         cudaFree(b->dev); cudaStreamDestroy(b->own_stream); delete b;
         return st;
     }
@@ -268,6 +299,9 @@ athad_status athad_batch_destroy(athad_batch* b)
     if (!b) return ATHAD_ERR_INVALID;
     cudaStreamSynchronize(b->stream);
     drop_graphs(b);
+    for (cudaStream_t s : b->side) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
     cudaFree(b->dev);
     cudaStreamDestroy(b->own_stream);
     delete b;

@@ -109,6 +109,36 @@ __device__ __forceinline__ float dqsat_f(double E, float L, float T, double p, d
     return A * L / ((float)R_H2O * T * T);
 }
 
+// The mixture heat capacity of the Newton step (MixtureAtm.h:123-178) with the three
+// Shomate polynomials sharing t, t^2, t^3 and 1/t^2, and products by the reciprocal molar
+// masses: one division instead of six.
+__device__ __forceinline__ double cp_of_r(double c, double co2, double T, double inv_M_b)
+{
+    double q_v, q_c, q_b;
+    split(c, co2, q_v, q_c, q_b);
+    const double t = smin(smax(T, 298.0), 2000.0) * 1.0e-3;
+    const double t2 = t * t, t3 = t2 * t, it2 = 1.0 / t2;
+    const double h2o = 30.09200 + 6.832514 * t + 6.793435 * t2 + -2.534480 * t3 + 0.082139 * it2;
+    const double co2s = 24.99735 + 55.18696 * t + -33.69137 * t2 + 7.948387 * t3 + -0.136638 * it2;
+    const double bg = 28.98641 + 1.853978 * t + -9.647459 * t2 + 16.63537 * t3 + 0.000117 * it2;
+    return q_v * (h2o * (1.0 / M_H2O)) + q_c * (co2s * (1.0 / M_CO2)) + q_b * (bg * inv_M_b);
+}
+__device__ __forceinline__ float cp_of_fr(float c, float co2, float T, float inv_M_b)
+{
+    float q_v = fminf(fmaxf(c, 0.0f), 1.0f), q_c = fminf(fmaxf(co2, 0.0f), 1.0f);
+    const float sum = q_v + q_c;
+    if (sum > 1.0f) { q_v /= sum; q_c /= sum; }
+    const float q_b = fmaxf(0.0f, 1.0f - q_v - q_c);
+    float t = (T < 298.0f) ? 298.0f : T;
+    t = (t > 2000.0f) ? 2000.0f : t;
+    t *= 1.0e-3f;
+    const float t2 = t * t, t3 = t2 * t, it2 = 1.0f / t2;
+    const float h2o = 30.09200f + 6.832514f * t + 6.793435f * t2 + -2.534480f * t3 + 0.082139f * it2;
+    const float co2s = 24.99735f + 55.18696f * t + -33.69137f * t2 + 7.948387f * t3 + -0.136638f * it2;
+    const float bg = 28.98641f + 1.853978f * t + -9.647459f * t2 + 16.63537f * t3 + 0.000117f * it2;
+    return q_v * (h2o * (float)(1.0 / M_H2O)) + q_c * (co2s * (float)(1.0 / M_CO2)) + q_b * (bg * inv_M_b);
+}
+
 // adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
 // Neither reads a neighbour, so the two passes of the reference fuse into one.
 #ifndef ATHAD_SATADJ_MIN_BLOCKS
@@ -161,7 +191,9 @@ saturation_adjust_kernel(const ColumnArgs a)
                     // zero, so skipping them changes no bit.
                     double L_T = MIXED ? (double)thermo_f::latent_heat((float)T) : latent_heat(T);
                     const double inv_p = 1.0 / p_local;
-                    const float M_bg_f = (float)a.M_bg, co2_f = (float)co2, M_other_f = (float)M_other;
+                    const float co2_f = (float)co2, M_other_f = (float)M_other;
+                    const double inv_M_b = 1.0 / a.M_bg;
+                    const float inv_M_b_f = (float)inv_M_b;
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
                         const double DEP = 1.0 - CND;
@@ -174,8 +206,8 @@ saturation_adjust_kernel(const ColumnArgs a)
                         q_v_b += d_q_v;
                         q_c_b = smax(0.0, q_c_b - d_cnd);
                         q_i_b = smax(0.0, q_i_b - d_dep);
-                        const double cp_loc = MIXED ? (double)thermo_f::cp_of((float)q_v_b, co2_f, (float)T, M_bg_f)
-                                                    : cp_of(q_v_b, co2, T, a.M_bg);
+                        const double cp_loc = MIXED ? (double)cp_of_fr((float)q_v_b, co2_f, (float)T, inv_M_b_f)
+                                                    : cp_of_r(q_v_b, co2, T, inv_M_b);
                         T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
                         const double invT = 1.0 / T;
                         const double E_sat = p_sat_r(T, invT);
@@ -189,7 +221,7 @@ saturation_adjust_kernel(const ColumnArgs a)
                         double omega;
                         if (MIXED) {
                             const float Tf = (float)T;
-                            const float cp_g = thermo_f::cp_of((float)q_v_b, co2_f, Tf, M_bg_f);
+                            const float cp_g = cp_of_fr((float)q_v_b, co2_f, Tf, inv_M_b_f);
                             const float L_cnd = thermo_f::latent_heat(Tf);
                             const float L_dep = L_cnd + 3.337e5f;
                             float Gain = (float)CND * (L_cnd / cp_g) * dqsat_f(E_sat, L_cnd, Tf, p_local, inv_p, M_other_f);
@@ -197,7 +229,7 @@ saturation_adjust_kernel(const ColumnArgs a)
                             L_T = (double)L_cnd;
                             omega = (double)(1.0f / (1.0f + Gain));
                         } else {
-                            const double cp_g = cp_of(q_v_b, co2, T, a.M_bg);
+                            const double cp_g = cp_of_r(q_v_b, co2, T, inv_M_b);
                             const double L_cnd = latent_heat(T);
                             const double L_dep = L_cnd + 3.337e5;
                             double Gain = CND * (L_cnd / cp_g) * dqsat_r(E_sat, L_cnd, T, invT, p_local, inv_p, M_other);

@@ -81,16 +81,17 @@ __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
     }
 }
 
-// one colour of the red-black sweep, PressureSolverAtm.h:225-486 (update :475-480)
+// one colour of the red-black sweep, PressureSolverAtm.h:225-486 (update :475-480); thread
+// kk of row (i, j) takes the kk-th cell of the colour, k = 2 kk + ((i + j + COLOUR) & 1),
+// so every lane of a warp updates a cell
 template <int COLOUR>
 __global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
 {
     const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
+    const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((i + j + COLOUR) & 1);
     if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1) return;
-    if (((i + j + k) & 1) != COLOUR) return;
     const long long c = idx3(d, i, j, k);
     const PoiIJ P = a.poi[i * d.jm + j];
     const long long sI = d.plane, sJ = d.pitch;
@@ -170,8 +171,9 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
     const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
-    poisson_colour_kernel<0><<<grid, block, 0, st>>>(a);
-    poisson_colour_kernel<1><<<grid, block, 0, st>>>(a);
+    const dim3 half_grid(((d.km + 1) / 2 + 31) / 32, (d.jm + 7) / 8, d.im);
+    poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
+    poisson_colour_kernel<1><<<half_grid, block, 0, st>>>(a);
     poisson_bc_radial_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
     poisson_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
     poisson_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);

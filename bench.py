@@ -48,6 +48,9 @@ E2E_DOWN = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis", 
 # 8 B, stage 1 296 B read + 176 B written, stages 2-3 176 + 88 B, stage 4 220 + 200 B (the
 # field lists of k_rk4m.cu) = 1428 B.
 RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62 + 11), 1: 8 + 472 + 264 + 264 + 332 + 88}
+# algorithmic bytes per grid point of one pressure call (PressureSolverAtm::run with one
+# sweep): source 24 + 8, sweep 24, ceiling 8
+PRESSURE_BYTES_PER_POINT = 64
 # DRAM bytes (read + write) of one RK4 step (level mean and the four stage launches, the
 # time-level copy fused) measured by ncu (profiles/rk4_stage_41x181x361.md): per form, grid
 RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.871e9, ("mixed", (41, 181, 361)): 3.871e9}
@@ -288,13 +291,18 @@ def run_form(args, rank, world, device, precision):
     torch.cuda.synchronize(device)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    rk_ev = []
+    rk_ev, ps_ev = [], []
     with ClockSampler(device.index if device.index is not None else 0) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             it += 1
             if it % 4 == 0:
+                pa = torch.cuda.Event(enable_timing=True)
+                pb = torch.cuda.Event(enable_timing=True)
+                pa.record(stream)
                 g.PressureSolverAtm_run(total_iter_count=it)
+                pb.record(stream)
+                ps_ev.append((pa, pb))
             if it % 2 == 0:
                 g.SaturationAdjustment_run()
                 g.MoistConvection_run(it)
@@ -310,6 +318,7 @@ def run_form(args, rank, world, device, precision):
     torch.cuda.synchronize(device)
     ms = ev0.elapsed_time(ev1)
     rk_ms = [a.elapsed_time(b) for a, b in rk_ev]
+    ps_ms = [a.elapsed_time(b) for a, b in ps_ev]
     if dist:
         tdist.barrier()
     ms = max_over_ranks(ms, device)
@@ -319,6 +328,7 @@ def run_form(args, rank, world, device, precision):
     res = {"value": whole_job_value(pts, args.steps, world, ms), "ms_per_step": ms / args.steps,
            "rk4_ms": rk_avg, "achieved": fields_per_point * pts / (rk_avg * 1e-3) / 1e9,
            "rk4_bytes_per_point": fields_per_point, "clocks": clk.summary(), "final": final,
+           "pressure_ms": (sum(ps_ms) / len(ps_ms)) if ps_ms else None,
            "e2e_value": None, "h2d": 0, "d2h": 0, "finite": True}
     if args.no_e2e:
         g.close()
@@ -636,6 +646,14 @@ def main():
                       "rk4_gbs": rr["achieved"], "rk4_roofline_frac": rr["achieved"] / peak,
                       "rk4_bytes_per_point": rr["rk4_bytes_per_point"], "e2e": rr["e2e_value"],
                       "finite": rr["finite"]}
+        if rr.get("pressure_ms"):
+            # one pressure call: the source from aux_u/v/w (24 B read, 8 B written per point),
+            # one red-black sweep (p and the source read, p written: 24 B) and the ceiling
+            # pass (8 B read)
+            pgbs = PRESSURE_BYTES_PER_POINT * im * jm * km / (rr["pressure_ms"] * 1e-3) / 1e9
+            summary[f]["pressure_ms"] = rr["pressure_ms"]
+            summary[f]["pressure_gbs"] = pgbs
+            summary[f]["pressure_roofline_frac"] = pgbs / peak
     errors = None
     if "fp64" in runs and "mixed" in runs:
         errors = {"after_iterations": args.warmup + args.steps, "fields": field_errors(
