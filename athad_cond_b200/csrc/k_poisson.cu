@@ -8,48 +8,47 @@
 // every red-black sweep then streams p and that source only.  Within one colour every
 // cell reads only cells of the other colour, so the in-place update is order-independent
 // and the result equals the serial red-black sweep bit for bit.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace athad {
 
-// aux radial boundary, PressureSolverAtm.h:106-121.  c43 and c13 are `const int` members
-// initialised from 4.0/3.0 and 1.0/3.0 (cAtmosphereModel.h:158): 1 and 0.
-__global__ void poisson_aux_bc_kernel(PoissonArgs a)
+// The aux radial boundary (PressureSolverAtm.h:106-121) and the clamped divergence source
+// (:415-473, central differences) in one launch.  c43 and c13 are `const int` members
+// initialised from 4.0/3.0 and 1.0/3.0 (cAtmosphereModel.h:158): 1 and 0.  The threads of
+// the planes i = 0 and im-1 write the boundary values; the interior cells next to them form
+// the same value from the interior instead of reading it, so the launch has no order.
+__device__ __forceinline__ double aux_u_lid(const PoissonArgs& a, double inner, double second)
 {
-    const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1) return;
-    const long long c0 = idx3(d, 0, j, k), c1 = idx3(d, 1, j, k), c2 = idx3(d, 2, j, k);
-    const long long t0 = idx3(d, d.im - 1, j, k), t1 = idx3(d, d.im - 2, j, k), t2 = idx3(d, d.im - 3, j, k);
     const double c43 = 1.0, c13 = 0.0;
-    if (a.anelastic) {
-        a.aux_u[c0] = 0.0;
-        a.aux_u[t0] = 0.0;
-    } else {
-        a.aux_u[c0] = c43 * a.aux_u[c1] - c13 * a.aux_u[c2];
-        a.aux_u[t0] = c43 * a.aux_u[t1] - c13 * a.aux_u[t2];
-    }
-    a.aux_v[c0] = c43 * a.aux_v[c1] - c13 * a.aux_v[c2];
-    a.aux_v[t0] = c43 * a.aux_v[t1] - c13 * a.aux_v[t2];
-    a.aux_w[c0] = c43 * a.aux_w[c1] - c13 * a.aux_w[c2];
-    a.aux_w[t0] = c43 * a.aux_w[t1] - c13 * a.aux_w[t2];
+    return a.anelastic ? 0.0 : c43 * inner - c13 * second;
 }
 
-// clamped divergence source, PressureSolverAtm.h:415-473 (central differences)
 __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
+    const long long sI = d.plane, sJ = d.pitch;
+    if ((i == 0 || i == d.im - 1) && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1) {
+        const double c43 = 1.0, c13 = 0.0;
+        const long long cb = idx3(d, i, j, k);
+        const long long s = (i == 0) ? sI : -sI;   // toward the interior
+        a.aux_u[cb] = aux_u_lid(a, a.aux_u[cb + s], a.aux_u[cb + 2 * s]);
+        a.aux_v[cb] = c43 * a.aux_v[cb + s] - c13 * a.aux_v[cb + 2 * s];
+        a.aux_w[cb] = c43 * a.aux_w[cb + s] - c13 * a.aux_w[cb + 2 * s];
+    }
     bool fluid = (k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1 && i >= 1 && i < d.im - 1);
     bool clamped = false;
     if (fluid) {
         const long long c = idx3(d, i, j, k);
         const PoiIJ P = a.poi[i * d.jm + j];
-        const long long sI = d.plane, sJ = d.pitch;
-        const double du_dr = (__ldg(a.aux_u + c + sI) - __ldg(a.aux_u + c - sI)) * a.inv_2dr;
+        const double u_c = __ldg(a.aux_u + c);
+        const double u_up = (i + 1 == d.im - 1) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c - sI)) : __ldg(a.aux_u + c + sI);
+        const double u_dn = (i - 1 == 0) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c + sI)) : __ldg(a.aux_u + c - sI);
+        const double du_dr = (u_up - u_dn) * a.inv_2dr;
         const double dv_dthe = (__ldg(a.aux_v + c + sJ) - __ldg(a.aux_v + c - sJ)) * a.inv_2dthe;
         const double dw_dphi = (__ldg(a.aux_w + c + 1) - __ldg(a.aux_w + c - 1)) * a.inv_2dphi;
         double div_src = du_dr * P.exp_rm + dv_dthe * P.inv_rm + dw_dphi * P.inv_rmsinthe;
@@ -105,43 +104,66 @@ __global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
             - __ldg(a.src + c)) * P.inv_denom;
 }
 
-// radial boundary (PressureSolverAtm.h:504-526): p[0] = 1*p[1] - 0*p[2], lid copy
-__global__ void poisson_bc_radial_kernel(PoissonArgs a)
+// The three boundary passes (radial, pole, seam, PressureSolverAtm.h:504-552) in one launch.
+// Run in that order, they leave every boundary cell a value that depends on interior cells
+// only: lin(a, b) = 1 * a - 0 * b (c43, c13) for the radial and seam extrapolations, copies
+// for the lid and the poles, the seam the average of its two extrapolations.  Each thread
+// forms the final value of one boundary cell from the interior, which this launch does not
+// write, so the cells need no order.  The face groups overlap at edges and corners, where
+// two threads write the same value.
+__device__ __forceinline__ double bc_lin(double a, double b) { return 1.0 * a - 0.0 * b; }
+
+// after the radial pass, at (i, j, k) with j and k interior
+__device__ __forceinline__ double bc_radial(const Dims& d, const double* p, int i, int j, int k)
 {
-    const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (k >= d.km) return;
-    double* p = a.p;
-    p[idx3(d, 0, j, k)] = 1.0 * p[idx3(d, 1, j, k)] - 0.0 * p[idx3(d, 2, j, k)];
-    p[idx3(d, d.im - 1, j, k)] = p[idx3(d, d.im - 2, j, k)];
+    if (i == 0) return bc_lin(p[idx3(d, 1, j, k)], p[idx3(d, 2, j, k)]);
+    if (i == d.im - 1) return p[idx3(d, d.im - 2, j, k)];
+    return p[idx3(d, i, j, k)];
+}
+// after the radial and pole passes, k interior
+__device__ __forceinline__ double bc_pole(const Dims& d, const double* p, int i, int j, int k)
+{
+    const int jj = (j == 0) ? 1 : (j == d.jm - 1) ? d.jm - 2 : j;
+    return bc_radial(d, p, i, jj, k);
+}
+__device__ __forceinline__ double bc_final(const Dims& d, const double* p, int i, int j, int k)
+{
+    if (k == 0 || k == d.km - 1) {
+        const double r0 = bc_lin(bc_pole(d, p, i, j, 1), bc_pole(d, p, i, j, 2));
+        const double r1 = bc_lin(bc_pole(d, p, i, j, d.km - 2), bc_pole(d, p, i, j, d.km - 3));
+        return (r0 + r1) / 2.0;
+    }
+    return bc_pole(d, p, i, j, k);
 }
 
-// pole copy (:535-541)
-__global__ void poisson_bc_pole_kernel(PoissonArgs a)
+__global__ void __launch_bounds__(128) poisson_bc_kernel(PoissonArgs a)
 {
     const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (k >= d.km) return;
-    double* p = a.p;
-    p[idx3(d, i, 0, k)] = p[idx3(d, i, 1, k)];
-    p[idx3(d, i, d.jm - 1, k)] = p[idx3(d, i, d.jm - 2, k)];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (blockIdx.z == 0) {            // the planes i = 0, im-1
+        if (t >= 2 * d.jm * d.km) return;
+        const int side = t / (d.jm * d.km), r = t % (d.jm * d.km);
+        i = side ? d.im - 1 : 0; j = r / d.km; k = r % d.km;
+    } else if (blockIdx.z == 1) {     // the rows j = 0, jm-1
+        if (t >= 2 * d.im * d.km) return;
+        const int side = t / (d.im * d.km), r = t % (d.im * d.km);
+        j = side ? d.jm - 1 : 0; i = r / d.km; k = r % d.km;
+    } else {                          // the seam columns k = 0, km-1
+        if (t >= 2 * d.im * d.jm) return;
+        const int side = t / (d.im * d.jm), r = t % (d.im * d.jm);
+        k = side ? d.km - 1 : 0; i = r / d.jm; j = r % d.jm;
+    }
+    a.p[idx3(d, i, j, k)] = bc_final(d, a.p, i, j, k);
 }
 
-// seam average (:544-552)
-__global__ void poisson_bc_seam_kernel(PoissonArgs a)
+static void launch_bcs(const PoissonArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= d.jm) return;
-    double* row = a.p + idx3(d, i, j, 0);
-    const double r0 = 1.0 * row[1] - 0.0 * row[2];
-    const double r1 = 1.0 * row[d.km - 2] - 0.0 * row[d.km - 3];
-    const double m = (r0 + r1) / 2.0;
-    row[0] = m;
-    row[d.km - 1] = m;
+    int most = 2 * d.jm * d.km;
+    most = std::max(most, 2 * d.im * d.km);
+    most = std::max(most, 2 * d.im * d.jm);
+    poisson_bc_kernel<<<dim3((most + 127) / 128, 1, 3), 128, 0, st>>>(a);
 }
 
 // |p_dyn| ceiling (:583-594); writes only where the value changes
@@ -162,7 +184,6 @@ __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
 void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
-    poisson_aux_bc_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
     const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
     poisson_src_kernel<<<grid, block, 0, st>>>(a);
 }
@@ -174,19 +195,14 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     const dim3 half_grid(((d.km + 1) / 2 + 31) / 32, (d.jm + 7) / 8, d.im);
     poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
     poisson_colour_kernel<1><<<half_grid, block, 0, st>>>(a);
-    poisson_bc_radial_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
-    poisson_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
-    poisson_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
+    launch_bcs(a, st);
     poisson_ceiling_kernel<<<grid, block, 0, st>>>(a);
 }
 
 // the boundary conditions of a sweep alone (radial, pole, seam), PressureSolverAtm.h:504-552
 void launch_poisson_bcs(const PoissonArgs& a, cudaStream_t st)
 {
-    const Dims& d = a.d;
-    poisson_bc_radial_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
-    poisson_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
-    poisson_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
+    launch_bcs(a, st);
 }
 
 // gradient correction of project_initial_velocity, PressureSolverAtm.h:728-749
