@@ -603,7 +603,11 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
 }
 
 
-__global__ void __launch_bounds__(128) moist_convection_kernel(const MoistArgs X)
+#ifndef ATHAD_MC_BLOCK
+#define ATHAD_MC_BLOCK 128   // columns per CTA
+#endif
+
+__global__ void __launch_bounds__(ATHAD_MC_BLOCK) moist_convection_kernel(const MoistArgs X)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -613,7 +617,7 @@ __global__ void __launch_bounds__(128) moist_convection_kernel(const MoistArgs X
 
 void launch_moist_convection(const MoistArgs& a, cudaStream_t st)
 {
-    moist_convection_kernel<<<dim3((a.d.km + 127) / 128, a.d.jm), 128, 0, st>>>(a);
+    moist_convection_kernel<<<dim3((a.d.km + ATHAD_MC_BLOCK - 1) / ATHAD_MC_BLOCK, a.d.jm), ATHAD_MC_BLOCK, 0, st>>>(a);
 }
 
 }  // namespace athad

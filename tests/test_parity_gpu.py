@@ -226,3 +226,30 @@ def test_fused_time_level_copy_equals_separate_copy(precision):
             b.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5, store_n_level=True)
         for n in PROG + [x + "n" for x in PROG] + ["P_rainn", "P_snown"]:
             assert np.array_equal(a.download(n), b.download(n)), n
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_pressure_boundaries_and_ceiling_bit_exact(grid):
+    """The boundary passes (radial, pole, seam) and the |p| ceiling in the reference's order,
+    with p far beyond the ceiling next to the seam, the poles and the lid, and non-finite
+    values beside them: the seam average is formed from unclamped values and clamped after,
+    a non-finite neighbour turns an extrapolation into NaN and the ceiling into 0."""
+    p = config_params()
+    st = make_state(*grid, seed=17)
+    im, jm, km = grid
+    rng = np.random.default_rng(3)
+    for n in ("aux_u", "aux_v", "aux_w"):
+        st[n] = 1e-3 * rng.standard_normal(st["t"].shape)
+    pd = 40.0 * rng.standard_normal(st["t"].shape)
+    pd[2, 3, 2] = np.inf
+    pd[im - 3, jm - 3, km - 3] = np.nan
+    pd[2, 2, km // 2] = -np.inf
+    st["p_dyn"] = pd
+    for it in (4, 400):          # ceiling 10, then 3
+        o = OracleState(st, p)
+        o.pressure_sweep(n_sweeps=1, total_iter_count=it)
+        with gpu_with(st, p) as g:
+            g.PressureSolverAtm_run(total_iter_count=it, n_sweeps=1)
+            a = g.download("p_dyn")
+        assert np.array_equal(a, o.f["p_dyn"], equal_nan=True), it
+        assert np.max(np.abs(a)) <= (10.0 if it <= 300 else 3.0)
