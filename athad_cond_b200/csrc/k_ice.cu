@@ -15,7 +15,9 @@
 // A column reads nothing of other columns, so the columns run independently.  The reference
 // keeps N_i, m_i, S_nuc and S_i_dep from one cell to the next where a branch does not
 // assign them; the thread carries them the same way.  Compiled without fused multiply-add;
-// pow, exp and the saturation curves are CUDA's.
+// exp, log and the saturation curves are CUDA's.  The reference's pow calls become powers of
+// one root per cell (Rain^(1/18), Snow^(1/26)), cbrt and x * sqrt(x): the same exponents
+// within a few ulp.
 #include "kernels.cuh"
 #include "thermo.cuh"
 
@@ -97,8 +99,6 @@ __global__ void __launch_bounds__(128) ice_columns_kernel(IceArgs a)
     if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1) return;
     const long long sI = d.plane;
     const double t_0 = a.t_0;
-    const double exp_1_6 = 1.0 / 6.0, exp_1_3 = 1.0 / 3.0, exp_2_3 = 2.0 / 3.0;
-    const double exp_8_13 = 8.0 / 13.0, exp_5_26 = 5.0 / 26.0, exp_3_2 = 3.0 / 2.0;
     const double P_max = 50.0 / 86400.0;
     const double Rain_check = a.P_rain[idx3(d, kIcheck, j, k)];
     double m_i = kMiMax, N_i = 0.0, S_nuc = 0.0, S_i_dep = 0.0;
@@ -108,20 +108,36 @@ __global__ void __launch_bounds__(128) ice_columns_kernel(IceArgs a)
         for (int i = d.im - 2; i >= 0; i--) {
             const long long c = idx3(d, i, j, k);
             const double t_u = a.t[c] * t_0;
-            // IceSchemeCommon::canCondense (IceSchemeCommon.h:108-111)
-            if (t_u >= T_CRIT || !(q_sat_at(a, c, saturation_pressure(t_u)) < 1.0)) {
+            // IceSchemeCommon::canCondense (IceSchemeCommon.h:108-111); its q_sat is the
+            // scheme's own
+            if (t_u >= T_CRIT) {
+                evaporate_cell(a, c, t_u);
+                continue;
+            }
+            const double q_sat = q_sat_at(a, c, saturation_pressure(t_u));
+            if (!(q_sat < 1.0)) {
                 evaporate_cell(a, c, t_u);
                 continue;
             }
             const double Rain = a.P_rain[c], Snow = a.P_snow[c];
-            double R49 = 0.0, R79 = 0.0, R139 = 0.0;
+            // the rain powers 4/9, 7/9, 13/9 and 1/6 from one logarithm: r18 = Rain^(1/18)
+            double R49 = 0.0, R79 = 0.0, R139 = 0.0, R16 = 0.0;
             if (Rain > 1e-12) {
-                const double rb = pow(Rain, 1.0 / 9.0);
+                const double r18 = exp(log(Rain) * (1.0 / 18.0));
+                const double rb = r18 * r18;
                 const double r2 = rb * rb;
                 const double r4 = r2 * r2;
-                R49 = r4; R79 = Rain / r2; R139 = Rain * r4;
+                R49 = r4; R79 = Rain / r2; R139 = Rain * r4; R16 = rb * r18;
             }
-            const double q_sat = q_sat_at(a, c, saturation_pressure(t_u));
+            // the snow powers 5/26 and 8/13 = 16/26 from one logarithm: s26 = Snow^(1/26)
+            double S526 = 0.0, S813 = 0.0;
+            if (Snow > 1e-12) {
+                const double s26 = exp(log(Snow) * (1.0 / 26.0));
+                const double s2 = s26 * s26;
+                const double s4 = s2 * s2;
+                const double s8 = s4 * s4;
+                S526 = s4 * s26; S813 = s8 * s8;
+            }
             const double q_Ice = q_sat_at(a, c, sublimation_pressure(t_u));
             const double step = a.step_f[i];
             const double rh = a.r_humid[c];
@@ -141,18 +157,22 @@ __global__ void __launch_bounds__(128) ice_columns_kernel(IceArgs a)
                 S_nuc = 0.0;
             }
             double S_c_frz = (t_u < kThn) ? cl / dt_snow_dim : 0.0;
-            if (cv > q_Ice) S_i_dep = kCiDep * N_i * pow(m_i, exp_1_3) * (cv - q_Ice);
+            if (cv > q_Ice) S_i_dep = kCiDep * N_i * cbrt(m_i) * (cv - q_Ice);
             if (cv < q_Ice) S_i_dep = dmax(-ic / dt_snow_dim, (cv - q_Ice) / dt_snow_dim);
             double S_c_au = (cl > kQcCrit) ? kCcAu * (cl - kQcCrit) : 0.0;
             double S_i_au = (ic > 0.0) ? dmax(kCiAu * ic, 0.0) : 0.0;
-            double S_d_au = (S_i_dep > 0.0) ? S_i_dep / (1.5 * (pow(kMs0 / m_i, exp_2_3) - 1.0)) : 0.0;
+            double S_d_au = 0.0;
+            if (S_i_dep > 0.0) {
+                const double r = cbrt(kMs0 / m_i);
+                S_d_au = S_i_dep / (1.5 * (r * r - 1.0));
+            }
             double S_ac = (t_u >= t_0 && cl > kQcCrit) ? kCac * (cl - kQcCrit) * R79 : 0.0;
             double S_rim = (t_u < t_0) ? kCrimSnow * cl * Snow : 0.0;
             double S_shed = (t_u >= t_0) ? kCrim * cl * Snow : 0.0;
             double S_s_melt = 0.0, S_i_melt = 0.0;
             if (t_u > t_0) {
                 if (Snow > 1e-12) {
-                    S_s_melt = kCsMelt * (1.0 + kBsMelt * pow(Snow, exp_5_26)) * (t_u - t_0) * pow(Snow, exp_1_3);
+                    S_s_melt = kCsMelt * (1.0 + kBsMelt * S526) * (t_u - t_0) * cbrt(Snow);
                     S_s_melt = dmin(S_s_melt, Snow / mass_layer);
                 }
                 S_i_melt = ic / dt_snow_dim;
@@ -165,18 +185,19 @@ __global__ void __launch_bounds__(128) ice_columns_kernel(IceArgs a)
             }
             double S_ev = 0.0;
             if (t_u > t_0 && Rain > 1e-12 && cv < q_sat) {
-                S_ev = kAev * (1.0 + kBev * pow(Rain, exp_1_6)) * (q_sat - cv) * R49;
+                S_ev = kAev * (1.0 + kBev * R16) * (q_sat - cv) * R49;
                 S_ev = dmin(S_ev, Rain / mass_layer);
             }
             double S_s_dep = 0.0;
             if (t_u < t_0 && Snow > 1e-12) {
-                S_s_dep = kCsDep * (1.0 + kBsDep * pow(Snow, exp_5_26)) * (cv - q_Ice) * pow(Snow, exp_8_13);
+                S_s_dep = kCsDep * (1.0 + kBsDep * S526) * (cv - q_Ice) * S813;
                 if (S_s_dep < 0.0) S_s_dep = dmax(S_s_dep, -Snow / mass_layer);
             }
             double S_r_frz = 0.0;
             if (t_u <= t_0) {
                 const double t_frz = dmax(kTrFrz - t_u, 0.0);
-                S_r_frz = kCrFrz * pow(t_frz, exp_3_2) * pow(Rain, exp_3_2);
+                // x^(3/2) = x * sqrt(x) for x >= 0; Rain >= 0 after the init kernel and the flux caps
+                S_r_frz = kCrFrz * (t_frz * sqrt(t_frz)) * (Rain * sqrt(Rain));
             }
             // the cloud-water and cloud-ice limiters (:413-434)
             const double S_cloud_total = S_c_au + S_ac + S_rim + S_c_frz + S_shed;

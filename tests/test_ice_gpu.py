@@ -1,8 +1,9 @@
 """athad_two_cat_ice_scheme (TwoCatIceScheme::run) on the device against the oracle, which is
 pinned bit for bit against the reference (test_pin_reference.py).
 
-Tolerance: 1e-10 of each field's largest magnitude.  The scheme calls pow and exp in every
-cell and the saturation curves (CUDA's exp/log against glibc's pow/exp); the differences
+Tolerance: 1e-10 of each field's largest magnitude.  The scheme forms a dozen fractional
+powers in every cell and the saturation curves (the device from exp/log/cbrt/sqrt, the
+oracle from glibc's pow/exp); the differences
 stay at rounding level because no threshold of the scheme sits on a rounding edge in these
 states.  A mirror-symmetric state stays mirror-symmetric, bit for bit.
 """
