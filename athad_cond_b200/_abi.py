@@ -58,6 +58,7 @@ FIELD_NAMES = [
     "P_conv", "CloudBase", "LevelFreeSinking", "Deep_beg", "Deep_end",
     "P_rainn", "P_snown",
     "radiation", "epsilon",
+    "TempStand", "TempDewPoint", "HumidityRel",
 ]
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 NFIELDS = len(FIELD_NAMES)
@@ -133,6 +134,14 @@ class MinMaxReport(ctypes.Structure):
         (n, ctypes.c_int32) for n in ("imax", "jmax", "kmax", "imin", "jmin", "kmin")]
 
 
+class ResiduumReport(ctypes.Structure):
+    """athad_residuum_report"""
+    _fields_ = [("residuum", ctypes.c_double), ("residuum_prev", ctypes.c_double),
+                ("avg_abs", ctypes.c_double), ("avg_rel", ctypes.c_double),
+                ("n_cells", ctypes.c_int64), ("n_nonfinite", ctypes.c_int64)] + [
+        (n, ctypes.c_int32) for n in ("i_error", "j_error", "k_error", "i_nan", "j_nan", "k_nan")]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -176,6 +185,9 @@ SIGNATURES = {
     "athad_moist_caps": (ctypes.c_int, [_P]),
     "athad_vapour_ceiling": (ctypes.c_int, [_P, _P]),
     "athad_min_max": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "athad_find_residuum": (ctypes.c_int, [_P, ctypes.POINTER(ResiduumReport)]),
+    "athad_set_tropopause_layers": (ctypes.c_int, [_P, _D, ctypes.c_int32]),
+    "athad_stand_atm_dew_point": (ctypes.c_int, [_P]),
     "athad_checkpoint_begin": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),
     "athad_checkpoint_wait": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),

@@ -185,6 +185,26 @@ class GpuAtmosphere:
         return {"max": r.max, "min": r.min, "at_max": (r.imax, r.jmax, r.kmax),
                 "at_min": (r.imin, r.jmin, r.kmin)}
 
+    def find_residuum(self) -> dict:
+        """UtilsAtm::findResiduumAtm (UtilsAtm.h:70-220): the largest rms velocity-derivative
+        residual of the band i = 10..30, its cell, the grid average and the non-finite cells."""
+        r = _abi.ResiduumReport()
+        self._check(self.lib.athad_find_residuum(self._h, ctypes.byref(r)))
+        return {"residuum": r.residuum, "residuum_prev": r.residuum_prev, "avg_abs": r.avg_abs,
+                "avg_rel": r.avg_rel, "n_cells": r.n_cells, "n_nonfinite": r.n_nonfinite,
+                "at": (r.i_error, r.j_error, r.k_error), "first_nonfinite": (r.i_nan, r.j_nan, r.k_nan)}
+
+    def set_tropopause_layers(self, layers):
+        """cAtmosphereModel::tropopause_layers (jm level indices) for stand_atm_dew_point."""
+        a = np.ascontiguousarray(layers, dtype=np.float64)
+        self._check(self.lib.athad_set_tropopause_layers(
+            self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size))
+
+    def stand_atm_dew_point(self):
+        """ThermoAtm::standAtm_DewPoint_HumidRel (ThermoAtm.h:400-516): TempStand,
+        TempDewPoint, HumidityRel."""
+        self._check(self.lib.athad_stand_atm_dew_point(self._h))
+
     def checkpoint_begin(self, names):
         """Snapshot the named fields and copy them to page-locked host arrays on a side
         stream (athad_checkpoint_begin); the arrays are valid after checkpoint_wait()."""

@@ -132,6 +132,9 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     c->coslat = (double*)take(nmax);
     c->step_mc = (double*)take(nmax);
     c->cose = (double*)take(nmax);
+    c->res_sin = (double*)take(nmax);
+    c->rad_d = (double*)take(nmax);
+    c->i_trop = (int*)take((size_t)jm * sizeof(int));
     c->row_sum = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->row_cnt = (double*)take(round_up((size_t)im * jm, 64) * sizeof(double));
     c->counters = (unsigned long long*)take(256);
@@ -281,6 +284,11 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->cose, cose.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "cose");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->polar_passes, polar.data(), jm * sizeof(int), cudaMemcpyHostToDevice, c->stream), "polar passes");
     if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->turb_lev, tlev.data(), im * sizeof(TurbLevel), cudaMemcpyHostToDevice, c->stream), "turbulence levels");
+    // findResiduumAtm's sin(theta) of the running-sum theta, floored at 0.55 (UtilsAtm.h:96)
+    std::vector<double> res_sin(jm);
+    for (int j = 0; j < jm; j++) res_sin[j] = std::max(0.55, std::sin(the[j]));
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->res_sin, res_sin.data(), jm * sizeof(double), cudaMemcpyHostToDevice, c->stream), "res_sin");
+    if (s == ATHAD_OK) s = cuda_check(c, cudaMemcpyAsync(c->rad_d, rad.data(), im * sizeof(double), cudaMemcpyHostToDevice, c->stream), "rad");
     std::vector<GeoF> geof;
     if (s == ATHAD_OK && c->geof) {   // FP32 factors rounded from the FP64 ones (mirror-exact)
         geof.resize(geo.size());
@@ -871,6 +879,92 @@ athad_status athad_min_max(athad_ctx* ctx, athad_field f, athad_min_max_report* 
         out->min = v[1];
         out->imin = (int32_t)(at[1] / plane); out->jmin = (int32_t)(at[1] / d.km % d.jm); out->kmin = (int32_t)(at[1] % d.km);
     }
+    return ATHAD_OK;
+}
+
+athad_status athad_find_residuum(athad_ctx* ctx, athad_residuum_report* out)
+{
+    if (!ctx || !out) return fail(ctx, ATHAD_ERR_INVALID, "find_residuum: bad argument");
+    const Dims& d = ctx->L.d;
+    ResiduumArgs a;
+    a.d = d;
+    a.u = ctx->field[ATHAD_U]; a.v = ctx->field[ATHAD_V]; a.w = ctx->field[ATHAD_W];
+    a.sinthe = ctx->res_sin;
+    a.rad = ctx->rad_d;
+    a.dr = ctx->dr; a.dthe = ctx->dthe; a.dphi = ctx->dphi;
+    a.i0 = 10;                                     // UtilsAtm.h:99
+    a.i1 = std::min(30, d.im - 2);
+    a.scratch = ctx->stB[0];                       // stage buffer B: 48 B per band row
+    a.out = ctx->counters + 16;
+    launch_find_residuum(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "find_residuum");
+    unsigned long long h[6];
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters + 16, sizeof h, cudaMemcpyDeviceToHost,
+                                                     ctx->stream), "find_residuum report");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "find_residuum sync");
+    if (s != ATHAD_OK) return s;
+    std::memset(out, 0, sizeof *out);
+    double mx, sum;
+    std::memcpy(&mx, &h[0], sizeof mx);
+    std::memcpy(&sum, &h[2], sizeof sum);
+    const long long at = (long long)h[1], key = (long long)h[5];
+    out->residuum_prev = ctx->residuum_old;
+    if (at >= 0) {
+        out->residuum = mx;
+        out->i_error = (int32_t)(at / ((long long)d.jm * d.km));
+        out->j_error = (int32_t)(at / d.km % d.jm);
+        out->k_error = (int32_t)(at % d.km);
+    }
+    out->n_cells = (int64_t)h[3];
+    out->n_nonfinite = (int64_t)h[4];
+    out->avg_abs = (out->n_cells > 0) ? sum / (double)out->n_cells : 0.0;   // UtilsAtm.h:175-176
+    out->avg_rel = (out->residuum > 0.0) ? out->avg_abs / out->residuum : 0.0;
+    out->i_nan = out->j_nan = out->k_nan = -1;
+    if (out->n_nonfinite > 0) {
+        out->i_nan = (int32_t)(key % d.im);
+        out->j_nan = (int32_t)(key / d.im / d.km);
+        out->k_nan = (int32_t)(key / d.im % d.km);
+    }
+    ctx->residuum_old = out->residuum;             // set once, after the reduction (:211-213)
+    return ATHAD_OK;
+}
+
+athad_status athad_set_tropopause_layers(athad_ctx* ctx, const double* layers, int32_t n)
+{
+    if (!ctx || !layers) return fail(ctx, ATHAD_ERR_INVALID, "set_tropopause_layers: bad argument");
+    const int im = ctx->grid.im, jm = ctx->grid.jm;
+    if (n != jm) return fail(ctx, ATHAD_ERR_INVALID, "set_tropopause_layers: n must be jm");
+    std::vector<int> lev(jm);
+    for (int j = 0; j < jm; j++) {
+        // ThermoAtm.h:414-419: the equator row takes its northern neighbour's level
+        const double v = (j == (jm - 1) / 2 && j > 0) ? layers[j - 1] : layers[j];
+        if (!(v >= 0.0) || !(v < (double)im)) return fail(ctx, ATHAD_ERR_INVALID, "set_tropopause_layers: level outside [0, im-1]");
+        lev[j] = (int)v;
+    }
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(ctx->i_trop, lev.data(), jm * sizeof(int), cudaMemcpyHostToDevice,
+                                                     ctx->stream), "tropopause levels");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "tropopause levels sync");
+    if (s == ATHAD_OK) ctx->trop_set = true;
+    return s;
+}
+
+athad_status athad_stand_atm_dew_point(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (!ctx->trop_set) return fail(ctx, ATHAD_ERR_INVALID, "stand_atm_dew_point: tropopause layers not set");
+    StandAtmArgs a;
+    a.d = ctx->L.d;
+    a.t = ctx->field[ATHAD_T]; a.c = ctx->field[ATHAD_C]; a.co2 = ctx->field[ATHAD_CO2];
+    a.p_stat = ctx->field[ATHAD_P_STAT];
+    a.height = ctx->height;
+    a.i_trop = ctx->i_trop;
+    a.temp_stand = ctx->field[ATHAD_TEMP_STAND];
+    a.temp_dew = ctx->field[ATHAD_TEMP_DEW_POINT];
+    a.humid_rel = ctx->field[ATHAD_HUMIDITY_REL];
+    a.t_0 = ctx->p.t_0;
+    a.M_bg = ctx->p.M_bg;
+    launch_stand_atm(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "stand_atm_dew_point");
     return ATHAD_OK;
 }
 

@@ -46,7 +46,8 @@ inline Layout make_layout(const athad_grid& g, int precision)
     b += ATHAD_NPROFILES * round_up((size_t)g.im, 64) * sizeof(double);
     b += round_up((size_t)g.im * g.jm * sizeof(GeoIJ), 256);
     b += round_up((size_t)g.im * g.jm * sizeof(PoiIJ), 256);
-    b += 6 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose
+    b += 8 * round_up((size_t)(g.im > g.jm ? g.im : g.jm), 64) * sizeof(double);  // sin_w, height, step, coslat, step_mc, cose, res_sin, rad
+    b += round_up((size_t)g.jm * sizeof(int), 256);                                   // tropopause levels
     b += 2 * round_up((size_t)g.im * g.jm, 64) * sizeof(double);                    // row sums
     b += 256;                                                                         // counters
     b += round_up((size_t)g.jm * sizeof(int), 256);                                   // polar passes
@@ -98,6 +99,11 @@ struct athad_ctx {
     unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
     int* polar_passes = nullptr;              // [jm] zonal filter passes per row
     TurbLevel* turb_lev = nullptr;            // [im] TurbulenceAtm per-level constants
+    double* res_sin = nullptr;                // [jm] findResiduumAtm's max(0.55, sin theta_j)
+    double* rad_d = nullptr;                  // [im] rad.z
+    int* i_trop = nullptr;                    // [jm] tropopause level per row (standAtm)
+    bool trop_set = false;
+    double residuum_old = 1.0e-5;             // cAtmosphereModel.h:164
     // asynchronous checkpoints (athad_checkpoint_begin): a device snapshot of the fields,
     // copied to the host on a side stream while the compute stream goes on
     double* ckpt_buf = nullptr;

@@ -1,14 +1,23 @@
-// k_diag.cu - diagnostics on the device: cAtmosphereModel::searchMinMax_3D
-// (MinMax_Atm.cpp:51-109), the largest and smallest finite value of a field and the first
-// cell in (i, j, k) order holding each.
+// k_diag.cu - diagnostics on the device that read the model state:
 //
-// One warp per (i, j) row scans its longitudes lane-strided, keeping the first position of a
-// strictly larger (smaller) value, and combines lanes preferring the smaller longitude on a
-// tie; one CTA then combines the rows in order, preferring the smaller row.  The result is
-// the serial scan's, whatever the launch shape.
+//   searchMinMax_3D (MinMax_Atm.cpp:51-109): the largest and smallest finite value of a field
+//     and the first cell in (i, j, k) order holding each;
+//   UtilsAtm::findResiduumAtm (UtilsAtm.h:70-220): the largest rms velocity-derivative
+//     residual of the band i = 10..30, its cell, the grid average and the non-finite cells;
+//   ThermoAtm::standAtm_DewPoint_HumidRel (ThermoAtm.h:400-516): standard-atmosphere
+//     temperature, dew point and relative humidity of every cell.
+//
+// The scans run one warp per (i, j) row, lane-strided over the longitudes, keeping the first
+// position of a strictly larger (smaller) value, and combine lanes preferring the smaller
+// longitude on a tie; one CTA then combines the rows in order, preferring the smaller row.
+// Positions are the serial scan's whatever the launch shape; sums run in a fixed order.
+// Compiled without fused multiply-add: the residuals and the standard-atmosphere profile
+// are the oracle's bit for bit.
 #include <cfloat>
+#include <climits>
 
 #include "kernels.cuh"
+#include "thermo.cuh"
 
 namespace athad {
 
@@ -99,7 +108,152 @@ __global__ void __launch_bounds__(1024) minmax_final_kernel(int rows, const doub
     }
 }
 
+// ---- findResiduumAtm ----------------------------------------------------------------
+
+struct ResRow {
+    Best mx;
+    double sum;
+    long long cnt, nnan, nkey;    // nkey: first non-finite cell's (j*km + k)*im + i
+};
+
+__device__ __forceinline__ ResRow res_combine(ResRow a, ResRow b)
+{
+    ResRow r;
+    r.mx = pick_max(a.mx, b.mx);
+    r.sum = a.sum + b.sum;
+    r.cnt = a.cnt + b.cnt;
+    r.nnan = a.nnan + b.nnan;
+    r.nkey = (b.nkey < a.nkey) ? b.nkey : a.nkey;
+    return r;
+}
+__device__ __forceinline__ ResRow res_shfl(ResRow x, int off)
+{
+    ResRow y;
+    y.mx = shfl(x.mx, off);
+    y.sum = __shfl_xor_sync(0xffffffffu, x.sum, off);
+    y.cnt = __shfl_xor_sync(0xffffffffu, x.cnt, off);
+    y.nnan = __shfl_xor_sync(0xffffffffu, x.nnan, off);
+    y.nkey = __shfl_xor_sync(0xffffffffu, x.nkey, off);
+    return y;
+}
+__device__ __forceinline__ ResRow res_empty() { return ResRow{Best{0.0, -1}, 0.0, 0, 0, LLONG_MAX}; }
+
+// one warp per (i, j) row of the band, j = 1..jm-2; lanes over k = 1..km-2
+__global__ void __launch_bounds__(256) residuum_rows_kernel(ResiduumArgs a, int rows)
+{
+    const Dims& d = a.d;
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= rows) return;
+    const int i = a.i0 + row / (d.jm - 2);
+    const int j = 1 + row % (d.jm - 2);
+    const double rm = a.rad[i];
+    const double exp_rm = 1.0 / (rm + 1.0);
+    const double rmsinthe = rm * a.sinthe[j];
+    const long long base = idx3(d, i, j, 0);
+    const long long sI = d.plane, sJ = d.pitch;
+    ResRow r = res_empty();
+    for (int k = 1 + lane; k < d.km - 1; k += 32) {
+        const long long c = base + k;
+        const double dudr = (a.u[c + sI] - a.u[c - sI]) / (2.0 * a.dr) * exp_rm;
+        const double dvdthe = (a.v[c + sJ] - a.v[c - sJ]) / (2.0 * rm * a.dthe);
+        const double dwdphi = (a.w[c + 1] - a.w[c - 1]) / (2.0 * rmsinthe * a.dphi);
+        const double res = sqrt((dudr * dudr + dvdthe * dvdthe + dwdphi * dwdphi) / 3.0);
+        if (!isfinite(res)) {
+            const long long key = ((long long)j * d.km + k) * d.im + i;
+            if (key < r.nkey) r.nkey = key;
+            r.nnan++;
+            continue;
+        }
+        r.sum += res;
+        r.cnt++;
+        // only residuals above the starting value 0 become the residuum (UtilsAtm.h:133)
+        if (res > 0.0 && (r.mx.at < 0 || res > r.mx.v)) { r.mx.v = res; r.mx.at = ((long long)i * d.jm + j) * d.km + k; }
+    }
+    for (int off = 16; off >= 1; off >>= 1) r = res_combine(r, res_shfl(r, off));
+    if (lane == 0) {
+        double* sv = a.scratch;
+        long long* sl = reinterpret_cast<long long*>(a.scratch);
+        sv[6 * (long long)row + 0] = r.mx.v;
+        sl[6 * (long long)row + 1] = r.mx.at;
+        sv[6 * (long long)row + 2] = r.sum;
+        sl[6 * (long long)row + 3] = r.cnt;
+        sl[6 * (long long)row + 4] = r.nnan;
+        sl[6 * (long long)row + 5] = r.nkey;
+    }
+}
+
+__global__ void __launch_bounds__(1024) residuum_final_kernel(ResiduumArgs a, int rows)
+{
+    const double* sv = a.scratch;
+    const long long* sl = reinterpret_cast<const long long*>(a.scratch);
+    ResRow r = res_empty();
+    for (int q = threadIdx.x; q < rows; q += blockDim.x) {
+        ResRow x{Best{sv[6 * (long long)q], sl[6 * (long long)q + 1]}, sv[6 * (long long)q + 2],
+                 sl[6 * (long long)q + 3], sl[6 * (long long)q + 4], sl[6 * (long long)q + 5]};
+        r = res_combine(r, x);
+    }
+    for (int off = 16; off >= 1; off >>= 1) r = res_combine(r, res_shfl(r, off));
+    __shared__ ResRow part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = r;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int nw = (blockDim.x + 31) >> 5;
+        r = (threadIdx.x < nw) ? part[threadIdx.x] : res_empty();
+        for (int off = 16; off >= 1; off >>= 1) r = res_combine(r, res_shfl(r, off));
+        if (threadIdx.x == 0) {
+            unsigned long long* o = a.out;
+            o[0] = (unsigned long long)__double_as_longlong(r.mx.v);
+            o[1] = (unsigned long long)r.mx.at;
+            o[2] = (unsigned long long)__double_as_longlong(r.sum);
+            o[3] = (unsigned long long)r.cnt;
+            o[4] = (unsigned long long)r.nnan;
+            o[5] = (unsigned long long)r.nkey;
+        }
+    }
+}
+
+// ---- standAtm_DewPoint_HumidRel ------------------------------------------------------
+
+// one thread per cell; every output is a function of the cell and of its column's surface
+// temperature, so the reference's column loop (and its copy of the tropopause value to the
+// levels above it) becomes TempStand = TS_surface - 6.5e-3 * height[min(i, i_trop)]
+__global__ void __launch_bounds__(128) stand_atm_kernel(StandAtmArgs a)
+{
+    using namespace thermo;
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.km) return;
+    const long long c = idx3(d, i, j, k);
+    const double t_0 = a.t_0;
+    const double ts_surface = a.t[idx3(d, 0, j, k)] * t_0 - t_0;
+    const int it = a.i_trop[j];
+    a.temp_stand[c] = ts_surface - 6.5e-3 * a.height[(i <= it) ? i : it];
+    const double t_u = a.t[c] * t_0;
+    const double E = (t_u > t_0) ? saturation_pressure(t_u) : sublimation_pressure(t_u);
+    const double x_v = x_H2O_of(a.c[c], a.co2[c], a.M_bg);
+    double e = x_v * a.p_stat[c];
+    const bool zero_vapour = (e <= 0.0);
+    if (zero_vapour) e = 1e-3;
+    a.temp_dew[c] = dew_point(e) - t_0;
+    a.humid_rel[c] = (E <= 0.0) ? NO_SATURATION : (zero_vapour ? 0.0 : e / E * 100.0);
+}
+
 }  // namespace
+
+void launch_find_residuum(const ResiduumArgs& a, cudaStream_t st)
+{
+    const int rows = (a.i1 >= a.i0 && a.d.jm > 2) ? (a.i1 - a.i0 + 1) * (a.d.jm - 2) : 0;
+    if (rows > 0) residuum_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a, rows);
+    residuum_final_kernel<<<1, 1024, 0, st>>>(a, rows);
+}
+
+void launch_stand_atm(const StandAtmArgs& a, cudaStream_t st)
+{
+    stand_atm_kernel<<<dim3((a.d.km + 127) / 128, a.d.jm, a.d.im), 128, 0, st>>>(a);
+}
 
 void launch_min_max(const Dims& d, const double* x, double* scratch, double* out_v, long long* out_a,
                     cudaStream_t st)

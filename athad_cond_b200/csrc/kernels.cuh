@@ -270,6 +270,32 @@ void launch_moist_caps(const CapsArgs& a, cudaStream_t st);
 void launch_min_max(const Dims& d, const double* x, double* scratch, double* out_v, long long* out_a,
                     cudaStream_t st);
 void launch_vapour_ceiling(const CapsArgs& a, cudaStream_t st);
+
+// findResiduumAtm (k_diag.cu).  scratch: 48 B per (i, j) row of the band; out: [6] words =
+// residuum, its linear (i, j, k) position, sum, finite count, non-finite count, first
+// non-finite key ((j*km + k)*im + i)
+struct ResiduumArgs {
+    Dims d;
+    const double* u; const double* v; const double* w;
+    const double* sinthe;         // [jm] max(0.55, sin theta_j), theta the running sum
+    const double* rad;            // [im] rad.z
+    double dr, dthe, dphi;
+    int i0, i1;                   // the band, inclusive
+    double* scratch;
+    unsigned long long* out;
+};
+void launch_find_residuum(const ResiduumArgs& a, cudaStream_t st);
+
+// standAtm_DewPoint_HumidRel (k_diag.cu)
+struct StandAtmArgs {
+    Dims d;
+    const double* t; const double* c; const double* co2; const double* p_stat;
+    const double* height;         // [im] get_layer_height
+    const int* i_trop;            // [jm] tropopause level per row
+    double* temp_stand; double* temp_dew; double* humid_rel;
+    double t_0, M_bg;
+};
+void launch_stand_atm(const StandAtmArgs& a, cudaStream_t st);
 void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
 
 }  // namespace athad

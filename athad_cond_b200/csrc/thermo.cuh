@@ -165,6 +165,31 @@ ATHAD_HD double M_nonwater(double c, double co2, double M_b)   // MixtureAtm.h:2
     return (inv > 0.0) ? 1.0 / inv : M_b;
 }
 
+// the water vapour mole fraction, MixtureAtm.h:181-187 (M_of) and :220-225 (x_H2O_of)
+ATHAD_HD double x_H2O_of(double c, double co2, double M_b)
+{
+    double q_v, q_c, q_b;
+    split(c, co2, q_v, q_c, q_b);
+    const double inv = q_v / M_H2O + q_c / M_CO2 + q_b / M_b;
+    const double M = (inv > 0.0) ? 1.0 / inv : M_b;
+    return q_v * M / M_H2O;
+}
+
+// SaturationH2O::dewPoint (SaturationH2O.h:189-202): bisection of the saturation curve
+// (liquid above the triple point, ice below) on [150 K, T_crit], 60 halvings
+ATHAD_HD double dew_point(double e)
+{
+    if (!(e > 0.0)) return 0.0;
+    if (e >= 220640.0) return T_CRIT;
+    double lo = 150.0, hi = T_CRIT;
+    if (saturation_pressure_auto(lo) >= e) return lo;
+    for (int it = 0; it < 60; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (saturation_pressure_auto(mid) < e) lo = mid; else hi = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+
 }  // namespace thermo
 
 // FP32 versions of the parts of the saturation adjustment's Newton step that are not the

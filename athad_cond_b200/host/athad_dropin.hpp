@@ -20,6 +20,8 @@
 //     TwoCatIceSchemeRun(m)     TwoCatIceScheme(m).run()                     :589, 1238
 //     MultiLayerRadiationRun(m) MultiLayerRadiation(m).run()                 :831-1007
 //     RadiativeHeating(m, w)    radiation mode 2's apply_radiative_heating   :864-879, 1656
+//     StandAtmDewPointHumidRel(m) ThermoAtm(m).standAtm_DewPoint_HumidRel()  :636, 1420
+//     FindResiduumAtm(m)        UtilsAtm(m).findResiduumAtm()                :668, 1645
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -329,6 +331,31 @@ public:
         down(ATHAD_PROD, m.prod); down(ATHAD_TKE_SOURCE, m.tke_source);
         down(ATHAD_DIS_SOURCE, m.dis_source);
         down2(ATHAD_2D_VEL_STAR, m.vel_star);
+    }
+
+    // ThermoAtm(m).standAtm_DewPoint_HumidRel() (cAtmosphereModel.cpp:636, 1420), flat
+    // terrain: TempStand, TempDewPoint, HumidityRel from t, c, co2, p_stat and the model's
+    // tropopause levels
+    void StandAtmDewPointHumidRel(Model& m)
+    {
+        check(ctx_, athad_set_tropopause_layers(ctx_, m.tropopause_layers.data(),
+                                                (int32_t)m.tropopause_layers.size()), "set_tropopause_layers");
+        up(ATHAD_T, m.t); up(ATHAD_C, m.c); up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat);
+        check(ctx_, athad_stand_atm_dew_point(ctx_), "stand_atm_dew_point");
+        down(ATHAD_TEMP_STAND, m.TempStand); down(ATHAD_TEMP_DEW_POINT, m.TempDewPoint);
+        down(ATHAD_HUMIDITY_REL, m.HumidityRel);
+    }
+
+    // UtilsAtm(m).findResiduumAtm() (cAtmosphereModel.cpp:668, 1645): the figures the
+    // reference prints, returned instead; m.residuum_old is set as the reference sets it
+    athad_residuum_report FindResiduumAtm(Model& m)
+    {
+        up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w);
+        athad_residuum_report r;
+        check(ctx_, athad_find_residuum(ctx_, &r), "find_residuum");
+        r.residuum_prev = m.residuum_old;
+        m.residuum_old = r.residuum;
+        return r;
     }
 
 private:

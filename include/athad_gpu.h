@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 5
+#define ATHAD_ABI_VERSION 6
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -154,6 +154,9 @@ typedef enum athad_field {
     /* MultiLayerRadiation outputs (MultiLayerRadiation.h): upward long-wave flux per layer
      * [W/m2] and the layer emissivity */
     ATHAD_RADIATION, ATHAD_EPSILON,
+    /* standAtm_DewPoint_HumidRel outputs (ThermoAtm.h:400-516): the standard-atmosphere
+     * temperature [deg C], the dew point [deg C] and the relative humidity [%] */
+    ATHAD_TEMP_STAND, ATHAD_TEMP_DEW_POINT, ATHAD_HUMIDITY_REL,
     ATHAD_NFIELDS
 } athad_field;
 
@@ -215,6 +218,21 @@ typedef struct athad_min_max_report {
     double  max, min;
     int32_t imax, jmax, kmax, imin, jmin, kmin;
 } athad_min_max_report;
+
+/* UtilsAtm::findResiduumAtm (UtilsAtm.h:70-220): the rms of the three normal velocity
+ * derivatives over the band i = 10..30, j and k interior. */
+typedef struct athad_residuum_report {
+    double  residuum;              /* largest finite cell residual (0 if none is above 0)    */
+    double  residuum_prev;         /* the previous call's residuum (residuum_old; 1e-5 before
+                                    * the first call, cAtmosphereModel.h:164)              */
+    double  avg_abs;               /* grid-average residual of the finite cells           */
+    double  avg_rel;               /* avg_abs / residuum (0 if residuum is 0)              */
+    int64_t n_cells;               /* finite cells of the band                            */
+    int64_t n_nonfinite;           /* non-finite residuals, left out of the average        */
+    int32_t i_error, j_error, k_error;   /* cell of the residuum: the smallest (i, j, k) on
+                                          * equal values; 0, 0, 0 if none                 */
+    int32_t i_nan, j_nan, k_nan;   /* first non-finite residual in (j, k, i) order; -1 if none */
+} athad_residuum_report;
 
 typedef struct athad_ctx athad_ctx;
 
@@ -371,6 +389,23 @@ athad_status athad_min_max(athad_ctx* ctx, athad_field f, athad_min_max_report* 
  * asynchronous) on a side stream while later calls proceed.  The host arrays must stay valid
  * until athad_checkpoint_wait returns.  The first call, and a call with more fields than
  * before, allocates the snapshot (n fields of device memory outside the context's slab). */
+/* UtilsAtm::findResiduumAtm (UtilsAtm.h:70-220; call sites cAtmosphereModel.cpp:668,
+ * 1645, the end of every iteration of run_3D_loop).  The band is i = 10..30 as in the reference,
+ * which needs im >= 32; on smaller grids it ends at im - 2 (and is empty for im < 12).  The
+ * sum behind the average runs in a fixed order.  Waits for the device.  Uses an RK4 stage
+ * buffer as scratch. */
+athad_status athad_find_residuum(athad_ctx* ctx, athad_residuum_report* out);
+/* The tropopause level of each colatitude row (cAtmosphereModel::tropopause_layers, built
+ * by init_tropopause_layers, InitValues_Atm.cpp:330-401): jm values, each a level index in
+ * [0, im-1].  Needed once before athad_stand_atm_dew_point. */
+athad_status athad_set_tropopause_layers(athad_ctx* ctx, const double* layers, int32_t n);
+/* ThermoAtm::standAtm_DewPoint_HumidRel (ThermoAtm.h:400-516; call sites
+ * cAtmosphereModel.cpp:636, 1420), flat terrain: ATHAD_TEMP_STAND, ATHAD_TEMP_DEW_POINT
+ * (SaturationH2O::dewPoint's 60-step bisection of the IAPWS curve at the exact vapour
+ * pressure x_H2O p) and ATHAD_HUMIDITY_REL.  The reference takes the equator row's
+ * tropopause from its neighbour by the literal row index 90; here that is the equator row
+ * (jm-1)/2, the same row at jm = 181 and mirror-symmetric on every grid. */
+athad_status athad_stand_atm_dew_point(athad_ctx* ctx);
 athad_status athad_checkpoint_begin(athad_ctx* ctx, const int32_t* fields, int32_t n, double* const* hosts);
 athad_status athad_checkpoint_wait(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,
@@ -391,9 +426,6 @@ athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n);
 /* Counters of the last calls. */
 athad_status athad_get_report(athad_ctx* ctx, athad_report* out);
 
-/* ---- allocation-free entry point --------------------------------------------- */
-
-/* Largest grid athad_density_profile_noalloc accepts: im*jm (i, j) rows, im levels. */
 /* ---- ensembles: batched iteration of many contexts ----------------------------
  * No counterpart in the reference, which runs one grid per process.  A batch advances
  * mixed-precision contexts (members, each with its own grid and parameters) together on
@@ -440,6 +472,9 @@ athad_status athad_batch_set_shape(athad_batch* b, int32_t shape);
 athad_status athad_batch_autotune(athad_batch* b, int32_t reps, int32_t* best_shape,
                                   float* ms_per_shape);
 
+/* ---- allocation-free entry point --------------------------------------------- */
+
+/* Largest grid athad_density_profile_noalloc accepts: im*jm (i, j) rows, im levels. */
 #define ATHAD_NOALLOC_MAX_ROWS 131072
 #define ATHAD_NOALLOC_MAX_IM   1024
 

@@ -71,6 +71,7 @@ enum {
     OF_P_CONV, OF_CLOUD_BASE, OF_LEVEL_FREE_SINKING, OF_DEEP_BEG, OF_DEEP_END,
     OF_P_RAINN, OF_P_SNOWN,
     OF_RADIATION, OF_EPSILON,
+    OF_TEMP_STAND, OF_TEMP_DEW_POINT, OF_HUMIDITY_REL,
     OF_NFIELDS
 };
 enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR,
@@ -159,6 +160,19 @@ void or_vapour_ceiling(int im, int jm, int km, const or_params* p, double* const
 /* searchMinMax_3D, MinMax_Atm.cpp:51-109 */
 void or_min_max(int im, int jm, int km, const double* x, double* out, int* idx);
 
+/* UtilsAtm::findResiduumAtm (UtilsAtm.h:70-220) over the band i = 10 .. min(30, im-2):
+ * out = residuum (largest finite residual, 0 if none above 0), grid-average residual,
+ * average / residuum; cnt = finite cells, non-finite cells; idx = i, j, k of the residuum
+ * (smallest (i, j, k) on ties; 0, 0, 0 if none) and of the first non-finite residual in the
+ * serial (j, k, i) order (-1, -1, -1 if none). */
+void or_find_residuum(int im, int jm, int km, double* const* f, double* out, int64_t* cnt, int* idx);
+
+/* ThermoAtm::standAtm_DewPoint_HumidRel (ThermoAtm.h:400-516), flat terrain: TempStand,
+ * TempDewPoint, HumidityRel.  i_trop[j] = the tropopause level the row uses (the equator
+ * row already given its neighbour's value). */
+void or_stand_atm_dew_point(int im, int jm, int km, const or_params* p, double* const* f,
+                            const int* i_trop);
+
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);
 
@@ -173,6 +187,7 @@ double or_moist_lapse(double T, double p, double M_other, double cp, double R_mi
 double or_cp_of(double c, double co2, double T, double M_bg);
 double or_R_of(double c, double co2, double R_bg);
 double or_M_nonwater(double c, double co2, double M_bg);
+double or_x_H2O_of(double c, double co2, double M_bg);
 void   or_resolve(const double* x8, double* out7);   /* M_mean, R_mix, q_H2O, q_CO2, q_bg, M_bg, R_bg */
 
 #ifdef __cplusplus

@@ -179,6 +179,16 @@ double or_M_nonwater(double c, double co2, double M_b)
     return (inv > 0.0) ? 1.0 / inv : M_b;
 }
 
+/* MixtureAtm.h:181-187 (M_of) and :220-225 (x_H2O_of): the water vapour mole fraction */
+double or_x_H2O_of(double c, double co2, double M_b)
+{
+    double q_v, q_c, q_b;
+    split(c, co2, &q_v, &q_c, &q_b);
+    const double inv = q_v / OR_M_H2O + q_c / OR_M_CO2 + q_b / M_b;
+    const double M = (inv > 0.0) ? 1.0 / inv : M_b;
+    return q_v * M / OR_M_H2O;
+}
+
 /* MixtureAtm.h:82-109.  x8 = H2O, CO2, N2, CH4, NH3, H2, CO, SO2 mole fractions;
  * out7 = M_mean, R_mix, q_H2O, q_CO2, q_bg, M_bg, R_bg. */
 void or_resolve(const double* x, double* out)

@@ -53,6 +53,8 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 10: d.TwoCatIceSchemeRun(*m); break;
             case 11: d.MultiLayerRadiationRun(*m); break;
             case 12: d.RadiativeHeating(*m, 0.05); break;
+            case 13: d.StandAtmDewPointHumidRel(*m); break;
+            case 14: d.FindResiduumAtm(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {
@@ -61,5 +63,8 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
     }
     return 0;
 }
+
+// the model's residuum_old (what findResiduumAtm leaves behind)
+double dropin_residuum_old(void* model) { return ((cAtmosphereModel*)model)->residuum_old; }
 
 }  // extern "C"

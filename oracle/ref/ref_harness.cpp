@@ -89,6 +89,7 @@ Array* field3(cAtmosphereModel* m, const std::string& n)
     F(c_u) F(e_l) F(e_d) F(e_p) F(g_p)
     F(P_conv) F(CloudBase) F(LevelFreeSinking) F(Deep_beg) F(Deep_end)
     F(P_rainn) F(P_snown) F(radiation) F(epsilon)
+    F(TempStand) F(TempDewPoint) F(HumidityRel)
     F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
     F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
 #undef F
@@ -417,6 +418,46 @@ void ref_radiative_heating(void* p, double omega_rad)
             }
 }
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
+
+// ThermoAtm::standAtm_DewPoint_HumidRel, and the tropopause levels it reads (jm doubles)
+void ref_stand_atm(void* p) { ThermoAtm(*(cAtmosphereModel*)p).standAtm_DewPoint_HumidRel(); }
+void ref_tropopause(void* p, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    for (int j = 0; j < m->jm; j++) out[j] = m->tropopause_layers[j];
+}
+
+// UtilsAtm::findResiduumAtm.  It reports through its printout (and keeps the residuum in
+// residuum_old), so the printout is captured and read back: out = residuum (exact),
+// residuum_old before the call, grid average (8 significant digits); idx = i, j, k of the
+// residuum, the finite cell count, the non-finite count (0 when the warning is absent).
+void ref_residuum(void* p, double* out, long long* idx)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    out[1] = m->residuum_old;
+    std::ostringstream cap;
+    std::streambuf* prev = std::cout.rdbuf(cap.rdbuf());
+    UtilsAtm(*m).findResiduumAtm();
+    std::cout.rdbuf(prev);
+    const std::string txt = cap.str();
+    out[0] = m->residuum_old;
+    auto after = [&](const char* key) -> std::string {
+        const size_t at = txt.find(key);
+        return (at == std::string::npos) ? std::string() : txt.substr(at + std::strlen(key));
+    };
+    std::string t = after("i_error = ");
+    idx[0] = t.empty() ? -1 : std::atoll(t.c_str());
+    t = after("j_error = ");
+    idx[1] = t.empty() ? -1 : std::atoll(t.c_str());
+    t = after("k_error = ");
+    idx[2] = t.empty() ? -1 : std::atoll(t.c_str());
+    t = after("grid average absolute error = ");
+    out[2] = t.empty() ? -1.0 : std::atof(t.c_str());
+    const size_t lp = t.find('(');
+    idx[3] = (lp == std::string::npos) ? -1 : std::atoll(t.c_str() + lp + 1);
+    t = after("WARNING \xe2\x80\x94 ");
+    idx[4] = t.empty() ? 0 : std::atoll(t.c_str());
+}
 
 // RHS_Atmosphere_Turb at one cell on the current state, with the CellGeometry the RK4
 // driver builds (RungeKutta_Atm_Turb.cpp:92-135).  out = rhs_t..rhs_dis (11), aux_u/v/w,

@@ -175,6 +175,25 @@ class OracleState:
         lib().or_min_max(im, jm, km, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out, idx)
         return {"max": out[0], "min": out[1], "at_max": tuple(idx[0:3]), "at_min": tuple(idx[3:6])}
 
+    def find_residuum(self) -> dict:
+        """or_find_residuum: UtilsAtm::findResiduumAtm."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        out = (ctypes.c_double * 3)()
+        cnt = (ctypes.c_int64 * 2)()
+        idx = (ctypes.c_int * 6)()
+        lib().or_find_residuum(im, jm, km, F, out, cnt, idx)
+        return {"residuum": out[0], "avg_abs": out[1], "avg_rel": out[2], "n_cells": cnt[0],
+                "n_nonfinite": cnt[1], "at": tuple(idx[0:3]), "first_nonfinite": tuple(idx[3:6])}
+
+    def stand_atm_dew_point(self, i_trop):
+        """or_stand_atm_dew_point: ThermoAtm::standAtm_DewPoint_HumidRel with the rows'
+        tropopause levels i_trop (the equator row's already taken from its neighbour)."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lev = (ctypes.c_int * jm)(*[int(x) for x in i_trop])
+        lib().or_stand_atm_dew_point(im, jm, km, ctypes.byref(self.params), F, lev)
+
     def moist_caps(self):
         F, _, _ = self._args()
         im, jm, km = self.shape

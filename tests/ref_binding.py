@@ -140,6 +140,43 @@ class Reference:
         f.argtypes = [ctypes.c_void_p]
         f(self.h)
 
+    def stand_atm(self):
+        """ThermoAtm::standAtm_DewPoint_HumidRel."""
+        f = self.lib.ref_stand_atm
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
+    def tropopause_layers(self):
+        out = np.empty(self.shape[1])
+        f = self.lib.ref_tropopause
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        f(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def find_residuum(self, threads=1) -> dict:
+        """UtilsAtm::findResiduumAtm, read back from its printout (one thread by default, so
+        the printed first non-finite cell and equal-value choices follow the serial order)."""
+        out = (ctypes.c_double * 3)()
+        idx = (ctypes.c_longlong * 5)()
+        f = self.lib.ref_residuum
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+        if threads:
+            self.lib.ref_set_threads(threads)
+        try:
+            f(self.h, out, idx)
+        finally:
+            if threads and self.threads:
+                self.lib.ref_set_threads(self.threads)
+        return {"residuum": out[0], "residuum_prev": out[1], "avg_abs_8": out[2],
+                "at": tuple(idx[0:3]), "n_cells": idx[3], "n_nonfinite": idx[4]}
+
+    def residuum_old(self) -> float:
+        """The model's residuum_old (needs the drop-in library)."""
+        f = self.lib.dropin_residuum_old
+        f.argtypes = [ctypes.c_void_p]
+        f.restype = ctypes.c_double
+        return f(self.h)
+
     def set_turb_model(self, name: str):
         f = self.lib.ref_set_turb_model
         f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]

@@ -206,3 +206,28 @@ def test_dropin_radiation(model):
         for n, (a, b) in out.items():
             assert relerr(a, b) <= 1e-12, (what, n, relerr(a, b))
     reset(R, snap)
+
+
+def test_dropin_stand_atm_dew_point(model):
+    """ThermoAtm::standAtm_DewPoint_HumidRel through the adapter against the reference's own
+    call: TempStand bit for bit, the dew point and relative humidity within 1e-12 (CUDA's exp,
+    log and sqrt against glibc's pow and exp in the saturation curves)."""
+    R, snap = model
+    names = ["TempStand", "TempDewPoint", "HumidityRel"]
+    out = run_both(R, snap, R.stand_atm, lambda: R.dropin(13), names)
+    reset(R, snap)
+    assert np.array_equal(*out["TempStand"])
+    for n in names[1:]:
+        a, b = out[n]
+        assert relerr(a, b) <= 1e-12, (n, relerr(a, b))
+
+
+def test_dropin_find_residuum(model):
+    """UtilsAtm::findResiduumAtm through the adapter: the residuum it leaves in residuum_old
+    is the reference's, bit for bit."""
+    R, snap = model
+    reset(R, snap)
+    want = R.find_residuum(threads=1)["residuum"]
+    reset(R, snap)
+    R.dropin(14)
+    assert R.residuum_old() == want

@@ -11,7 +11,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
   * the filters after the RK4 step and the moist iteration's damp_wiggles;
   * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
-  * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating.
+  * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating;
+  * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -279,3 +280,47 @@ def test_precipitation_sum_bit_exact(ref):
     R.precipitation_sum()
     o.moist_caps()
     assert np.array_equal(R.get("Precipitation"), o.f["Precipitation"])
+
+
+def equator_rule(layers):
+    """ThermoAtm.h:414-419: the equator row (row 90 of the reference's 181) takes its
+    northern neighbour's tropopause level."""
+    jm = len(layers)
+    return [int(layers[j - 1] if j == (jm - 1) // 2 else layers[j]) for j in range(jm)]
+
+
+def test_stand_atm_dew_point_bit_exact(ref):
+    """ThermoAtm::standAtm_DewPoint_HumidRel on the reference's state, with a supercritical
+    patch (no saturation state: the -1 sentinel) and a dry patch (zero vapour)."""
+    R, o = fresh(ref)
+    t = R.get("t")
+    t[5:8, 20:24, 100:110] = 700.0 / 273.15
+    c = R.get("c")
+    c[10:12, 60:64, 200:210] = 0.0
+    for n, a in (("t", t), ("c", c)):
+        R.set(n, a)
+        o.f[n][...] = a
+    R.stand_atm()
+    o.stand_atm_dew_point(equator_rule(R.tropopause_layers()))
+    assert_identical(R, o, ["TempStand", "TempDewPoint", "HumidityRel"])
+    hr = o.f["HumidityRel"]
+    assert np.all(hr[5:8, 20:24, 100:110] == -1.0) and np.all(hr[10:12, 60:64, 200:210] == 0.0)
+
+
+def test_find_residuum_bit_exact(ref):
+    """UtilsAtm::findResiduumAtm on the reference's state and with a non-finite velocity
+    planted in the band: the residuum and its cell exactly, the finite and non-finite counts,
+    the grid average to the 8 digits the reference prints."""
+    for plant in (False, True):
+        R, o = fresh(ref)
+        if plant:
+            u = R.get("u")
+            u[15, 40, 100] = np.nan
+            R.set("u", u)
+            o.f["u"][...] = u
+        r, q = R.find_residuum(threads=1), o.find_residuum()
+        assert r["residuum"] == q["residuum"] and r["at"] == q["at"]
+        assert r["n_cells"] == q["n_cells"] and r["n_nonfinite"] == q["n_nonfinite"]
+        assert abs(r["avg_abs_8"] - q["avg_abs"]) <= 1e-7 * q["avg_abs"]
+        if plant:
+            assert q["n_nonfinite"] == 2 and q["first_nonfinite"] == (14, 40, 100)
