@@ -59,6 +59,7 @@ FIELD_NAMES = [
     "P_rainn", "P_snown",
     "radiation", "epsilon",
     "TempStand", "TempDewPoint", "HumidityRel",
+    "Q_Latent", "Q_Sensible",
 ]
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 NFIELDS = len(FIELD_NAMES)
@@ -66,7 +67,8 @@ PROGNOSTIC = FIELD_NAMES[0:11]
 N_LEVEL = FIELD_NAMES[11:22]
 
 FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star",
-                 "epsilon_2D", "albedo"]
+                 "epsilon_2D", "albedo", "Evaporation_Dalton", "Evaporation_Meyer",
+                 "Evaporation_Rohwer", "c_fix"]
 FIELD2D = {n: i for i, n in enumerate(FIELD2D_NAMES)}
 PROFILE_NAMES = ["t_ref_level", "rho_base", "dlnrho_dr"]
 PROFILE = {n: i for i, n in enumerate(PROFILE_NAMES)}
@@ -90,7 +92,7 @@ _PARAM_DOUBLES = [
     "M_bg", "R_bg", "R_mix",
     "abl_height", "t_000",
     "sigma", "kappa_H2O", "kappa_CO2", "kappa_bg", "geothermal_flux", "albedo_surface",
-    "albedo_cloud", "rad_equator_short", "rad_pole_short",
+    "albedo_cloud", "rad_equator_short", "rad_pole_short", "coeff_Dalton",
 ]
 
 
@@ -188,6 +190,8 @@ SIGNATURES = {
     "athad_find_residuum": (ctypes.c_int, [_P, ctypes.POINTER(ResiduumReport)]),
     "athad_set_tropopause_layers": (ctypes.c_int, [_P, _D, ctypes.c_int32]),
     "athad_stand_atm_dew_point": (ctypes.c_int, [_P]),
+    "athad_water_vapour_evaporation": (ctypes.c_int, [_P]),
+    "athad_latent_sensible_heat": (ctypes.c_int, [_P]),
     "athad_checkpoint_begin": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),
     "athad_checkpoint_wait": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),
@@ -266,7 +270,7 @@ def config_params() -> Params:
                 co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5, abl_height=10000.0,
                 t_000=253.15, sigma=5.67028e-08, kappa_H2O=0.01, kappa_CO2=0.001, kappa_bg=1e-06,
                 geothermal_flux=150.0, albedo_surface=0.08, albedo_cloud=0.5,
-                rad_equator_short=298.0, rad_pole_short=0.0)
+                rad_equator_short=298.0, rad_pole_short=0.0, coeff_Dalton=0.7)
     for k, v in vals.items():
         setattr(p, k, v)
     R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010

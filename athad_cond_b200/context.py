@@ -205,6 +205,15 @@ class GpuAtmosphere:
         TempDewPoint, HumidityRel."""
         self._check(self.lib.athad_stand_atm_dew_point(self._h))
 
+    def water_vapour_evaporation(self):
+        """ThermoAtm::waterVapourEvaporation (ThermoAtm.h:115-398): surface water vapour
+        relaxed toward the sea's saturation, Evaporation and the three evaporation laws."""
+        self._check(self.lib.athad_water_vapour_evaporation(self._h))
+
+    def latent_sensible_heat(self):
+        """ThermoAtm::latentSensibleHeat (ThermoAtm.h:36-112): Q_Latent, Q_Sensible."""
+        self._check(self.lib.athad_latent_sensible_heat(self._h))
+
     def checkpoint_begin(self, names):
         """Snapshot the named fields and copy them to page-locked host arrays on a side
         stream (athad_checkpoint_begin); the arrays are valid after checkpoint_wait()."""

@@ -45,6 +45,7 @@ void athad_default_params(athad_params* p)
     p->sigma = 5.67028e-08; p->kappa_H2O = 0.01; p->kappa_CO2 = 0.001; p->kappa_bg = 1e-06;
     p->geothermal_flux = 150.0; p->albedo_surface = 0.08; p->albedo_cloud = 0.5;
     p->rad_equator_short = 298.0; p->rad_pole_short = 0.0;
+    p->coeff_Dalton = 0.7;
     const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
     const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
     const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
@@ -965,6 +966,48 @@ athad_status athad_stand_atm_dew_point(athad_ctx* ctx)
     a.M_bg = ctx->p.M_bg;
     launch_stand_atm(a, ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "stand_atm_dew_point");
+    return ATHAD_OK;
+}
+
+static SurfaceArgs surface_args(athad_ctx* ctx)
+{
+    SurfaceArgs a;
+    a.d = ctx->L.d;
+    a.c = ctx->field[ATHAD_C]; a.t = ctx->field[ATHAD_T]; a.co2 = ctx->field[ATHAD_CO2];
+    a.p_stat = ctx->field[ATHAD_P_STAT];
+    a.u = ctx->field[ATHAD_U]; a.v = ctx->field[ATHAD_V]; a.w = ctx->field[ATHAD_W];
+    a.evap = ctx->f2d[ATHAD_2D_EVAPORATION];
+    a.evap_dalton = ctx->f2d[ATHAD_2D_EVAPORATION_DALTON];
+    a.evap_meyer = ctx->f2d[ATHAD_2D_EVAPORATION_MEYER];
+    a.evap_rohwer = ctx->f2d[ATHAD_2D_EVAPORATION_ROHWER];
+    a.c_fix = ctx->f2d[ATHAD_2D_C_FIX];
+    a.q_latent = ctx->field[ATHAD_Q_LATENT];
+    a.q_sensible = ctx->field[ATHAD_Q_SENSIBLE];
+    a.sin_w = ctx->sin_w;
+    a.rad = ctx->rad_d;
+    a.t_0 = ctx->p.t_0; a.u_0 = ctx->p.u_0; a.M_bg = ctx->p.M_bg;
+    a.coeff_Dalton = ctx->p.coeff_Dalton; a.cp_l = ctx->p.cp_l;
+    // the vertical spread of ThermoAtm.h:130-132: r = e^-1 over n_spread = 3 levels
+    const double r = std::exp(-1.0);
+    a.w_norm = (1.0 - r) / (1.0 - std::pow(r, 3 + 1));
+    for (int i = 1; i <= 3; i++) a.weight[i - 1] = std::pow(r, i) * a.w_norm;
+    a.dr = ctx->dr; a.dthe = ctx->dthe; a.dphi = ctx->dphi;
+    return a;
+}
+
+athad_status athad_water_vapour_evaporation(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    launch_water_vapour_evaporation(surface_args(ctx), ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "water_vapour_evaporation");
+    return ATHAD_OK;
+}
+
+athad_status athad_latent_sensible_heat(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    launch_latent_sensible_heat(surface_args(ctx), ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "latent_sensible_heat");
     return ATHAD_OK;
 }
 

@@ -296,6 +296,21 @@ struct StandAtmArgs {
     double t_0, M_bg;
 };
 void launch_stand_atm(const StandAtmArgs& a, cudaStream_t st);
+// waterVapourEvaporation and latentSensibleHeat (k_surface.cu)
+struct SurfaceArgs {
+    Dims d;
+    double* c; const double* t; const double* co2; const double* p_stat;
+    const double* u; const double* v; const double* w;
+    double* evap; double* evap_dalton; double* evap_meyer; double* evap_rohwer; double* c_fix;  // 2-D
+    double* q_latent; double* q_sensible;
+    const double* sin_w;          // [jm] mirror-exact sin theta
+    const double* rad;            // [im] rad.z
+    double t_0, u_0, M_bg, coeff_Dalton, cp_l;
+    double w_norm, weight[3];     // the vertical spread: w_norm, e^-i w_norm for i = 1..3
+    double dr, dthe, dphi;
+};
+void launch_water_vapour_evaporation(const SurfaceArgs& a, cudaStream_t st);
+void launch_latent_sensible_heat(const SurfaceArgs& a, cudaStream_t st);
 void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
 
 }  // namespace athad

@@ -22,6 +22,8 @@
 //     RadiativeHeating(m, w)    radiation mode 2's apply_radiative_heating   :864-879, 1656
 //     StandAtmDewPointHumidRel(m) ThermoAtm(m).standAtm_DewPoint_HumidRel()  :636, 1420
 //     FindResiduumAtm(m)        UtilsAtm(m).findResiduumAtm()                :668, 1645
+//     WaterVapourEvaporation(m) ThermoAtm(m).waterVapourEvaporation()        :637, 1421
+//     LatentSensibleHeat(m)     ThermoAtm(m).latentSensibleHeat()            :638, 1422
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -75,6 +77,7 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.geothermal_flux = m.geothermal_flux; p.albedo_surface = m.albedo_surface;
     p.albedo_cloud = m.albedo_cloud; p.rad_equator_short = m.rad_equator_short;
     p.rad_pole_short = m.rad_pole_short;
+    p.coeff_Dalton = m.coeff_Dalton;
     return p;
 }
 
@@ -256,7 +259,8 @@ public:
         X(ATHAD_S_G, S_g) X(ATHAD_Q_V_U, q_v_u) X(ATHAD_Q_C_U, q_c_u) X(ATHAD_U_U, u_u) \
         X(ATHAD_V_U, v_u) X(ATHAD_W_U, w_u) X(ATHAD_MC_S, s) X(ATHAD_MC_S_U, s_u) X(ATHAD_MC_S_D, s_d) \
         X(ATHAD_M_U, M_u) X(ATHAD_M_D, M_d) X(ATHAD_C_U, c_u) X(ATHAD_E_DD, e_d) X(ATHAD_E_L, e_l) \
-        X(ATHAD_E_P, e_p) X(ATHAD_G_P, g_p) X(ATHAD_P_CONV, P_conv)
+        X(ATHAD_E_P, e_p) X(ATHAD_G_P, g_p) X(ATHAD_P_CONV, P_conv) X(ATHAD_Q_LATENT, Q_Latent) \
+        X(ATHAD_Q_SENSIBLE, Q_Sensible)
 #define ATHAD_BC_UP(F, N) up(F, m.N);
 #define ATHAD_BC_DOWN(F, N) down(F, m.N);
         ATHAD_BC_FIELDS(ATHAD_BC_UP)
@@ -356,6 +360,31 @@ public:
         r.residuum_prev = m.residuum_old;
         m.residuum_old = r.residuum;
         return r;
+    }
+
+    // ThermoAtm(m).waterVapourEvaporation() (cAtmosphereModel.cpp:637, 1421), flat terrain
+    void WaterVapourEvaporation(Model& m)
+    {
+        up(ATHAD_T, m.t); up(ATHAD_C, m.c); up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat);
+        up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w);
+        // a supercritical column leaves c_fix as it was
+        up2(ATHAD_2D_C_FIX, m.c_fix);
+        check(ctx_, athad_water_vapour_evaporation(ctx_), "water_vapour_evaporation");
+        down(ATHAD_C, m.c);
+        down2(ATHAD_2D_EVAPORATION, m.Evaporation);
+        down2(ATHAD_2D_EVAPORATION_DALTON, m.Evaporation_Dalton);
+        down2(ATHAD_2D_EVAPORATION_MEYER, m.Evaporation_Meyer);
+        down2(ATHAD_2D_EVAPORATION_ROHWER, m.Evaporation_Rohwer);
+        down2(ATHAD_2D_C_FIX, m.c_fix);
+    }
+
+    // ThermoAtm(m).latentSensibleHeat() (cAtmosphereModel.cpp:638, 1422), flat terrain
+    void LatentSensibleHeat(Model& m)
+    {
+        up(ATHAD_T, m.t);
+        up(ATHAD_Q_LATENT, m.Q_Latent); up(ATHAD_Q_SENSIBLE, m.Q_Sensible);   // the boundary cells keep theirs
+        check(ctx_, athad_latent_sensible_heat(ctx_), "latent_sensible_heat");
+        down(ATHAD_Q_LATENT, m.Q_Latent); down(ATHAD_Q_SENSIBLE, m.Q_Sensible);
     }
 
 private:

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 6
+#define ATHAD_ABI_VERSION 7
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -118,6 +118,8 @@ typedef struct athad_params {
     double geothermal_flux;      /* [W/m2], 150                                          */
     double albedo_surface, albedo_cloud;
     double rad_equator_short, rad_pole_short;   /* TOA short-wave insolation [W/m2]     */
+    double coeff_Dalton;         /* XML coeff_Dalton, 0.7 (cli/config_cond.xml:54): the
+                                  * Dalton evaporation coefficient (AtomUtils::C_Dalton)   */
 } athad_params;
 
 /* 3-D fields, one per cAtmosphereModel Array member of the same name. */
@@ -157,6 +159,8 @@ typedef enum athad_field {
     /* standAtm_DewPoint_HumidRel outputs (ThermoAtm.h:400-516): the standard-atmosphere
      * temperature [deg C], the dew point [deg C] and the relative humidity [%] */
     ATHAD_TEMP_STAND, ATHAD_TEMP_DEW_POINT, ATHAD_HUMIDITY_REL,
+    /* latentSensibleHeat outputs (ThermoAtm.h:36-112) */
+    ATHAD_Q_LATENT, ATHAD_Q_SENSIBLE,
     ATHAD_NFIELDS
 } athad_field;
 
@@ -170,6 +174,10 @@ typedef enum athad_field2d {
                                      * (TurbulenceAtm::compute_vel_star; wall BC input) */
     ATHAD_2D_EPSILON,               /* Array_2D epsilon_2D, surface-layer emissivity     */
     ATHAD_2D_ALBEDO,                /* Array_2D albedo (MultiLayerRadiation)             */
+    /* waterVapourEvaporation (ThermoAtm.h:115-398) outputs: the three evaporation laws
+     * [mm/d] and the surface water vapour before the update */
+    ATHAD_2D_EVAPORATION_DALTON, ATHAD_2D_EVAPORATION_MEYER, ATHAD_2D_EVAPORATION_ROHWER,
+    ATHAD_2D_C_FIX,
     ATHAD_NFIELDS2D
 } athad_field2d;
 
@@ -406,6 +414,18 @@ athad_status athad_set_tropopause_layers(athad_ctx* ctx, const double* layers, i
  * tropopause from its neighbour by the literal row index 90; here that is the equator row
  * (jm-1)/2, the same row at jm = 181 and mirror-symmetric on every grid. */
 athad_status athad_stand_atm_dew_point(athad_ctx* ctx);
+/* ThermoAtm::waterVapourEvaporation (ThermoAtm.h:115-398; call sites
+ * cAtmosphereModel.cpp:637, 1421), flat terrain: the sea surface as a saturation boundary.
+ * Per (j, k) column below the critical temperature, the surface water vapour relaxes toward
+ * the sea's saturation mass fraction and the change spreads over levels 1-3 with weights
+ * e^-i, capped at each level's saturation; the Dalton, Meyer and Rohwer evaporation rates of
+ * the saturation deficit are reported (ATHAD_2D_EVAPORATION = Dalton's).  The reference's
+ * Earth branch after this block is unreachable and not built. */
+athad_status athad_water_vapour_evaporation(athad_ctx* ctx);
+/* ThermoAtm::latentSensibleHeat (ThermoAtm.h:36-112; call sites cAtmosphereModel.cpp:638,
+ * 1422): Q_Latent zeroed at the surface, Q_Sensible = cp_l t_0 |grad t| / sqrt(3) in the
+ * interior. */
+athad_status athad_latent_sensible_heat(athad_ctx* ctx);
 athad_status athad_checkpoint_begin(athad_ctx* ctx, const int32_t* fields, int32_t n, double* const* hosts);
 athad_status athad_checkpoint_wait(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,

@@ -45,6 +45,7 @@ typedef struct or_params {
     double abl_height, t_000;
     double sigma, kappa_H2O, kappa_CO2, kappa_bg, geothermal_flux, albedo_surface, albedo_cloud;
     double rad_equator_short, rad_pole_short;
+    double coeff_Dalton;
 } or_params;
 
 typedef struct or_step {
@@ -72,10 +73,12 @@ enum {
     OF_P_RAINN, OF_P_SNOWN,
     OF_RADIATION, OF_EPSILON,
     OF_TEMP_STAND, OF_TEMP_DEW_POINT, OF_HUMIDITY_REL,
+    OF_Q_LATENT, OF_Q_SENSIBLE,
     OF_NFIELDS
 };
 enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR,
-       OF2_EPSILON, OF2_ALBEDO, OF2_N };
+       OF2_EPSILON, OF2_ALBEDO, OF2_EVAPORATION_DALTON, OF2_EVAPORATION_MEYER,
+       OF2_EVAPORATION_ROHWER, OF2_C_FIX, OF2_N };
 enum { OFP_T_REF_LEVEL = 0, OFP_RHO_BASE, OFP_DLNRHO_DR, OFP_N };
 
 size_t or_params_size(void);
@@ -172,6 +175,12 @@ void or_find_residuum(int im, int jm, int km, double* const* f, double* out, int
  * row already given its neighbour's value). */
 void or_stand_atm_dew_point(int im, int jm, int km, const or_params* p, double* const* f,
                             const int* i_trop);
+
+/* ThermoAtm::waterVapourEvaporation (ThermoAtm.h:115-398) and ::latentSensibleHeat
+ * (:36-112), flat terrain */
+void or_water_vapour_evaporation(int im, int jm, int km, const or_params* p, double* const* f,
+                                 double* const* f2);
+void or_latent_sensible_heat(int im, int jm, int km, const or_params* p, int compat, double* const* f);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

@@ -6,8 +6,8 @@
  *
  * Only the fields the device context holds are treated; the reference's diagnostic
  * arrays in the same lists (radiation, PrecipitableWaterLocal, CoriolisForce,
- * CentrifugalForce, BuoyancyForce, PresGradForce, Q_Latent, Q_Sensible) are not state of
- * the hot path.  c43 and c13 are `const int` members initialised from 4.0/3.0 and 1.0/3.0
+ * CentrifugalForce, BuoyancyForce, PresGradForce) are not state of the hot path; Q_Latent
+ * and Q_Sensible (latentSensibleHeat's outputs) are treated.  c43 and c13 are `const int` members initialised from 4.0/3.0 and 1.0/3.0
  * (cAtmosphereModel.h:158), i.e. 1 and 0, and are applied as such.
  */
 #include "or_internal.h"
@@ -16,7 +16,7 @@ static const int bc_both_cubic[] = {            /* BC_Atm.h:567-574, Pattern A *
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U,
     OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_M_U, OF_M_D
+    OF_M_U, OF_M_D, OF_Q_LATENT, OF_Q_SENSIBLE
 };
 static const int bc_vn_bot[] = { OF_U, OF_V, OF_W, OF_P_CONV };   /* :586-590, Pattern B */
 static const int bc_cubic_bot_vn_top[] = {      /* :599-603, Pattern C */
@@ -30,13 +30,13 @@ static const int bc_theta[] = {                 /* :760-776 */
     OF_CO2, OF_TKE, OF_DIS, OF_NUE, OF_PROD, OF_TKE_SOURCE, OF_DIS_SOURCE,
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U, OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P
+    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE
 };
 static const int bc_phi_avg[] = {               /* :806-817 */
     OF_T, OF_P_STAT, OF_R_HUMID, OF_R_DRY, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR, OF_CO2,
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U, OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P
+    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE
 };
 static const int bc_phi_extrap[] = { OF_TKE, OF_DIS, OF_NUE, OF_PROD, OF_TKE_SOURCE, OF_DIS_SOURCE };  /* :822-825 */
 

@@ -55,6 +55,8 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 12: d.RadiativeHeating(*m, 0.05); break;
             case 13: d.StandAtmDewPointHumidRel(*m); break;
             case 14: d.FindResiduumAtm(*m); break;
+            case 15: d.WaterVapourEvaporation(*m); break;
+            case 16: d.LatentSensibleHeat(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

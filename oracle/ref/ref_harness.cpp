@@ -89,7 +89,7 @@ Array* field3(cAtmosphereModel* m, const std::string& n)
     F(c_u) F(e_l) F(e_d) F(e_p) F(g_p)
     F(P_conv) F(CloudBase) F(LevelFreeSinking) F(Deep_beg) F(Deep_end)
     F(P_rainn) F(P_snown) F(radiation) F(epsilon)
-    F(TempStand) F(TempDewPoint) F(HumidityRel)
+    F(TempStand) F(TempDewPoint) F(HumidityRel) F(Q_Latent) F(Q_Sensible)
     F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
     F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
 #undef F
@@ -104,6 +104,10 @@ Array_2D* field2(cAtmosphereModel* m, const std::string& n)
     if (n == "vel_star") return &m->vel_star;
     if (n == "epsilon_2D") return &m->epsilon_2D;
     if (n == "albedo") return &m->albedo;
+    if (n == "Evaporation_Dalton") return &m->Evaporation_Dalton;
+    if (n == "Evaporation_Meyer") return &m->Evaporation_Meyer;
+    if (n == "Evaporation_Rohwer") return &m->Evaporation_Rohwer;
+    if (n == "c_fix") return &m->c_fix;
     return nullptr;
 }
 
@@ -418,6 +422,10 @@ void ref_radiative_heating(void* p, double omega_rad)
             }
 }
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
+
+// ThermoAtm::waterVapourEvaporation and ::latentSensibleHeat
+void ref_evaporation(void* p) { ThermoAtm(*(cAtmosphereModel*)p).waterVapourEvaporation(); }
+void ref_latent_sensible(void* p) { ThermoAtm(*(cAtmosphereModel*)p).latentSensibleHeat(); }
 
 // ThermoAtm::standAtm_DewPoint_HumidRel, and the tropopause levels it reads (jm doubles)
 void ref_stand_atm(void* p) { ThermoAtm(*(cAtmosphereModel*)p).standAtm_DewPoint_HumidRel(); }

@@ -186,6 +186,19 @@ class OracleState:
         return {"residuum": out[0], "avg_abs": out[1], "avg_rel": out[2], "n_cells": cnt[0],
                 "n_nonfinite": cnt[1], "at": tuple(idx[0:3]), "first_nonfinite": tuple(idx[3:6])}
 
+    def water_vapour_evaporation(self):
+        """or_water_vapour_evaporation: ThermoAtm::waterVapourEvaporation."""
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_water_vapour_evaporation(im, jm, km, ctypes.byref(self.params), F, F2)
+
+    def latent_sensible_heat(self, compat=0):
+        """or_latent_sensible_heat: ThermoAtm::latentSensibleHeat; compat=1 the reference's
+        (not mirror-exact) sin table."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        lib().or_latent_sensible_heat(im, jm, km, ctypes.byref(self.params), int(compat), F)
+
     def stand_atm_dew_point(self, i_trop):
         """or_stand_atm_dew_point: ThermoAtm::standAtm_DewPoint_HumidRel with the rows'
         tropopause levels i_trop (the equator row's already taken from its neighbour)."""

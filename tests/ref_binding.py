@@ -140,6 +140,18 @@ class Reference:
         f.argtypes = [ctypes.c_void_p]
         f(self.h)
 
+    def evaporation(self):
+        """ThermoAtm::waterVapourEvaporation."""
+        f = self.lib.ref_evaporation
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
+    def latent_sensible(self):
+        """ThermoAtm::latentSensibleHeat."""
+        f = self.lib.ref_latent_sensible
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
     def stand_atm(self):
         """ThermoAtm::standAtm_DewPoint_HumidRel."""
         f = self.lib.ref_stand_atm

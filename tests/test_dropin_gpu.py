@@ -231,3 +231,25 @@ def test_dropin_find_residuum(model):
     reset(R, snap)
     R.dropin(14)
     assert R.residuum_old() == want
+
+
+def test_dropin_surface_fluxes(model):
+    """ThermoAtm::waterVapourEvaporation and ::latentSensibleHeat through the adapter against
+    the reference's own calls: c and the evaporation fields within 1e-12 (CUDA's exp, log and
+    sqrt against glibc's pow and exp), Q_Sensible within 1e-12 (the reference's sin(theta)
+    table is not mirror-exact; the device's is)."""
+    R, snap = model
+    out = run_both(R, snap, R.evaporation, lambda: R.dropin(15), ["c"])
+    a, b = out["c"]
+    assert relerr(a, b) <= 1e-12
+    reset(R, snap)
+    R.evaporation()
+    want = {n: R.get2(n) for n in ("Evaporation", "Evaporation_Meyer", "c_fix")}
+    reset(R, snap)
+    R.dropin(15)
+    for n, b in want.items():
+        assert relerr(R.get2(n), b) <= 1e-12, n
+    out = run_both(R, snap, R.latent_sensible, lambda: R.dropin(16), ["Q_Sensible", "Q_Latent"])
+    reset(R, snap)
+    for n, (a, b) in out.items():
+        assert relerr(a, b) <= 1e-12, (n, relerr(a, b))

@@ -12,7 +12,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * the filters after the RK4 step and the moist iteration's damp_wiggles;
   * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
   * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating;
-  * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm.
+  * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm;
+  * the surface fluxes waterVapourEvaporation and latentSensibleHeat.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -324,3 +325,27 @@ def test_find_residuum_bit_exact(ref):
         assert abs(r["avg_abs_8"] - q["avg_abs"]) <= 1e-7 * q["avg_abs"]
         if plant:
             assert q["n_nonfinite"] == 2 and q["first_nonfinite"] == (14, 40, 100)
+
+
+def test_surface_fluxes_bit_exact(ref):
+    """ThermoAtm::waterVapourEvaporation (with one supercritical surface column, where the
+    reference leaves c and c_fix alone and reports no evaporation) and ::latentSensibleHeat
+    on the reference's state."""
+    R, o = fresh(ref)
+    t = R.get("t")
+    t[0, 5, 10] = 700.0 / 273.15
+    R.set("t", t)
+    o.f["t"][...] = t
+    cf = R.get2("c_fix")
+    o.f2["c_fix"][...] = cf
+    R.evaporation()
+    o.water_vapour_evaporation()
+    assert_identical(R, o, ["c"])
+    for n in ("Evaporation", "Evaporation_Dalton", "Evaporation_Meyer", "Evaporation_Rohwer", "c_fix"):
+        assert np.array_equal(R.get2(n), o.f2[n]), n
+    assert o.f2["Evaporation"][5, 10] == 0.0 and o.f2["c_fix"][5, 10] == cf[5, 10]
+    R.latent_sensible()
+    o.latent_sensible_heat(compat=1)
+    for n in ("Q_Sensible", "Q_Latent"):
+        a, b = R.get(n), o.f[n]
+        assert np.array_equal(a[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]) and np.array_equal(a[0], b[0]), n
