@@ -68,7 +68,7 @@ N_LEVEL = FIELD_NAMES[11:22]
 
 FIELD2D_NAMES = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star",
                  "epsilon_2D", "albedo", "Evaporation_Dalton", "Evaporation_Meyer",
-                 "Evaporation_Rohwer", "c_fix"]
+                 "Evaporation_Rohwer", "c_fix", "co2_total"]
 FIELD2D = {n: i for i, n in enumerate(FIELD2D_NAMES)}
 PROFILE_NAMES = ["t_ref_level", "rho_base", "dlnrho_dr"]
 PROFILE = {n: i for i, n in enumerate(PROFILE_NAMES)}
@@ -144,6 +144,13 @@ class ResiduumReport(ctypes.Structure):
         (n, ctypes.c_int32) for n in ("i_error", "j_error", "k_error", "i_nan", "j_nan", "k_nan")]
 
 
+class BudgetReport(ctypes.Structure):
+    """athad_budget_report"""
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "q_mean", "q_ref", "drift_pct", "q_fixed", "q_fixed_ref", "fixed_drift_pct",
+        "air_now", "air_ref", "air_drift_pct")]
+
+
 class Report(ctypes.Structure):
     _fields_ = [("poisson_src_cells", ctypes.c_int64), ("poisson_src_clamped", ctypes.c_int64),
                 ("satadj_ceiling_hits", ctypes.c_int64), ("nonfinite_inputs", ctypes.c_int64),
@@ -192,6 +199,8 @@ SIGNATURES = {
     "athad_stand_atm_dew_point": (ctypes.c_int, [_P]),
     "athad_water_vapour_evaporation": (ctypes.c_int, [_P]),
     "athad_latent_sensible_heat": (ctypes.c_int, [_P]),
+    "athad_co2_column": (ctypes.c_int, [_P, ctypes.POINTER(BudgetReport)]),
+    "athad_water_budget": (ctypes.c_int, [_P, ctypes.POINTER(BudgetReport), _D]),
     "athad_checkpoint_begin": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),
     "athad_checkpoint_wait": (ctypes.c_int, [_P]),
     "athad_pressure_solve": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(SolveReport)]),

@@ -205,6 +205,22 @@ class GpuAtmosphere:
         TempDewPoint, HumidityRel."""
         self._check(self.lib.athad_stand_atm_dew_point(self._h))
 
+    def co2_column(self) -> dict:
+        """ThermoAtm::co2Column (ThermoAtm.h:1096-1137): co2_total and the CO2 budget."""
+        r = _abi.BudgetReport()
+        self._check(self.lib.athad_co2_column(self._h, ctypes.byref(r)))
+        return {n: getattr(r, n) for n in ("q_mean", "q_ref", "drift_pct")}
+
+    def water_budget(self) -> dict:
+        """ThermoAtm::waterBudget (ThermoAtm.h:934-1094): the water budget and the per-level
+        drift from the first call."""
+        r = _abi.BudgetReport()
+        lev = np.zeros(self.shape[0])
+        self._check(self.lib.athad_water_budget(self._h, ctypes.byref(r), _dptr(lev)))
+        out = {n: getattr(r, n) for n, _ in r._fields_}
+        out["level_drift"] = lev
+        return out
+
     def water_vapour_evaporation(self):
         """ThermoAtm::waterVapourEvaporation (ThermoAtm.h:115-398): surface water vapour
         relaxed toward the sea's saturation, Evaporation and the three evaporation laws."""

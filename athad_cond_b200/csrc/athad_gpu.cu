@@ -969,6 +969,87 @@ athad_status athad_stand_atm_dew_point(athad_ctx* ctx)
     return ATHAD_OK;
 }
 
+// the per-level sums of co2Column / waterBudget on the device, read back (6 per level)
+static athad_status budget_levels(athad_ctx* ctx, bool co2_total, std::vector<double>& lv)
+{
+    BudgetArgs a;
+    a.d = ctx->L.d;
+    a.p_stat = ctx->field[ATHAD_P_STAT];
+    a.c = ctx->field[ATHAD_C]; a.cloud = ctx->field[ATHAD_CLOUD]; a.ice = ctx->field[ATHAD_ICE];
+    a.gr = ctx->field[ATHAD_GR]; a.co2 = ctx->field[ATHAD_CO2];
+    a.coslat = ctx->coslat;
+    a.g = ctx->p.g;
+    a.rows = ctx->stB[0];                          // stage buffers B: scratch
+    a.levels = ctx->stB[1];
+    a.co2_total = co2_total ? ctx->f2d[ATHAD_2D_CO2_TOTAL] : nullptr;
+    launch_budgets(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "budgets");
+    const int im = ctx->grid.im;
+    lv.assign(6 * (size_t)im, 0.0);
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(lv.data(), a.levels, lv.size() * sizeof(double),
+                                                     cudaMemcpyDeviceToHost, ctx->stream), "budgets report");
+    if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "budgets sync");
+    return s;
+}
+
+static double pct(double now, double ref) { return (ref > 0.0) ? 100.0 * (now / ref - 1.0) : 0.0; }
+
+athad_status athad_co2_column(athad_ctx* ctx, athad_budget_report* out)
+{
+    if (!ctx || !out) return fail(ctx, ATHAD_ERR_INVALID, "co2_column: bad argument");
+    std::vector<double> lv;
+    athad_status s = budget_levels(ctx, true, lv);
+    if (s != ATHAD_OK) return s;
+    double w_num = 0.0, w_den = 0.0;
+    for (int i = 0; i < ctx->grid.im; i++) { w_den += lv[6 * i + 0]; w_num += lv[6 * i + 2]; }
+    std::memset(out, 0, sizeof *out);
+    out->q_mean = (w_den > 0.0) ? w_num / w_den : 0.0;           // ThermoAtm.h:1125-1126
+    if (ctx->q_co2_ref <= 0.0) ctx->q_co2_ref = out->q_mean;
+    out->q_ref = ctx->q_co2_ref;
+    out->drift_pct = pct(out->q_mean, out->q_ref);
+    return ATHAD_OK;
+}
+
+athad_status athad_water_budget(athad_ctx* ctx, athad_budget_report* out, double* level_drift)
+{
+    if (!ctx || !out) return fail(ctx, ATHAD_ERR_INVALID, "water_budget: bad argument");
+    std::vector<double> lv;
+    athad_status s = budget_levels(ctx, false, lv);
+    if (s != ATHAD_OK) return s;
+    const int im = ctx->grid.im;
+    double w_num = 0.0, w_den = 0.0;
+    for (int i = 0; i < im; i++) { w_den += lv[6 * i + 0]; w_num += lv[6 * i + 1]; }
+    std::memset(out, 0, sizeof *out);
+    out->q_mean = (w_den > 0.0) ? w_num / w_den : 0.0;           // ThermoAtm.h:963-964
+    if (ctx->q_h2o_ref <= 0.0) ctx->q_h2o_ref = out->q_mean;
+    out->q_ref = ctx->q_h2o_ref;
+    out->drift_pct = pct(out->q_mean, out->q_ref);
+    // level means and air masses (:974-996), frozen weights (:1003-1014), levels (:1020-1033)
+    std::vector<double> qbar(im), abar(im), lev(im);
+    for (int i = 0; i < im; i++) {
+        qbar[i] = (lv[6 * i + 4] > 0.0) ? lv[6 * i + 3] / lv[6 * i + 4] : 0.0;
+        abar[i] = lv[6 * i + 0];
+        lev[i] = (w_den > 0.0) ? lv[6 * i + 1] / w_den : 0.0;
+    }
+    if (ctx->air_levels.empty()) ctx->air_levels = abar;
+    double qf_num = 0.0, qf_den = 0.0;
+    for (int i = 0; i < im; i++) {
+        qf_num += ctx->air_levels[i] * qbar[i];
+        qf_den += ctx->air_levels[i];
+        out->air_now += abar[i];
+    }
+    out->air_ref = qf_den;
+    out->q_fixed = (qf_den > 0.0) ? qf_num / qf_den : 0.0;
+    if (ctx->q_h2o_fixed_ref <= 0.0) ctx->q_h2o_fixed_ref = out->q_fixed;
+    out->q_fixed_ref = ctx->q_h2o_fixed_ref;
+    out->fixed_drift_pct = pct(out->q_fixed, out->q_fixed_ref);
+    out->air_drift_pct = pct(out->air_now, out->air_ref);
+    if (ctx->h2o_levels.empty()) ctx->h2o_levels = lev;
+    if (level_drift)
+        for (int i = 0; i < im; i++) level_drift[i] = lev[i] - ctx->h2o_levels[i];
+    return ATHAD_OK;
+}
+
 static SurfaceArgs surface_args(athad_ctx* ctx)
 {
     SurfaceArgs a;

@@ -104,6 +104,9 @@ struct athad_ctx {
     int* i_trop = nullptr;                    // [jm] tropopause level per row (standAtm)
     bool trop_set = false;
     double residuum_old = 1.0e-5;             // cAtmosphereModel.h:164
+    // the budgets' first-call references (cAtmosphereModel.h:89-109; <= 0 / empty = unset)
+    double q_co2_ref = -1.0, q_h2o_ref = -1.0, q_h2o_fixed_ref = -1.0;
+    std::vector<double> air_levels, h2o_levels;
     // asynchronous checkpoints (athad_checkpoint_begin): a device snapshot of the fields,
     // copied to the host on a side stream while the compute stream goes on
     double* ckpt_buf = nullptr;

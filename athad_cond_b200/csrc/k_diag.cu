@@ -213,6 +213,92 @@ __global__ void __launch_bounds__(1024) residuum_final_kernel(ResiduumArgs a, in
     }
 }
 
+// ---- co2Column / waterBudget ----------------------------------------------------------
+
+__device__ __forceinline__ double budget_dp(const BudgetArgs& a, long long c, int i)
+{
+    return (i < a.d.im - 1) ? (a.p_stat[c] - a.p_stat[c + a.d.plane]) * 100.0 : a.p_stat[c] * 100.0;
+}
+
+// one warp per (i, j) row: air mass, water mass, CO2 mass of the cells with a positive layer
+// pressure drop, and the plain sum of the water mass fraction (ThermoAtm.h:942-1034, 1102-1122)
+__global__ void __launch_bounds__(256) budget_rows_kernel(BudgetArgs a)
+{
+    const Dims& d = a.d;
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= d.im * d.jm) return;
+    const int i = row / d.jm;
+    const long long base = (long long)row * d.pitch;
+    double s_air = 0.0, s_w = 0.0, s_c = 0.0, s_q = 0.0;
+    for (int k = lane; k < d.km; k += 32) {
+        const long long c = base + k;
+        const double q_w = fmax(0.0, a.c[c]) + fmax(0.0, a.cloud[c]) + fmax(0.0, a.ice[c]) + fmax(0.0, a.gr[c]);
+        s_q += q_w;
+        const double dp = budget_dp(a, c, i);
+        if (!(dp > 0.0)) continue;
+        const double u_air = dp / a.g;
+        s_air += u_air;
+        s_w += q_w * u_air;
+        s_c += fmax(0.0, a.co2[c]) * u_air;
+    }
+    for (int off = 16; off >= 1; off >>= 1) {
+        s_air += __shfl_xor_sync(0xffffffffu, s_air, off);
+        s_w += __shfl_xor_sync(0xffffffffu, s_w, off);
+        s_c += __shfl_xor_sync(0xffffffffu, s_c, off);
+        s_q += __shfl_xor_sync(0xffffffffu, s_q, off);
+    }
+    if (lane == 0) {
+        double* r = a.rows + 4 * (long long)row;
+        r[0] = s_air; r[1] = s_w; r[2] = s_c; r[3] = s_q;
+    }
+}
+
+// one CTA per level: the rows weighted by cos(latitude), summed in a fixed order
+__global__ void __launch_bounds__(256) budget_levels_kernel(BudgetArgs a)
+{
+    const Dims& d = a.d;
+    const int i = blockIdx.x;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < d.jm; j += blockDim.x) {
+        const double w = a.coslat[j];
+        const double* r = a.rows + 4 * ((long long)i * d.jm + j);
+        v[0] += w * r[0]; v[1] += w * r[1]; v[2] += w * r[2]; v[3] += w * r[3];
+        v[4] += w;
+    }
+    __shared__ double part[5][8];
+    for (int q = 0; q < 5; q++) {
+        double x = v[q];
+        for (int off = 16; off >= 1; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) x += part[threadIdx.x][w];
+        if (threadIdx.x == 4) x *= (double)d.km;       // sum of coslat over every (j, k)
+        a.levels[6 * i + threadIdx.x] = x;
+    }
+    if (threadIdx.x == 5) a.levels[6 * i + 5] = 0.0;
+}
+
+// co2_total: the column CO2 path, summed up the column as ThermoAtm.h:1105-1120 does
+__global__ void __launch_bounds__(128) co2_column_kernel(BudgetArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k >= d.km) return;
+    double col = 0.0;
+    for (int i = 0; i < d.im; i++) {
+        const long long c = idx3(d, i, j, k);
+        const double dp = budget_dp(a, c, i);
+        if (!(dp > 0.0)) continue;
+        col += fmax(0.0, a.co2[c]) * (dp / a.g);
+    }
+    a.co2_total[(long long)j * d.pitch + k] = col;
+}
+
 // ---- standAtm_DewPoint_HumidRel ------------------------------------------------------
 
 // one thread per cell; every output is a function of the cell and of its column's surface
@@ -248,6 +334,14 @@ void launch_find_residuum(const ResiduumArgs& a, cudaStream_t st)
     const int rows = (a.i1 >= a.i0 && a.d.jm > 2) ? (a.i1 - a.i0 + 1) * (a.d.jm - 2) : 0;
     if (rows > 0) residuum_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a, rows);
     residuum_final_kernel<<<1, 1024, 0, st>>>(a, rows);
+}
+
+void launch_budgets(const BudgetArgs& a, cudaStream_t st)
+{
+    const int rows = a.d.im * a.d.jm;
+    budget_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a);
+    budget_levels_kernel<<<a.d.im, 256, 0, st>>>(a);
+    if (a.co2_total) co2_column_kernel<<<dim3((a.d.km + 127) / 128, a.d.jm), 128, 0, st>>>(a);
 }
 
 void launch_stand_atm(const StandAtmArgs& a, cudaStream_t st)

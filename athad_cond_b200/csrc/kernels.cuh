@@ -286,6 +286,21 @@ struct ResiduumArgs {
 };
 void launch_find_residuum(const ResiduumArgs& a, cudaStream_t st);
 
+// co2Column / waterBudget (k_diag.cu): per (i, j) row sums, then per level
+// levels[6 i ..] = sum_j coslat_j x {air mass, water mass, CO2 mass, water fraction, 1 (km
+// times)} and the column CO2 path co2_total
+struct BudgetArgs {
+    Dims d;
+    const double* p_stat; const double* c; const double* cloud; const double* ice;
+    const double* gr; const double* co2;
+    const double* coslat;         // [jm]
+    double g;
+    double* rows;                 // [4 im jm]
+    double* levels;               // [6 im]
+    double* co2_total;            // 2-D [jm][pitch], or nullptr
+};
+void launch_budgets(const BudgetArgs& a, cudaStream_t st);
+
 // standAtm_DewPoint_HumidRel (k_diag.cu)
 struct StandAtmArgs {
     Dims d;

@@ -24,6 +24,8 @@
 //     FindResiduumAtm(m)        UtilsAtm(m).findResiduumAtm()                :668, 1645
 //     WaterVapourEvaporation(m) ThermoAtm(m).waterVapourEvaporation()        :637, 1421
 //     LatentSensibleHeat(m)     ThermoAtm(m).latentSensibleHeat()            :638, 1422
+//     Co2Column(m)              ThermoAtm(m).co2Column(report)               :632, 1416
+//     WaterBudget(m)            ThermoAtm(m).waterBudget(report, stage)      :633, 1216, 1417
 //
 // The model's fields stay resident on the device.  While the reference's other modules
 // (boundary conditions, filters, ice scheme, turbulence, radiation) still run on the host,
@@ -385,6 +387,36 @@ public:
         up(ATHAD_Q_LATENT, m.Q_Latent); up(ATHAD_Q_SENSIBLE, m.Q_Sensible);   // the boundary cells keep theirs
         check(ctx_, athad_latent_sensible_heat(ctx_), "latent_sensible_heat");
         down(ATHAD_Q_LATENT, m.Q_Latent); down(ATHAD_Q_SENSIBLE, m.Q_Sensible);
+    }
+
+    // ThermoAtm(m).co2Column(report) (cAtmosphereModel.cpp:632, 1416): m.co2_total and the
+    // CO2 budget, returned for the caller to print; m.m_q_co2_ref set on the first call as
+    // the reference sets it
+    athad_budget_report Co2Column(Model& m)
+    {
+        up(ATHAD_P_STAT, m.p_stat); up(ATHAD_CO2, m.co2);
+        athad_budget_report r;
+        check(ctx_, athad_co2_column(ctx_, &r), "co2_column");
+        down2(ATHAD_2D_CO2_TOTAL, m.co2_total);
+        if (m.m_q_co2_ref <= 0.0) m.m_q_co2_ref = r.q_mean;
+        return r;
+    }
+
+    // ThermoAtm(m).waterBudget(report, stage) (cAtmosphereModel.cpp:633, 1216, 1417): the
+    // water budget, returned for the caller to print; the model's first-call references
+    // (m_q_h2o_ref, m_air_levels, m_q_h2o_fixed_ref, m_q_h2o_levels) set as the reference
+    // sets them.  The context keeps its own references from its first call.
+    athad_budget_report WaterBudget(Model& m, std::vector<double>* level_drift = nullptr)
+    {
+        up(ATHAD_P_STAT, m.p_stat); up(ATHAD_C, m.c); up(ATHAD_CLOUD, m.cloud);
+        up(ATHAD_ICE, m.ice); up(ATHAD_GR, m.gr);
+        athad_budget_report r;
+        std::vector<double> lev(im_);
+        check(ctx_, athad_water_budget(ctx_, &r, lev.data()), "water_budget");
+        if (m.m_q_h2o_ref <= 0.0) m.m_q_h2o_ref = r.q_ref;
+        if (m.m_q_h2o_fixed_ref <= 0.0) m.m_q_h2o_fixed_ref = r.q_fixed_ref;
+        if (level_drift) *level_drift = lev;
+        return r;
     }
 
 private:

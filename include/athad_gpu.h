@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 7
+#define ATHAD_ABI_VERSION 8
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -178,6 +178,7 @@ typedef enum athad_field2d {
      * [mm/d] and the surface water vapour before the update */
     ATHAD_2D_EVAPORATION_DALTON, ATHAD_2D_EVAPORATION_MEYER, ATHAD_2D_EVAPORATION_ROHWER,
     ATHAD_2D_C_FIX,
+    ATHAD_2D_CO2_TOTAL,             /* Array_2D co2_total, the column CO2 path [kg/m2]   */
     ATHAD_NFIELDS2D
 } athad_field2d;
 
@@ -241,6 +242,17 @@ typedef struct athad_residuum_report {
                                           * equal values; 0, 0, 0 if none                 */
     int32_t i_nan, j_nan, k_nan;   /* first non-finite residual in (j, k, i) order; -1 if none */
 } athad_residuum_report;
+
+/* The global mass budgets of ThermoAtm::co2Column (ThermoAtm.h:1096-1137) and
+ * ::waterBudget (:934-1094): the cos-latitude-weighted, air-mass-weighted mean mass fraction
+ * of the species and its drift from the context's first call (the reference's m_q_co2_ref /
+ * m_q_h2o_ref), summed in FP64 in a fixed order. */
+typedef struct athad_budget_report {
+    double q_mean, q_ref, drift_pct;   /* mean, first call's mean, 100 (q_mean / q_ref - 1)  */
+    double q_fixed, q_fixed_ref, fixed_drift_pct;  /* water: the level means weighted by the
+                                        * first call's level air masses, and its drift       */
+    double air_now, air_ref, air_drift_pct;        /* water: total air mass and its drift   */
+} athad_budget_report;
 
 typedef struct athad_ctx athad_ctx;
 
@@ -426,6 +438,14 @@ athad_status athad_water_vapour_evaporation(athad_ctx* ctx);
  * 1422): Q_Latent zeroed at the surface, Q_Sensible = cp_l t_0 |grad t| / sqrt(3) in the
  * interior. */
 athad_status athad_latent_sensible_heat(athad_ctx* ctx);
+/* ThermoAtm::co2Column (ThermoAtm.h:1096-1137; call sites cAtmosphereModel.cpp:632, 1416):
+ * ATHAD_2D_CO2_TOTAL and the CO2 budget.  Waits for the device. */
+athad_status athad_co2_column(athad_ctx* ctx, athad_budget_report* out);
+/* ThermoAtm::waterBudget (ThermoAtm.h:934-1094; call sites cAtmosphereModel.cpp:633, 1216,
+ * 1417): the water budget (c + cloud + ice + graupel); level_drift, if not NULL, receives the
+ * im per-level drifts of the water mass fraction from the first call (the reference prints
+ * the six largest).  Waits for the device. */
+athad_status athad_water_budget(athad_ctx* ctx, athad_budget_report* out, double* level_drift);
 athad_status athad_checkpoint_begin(athad_ctx* ctx, const int32_t* fields, int32_t n, double* const* hosts);
 athad_status athad_checkpoint_wait(athad_ctx* ctx);
 athad_status athad_project_initial_velocity(athad_ctx* ctx, int32_t n_sweeps,

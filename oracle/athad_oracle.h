@@ -78,7 +78,7 @@ enum {
 };
 enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR,
        OF2_EPSILON, OF2_ALBEDO, OF2_EVAPORATION_DALTON, OF2_EVAPORATION_MEYER,
-       OF2_EVAPORATION_ROHWER, OF2_C_FIX, OF2_N };
+       OF2_EVAPORATION_ROHWER, OF2_C_FIX, OF2_CO2_TOTAL, OF2_N };
 enum { OFP_T_REF_LEVEL = 0, OFP_RHO_BASE, OFP_DLNRHO_DR, OFP_N };
 
 size_t or_params_size(void);
@@ -181,6 +181,15 @@ void or_stand_atm_dew_point(int im, int jm, int km, const or_params* p, double* 
 void or_water_vapour_evaporation(int im, int jm, int km, const or_params* p, double* const* f,
                                  double* const* f2);
 void or_latent_sensible_heat(int im, int jm, int km, const or_params* p, int compat, double* const* f);
+
+/* ThermoAtm::co2Column (ThermoAtm.h:1096-1137): co2_total and the mass-weighted mean q_CO2,
+ * in the reference's serial (j, k, i) order; out = w_num, w_den. */
+void or_co2_column(int im, int jm, int km, const or_params* p, double* const* f, double* const* f2,
+                   double* out);
+/* ThermoAtm::waterBudget (ThermoAtm.h:934-1094), the sums before the reference's first-call
+ * bookkeeping: out = w_num, w_den; qbar, abar, lev [im] */
+void or_water_budget(int im, int jm, int km, const or_params* p, double* const* f, double* out,
+                     double* qbar, double* abar, double* lev);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

@@ -57,6 +57,12 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
             case 14: d.FindResiduumAtm(*m); break;
             case 15: d.WaterVapourEvaporation(*m); break;
             case 16: d.LatentSensibleHeat(*m); break;
+            case 17: {   // first calls of both budgets (the model's references cleared)
+                m->m_q_co2_ref = -1.0; m->m_q_h2o_ref = -1.0; m->m_q_h2o_fixed_ref = -1.0;
+                d.Co2Column(*m);
+                d.WaterBudget(*m);
+                break;
+            }
             default: return -1;
         }
     } catch (const std::exception& e) {
@@ -64,6 +70,13 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
         return -1;
     }
     return 0;
+}
+
+// the model's budget references: m_q_co2_ref, m_q_h2o_ref, m_q_h2o_fixed_ref
+void dropin_budget_refs(void* model, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)model;
+    out[0] = m->m_q_co2_ref; out[1] = m->m_q_h2o_ref; out[2] = m->m_q_h2o_fixed_ref;
 }
 
 // the model's residuum_old (what findResiduumAtm leaves behind)

@@ -108,6 +108,7 @@ Array_2D* field2(cAtmosphereModel* m, const std::string& n)
     if (n == "Evaporation_Meyer") return &m->Evaporation_Meyer;
     if (n == "Evaporation_Rohwer") return &m->Evaporation_Rohwer;
     if (n == "c_fix") return &m->c_fix;
+    if (n == "co2_total") return &m->co2_total;
     return nullptr;
 }
 
@@ -422,6 +423,28 @@ void ref_radiative_heating(void* p, double omega_rad)
             }
 }
 void ref_level_mean(void* p) { ((cAtmosphereModel*)p)->computeLevelMeanTemperature(); }
+
+// ThermoAtm::co2Column and ::waterBudget as first calls (the references they keep cleared
+// first): out = m_q_co2_ref, m_q_h2o_ref, m_q_h2o_fixed_ref, m_air_levels [im],
+// m_q_h2o_levels [im]
+void ref_budgets(void* p, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->m_q_co2_ref = -1.0;
+    m->m_q_h2o_ref = -1.0;
+    m->m_q_h2o_fixed_ref = -1.0;
+    m->m_air_levels.clear();
+    m->m_q_h2o_levels.clear();
+    ThermoAtm(*m).co2Column(false);
+    ThermoAtm(*m).waterBudget(false);
+    out[0] = m->m_q_co2_ref;
+    out[1] = m->m_q_h2o_ref;
+    out[2] = m->m_q_h2o_fixed_ref;
+    for (int i = 0; i < m->im; i++) {
+        out[3 + i] = m->m_air_levels[i];
+        out[3 + m->im + i] = m->m_q_h2o_levels[i];
+    }
+}
 
 // ThermoAtm::waterVapourEvaporation and ::latentSensibleHeat
 void ref_evaporation(void* p) { ThermoAtm(*(cAtmosphereModel*)p).waterVapourEvaporation(); }

@@ -186,6 +186,29 @@ class OracleState:
         return {"residuum": out[0], "avg_abs": out[1], "avg_rel": out[2], "n_cells": cnt[0],
                 "n_nonfinite": cnt[1], "at": tuple(idx[0:3]), "first_nonfinite": tuple(idx[3:6])}
 
+    def budgets(self) -> dict:
+        """or_co2_column and or_water_budget, finished as the reference's first calls finish
+        them (ThermoAtm.h:1016-1031, 1126-1127): the references those calls would set."""
+        F, F2, _ = self._args()
+        im, jm, km = self.shape
+        co2 = (ctypes.c_double * 2)()
+        lib().or_co2_column(im, jm, km, ctypes.byref(self.params), F, F2, co2)
+        w = (ctypes.c_double * 2)()
+        qbar, abar, lev = np.zeros(im), np.zeros(im), np.zeros(im)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib().or_water_budget(im, jm, km, ctypes.byref(self.params), F, w, qbar.ctypes.data_as(dp),
+                              abar.ctypes.data_as(dp), lev.ctypes.data_as(dp))
+        q_co2 = co2[0] / co2[1] if co2[1] > 0 else 0.0
+        q_h2o = w[0] / w[1] if w[1] > 0 else 0.0
+        qf_num = qf_den = 0.0
+        for i in range(im):
+            qf_num += abar[i] * qbar[i]
+            qf_den += abar[i]
+        q_fixed = qf_num / qf_den if qf_den > 0 else 0.0
+        levels = lev / w[1] if w[1] > 0 else np.zeros(im)
+        return {"q_co2_ref": q_co2, "q_h2o_ref": q_h2o, "q_h2o_fixed_ref": q_fixed,
+                "air_levels": abar, "h2o_levels": levels, "qbar": qbar}
+
     def water_vapour_evaporation(self):
         """or_water_vapour_evaporation: ThermoAtm::waterVapourEvaporation."""
         F, F2, _ = self._args()

@@ -140,6 +140,23 @@ class Reference:
         f.argtypes = [ctypes.c_void_p]
         f(self.h)
 
+    def budgets(self, threads=1) -> dict:
+        """ThermoAtm::co2Column and ::waterBudget as first calls: the references they set
+        (one thread by default, so the OpenMP sums run in the serial order)."""
+        im = self.shape[0]
+        out = np.empty(3 + 2 * im)
+        f = self.lib.ref_budgets
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        if threads:
+            self.lib.ref_set_threads(threads)
+        try:
+            f(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        finally:
+            if threads and self.threads:
+                self.lib.ref_set_threads(self.threads)
+        return {"q_co2_ref": out[0], "q_h2o_ref": out[1], "q_h2o_fixed_ref": out[2],
+                "air_levels": out[3:3 + im].copy(), "h2o_levels": out[3 + im:].copy()}
+
     def evaporation(self):
         """ThermoAtm::waterVapourEvaporation."""
         f = self.lib.ref_evaporation
@@ -181,6 +198,14 @@ class Reference:
                 self.lib.ref_set_threads(self.threads)
         return {"residuum": out[0], "residuum_prev": out[1], "avg_abs_8": out[2],
                 "at": tuple(idx[0:3]), "n_cells": idx[3], "n_nonfinite": idx[4]}
+
+    def budget_refs(self):
+        """The model's m_q_co2_ref, m_q_h2o_ref, m_q_h2o_fixed_ref (needs the drop-in library)."""
+        out = (ctypes.c_double * 3)()
+        f = self.lib.dropin_budget_refs
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        f(self.h, out)
+        return list(out)
 
     def residuum_old(self) -> float:
         """The model's residuum_old (needs the drop-in library)."""

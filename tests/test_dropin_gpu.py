@@ -253,3 +253,18 @@ def test_dropin_surface_fluxes(model):
     reset(R, snap)
     for n, (a, b) in out.items():
         assert relerr(a, b) <= 1e-12, (n, relerr(a, b))
+
+
+def test_dropin_mass_budgets(model):
+    """ThermoAtm::co2Column and ::waterBudget through the adapter: co2_total bit for bit and the
+    first-call references within 1e-12 of the reference's (sums in another fixed order)."""
+    R, snap = model
+    reset(R, snap)
+    want = R.budgets(threads=1)
+    co2_total = R.get2("co2_total")
+    reset(R, snap)
+    R.dropin(17)
+    got = R.budget_refs()
+    assert np.array_equal(R.get2("co2_total"), co2_total)
+    for g, key in zip(got, ("q_co2_ref", "q_h2o_ref", "q_h2o_fixed_ref")):
+        assert abs(g - want[key]) <= 1e-12 * want[key], key

@@ -13,7 +13,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
   * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating;
   * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm;
-  * the surface fluxes waterVapourEvaporation and latentSensibleHeat.
+  * the surface fluxes waterVapourEvaporation and latentSensibleHeat;
+  * the mass budgets co2Column and waterBudget (their sums on one thread).
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -349,3 +350,15 @@ def test_surface_fluxes_bit_exact(ref):
     for n in ("Q_Sensible", "Q_Latent"):
         a, b = R.get(n), o.f[n]
         assert np.array_equal(a[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]) and np.array_equal(a[0], b[0]), n
+
+
+def test_mass_budgets_bit_exact(ref):
+    """ThermoAtm::co2Column and ::waterBudget as first calls, the reference on one thread: the
+    references they set (mass-weighted means, level air masses, level water) and co2_total."""
+    R, o = fresh(ref)
+    r, q = R.budgets(threads=1), o.budgets()
+    for key in ("q_co2_ref", "q_h2o_ref", "q_h2o_fixed_ref"):
+        assert r[key] == q[key], key
+    for key in ("air_levels", "h2o_levels"):
+        assert np.array_equal(r[key], q[key]), key
+    assert np.array_equal(R.get2("co2_total"), o.f2["co2_total"])

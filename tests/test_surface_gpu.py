@@ -7,7 +7,9 @@ largest magnitude (CUDA's exp, log and sqrt in the saturation curves against gli
 exp), a supercritical surface column left alone.  athad_latent_sensible_heat
 (ThermoAtm::latentSensibleHeat, ThermoAtm.h:36-112): Q_Sensible and Q_Latent bit for bit (no
 transcendental but the correctly rounded sqrt).  A mirror-symmetric state stays
-mirror-symmetric, bit for bit.
+mirror-symmetric, bit for bit.  athad_co2_column / athad_water_budget (co2Column,
+waterBudget): co2_total bit for bit, the mass-weighted means and first-call references within
+1e-12 (FP64 sums in another fixed order), the drifts after the state changes.
 """
 import numpy as np
 import pytest
@@ -76,3 +78,25 @@ def test_surface_fluxes_mirror_symmetric():
         for n in EVAP2D:
             a = g.download_2d(n)
             assert np.array_equal(a, a[::-1, :]), n
+
+
+@pytest.mark.parametrize("grid", [(11, 21, 41), (41, 181, 361)])
+def test_mass_budgets_match_oracle(grid):
+    st = make_state(*grid, seed=149)
+    o = OracleState(st, config_params())
+    want = o.budgets()
+    with GpuAtmosphere(*grid, config_params()) as g:
+        g.upload_state(st)
+        co2 = g.co2_column()
+        h2o = g.water_budget()
+        assert np.array_equal(g.download_2d("co2_total"), o.f2["co2_total"])
+        for got, key in ((co2["q_mean"], "q_co2_ref"), (h2o["q_mean"], "q_h2o_ref"),
+                         (h2o["q_fixed"], "q_h2o_fixed_ref")):
+            assert abs(got - want[key]) <= 1e-12 * want[key], key
+        assert co2["drift_pct"] == 0.0 and h2o["drift_pct"] == 0.0 and not np.any(h2o["level_drift"])
+        assert abs(h2o["air_now"] - want["air_levels"].sum()) <= 1e-12 * want["air_levels"].sum()
+        # more water: the budget drifts by the change, the references stay
+        g.upload("c", 1.01 * st["c"])
+        h2o2 = g.water_budget()
+        assert h2o2["q_ref"] == h2o["q_mean"] and h2o2["drift_pct"] > 0.0
+        assert h2o2["air_drift_pct"] == 0.0 and np.all(h2o2["level_drift"] >= 0.0)
