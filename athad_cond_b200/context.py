@@ -205,6 +205,13 @@ class GpuAtmosphere:
         TempDewPoint, HumidityRel."""
         self._check(self.lib.athad_stand_atm_dew_point(self._h))
 
+    def update_skin_temperature(self, t_skin_relax: float = 0.25) -> float:
+        """cAtmosphereModel::updateSkinTemperature (cAtmosphereModel.cpp:291-327): the new
+        t_skin, which the context's densities use from now on."""
+        out = np.zeros(1)
+        self._check(self.lib.athad_update_skin_temperature(self._h, float(t_skin_relax), _dptr(out)))
+        return float(out[0])
+
     def co2_column(self) -> dict:
         """ThermoAtm::co2Column (ThermoAtm.h:1096-1137): co2_total and the CO2 budget."""
         r = _abi.BudgetReport()

@@ -969,6 +969,49 @@ athad_status athad_stand_atm_dew_point(athad_ctx* ctx)
     return ATHAD_OK;
 }
 
+athad_status athad_update_skin_temperature(athad_ctx* ctx, double t_skin_relax, double* t_skin)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    const int jm = ctx->grid.jm, km = ctx->grid.km;
+    if (t_skin_relax > 0.0) {                                  // cAtmosphereModel.cpp:293
+        launch_albedo_rows(ctx->L.d, ctx->f2d[ATHAD_2D_ALBEDO], ctx->stB[0], ctx->stream);
+        ATHAD_CHECK_LAUNCH(ctx, "albedo rows");
+        std::vector<double> rows(jm);
+        athad_status s = cuda_check(ctx, cudaMemcpyAsync(rows.data(), ctx->stB[0], jm * sizeof(double),
+                                                         cudaMemcpyDeviceToHost, ctx->stream), "albedo rows");
+        if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "albedo rows sync");
+        if (s != ATHAD_OK) return s;
+        // the insolation profile of MultiLayerRadiation.h:102-108 (AtomUtils::parabola)
+        const athad_params& p = ctx->p;
+        const int j_max = jm - 1, j_half = j_max / 2;
+        std::vector<double> sw(jm, p.rad_pole_short);
+        const double eff = p.rad_pole_short - p.rad_equator_short;
+        for (int j = j_half; j >= 0; j--) {
+            const double x = (double)j / (double)j_half;
+            sw[j] = eff * (x * x - 2.0 * x) + p.rad_pole_short;
+        }
+        for (int j = j_max; j > j_half; j--) sw[j] = sw[j_max - j];
+        // planetaryShortWave (:240-264)
+        double w_sum = 0.0, abs_w = 0.0, alb_max = 0.0;
+        for (int j = 0; j < jm; j++) {
+            const double w = std::cos((j / (double)(jm - 1) - 0.5) * M_PI);
+            const double alb_k = rows[j] / (double)km;
+            alb_max = std::max(alb_max, alb_k);
+            w_sum += w;
+            abs_w += w * (1.0 - alb_k) * sw[j];
+        }
+        if (w_sum > 0.0 && alb_max > 0.0) {
+            const double in_mean = abs_w / w_sum + p.geothermal_flux;    // :296-297
+            if (in_mean > 0.0) {
+                const double target = std::pow(in_mean / p.sigma, 0.25);
+                ctx->p.t_skin += std::min(1.0, t_skin_relax) * (target - ctx->p.t_skin);
+            }
+        }
+    }
+    if (t_skin) *t_skin = ctx->p.t_skin;
+    return ATHAD_OK;
+}
+
 // the per-level sums of co2Column / waterBudget on the device, read back (6 per level)
 static athad_status budget_levels(athad_ctx* ctx, bool co2_total, std::vector<double>& lv)
 {

@@ -76,7 +76,10 @@ __global__ void __launch_bounds__(128) radial_columns_kernel(FilterArgs a)
     }
 }
 
-// damp_wiggles along j (clamped): out of place
+// damp_wiggles along j (clamped): out of place.  The two neighbours are added first, so the
+// result at row jm-1-j is bit for bit the result at row j of the mirrored field; the
+// reference's left-to-right (v[j-1] - 2 v[j]) + v[j+1] rounds the mirrored rows differently
+// (one rounding, an ulp of the field at most).
 __global__ void __launch_bounds__(128) wiggle_j_kernel(Dims d, const double* __restrict__ src, double* __restrict__ dst)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -84,7 +87,7 @@ __global__ void __launch_bounds__(128) wiggle_j_kernel(Dims d, const double* __r
     if (k >= d.km) return;
     const int jm1 = (j > 0) ? j - 1 : 0, jp1 = (j < d.jm - 1) ? j + 1 : d.jm - 1;
     const double c = src[idx3(d, i, j, k)];
-    dst[idx3(d, i, j, k)] = c + 0.25 * (src[idx3(d, i, jm1, k)] - 2.0 * c + src[idx3(d, i, jp1, k)]);
+    dst[idx3(d, i, j, k)] = c + 0.25 * ((src[idx3(d, i, jm1, k)] + src[idx3(d, i, jp1, k)]) - 2.0 * c);
 }
 
 // damp_wiggles along i (clamped): in place, one column per thread

@@ -126,7 +126,24 @@ __global__ void __launch_bounds__(256) rad_blend_kernel(long long n, const doubl
         t[q] = t_before[q] * (1.0 - omega) + t[q] * omega;
 }
 
+// cAtmosphereModel::planetaryShortWave's row sums (cAtmosphereModel.cpp:244-246): one thread
+// per row, the longitudes in order, so the host finishes the budget bit for bit
+__global__ void albedo_rows_kernel(Dims d, const double* __restrict__ albedo, double* __restrict__ out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d.jm) return;
+    const double* row = albedo + (long long)j * d.pitch;
+    double s = 0.0;
+    for (int k = 0; k < d.km; k++) s += row[k];
+    out[j] = s;
+}
+
 }  // namespace
+
+void launch_albedo_rows(const Dims& d, const double* albedo, double* out, cudaStream_t st)
+{
+    albedo_rows_kernel<<<(d.jm + 127) / 128, 128, 0, st>>>(d, albedo, out);
+}
 
 void launch_multilayer_radiation(const RadArgs& a, cudaStream_t st)
 {

@@ -326,6 +326,8 @@ struct SurfaceArgs {
 };
 void launch_water_vapour_evaporation(const SurfaceArgs& a, cudaStream_t st);
 void launch_latent_sensible_heat(const SurfaceArgs& a, cudaStream_t st);
+// planetaryShortWave's per-row albedo sums, summed over k in order (k_rad.cu)
+void launch_albedo_rows(const Dims& d, const double* albedo, double* out, cudaStream_t st);
 void launch_rad_blend(const Dims& d, const double* t_before, double* t, double omega, cudaStream_t st);
 
 }  // namespace athad

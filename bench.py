@@ -545,6 +545,41 @@ def run_poisson(args, device) -> dict:
             "levels": best["levels"], "history": best["history"], "clocks": clk.summary()}
 
 
+def run_loop(args, device) -> dict:
+    """The whole model iteration on the device (athad_cond_b200.loop.ModelLoop): every module
+    of the reference's run_3D_loop at its cadence, through the C ABI, on one mixed-precision
+    (or FP64) context; the readbacks the reference prints (residuum, budgets, skin
+    temperature) inside the timed region."""
+    import torch
+    from athad_cond_b200 import GpuAtmosphere, make_state
+    from athad_cond_b200._abi import Precision, config_params
+    from athad_cond_b200.loop import ModelLoop
+    import numpy as np
+    im, jm, km = tuple(int(x) for x in args.grid.lower().split("x")) if args.grid else GRID
+    p = config_params()
+    p.precision = int(Precision.MIXED if args.precision != "fp64" else Precision.FP64)
+    g = GpuAtmosphere(im, jm, km, p)
+    stream = torch.cuda.Stream(device=device)
+    g.set_stream(stream.cuda_stream)
+    g.upload_state(make_state(im, jm, km, seed=20261203))
+    loop = ModelLoop(g)
+    for _ in range(args.warmup):
+        loop.iteration()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    last = None
+    for _ in range(args.steps):
+        last = loop.iteration()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    finite = all(bool(np.isfinite(g.download(n)).all()) for n in ("t", "u", "v", "w", "c", "p_dyn"))
+    g.close()
+    return {"grid": [im, jm, km], "ms_per_iteration": ms, "value": im * jm * km / (ms * 1e-3),
+            "finite": finite, "residuum": last["residuum"]["residuum"], "t_skin": last["t_skin"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -556,7 +591,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="forms to run; the headline value is the mixed form when it runs")
-    ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving", "poisson"],
+    ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving", "poisson", "loop"],
                     help="iteration: the 41x181x361 model iteration (default); ensemble: the "
                          "batched ensemble; serving: the serving loop")
     ap.add_argument("--members", type=int, default=64, help="ensemble members")
@@ -591,7 +626,8 @@ def main():
     if args.workload != "iteration":
         if world > 1 and rank != 0:
             return
-        fn = {"ensemble": run_ensemble, "serving": run_serving, "poisson": run_poisson}[args.workload]
+        fn = {"ensemble": run_ensemble, "serving": run_serving, "poisson": run_poisson,
+              "loop": run_loop}[args.workload]
         r = fn(args, device)
         if args.workload == "poisson":
             line = {"metric": "pressure-Poisson solve to 1e-10 relative residual: seconds",
@@ -600,6 +636,15 @@ def main():
                     "config": {"workload": "61x361x721 stress solve, mirror-symmetric Gaussian "
                                            "velocity perturbation 0.5 m/s", "grid": r["grid"]},
                     "detail": r}
+        elif args.workload == "loop":
+            line = {"metric": "grid-point steps/s of the whole model iteration on the device",
+                    "value": r["value"], "unit": "grid-point steps/s", "n_gpus": 1,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_iteration"],
+                    "higher_is_better": True, "dtype": "f32+f64" if args.precision != "fp64" else "f64",
+                    "data": "synthetic",
+                    "config": {"workload": "run_3D_loop with every module on the device, "
+                                           f"{r['grid'][0]}x{r['grid'][1]}x{r['grid'][2]} grid",
+                               "grid": r["grid"]}, "detail": r}
         elif args.workload == "ensemble":
             line = {"metric": "ensemble grid-point steps/s (batched mixed-precision model iterations)",
                     "value": r["batched_mixed"]["value"], "unit": "grid-point steps/s", "n_gpus": 1,

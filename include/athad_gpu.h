@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 8
+#define ATHAD_ABI_VERSION 9
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -438,6 +438,15 @@ athad_status athad_water_vapour_evaporation(athad_ctx* ctx);
  * 1422): Q_Latent zeroed at the surface, Q_Sensible = cp_l t_0 |grad t| / sqrt(3) in the
  * interior. */
 athad_status athad_latent_sensible_heat(athad_ctx* ctx);
+/* cAtmosphereModel::updateSkinTemperature (cAtmosphereModel.cpp:291-327; called after the
+ * radiative heating of radiation mode 2, :1661) with planetaryShortWave (:236-265): the
+ * optically thin top's skin temperature relaxed by t_skin_relax (XML, 0.25) toward
+ * ((absorbed short wave + geothermal flux) / sigma)^(1/4), the absorbed short wave being the
+ * cos-latitude mean of (1 - albedo) times the pole-to-equator insolation profile, from
+ * ATHAD_2D_ALBEDO.  Changes the context's t_skin (read by athad_densities); t_skin, if not
+ * NULL, receives it.  Nothing changes where the reference returns early (t_skin_relax <= 0,
+ * no positive albedo, no positive absorbed flux).  Waits for the device. */
+athad_status athad_update_skin_temperature(athad_ctx* ctx, double t_skin_relax, double* t_skin);
 /* ThermoAtm::co2Column (ThermoAtm.h:1096-1137; call sites cAtmosphereModel.cpp:632, 1416):
  * ATHAD_2D_CO2_TOTAL and the CO2 budget.  Waits for the device. */
 athad_status athad_co2_column(athad_ctx* ctx, athad_budget_report* out);

@@ -131,7 +131,7 @@ void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* 
  * terrain) */
 void or_post_rk4_filters(int im, int jm, int km, const or_params* p, double* const* f);
 /* AtomUtils::damp_wiggles(field, along i, j, k), lib/Utils.cpp:429-531 */
-void or_damp_wiggles(int im, int jm, int km, double* field);
+void or_damp_wiggles(int im, int jm, int km, double* field, int compat);
 int  or_polar_passes(int jm, int j, const double* sin_w);
 
 /* TurbulenceAtm::run, TurbulenceAtm.h:62-79 (compute_vel_star, compute_sources with the
@@ -181,6 +181,11 @@ void or_stand_atm_dew_point(int im, int jm, int km, const or_params* p, double* 
 void or_water_vapour_evaporation(int im, int jm, int km, const or_params* p, double* const* f,
                                  double* const* f2);
 void or_latent_sensible_heat(int im, int jm, int km, const or_params* p, int compat, double* const* f);
+
+/* cAtmosphereModel::updateSkinTemperature (cAtmosphereModel.cpp:291-327) with
+ * planetaryShortWave (:236-265) from the albedo [jm][km]: the new t_skin */
+double or_update_skin_temperature(int jm, int km, const or_params* p, const double* albedo,
+                                  double t_skin, double t_skin_relax);
 
 /* ThermoAtm::co2Column (ThermoAtm.h:1096-1137): co2_total and the mass-weighted mean q_CO2,
  * in the reference's serial (j, k, i) order; out = w_num, w_den. */

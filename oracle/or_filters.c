@@ -78,7 +78,9 @@ void or_post_rk4_filters(int im, int jm, int km, const or_params* p, double* con
     or_geom_free(&g);
 }
 
-void or_damp_wiggles(int im, int jm, int km, double* x)
+/* compat = 1: the reference's expression order; 0: the j pass adds the two neighbours first
+ * (mirror-exact), as the device does */
+void or_damp_wiggles(int im, int jm, int km, double* x, int compat)
 {
     const size_t n = (size_t)im * jm * km;
     double* tmp = (double*)malloc(sizeof(double) * n);
@@ -98,8 +100,11 @@ void or_damp_wiggles(int im, int jm, int km, double* x)
         for (int j = 0; j < jm; j++) {
             const int jm1 = (j - 1 < 0) ? 0 : j - 1, jp1 = (j + 1 > jm - 1) ? jm - 1 : j + 1;
             for (int k = 0; k < km; k++)
-                x[OR_IDX(i, j, k)] = tmp[OR_IDX(i, j, k)]
-                    + coeff * (tmp[OR_IDX(i, jm1, k)] - 2.0 * tmp[OR_IDX(i, j, k)] + tmp[OR_IDX(i, jp1, k)]);
+                x[OR_IDX(i, j, k)] = compat
+                    ? tmp[OR_IDX(i, j, k)]
+                      + coeff * (tmp[OR_IDX(i, jm1, k)] - 2.0 * tmp[OR_IDX(i, j, k)] + tmp[OR_IDX(i, jp1, k)])
+                    : tmp[OR_IDX(i, j, k)]
+                      + coeff * ((tmp[OR_IDX(i, jm1, k)] + tmp[OR_IDX(i, jp1, k)]) - 2.0 * tmp[OR_IDX(i, j, k)]);
         }
     /* along i, clamped at the surface and the lid */
     memcpy(tmp, x, sizeof(double) * n);

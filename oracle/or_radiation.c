@@ -116,3 +116,33 @@ void or_radiative_heating(int im, int jm, int km, const or_params* p, double ome
     for (size_t q = 0; q < n; q++) f[OF_T][q] = t_backup[q] * (1.0 - omega_rad) + f[OF_T][q] * omega_rad;
     free(t_backup);
 }
+
+/* cAtmosphereModel::updateSkinTemperature (cAtmosphereModel.cpp:291-327) with
+ * planetaryShortWave (:236-265) and the insolation profile of MultiLayerRadiation.h:102-108 */
+double or_update_skin_temperature(int jm, int km, const or_params* p, const double* albedo,
+                                  double t_skin, double t_skin_relax)
+{
+    if (t_skin_relax <= 0.0) return t_skin;
+    const int j_max = jm - 1, j_half = j_max / 2;
+    double* sw = (double*)malloc(sizeof(double) * jm);
+    for (int j = 0; j < jm; j++) sw[j] = p->rad_pole_short;
+    const double rad_short_eff = p->rad_pole_short - p->rad_equator_short;
+    for (int j = j_half; j >= 0; j--) sw[j] = rad_short_eff * parabola((double)j / (double)j_half) + p->rad_pole_short;
+    for (int j = j_max; j > j_half; j--) sw[j] = sw[j_max - j];
+    double w_sum = 0.0, abs_w = 0.0, alb_max = 0.0;
+    for (int j = 0; j < jm; j++) {
+        const double w = cos((j / (double)(jm - 1) - 0.5) * M_PI);
+        double alb_k = 0.0;
+        for (int k = 0; k < km; k++) alb_k += albedo[(size_t)j * km + k];
+        alb_k /= (double)km;
+        alb_max = or_max(alb_max, alb_k);
+        w_sum += w;
+        abs_w += w * (1.0 - alb_k) * sw[j];
+    }
+    free(sw);
+    if (!(w_sum > 0.0) || !(alb_max > 0.0)) return t_skin;
+    const double in_mean = abs_w / w_sum + p->geothermal_flux;
+    if (!(in_mean > 0.0)) return t_skin;
+    const double target = pow(in_mean / p->sigma, 0.25);
+    return t_skin + or_min(1.0, t_skin_relax) * (target - t_skin);
+}

@@ -70,6 +70,7 @@ struct NullBuf : std::streambuf {
 };
 NullBuf g_null;
 std::streambuf* g_saved = nullptr;
+std::streambuf* g_null_buf() { return &g_null; }
 
 Array* field3(cAtmosphereModel* m, const std::string& n)
 {
@@ -444,6 +445,17 @@ void ref_budgets(void* p, double* out)
         out[3 + i] = m->m_air_levels[i];
         out[3 + m->im + i] = m->m_q_h2o_levels[i];
     }
+}
+
+// cAtmosphereModel::updateSkinTemperature with the given relaxation: the new t_skin
+double ref_skin(void* p, double relax)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->t_skin_relax = relax;
+    std::streambuf* prev = std::cout.rdbuf(g_null_buf());
+    m->updateSkinTemperature(false);
+    std::cout.rdbuf(prev);
+    return m->t_skin;
 }
 
 // ThermoAtm::waterVapourEvaporation and ::latentSensibleHeat

@@ -50,6 +50,18 @@ def lib():
     return _lib
 
 
+def update_skin_temperature(params, albedo, t_skin, relax):
+    """or_update_skin_temperature: cAtmosphereModel::updateSkinTemperature on a (jm, km)
+    albedo."""
+    a = np.ascontiguousarray(albedo, dtype=np.float64)
+    fn = lib().or_update_skin_temperature
+    fn.restype = ctypes.c_double
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                   ctypes.c_double, ctypes.c_double]
+    return fn(a.shape[0], a.shape[1], ctypes.byref(params), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+              t_skin, relax)
+
+
 class Step(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("diffusion_ramp", ctypes.c_double),
                 ("buoyancy_ramp", ctypes.c_double), ("write_diagnostics", ctypes.c_int32),
@@ -261,7 +273,9 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_two_cat_ice_scheme(im, jm, km, ctypes.byref(self.params), F)
 
-    def damp_wiggles(self, name):
+    def damp_wiggles(self, name, compat=0):
+        """or_damp_wiggles: AtomUtils::damp_wiggles; compat=1 the reference's summation order
+        in the j pass, 0 the mirror-exact one of the device."""
         im, jm, km = self.shape
         a = self.f[name]
-        lib().or_damp_wiggles(im, jm, km, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        lib().or_damp_wiggles(im, jm, km, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(compat))

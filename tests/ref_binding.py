@@ -140,6 +140,14 @@ class Reference:
         f.argtypes = [ctypes.c_void_p]
         f(self.h)
 
+    def skin(self, relax: float) -> float:
+        """cAtmosphereModel::updateSkinTemperature with t_skin_relax = relax: the new t_skin
+        (relax = 0 reads it unchanged)."""
+        f = self.lib.ref_skin
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        f.restype = ctypes.c_double
+        return f(self.h, relax)
+
     def budgets(self, threads=1) -> dict:
         """ThermoAtm::co2Column and ::waterBudget as first calls: the references they set
         (one thread by default, so the OpenMP sums run in the serial order)."""

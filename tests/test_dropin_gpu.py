@@ -117,8 +117,10 @@ def test_dropin_boundary_conditions(model):
 
 def test_dropin_filters(model):
     """The post-RK4 filters and the moist iteration's damp_wiggles through the adapter, on
-    the reference's state with grid-scale noise added: bit-identical to the reference's own
-    AtomUtils calls."""
+    the reference's state with grid-scale noise added: the filtered velocities bit-identical
+    to the reference's own AtomUtils calls; the damped fields within 1e-15 of each field's
+    largest magnitude (the device adds the two meridional neighbours first, so that mirrored
+    rows round alike; the reference subtracts first)."""
     R, snap = model
     im, jm, km = R.shape
     rng = np.random.default_rng(7)
@@ -138,7 +140,10 @@ def test_dropin_filters(model):
     out = run_both(R, noisy, cpu, gpu, ["u", "v", "w", "t", "c", "cloud", "ice"])
     reset(R, snap)
     for n, (a, b) in out.items():
-        assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))
+        if n in ("u", "v", "w"):
+            assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))
+        else:
+            assert relerr(a, b) <= 1e-15, (n, relerr(a, b))
 
 
 def test_dropin_turbulence(model):

@@ -1,7 +1,8 @@
 """The smoothing filters on the device against the oracle (pinned bit for bit against the
 reference in test_pin_reference.py): athad_post_rk4_filters (polar zonal filter of u, v, w;
 radial Shapiro filters) and athad_damp_wiggles.  Tolerance: bit-identical (1-2-1 and
-4th-order sums in the reference's order, no fused multiply-add).  Both filters keep a
+4th-order sums in the oracle's order, no fused multiply-add; damp_wiggles' meridional pass
+adds the two neighbours first, the oracle's mirror-exact form).  Both filters keep a
 mirror-symmetric state mirror-symmetric.
 """
 import numpy as np

@@ -14,7 +14,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating;
   * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm;
   * the surface fluxes waterVapourEvaporation and latentSensibleHeat;
-  * the mass budgets co2Column and waterBudget (their sums on one thread).
+  * the mass budgets co2Column and waterBudget (their sums on one thread);
+  * updateSkinTemperature with planetaryShortWave.
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
@@ -25,7 +26,7 @@ import pytest
 
 import ref_binding
 from athad_cond_b200._abi import FIELD_NAMES, config_params, Wall
-from oracle_binding import OracleState
+from oracle_binding import OracleState, update_skin_temperature
 
 pytestmark = pytest.mark.skipif(not ref_binding.available("pin"),
                                 reason="reference not built (oracle/_ref/pin)")
@@ -188,7 +189,7 @@ def test_damp_wiggles_bit_exact(ref):
     R, o = fresh(ref)
     for n in ("t", "ice", "c", "cloud"):
         R.damp_wiggles(n)
-        o.damp_wiggles(n)
+        o.damp_wiggles(n, compat=1)
     assert_identical(R, o, ["t", "ice", "c", "cloud"])
 
 
@@ -362,3 +363,17 @@ def test_mass_budgets_bit_exact(ref):
     for key in ("air_levels", "h2o_levels"):
         assert np.array_equal(r[key], q[key]), key
     assert np.array_equal(R.get2("co2_total"), o.f2["co2_total"])
+
+
+def test_skin_temperature_bit_exact(ref):
+    """cAtmosphereModel::updateSkinTemperature after MultiLayerRadiation::run (which sets the
+    albedo and the insolation profile), twice in a row."""
+    R, o = fresh(ref)
+    R.mlr()
+    albedo = R.get2("albedo")
+    p = config_params()
+    t = R.skin(0.0)
+    for _ in range(2):
+        want = update_skin_temperature(p, albedo, t, 0.25)
+        t = R.skin(0.25)
+        assert t == want

@@ -10,7 +10,7 @@ import pytest
 
 from athad_cond_b200 import GpuAtmosphere, make_state, mirror
 from athad_cond_b200._abi import config_params
-from oracle_binding import OracleState
+from oracle_binding import OracleState, update_skin_temperature
 
 pytestmark = pytest.mark.gpu
 
@@ -66,3 +66,21 @@ def test_radiation_keeps_mirror_symmetry():
         for n in ("epsilon_2D", "albedo"):
             a = g.download_2d(n)
             assert np.array_equal(a, a[::-1, :]), n
+
+
+def test_skin_temperature_matches_oracle():
+    """athad_update_skin_temperature (cAtmosphereModel::updateSkinTemperature): the new t_skin
+    identical to the oracle's, twice in a row from the albedo on the device; t_skin_relax = 0
+    leaves it."""
+    grid = (11, 21, 41)
+    rng = np.random.default_rng(151)
+    albedo = 0.05 + 0.5 * rng.random(grid[1:])
+    p = config_params()
+    with GpuAtmosphere(*grid, p) as g:
+        g.upload_2d("albedo", albedo)
+        t = p.t_skin
+        assert g.update_skin_temperature(0.0) == t
+        for _ in range(2):
+            want = update_skin_temperature(p, albedo, t, 0.25)
+            t = g.update_skin_temperature(0.25)
+            assert t == want and t != p.t_skin
