@@ -76,34 +76,27 @@ __global__ void __launch_bounds__(128) radial_columns_kernel(FilterArgs a)
     }
 }
 
-// damp_wiggles along j (clamped): out of place.  The two neighbours are added first, so the
-// result at row jm-1-j is bit for bit the result at row j of the mirrored field; the
-// reference's left-to-right (v[j-1] - 2 v[j]) + v[j+1] rounds the mirrored rows differently
-// (one rounding, an ulp of the field at most).
-__global__ void __launch_bounds__(128) wiggle_j_kernel(Dims d, const double* __restrict__ src, double* __restrict__ dst)
+// damp_wiggles along j then along i (both clamped), one thread per cell, out of place: the
+// radial pass reads only the meridional pass's values at i-1, i, i+1 of its own column, so
+// the thread forms those three (from the zonal pass's output) and writes the cell's result.
+// The meridional pass adds the two neighbours first, so the result at row jm-1-j is bit for
+// bit the result at row j of the mirrored field; the reference's left-to-right
+// (v[j-1] - 2 v[j]) + v[j+1] rounds the mirrored rows differently (an ulp at most).
+__global__ void __launch_bounds__(128) wiggle_ji_kernel(Dims d, const double* __restrict__ src, double* __restrict__ dst)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, i = blockIdx.z;
     if (k >= d.km) return;
     const int jm1 = (j > 0) ? j - 1 : 0, jp1 = (j < d.jm - 1) ? j + 1 : d.jm - 1;
-    const double c = src[idx3(d, i, j, k)];
-    dst[idx3(d, i, j, k)] = c + 0.25 * ((src[idx3(d, i, jm1, k)] + src[idx3(d, i, jp1, k)]) - 2.0 * c);
-}
-
-// damp_wiggles along i (clamped): in place, one column per thread
-__global__ void __launch_bounds__(128) wiggle_i_kernel(Dims d, double* __restrict__ x)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (k >= d.km) return;
-    double* col = x + idx3(d, 0, j, k);
-    const long long s = d.plane;
-    double om1 = col[0], o0 = col[0];
-    for (int i = 0; i < d.im; i++) {
-        const double op1 = (i + 1 <= d.im - 1) ? col[(i + 1) * s] : o0;
-        col[i * s] = o0 + 0.25 * (om1 - 2.0 * o0 + op1);
-        om1 = o0; o0 = op1;
+    const int im1 = (i > 0) ? i - 1 : 0, ip1 = (i < d.im - 1) ? i + 1 : d.im - 1;
+    double v[3];
+    const int ii[3] = {im1, i, ip1};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const double c = src[idx3(d, ii[q], j, k)];
+        v[q] = c + 0.25 * ((src[idx3(d, ii[q], jm1, k)] + src[idx3(d, ii[q], jp1, k)]) - 2.0 * c);
     }
+    dst[idx3(d, i, j, k)] = v[1] + 0.25 * (v[0] - 2.0 * v[1] + v[2]);
 }
 
 }  // namespace
@@ -123,8 +116,7 @@ void launch_damp_wiggles(const Dims& d, double* f, double* scratch, cudaStream_t
     // along k: the row kernel with one pass, from f into scratch (the copy-in reads f)
     cudaMemcpyAsync(scratch, f, d.fstride * sizeof(double), cudaMemcpyDeviceToDevice, st);
     zonal_rows_kernel<<<dim3(d.jm, d.im, 1), 128, 2 * d.km * sizeof(double), st>>>(a, 1, 1);
-    wiggle_j_kernel<<<dim3((d.km + 127) / 128, d.jm, d.im), 128, 0, st>>>(d, scratch, f);
-    wiggle_i_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(d, f);
+    wiggle_ji_kernel<<<dim3((d.km + 127) / 128, d.jm, d.im), 128, 0, st>>>(d, scratch, f);
 }
 
 }  // namespace athad
