@@ -166,19 +166,31 @@ static void launch_bcs(const PoissonArgs& a, cudaStream_t st)
     poisson_bc_kernel<<<dim3((most + 127) / 128, 1, 3), 128, 0, st>>>(a);
 }
 
-// |p_dyn| ceiling (:583-594); writes only where the value changes
+// |p_dyn| ceiling (:583-594); writes only where the value changes.  A thread takes four
+// consecutive longitudes of one pitched row (two 16-byte loads; the pitch is a multiple of
+// 32), so a warp has 1 KB of loads in flight
+__device__ __forceinline__ bool ceiling_of(double v, double cap, double& out)
+{
+    if (!is_finite_bits(v)) { out = 0.0; return true; }
+    if (v > cap) { out = cap; return true; }
+    if (v < -cap) { out = -cap; return true; }
+    return false;
+}
+
 __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
 {
     const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= d.km || j >= d.jm) return;
-    const long long c = idx3(d, i, j, k);
-    const double v = a.p[c];
-    if (!is_finite_bits(v)) a.p[c] = 0.0;
-    else if (v > a.ceiling) a.p[c] = a.ceiling;
-    else if (v < -a.ceiling) a.p[c] = -a.ceiling;
+    const long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (q >= (long long)d.im * d.plane) return;
+    const int k0 = (int)(q % d.pitch);
+    const double2* p2 = reinterpret_cast<const double2*>(a.p + q);
+    const double2 v01 = p2[0], v23 = p2[1];
+    const double v[4] = {v01.x, v01.y, v23.x, v23.y};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        double w;
+        if (k0 + e < d.km && ceiling_of(v[e], a.ceiling, w)) a.p[q + e] = w;
+    }
 }
 
 void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st)
@@ -196,7 +208,8 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
     poisson_colour_kernel<1><<<half_grid, block, 0, st>>>(a);
     launch_bcs(a, st);
-    poisson_ceiling_kernel<<<grid, block, 0, st>>>(a);
+    const long long quads = (long long)d.im * d.plane / 4;
+    poisson_ceiling_kernel<<<(unsigned)((quads + 255) / 256), 256, 0, st>>>(a);
 }
 
 // the boundary conditions of a sweep alone (radial, pole, seam), PressureSolverAtm.h:504-552
