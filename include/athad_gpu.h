@@ -36,7 +36,7 @@ typedef enum athad_status {
     ATHAD_OK              = 0,
     ATHAD_ERR_INVALID     = 1,  /* bad argument (null pointer, size mismatch, bad id)  */
     ATHAD_ERR_CUDA        = 2,  /* a CUDA runtime call failed                          */
-    ATHAD_ERR_UNSUPPORTED = 3,  /* a configuration this build does not implement       */
+    ATHAD_ERR_UNSUPPORTED = 3,  /* a configuration this library does not implement     */
     ATHAD_ERR_OOM         = 4,  /* device allocation failed / budget exceeded          */
     ATHAD_ERR_NONFINITE   = 5,  /* a kernel's status word reported non-finite input    */
     ATHAD_ERR_TIMEOUT     = 6,  /* a bounded device-side wait gave up                  */

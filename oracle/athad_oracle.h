@@ -1,7 +1,7 @@
 /*
  * athad_oracle.h - CPU restatement of the ATHAD_COND model-iteration hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared against; it
+ * TEST INFRASTRUCTURE ONLY.  This is what the CUDA path is compared against; it
  * is never linked into, loaded by or called from the product.  Only tests/, the smoke()
  * entry point and the cpu_baseline leg of bench.py use it.
  *

@@ -1,6 +1,6 @@
 // ref_harness.cpp - a C entry layer around the unmodified reference, so the tests can run
 // the reference's own hot-path functions on a state they choose and read the results.
-// TEST INFRASTRUCTURE ONLY (the checker of the oracle); built into oracle/_ref/ by
+// TEST INFRASTRUCTURE ONLY (the oracle's pin); built into oracle/_ref/ by
 // oracle/ref/Makefile from the reference sources where they lie.
 //
 // The reference keeps its model state in private members of cAtmosphereModel and runs its

@@ -5,7 +5,7 @@ test_parity_gpu.py).  Stated tolerances, max |mixed - oracle| / max |oracle| per
   * one RK4 step: 1e-8 (the FP32 right-hand side perturbs only the dt-sized increment);
   * 100 RK4 steps on 21 x 91 x 181: 1e-6;
   * 1000 RK4 steps on 41 x 181 x 361 against the FP64 GPU form: 1e-5 for every
-    prognostic field (the north_star's bar for the dynamics).
+    prognostic field (the accuracy bar the mixed form is held to for the dynamics).
 Mirror symmetry is exact (bit for bit) for the mixed form too, as for the FP64 form.
 """
 import numpy as np
