@@ -5,11 +5,11 @@ CUDA sources (csrc/), the Python view of the ABI used by the tests and the bench
 a seeded synthetic-state builder.  Importing the package does not require a GPU; creating a
 GpuAtmosphere does, and fails loudly without one or without the built library.
 """
-from ._abi import (FIELD, FIELD_NAMES, FIELD2D, PROFILE, Params, Precision, Status, Turb, Wall,  # noqa: F401
-                   default_params, load_library, LIB_PATH)
-from .context import AthadError, GpuAtmosphere, GpuBatch  # noqa: F401
+from ._abi import (FIELD, FIELD_NAMES, FIELD2D, PROFILE, InitConfig, Params, Precision, Status, Turb,  # noqa: F401
+                   Wall, config_init, default_params, load_library, LIB_PATH)
+from .context import AthadError, GpuAtmosphere, GpuBatch, default_init_config  # noqa: F401
 from .synthetic import make_state, mirror, layer_heights  # noqa: F401
 
 __all__ = ["GpuAtmosphere", "GpuBatch", "AthadError", "make_state", "mirror", "layer_heights",
            "default_params", "load_library", "Params", "FIELD", "FIELD_NAMES", "Turb", "Wall",
-           "Precision"]
+           "Precision", "InitConfig", "config_init", "default_init_config"]

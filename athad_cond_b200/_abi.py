@@ -105,6 +105,45 @@ class Params(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class InitConfig(ctypes.Structure):
+    """athad_init_config: the configuration members the reference's initial state reads
+    beyond athad_params (cli/config_cond.xml values by default)."""
+    _fields_ = [("struct_size", ctypes.c_uint32), ("n_cells_hemisphere", ctypes.c_int32),
+                ("cell_amp_mode", ctypes.c_int32), ("pad0", ctypes.c_int32)] + [
+        (n, ctypes.c_double) for n in ("t_surf_equator", "t_surf_pole", "tropopause_equator",
+                                       "tropopause_pole", "cell_lat_scale", "co2_scale", "q_CO2",
+                                       "q_bg", "vel_star_init")]
+
+
+def composition(x):
+    """AtmMixture::resolve (MixtureAtm.h:82-109) of the eight mole fractions x_H2O, x_CO2,
+    x_N2, x_CH4, x_NH3, x_H2, x_CO, x_SO2: M_mean, R_mix, q_H2O, q_CO2, q_bg, M_bg, R_bg."""
+    R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010
+    m_H2O, m_CO2 = x[0] * M_H2O, x[1] * M_CO2
+    m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031 + x[5] * 0.002016 + x[6] * 0.028010 + x[7] * 0.064066
+    M_mean = m_H2O + m_CO2 + m_bg
+    x_bg = x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
+    M_bg = (m_bg / x_bg) if x_bg > 0.0 else 0.028014
+    return {"M_mean": M_mean, "R_mix": R_STAR / M_mean, "q_H2O": m_H2O / M_mean,
+            "q_CO2": m_CO2 / M_mean, "q_bg": m_bg / M_mean, "M_bg": M_bg, "R_bg": R_STAR / M_bg}
+
+
+CONFIG_X = (0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0)   # cli/config_cond.xml:77-84
+
+
+def config_init() -> InitConfig:
+    """cli/config_cond.xml's initial-state members (same as athad_default_init_config)."""
+    c = InitConfig()
+    c.struct_size = ctypes.sizeof(InitConfig)
+    c.n_cells_hemisphere, c.cell_amp_mode = 5, 0
+    c.t_surf_equator, c.t_surf_pole = 513.15, 503.15
+    c.tropopause_equator, c.tropopause_pole = 207000.0, 195000.0
+    c.cell_lat_scale, c.co2_scale, c.vel_star_init = 0.11, 1.0, 0.4
+    comp = composition(CONFIG_X)
+    c.q_CO2, c.q_bg = comp["q_CO2"], comp["q_bg"]
+    return c
+
+
 class StepScalars(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("diffusion_ramp", ctypes.c_double),
                 ("buoyancy_ramp", ctypes.c_double), ("write_diagnostics", ctypes.c_int32),
@@ -180,6 +219,8 @@ SIGNATURES = {
     "athad_download_profile": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_field_device_ptr": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_size_t)]),
     "athad_fill": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_double]),
+    "athad_default_init_config": (None, [ctypes.POINTER(InitConfig)]),
+    "athad_initial_state": (ctypes.c_int, [_P, ctypes.POINTER(InitConfig)]),
     "athad_store_n_level": (ctypes.c_int, [_P]),
     "athad_level_mean": (ctypes.c_int, [_P]),
     "athad_rk4_step": (ctypes.c_int, [_P, ctypes.POINTER(StepScalars)]),
@@ -283,13 +324,6 @@ def config_params() -> Params:
                 rad_equator_short=298.0, rad_pole_short=0.0, coeff_Dalton=0.7)
     for k, v in vals.items():
         setattr(p, k, v)
-    R_STAR, M_H2O, M_CO2 = 8.314462618, 0.018015, 0.044010
-    x = [0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0]
-    m_H2O, m_CO2 = x[0] * M_H2O, x[1] * M_CO2
-    m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031 + x[5] * 0.002016 + x[6] * 0.028010 + x[7] * 0.064066
-    M_mean = m_H2O + m_CO2 + m_bg
-    p.R_mix = R_STAR / M_mean
-    x_bg = x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
-    p.M_bg = (m_bg / x_bg) if x_bg > 0.0 else 0.028014
-    p.R_bg = R_STAR / p.M_bg
+    comp = composition(CONFIG_X)
+    p.R_mix, p.M_bg, p.R_bg = comp["R_mix"], comp["M_bg"], comp["R_bg"]
     return p

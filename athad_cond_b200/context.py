@@ -15,6 +15,13 @@ from . import _abi
 from ._abi import FIELD, FIELD2D, PROFILE, Status
 
 
+def default_init_config() -> _abi.InitConfig:
+    """athad_default_init_config: cli/config_cond.xml's initial-state members."""
+    c = _abi.InitConfig()
+    _abi.load_library().athad_default_init_config(ctypes.byref(c))
+    return c
+
+
 class AthadError(RuntimeError):
     def __init__(self, status: int, message: str):
         self.status = Status(status) if status in Status._value2member_map_ else status
@@ -115,6 +122,15 @@ class GpuAtmosphere:
         self._check(self.lib.athad_download_profile(self._h, PROFILE[name], _dptr(out), out.size))
         return out
 
+    # ---- the initial state ----
+    def initial_state(self, config: _abi.InitConfig | None = None):
+        """cAtmosphereModel::RunTimeSlice's deterministic initial state (cAtmosphereModel.cpp:
+        468-668), built on the device for this grid: every field, 2-D field and profile is
+        overwritten.  config: the initial-state members (default cli/config_cond.xml)."""
+        cfg = config if config is not None else default_init_config()
+        cfg.struct_size = ctypes.sizeof(_abi.InitConfig)
+        self._check(self.lib.athad_initial_state(self._h, ctypes.byref(cfg)))
+
     def upload_state(self, state: dict):
         for name, a in state.items():
             if name in FIELD:
@@ -156,8 +172,8 @@ class GpuAtmosphere:
         self._check(self.lib.athad_pressure_sweep(self._h, n_sweeps, total_iter_count))
 
     def boundary_conditions(self):
-        """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi
-        (call site cAtmosphereModel.cpp:1439-1442)."""
+        """BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, bcTheta, bcPhi, bcScalarSurfSur,
+        bcSolidGround (call site cAtmosphereModel.cpp:1439-1446)."""
         self._check(self.lib.athad_boundary_conditions(self._h))
 
     def post_rk4_filters(self):

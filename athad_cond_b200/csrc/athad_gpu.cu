@@ -194,6 +194,7 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     for (int i = 0; i < im; i++)
         height[i] = (double)(float)((std::exp(params->zeta * (rad[i] - rad[0])) - 1) * (double)hL);
     c->layer_height1 = height[1];
+    c->height_h = height;
     for (int i = 0; i < im; i++) {   // SaturationAdjustment::computeSteps: float difference
         const float h1 = (i + 1 <= im - 1) ? (float)height[i + 1] : -1.0f;
         const float h0 = (float)height[i];
@@ -753,7 +754,10 @@ athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
     return ATHAD_OK;
 }
 
-athad_status athad_boundary_conditions(athad_ctx* ctx)
+}  // extern "C"
+
+namespace athad {
+athad_status boundary_conditions(athad_ctx* ctx, int wall_bc)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
     const athad_params& p = ctx->p;
@@ -775,10 +779,19 @@ athad_status athad_boundary_conditions(athad_ctx* ctx)
     } else {
         a.dis_wall = 60.0 * nue_air / (0.0333 * y1_safe * y1_safe) * nd_omega; a.set_dis_wall = 1;
     }
+    a.wall_bc = wall_bc;
+    a.tke_max_nd = 1000.0 / (p.u_0 * p.u_0);
+    a.nue_max = 1000.0 / (p.u_0 * p.L_atm);
+    a.vel_max_nd = 100.0 / p.u_0;
     launch_boundary_conditions(a, ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "boundary_conditions");
     return ATHAD_OK;
 }
+}  // namespace athad
+
+extern "C" {
+
+athad_status athad_boundary_conditions(athad_ctx* ctx) { return athad::boundary_conditions(ctx, 1); }
 
 athad_status athad_post_rk4_filters(athad_ctx* ctx)
 {

@@ -116,6 +116,7 @@ struct athad_ctx {
     double dr = 0, dthe = 0, dphi = 0, shell_len = 0, metric_r0 = 0;
     double layer_height1 = 0;   // get_layer_height(1): the first layer's height, float-rounded
     std::vector<double> rad;
+    std::vector<double> height_h;             // [im] get_layer_height(i), float values (host copy)
     int64_t poisson_sweeps_since_reset = 0;
     MGSolver* mg = nullptr;
     std::string err;
@@ -142,4 +143,7 @@ inline athad_status cuda_check(athad_ctx* c, cudaError_t e, const char* what)
 
 namespace athad {
 void mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a);
+// the boundary conditions of athad_boundary_conditions, with (wall_bc = 1) or without the
+// turbulence wall values
+athad_status boundary_conditions(athad_ctx* ctx, int wall_bc);
 }

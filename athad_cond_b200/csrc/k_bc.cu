@@ -1,12 +1,12 @@
 // k_bc.cu - the per-iteration boundary conditions of the atmosphere on sm_100a
 // (athad_boundary_conditions): BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc,
-// BC_Atm::bcTheta and BC_Atm::bcPhi, in the order of their call site
-// (cAtmosphereModel.cpp:1439-1442), for flat terrain (every cell is air, so
-// bcScalarSurfSur and bcSolidGround change nothing).
+// BC_Atm::bcTheta, BC_Atm::bcPhi, BC_Atm::bcScalarSurfSur and BC_Atm::bcSolidGround, in the
+// order of their call site (cAtmosphereModel.cpp:1439-1446), for flat terrain (every cell is
+// air, so of the last two only bcSolidGround's value limits over every cell change anything).
 //
 // Three launches, one per direction, because each reads the boundary cells the previous
 // one wrote (the corners): radial columns (one thread per (j, k)), polar rows (one thread
-// per (i, k)), seam rows (one thread per (i, j)).  Every formula is a copy or a short sum
+// per (i, k)), seam rows (one thread per (i, j)); then the value limits, cell by cell.  Every formula is a copy or a short sum
 // evaluated in the reference's order; the file is compiled without fused multiply-add, so
 // the results are bit-identical to the reference's.
 //
@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(128) bc_radius_kernel(BcArgs a)
     if (F[ATHAD_Q_V_U][c0] < 0.0) F[ATHAD_Q_V_U][c0] = 0.0;                            // :734-735
     if (F[ATHAD_Q_C_U][c0] < 0.0) F[ATHAD_Q_C_U][c0] = 0.0;
     // apply_wall_bc: the wall values of tke, nue and dis
+    if (!a.wall_bc) return;
     const double vs = a.vel_star[(long long)j * d.pitch + k];
     F[ATHAD_TKE][c0] = vs * vs / a.tke_wall_den;
     F[ATHAD_NUE][c0] = 0.0;
@@ -165,6 +166,38 @@ __global__ void __launch_bounds__(128) bc_phi_kernel(BcArgs a)
     }
 }
 
+// bcScalarSurfSur and bcSolidGround (BC_Atm.h:1026-1123, 23-547) with flat terrain: their
+// land branches and the surface copies x[0] := x[i_mount = 0] change nothing, which leaves
+// bcSolidGround's value limits over every cell (:470-545), one (i, j) row per block row
+__global__ void __launch_bounds__(256) bc_limits_kernel(BcArgs a)
+{
+    const Dims& d = a.d;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.km) return;
+    const long long c = (long long)blockIdx.y * d.pitch + k;
+    double* const* F = a.F;
+    const int sign[5] = {ATHAD_C, ATHAD_CLOUD, ATHAD_ICE, ATHAD_TKE, ATHAD_DIS};
+#pragma unroll
+    for (int q = 0; q < 5; q++)
+        if (F[sign[q]][c] < 0.0) F[sign[q]][c] = 0.0;
+    const double prod_max = 1.0e4, dis_max = 1.0e6;
+    F[ATHAD_TKE][c] = safe_clamp(F[ATHAD_TKE][c], 0.0, a.tke_max_nd);
+    F[ATHAD_TKEN][c] = safe_clamp(F[ATHAD_TKEN][c], 0.0, a.tke_max_nd);
+    F[ATHAD_DIS][c] = safe_clamp(F[ATHAD_DIS][c], 1.0e-10, dis_max);
+    F[ATHAD_DISN][c] = safe_clamp(F[ATHAD_DISN][c], 1.0e-10, dis_max);
+    F[ATHAD_NUE][c] = safe_clamp(F[ATHAD_NUE][c], 0.0, a.nue_max);
+    F[ATHAD_PROD][c] = safe_clamp(F[ATHAD_PROD][c], 0.0, prod_max);
+    F[ATHAD_TKE_SOURCE][c] = safe_clamp(F[ATHAD_TKE_SOURCE][c], -prod_max, prod_max);
+    F[ATHAD_DIS_SOURCE][c] = safe_clamp(F[ATHAD_DIS_SOURCE][c], -prod_max, prod_max);
+    const int vel[6] = {ATHAD_U, ATHAD_UN, ATHAD_V, ATHAD_VN, ATHAD_W, ATHAD_WN};
+    const double vm = a.vel_max_nd;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const double v = F[vel[q]][c];
+        F[vel[q]][c] = !is_finite_bits(v) ? 0.0 : (v < -vm) ? -vm : (v > vm) ? vm : v;
+    }
+}
+
 }  // namespace
 
 void launch_boundary_conditions(const BcArgs& a, cudaStream_t st)
@@ -173,6 +206,7 @@ void launch_boundary_conditions(const BcArgs& a, cudaStream_t st)
     bc_radius_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
     bc_theta_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
     bc_phi_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
+    bc_limits_kernel<<<dim3((d.km + 255) / 256, d.im * d.jm), 256, 0, st>>>(a);
 }
 
 }  // namespace athad

@@ -194,6 +194,9 @@ struct BcArgs {
     double tke_wall_den;        // sqrt(C_nue) * u_0 * u_0
     double dis_wall;            // omega (or epsilon) at the wall, non-dimensional
     int set_dis_wall;
+    int wall_bc;                // 0: no wall values (RunTimeSlice's boundary conditions)
+    // bcSolidGround's value limits (BC_Atm.h:470-545), non-dimensional
+    double tke_max_nd, nue_max, vel_max_nd;
 };
 void launch_boundary_conditions(const BcArgs& a, cudaStream_t st);
 

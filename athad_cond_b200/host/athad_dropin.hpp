@@ -13,7 +13,8 @@
 //     MoistConvectionRun(m, it) MoistConvection(m).run(it)                   :1247
 //     Densities(m, water)       ThermoAtm(m).densities(water)                :567, 634, 1418
 //     BoundaryConditions(m)     BC_Atm(m).bcRadius(); TurbulenceAtm(m).apply_wall_bc();
-//                               BC_Atm(m).bcTheta(); BC_Atm(m).bcPhi()       :1439-1442
+//                               BC_Atm(m).bcTheta(); BC_Atm(m).bcPhi();
+//                               bcScalarSurfSur(); bcSolidGround()           :1439-1446
 //     PostRK4Filters(m)         the polar zonal and radial Shapiro filters   :1507-1520
 //     DampMoistWiggles(m)       AtomUtils::damp_wiggles of t, ice, c, cloud  :1225-1228
 //     TurbulenceRun(m)          TurbulenceAtm(m).run()                       :614, 1426
@@ -249,13 +250,14 @@ public:
         down_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
     }
 
-    // the per-iteration boundary conditions (cAtmosphereModel.cpp:1439-1442), flat terrain
+    // the per-iteration boundary conditions (cAtmosphereModel.cpp:1439-1446), flat terrain
     void BoundaryConditions(Model& m)
     {
 #define ATHAD_BC_FIELDS(X) X(ATHAD_T, t) X(ATHAD_U, u) X(ATHAD_V, v) X(ATHAD_W, w) X(ATHAD_C, c) \
         X(ATHAD_CLOUD, cloud) X(ATHAD_ICE, ice) X(ATHAD_GR, gr) X(ATHAD_CO2, co2) X(ATHAD_TKE, tke) \
         X(ATHAD_DIS, dis) X(ATHAD_NUE, nue) X(ATHAD_PROD, prod) X(ATHAD_TKE_SOURCE, tke_source) \
         X(ATHAD_DIS_SOURCE, dis_source) X(ATHAD_UN, un) X(ATHAD_VN, vn) X(ATHAD_WN, wn) \
+        X(ATHAD_TKEN, tken) X(ATHAD_DISN, disn) \
         X(ATHAD_P_STAT, p_stat) X(ATHAD_R_HUMID, r_humid) X(ATHAD_R_DRY, r_dry) X(ATHAD_S_C_C, S_c_c) \
         X(ATHAD_S_V, S_v) X(ATHAD_S_C, S_c) X(ATHAD_S_I, S_i) X(ATHAD_S_R, S_r) X(ATHAD_S_S, S_s) \
         X(ATHAD_S_G, S_g) X(ATHAD_Q_V_U, q_v_u) X(ATHAD_Q_C_U, q_c_u) X(ATHAD_U_U, u_u) \

@@ -8,13 +8,17 @@ densities every 2nd, and the time-level copy (storeIntermediateData3D) that clos
 written by the last RK4 stage (athad_step_scalars.store_n_level: nothing runs in between).
 Metric: grid-point RK4 steps per second = im*jm*km * steps / time.
 
-Workload: the 41 x 181 x 361 grid, 1000 iterations, run twice from the same seeded
-synthetic state (the reference's shapes and value ranges): the plain FP64 form and the
-mixed-precision form (athad_params.precision = MIXED: FP32 RK4 stencil arithmetic and stage
-storage, FP64 time level and column physics).  The headline value is the mixed form; both
-forms' rates, their RK4 rooflines and the mixed form's per-field error against the FP64
-form after the same iterations are in the line.  The inputs (about 40 fields of 21 MB) are
-far larger than the 126 MB L2, so no flush is needed between steps.
+Workload: the 41 x 181 x 361 grid, 1000 iterations, run twice from the reference's
+deterministic initial state (cAtmosphereModel::RunTimeSlice: the integrated moist adiabat
+over the symmetric parabolic sea-surface temperature, built on the device by
+athad_initial_state): the plain FP64 form and the mixed-precision form
+(athad_params.precision = MIXED: FP32 RK4 stencil arithmetic and stage storage, FP64 time
+level and column physics).  The headline value is the mixed form; both forms' rates, their
+RK4 rooflines, the mixed form's per-field error against the FP64 form after the same
+iterations, the FP64 form's own one-ulp sensitivity over those iterations and a leg on the
+reference's own 61 x 181 x 361 grid (the grid, state and cadence of the reference arm) are
+in the line.  The inputs (about 40 fields of 21 MB) are far larger than the 126 MB L2, so
+no flush is needed between steps.
 
 --gpus N > 1 (under torchrun): independent replicas, one per GPU (the path has no
 cross-replica exchange), weak scaling; value = all ranks' grid-point steps / max time.
@@ -36,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 GRID = (41, 181, 361)
+NATIVE_GRID = (61, 181, 361)   # the reference's compiled-in grid (cAtmosphereModel.h:162)
 # fields the reference's off-path modules (boundary conditions, filters, turbulence, ice
 # scheme, radiation) write between hot-path calls: uploaded every step in the end-to-end
 # measurement; and the fields they read back afterwards.
@@ -151,20 +156,15 @@ def whole_job_value(points: int, steps: int, world: int, ms: float) -> float:
     return points * steps * world / (ms * 1e-3)
 
 
-def replica_seed(rank: int) -> int:
-    """Each replica integrates its own seeded state."""
-    return 20261203 + rank
-
-
 def cpu_baseline(seconds_budget: float = 20.0):
     """The oracle (single-threaded C restatement of the reference path) on a bounded
-    sample: whole model iterations of the same grid until the budget is used."""
+    sample: whole model iterations of the same grid, from the same initial state (the
+    oracle's own restatement of it, not timed), until the budget is used."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from athad_cond_b200 import make_state
-    from athad_cond_b200._abi import config_params
+    from athad_cond_b200._abi import config_init, config_params
     from oracle_binding import OracleState
     im, jm, km = GRID
-    o = OracleState(make_state(im, jm, km, seed=20261203), config_params())
+    o = OracleState.initial(im, jm, km, config_params(), config_init(), compat=0)
     t0 = time.perf_counter()
     it = 0
     while True:
@@ -256,24 +256,28 @@ def reference_arm(args):
     return line
 
 
-def run_form(args, rank, world, device, precision):
-    """One form (FP64 or mixed) of the model iteration: warm-up, the device-timed region
-    of args.steps iterations, then the end-to-end leg through the C ABI with host buffers.
-    Returns the timings and the final fields of ERR_FIELDS (for the error report)."""
+def run_form(args, rank, world, device, precision, grid=None, steps=None, perturb_t=False, e2e=True):
+    """One form (FP64 or mixed) of the model iteration from the reference's initial state
+    (built on the device by athad_initial_state): warm-up, the device-timed region of
+    `steps` iterations, then the end-to-end leg through the C ABI with host buffers.
+    perturb_t: t raised by one ulp everywhere after the initial state (the FP64 form's own
+    sensitivity to rounding).  Returns the timings and the final fields of ERR_FIELDS."""
     import numpy as np
     import torch
-    from athad_cond_b200 import GpuAtmosphere, make_state
-    from athad_cond_b200._abi import config_params, Precision
+    from athad_cond_b200 import GpuAtmosphere
+    from athad_cond_b200._abi import config_params
 
-    im, jm, km = GRID
+    im, jm, km = grid or GRID
+    steps = args.steps if steps is None else steps
     pts = im * jm * km
     p = config_params()
     p.precision = int(precision)
-    st = make_state(im, jm, km, seed=replica_seed(rank))
-    st["Evaporation"] = np.full((jm, km), 20.0)
     g = GpuAtmosphere(im, jm, km, p)
-    g.upload_state(st)
     stream = torch.cuda.Stream(device=device)
+    g.initial_state()
+    if perturb_t:
+        t = g.download("t")
+        g.upload("t", np.nextafter(t, np.inf))
     g.set_stream(stream.cuda_stream)
     dt = 4e-5
     dist = world > 1
@@ -294,7 +298,7 @@ def run_form(args, rank, world, device, precision):
     rk_ev, ps_ev = [], []
     with ClockSampler(device.index if device.index is not None else 0) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             it += 1
             if it % 4 == 0:
                 pa = torch.cuda.Event(enable_timing=True)
@@ -325,21 +329,21 @@ def run_form(args, rank, world, device, precision):
     final = {n: g.download(n) for n in ERR_FIELDS}
     fields_per_point = RK4_BYTES_PER_POINT[int(precision)]
     rk_avg = sum(rk_ms) / len(rk_ms)
-    res = {"value": whole_job_value(pts, args.steps, world, ms), "ms_per_step": ms / args.steps,
+    res = {"value": whole_job_value(pts, steps, world, ms), "ms_per_step": ms / steps,
            "rk4_ms": rk_avg, "achieved": fields_per_point * pts / (rk_avg * 1e-3) / 1e9,
            "rk4_bytes_per_point": fields_per_point, "clocks": clk.summary(), "final": final,
            "pressure_ms": (sum(ps_ms) / len(ps_ms)) if ps_ms else None,
            "e2e_value": None, "h2d": 0, "d2h": 0, "finite": True}
-    if args.no_e2e:
+    if args.no_e2e or not e2e:
         g.close()
         return res
 
     # ---- end to end through the C ABI with host buffers ----
-    host_up = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in E2E_UP}
-    host_down = {n: torch.empty(GRID, dtype=torch.float64).pin_memory() for n in E2E_DOWN}
+    host_up = {n: torch.from_numpy(g.download(n)).pin_memory() for n in E2E_UP}
+    host_down = {n: torch.empty((im, jm, km), dtype=torch.float64).pin_memory() for n in E2E_DOWN}
     lib = g.lib
     from athad_cond_b200._abi import FIELD
-    e2e_steps = max(4, min(args.steps, 40))
+    e2e_steps = max(4, min(steps, 40))
     g.synchronize()
     if dist:
         tdist.barrier()
@@ -365,14 +369,17 @@ def run_form(args, rank, world, device, precision):
     return res
 
 
-def field_errors(a: dict, b: dict) -> dict:
-    """max |a - b| / max |b| per field (b the FP64 form)."""
+def field_errors(a: dict, b: dict, beyond: float = 1e-5) -> dict:
+    """Per field: max |a - b| / max |b| (b the FP64 form) and the fraction of cells where
+    |a - b| / max |b| exceeds `beyond`."""
     import numpy as np
-    out = {}
+    out, frac = {}, {}
     for n in ERR_FIELDS:
         den = float(np.max(np.abs(b[n])))
-        out[n] = float(np.max(np.abs(a[n] - b[n]))) / den if den > 0 else float(np.max(np.abs(a[n])))
-    return out
+        d = np.abs(a[n] - b[n])
+        out[n] = float(np.max(d)) / den if den > 0 else float(np.max(np.abs(a[n])))
+        frac[n] = float(np.count_nonzero(d > beyond * den)) / d.size if den > 0 else 0.0
+    return out, frac
 
 
 def _iteration_fp64(g, it: int, dt: float = 4e-5):
@@ -551,7 +558,7 @@ def run_loop(args, device) -> dict:
     (or FP64) context; the readbacks the reference prints (residuum, budgets, skin
     temperature) inside the timed region."""
     import torch
-    from athad_cond_b200 import GpuAtmosphere, make_state
+    from athad_cond_b200 import GpuAtmosphere
     from athad_cond_b200._abi import Precision, config_params
     from athad_cond_b200.loop import ModelLoop
     import numpy as np
@@ -560,8 +567,8 @@ def run_loop(args, device) -> dict:
     p.precision = int(Precision.MIXED if args.precision != "fp64" else Precision.FP64)
     g = GpuAtmosphere(im, jm, km, p)
     stream = torch.cuda.Stream(device=device)
+    g.initial_state()
     g.set_stream(stream.cuda_stream)
-    g.upload_state(make_state(im, jm, km, seed=20261203))
     loop = ModelLoop(g)
     for _ in range(args.warmup):
         loop.iteration()
@@ -589,6 +596,10 @@ def main():
     ap.add_argument("--grid", default=None, help="IMxJMxKM (default: the 41x181x361 workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-envelope", action="store_true",
+                    help="skip the FP64 one-ulp sensitivity run of the error report")
+    ap.add_argument("--native-steps", type=int, default=100,
+                    help="iterations of the leg on the reference's own 61x181x361 grid (0: skip)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="forms to run; the headline value is the mixed form when it runs")
     ap.add_argument("--workload", default="iteration", choices=["iteration", "ensemble", "serving", "poisson", "loop"],
@@ -641,7 +652,7 @@ def main():
                     "value": r["value"], "unit": "grid-point steps/s", "n_gpus": 1,
                     "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_iteration"],
                     "higher_is_better": True, "dtype": "f32+f64" if args.precision != "fp64" else "f64",
-                    "data": "synthetic",
+                    "data": "the reference's deterministic initial state, built on the device",
                     "config": {"workload": "run_3D_loop with every module on the device, "
                                            f"{r['grid'][0]}x{r['grid'][1]}x{r['grid'][2]} grid",
                                "grid": r["grid"]}, "detail": r}
@@ -670,6 +681,22 @@ def main():
     forms = {"fp64": Precision.FP64, "mixed": Precision.MIXED}
     wanted = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     runs = {f: run_form(args, rank, world, device, forms[f]) for f in wanted}
+    envelope = None
+    if "fp64" in runs and "mixed" in runs and not args.no_envelope:
+        # the FP64 form against itself with t one ulp higher: how far rounding alone moves
+        # each field over the same iterations
+        pert = run_form(args, rank, world, device, Precision.FP64, perturb_t=True, e2e=False)
+        envelope = field_errors(pert["final"], runs["fp64"]["final"])
+    native = None
+    if args.native_steps > 0:
+        # the reference's own grid, initial state and cadence (what the reference arm runs)
+        native = {}
+        for f in wanted:
+            rr = run_form(args, rank, world, device, forms[f], grid=NATIVE_GRID, steps=args.native_steps)
+            native[f] = {"value": rr["value"], "ms_per_step": rr["ms_per_step"], "rk4_ms": rr["rk4_ms"],
+                         "e2e": rr["e2e_value"], "finite": rr["finite"]}
+        native["grid"] = list(NATIVE_GRID)
+        native["steps"] = args.native_steps
     base = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     if world > 1:
         import torch.distributed as tdist
@@ -701,8 +728,15 @@ def main():
             summary[f]["pressure_roofline_frac"] = pgbs / peak
     errors = None
     if "fp64" in runs and "mixed" in runs:
-        errors = {"after_iterations": args.warmup + args.steps, "fields": field_errors(
-            runs["mixed"]["final"], runs["fp64"]["final"]), "measure": "max|mixed-fp64| / max|fp64|"}
+        err, frac = field_errors(runs["mixed"]["final"], runs["fp64"]["final"])
+        errors = {"after_iterations": args.warmup + args.steps, "fields": err,
+                  "fraction_of_cells_beyond_1e-5": frac, "measure": "max|mixed-fp64| / max|fp64|"}
+        if envelope is not None:
+            errors["fp64_one_ulp_envelope"] = {
+                "fields": envelope[0], "fraction_of_cells_beyond_1e-5": envelope[1],
+                "measure": "max|fp64(t + 1 ulp) - fp64| / max|fp64| after the same iterations"}
+            errors["within_max_1e-5_envelope"] = {
+                n: bool(err[n] <= max(1e-5, envelope[0][n])) for n in ERR_FIELDS}
         summary["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
     form_text = {"mixed": "mixed-precision (FP32 RK4 stencil arithmetic and stage storage, FP64 time "
                           "level, final combination and column physics)",
@@ -712,7 +746,9 @@ def main():
         "value": r["value"], "unit": "grid-point steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64" if head_name == "mixed" else "f64", "data": "synthetic",
+        "dtype": "f32+f64" if head_name == "mixed" else "f64",
+        "data": "the reference's deterministic initial state (integrated moist adiabat, symmetric "
+                "parabolic sea-surface temperature, prescribed circulation cells), built on the device",
         "config": {"workload": f"{form_text} model iteration, {im}x{jm}x{km} grid "
                                "(RK4 every step, pressure sweep every 4th, saturation adjustment, "
                                "moist convection and densities every 2nd)",
@@ -729,6 +765,7 @@ def main():
                      "peak_source": peak_kind},
         "forms": summary,
         "error_vs_fp64": errors,
+        "native_grid": native,
         "cpu_baseline": base,
         "gpu_launches": launches,
         "clocks": r["clocks"],

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 9
+#define ATHAD_ABI_VERSION 10
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -296,6 +296,46 @@ athad_status athad_field_device_ptr(athad_ctx* ctx, athad_field f, double** ptr,
 /* Fill a field with a constant on the device. */
 athad_status athad_fill(athad_ctx* ctx, athad_field f, double value);
 
+/* ---- the initial state --------------------------------------------------------- */
+
+/* The configuration members the reference's initial state reads beyond athad_params
+ * (cAtmosphereModel members of the same name; athad_default_init_config fills the values of
+ * cli/config_cond.xml). */
+typedef struct athad_init_config {
+    uint32_t struct_size;        /* sizeof(athad_init_config)                             */
+    int32_t  n_cells_hemisphere; /* prescribed circulation cells per hemisphere, 5        */
+    int32_t  cell_amp_mode;      /* 0: unscaled amplitudes; 1, 2: scaled with cell_lat_scale */
+    int32_t  pad0;
+    double   t_surf_equator;     /* sea-surface temperature at the equator [K], 513.15   */
+    double   t_surf_pole;        /* ... at the poles [K], 503.15                          */
+    double   tropopause_equator; /* top of the convective column at the equator [m], 207000 */
+    double   tropopause_pole;    /* ... at the poles [m], 195000                          */
+    double   cell_lat_scale;     /* Hadley edge as a fraction of Earth's 30 degrees, 0.11 */
+    double   co2_scale;          /* multiplier of the CO2 field, 1                        */
+    double   q_CO2, q_bg;        /* mass fractions of CO2 and the background gas of the
+                                  * configured composition (AtmMixture::resolve, m_comp):
+                                  * co2Atmosphere's dry-air CO2 share q_CO2 / (q_CO2 + q_bg) */
+    double   vel_star_init;      /* resetArrays' friction velocity [m/s], 0.4              */
+} athad_init_config;
+
+void athad_default_init_config(athad_init_config* c);
+
+/* The reference's deterministic initial state, cAtmosphereModel::RunTimeSlice for Ma = 0
+ * (cAtmosphereModel.cpp:468-668), built on the device for this context's grid, followed by
+ * run_3D_loop's Held-Suarez target t_eq := t (:750-753): resetArrays, the tropopause levels,
+ * the prescribed Hadley/Ferrel velocities (VelocityInitializer.h:23-105), the symmetric
+ * parabolic sea-surface temperature with the dry adiabat (InitValues_Atm.cpp:466-620), the
+ * saturated water profile (:843-926), two passes of co2Atmosphere and densities(true), the
+ * cloud and ice profile (:930-1117), the saturation adjustment, the ice scheme, the moist
+ * convection, the turbulence initialisation, the diagnosis block, the boundary conditions
+ * and the 200-sweep initial projection, with every damp_wiggles between them.  Overwrites
+ * every field, 2-D field and profile, the tropopause levels and the budgets' first-call
+ * references; leaves out the outputs no field reads (precipitableWater, forces,
+ * standAtm_DewPoint_HumidRel).  Rows are evaluated on the northern half and mirrored, so the
+ * state is exactly north-south symmetric; the anchor row of latitude phi is
+ * lround((90 - phi) (jm - 1) / 180), the reference's row at jm = 181.  Waits for the device. */
+athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* config);
+
 /* ---- the hot path ----------------------------------------------------------- */
 
 /* storeIntermediateData3D(1.0) (UtilsAtm.h:25-49; call sites cAtmosphereModel.cpp:667,
@@ -346,10 +386,13 @@ typedef struct athad_solve_report {
  * call: it relaxes one sweep per call (athad_pressure_sweep). */
 athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int32_t max_iter,
                                   athad_solve_report* report);
-/* The per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1442 for flat
+/* The per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1446 for flat
  * terrain: BC_Atm::bcRadius (BC_Atm.h:556-746), TurbulenceAtm::apply_wall_bc
  * (TurbulenceAtm.h:109-147; reads the 2-D field ATHAD_2D_VEL_STAR), BC_Atm::bcTheta
- * (:750-796) and BC_Atm::bcPhi (:803-918), on the fields the context holds. */
+ * (:750-796), BC_Atm::bcPhi (:803-918), BC_Atm::bcScalarSurfSur and BC_Atm::bcSolidGround
+ * (without land only bcSolidGround's value limits over every cell act, :470-545: c, cloud,
+ * ice, tke, dis >= 0; tke, dis, nue, prod, tke_source, dis_source, u, v, w and their time
+ * level n bounded, non-finite values replaced), on the fields the context holds. */
 athad_status athad_boundary_conditions(athad_ctx* ctx);
 /* The filters after the RK4 step (cAtmosphereModel.cpp:1507-1520), flat terrain:
  * AtomUtils::polar_zonal_filter of u, v, w (lib/Utils.cpp:542-611), radial_shapiro_filter

@@ -121,8 +121,9 @@ void or_densities(int im, int jm, int km, const or_params* p, int compat,
 int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, int iter_n,
                         double* const* f, double* const* f2);
 
-/* the per-iteration boundary conditions, cAtmosphereModel.cpp:1439-1442: BC_Atm::bcRadius,
- * TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta, BC_Atm::bcPhi (flat terrain) */
+/* the per-iteration boundary conditions, cAtmosphereModel.cpp:1439-1446: BC_Atm::bcRadius,
+ * TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta, BC_Atm::bcPhi, BC_Atm::bcScalarSurfSur and
+ * BC_Atm::bcSolidGround (flat terrain: the value limits of BC_Atm.h:470-545) */
 void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* const* f,
                             double* const* f2);
 
@@ -195,6 +196,33 @@ void or_co2_column(int im, int jm, int km, const or_params* p, double* const* f,
  * bookkeeping: out = w_num, w_den; qbar, abar, lev [im] */
 void or_water_budget(int im, int jm, int km, const or_params* p, double* const* f, double* out,
                      double* qbar, double* abar, double* lev);
+
+/* the per-iteration boundary conditions without (wall_bc = 0) or with (1) the turbulence wall
+ * values; RunTimeSlice's boundary conditions (cAtmosphereModel.cpp:651-653) have none.
+ * or_turb_wall_bc: TurbulenceAtm::apply_wall_bc alone (TurbulenceAtm.h:109-147). */
+void or_boundary_conditions_ex(int im, int jm, int km, const or_params* p, double* const* f,
+                               double* const* f2, int wall_bc);
+void or_turb_wall_bc(int im, int jm, int km, const or_params* p, double* const* f, double* const* f2);
+
+/* The reference's deterministic initial state (cAtmosphereModel::RunTimeSlice, Ma = 0,
+ * cAtmosphereModel.cpp:468-668, then run_3D_loop's t_eq := t, :750-753): the configuration
+ * members it reads beyond or_params, laid out as athad_init_config. */
+typedef struct or_init_cfg {
+    uint32_t struct_size;
+    int32_t  n_cells_hemisphere, cell_amp_mode, pad0;
+    double   t_surf_equator, t_surf_pole, tropopause_equator, tropopause_pole;
+    double   cell_lat_scale, co2_scale, q_CO2, q_bg, vel_star_init;
+} or_init_cfg;
+/* stages of or_init_state's `upto`, in the reference's order */
+enum { OR_INIT_VELOCITY = 1, OR_INIT_TEMPERATURE, OR_INIT_WATER, OR_INIT_CLOUD, OR_INIT_SATADJ,
+       OR_INIT_ICE, OR_INIT_MOIST, OR_INIT_TURBULENCE, OR_INIT_DIAGNOSE, OR_INIT_BC,
+       OR_INIT_PROJECT, OR_INIT_ALL };
+size_t or_init_cfg_size(void);
+/* init_tropopause_layers (InitValues_Atm.cpp:330-401): jm levels */
+void or_tropopause_layers(int im, int jm, const or_params* p, const or_init_cfg* c, double* levels);
+/* every field, 2-D field and profile is overwritten; returns 0, -1 on a bad config */
+int or_init_state(int im, int jm, int km, const or_params* p, const or_init_cfg* c, int compat, int upto,
+                  double* const* f, double* const* f2, double* const* prof);
 
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);

@@ -1,8 +1,9 @@
 /*
  * or_bc.c - the per-iteration boundary conditions of the atmosphere (TEST INFRASTRUCTURE
- * ONLY): BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta and
- * BC_Atm::bcPhi in the order of their call site (cAtmosphereModel.cpp:1439-1442), flat
- * terrain (every cell is air, so bcScalarSurfSur and bcSolidGround do nothing).
+ * ONLY): BC_Atm::bcRadius, TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta, BC_Atm::bcPhi,
+ * BC_Atm::bcScalarSurfSur and BC_Atm::bcSolidGround in the order of their call site
+ * (cAtmosphereModel.cpp:1439-1446), flat terrain: every cell is air, so the last two keep
+ * only bcSolidGround's value limits over every cell (BC_Atm.h:470-545).
  *
  * Only the fields the device context holds are treated; the reference's diagnostic
  * arrays in the same lists (radiation, PrecipitableWaterLocal, CoriolisForce,
@@ -58,8 +59,42 @@ static void smooth_seam(double* f, int jm, int km, int i, int j)
     x[1] = f_1 + c * (w_1 - 2.0 * f_1 + e_1);
 }
 
+/* TurbulenceAtm::apply_wall_bc, TurbulenceAtm.h:109-147 (C_nue 0.028, nue_air 1.5e-5 of its
+ * constructor; y1 = get_layer_height(1), a float) */
+void or_turb_wall_bc(int im, int jm, int km, const or_params* p, double* const* f, double* const* f2)
+{
+    or_geom g;
+    or_geom_init(&g, im, jm, km, p, 0);
+    const double y1 = g.height[1];
+    const double y1_safe = or_max(y1, 1.0e-6);
+    const double nd_omega = p->L_atm / p->u_0;
+    const double nue_air = 1.5e-5;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            const double vs = f2[OF2_VEL_STAR][(size_t)j * km + k];
+            f[OF_TKE][OR_IDX(0, j, k)] = vs * vs / (sqrt(0.028) * p->u_0 * p->u_0);
+            f[OF_NUE][OR_IDX(0, j, k)] = 0.0;
+            if (p->turb_model == 1) {
+                f[OF_DIS][OR_IDX(0, j, k)] = 0.0;
+            } else if (p->turb_model == 2) {
+                const double om = 6.0 * nue_air / (0.075 * y1_safe * y1_safe);
+                f[OF_DIS][OR_IDX(0, j, k)] = om * nd_omega;
+            } else if (p->turb_model == 3) {
+                const double om = 60.0 * nue_air / (0.0333 * y1_safe * y1_safe);
+                f[OF_DIS][OR_IDX(0, j, k)] = om * nd_omega;
+            }
+        }
+    or_geom_free(&g);
+}
+
 void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* const* f,
                             double* const* f2)
+{
+    or_boundary_conditions_ex(im, jm, km, p, f, f2, 1);
+}
+
+void or_boundary_conditions_ex(int im, int jm, int km, const or_params* p, double* const* f,
+                               double* const* f2, int wall_bc)
 {
     const int c43 = 1, c13 = 0;               /* (int)(4.0/3.0), (int)(1.0/3.0) */
     const int iml = im - 1, jml = jm - 1;
@@ -104,29 +139,8 @@ void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* 
             if (f[OF_Q_C_U][OR_IDX(0, j, k)] < 0.0) f[OF_Q_C_U][OR_IDX(0, j, k)] = 0.0;
         }
 
-    /* ---- TurbulenceAtm::apply_wall_bc, TurbulenceAtm.h:109-147 (C_nue 0.028, nue_air
-     *      1.5e-5 of its constructor; y1 = get_layer_height(1), a float) ---- */
-    {
-        const double y1 = g.height[1];
-        const double y1_safe = or_max(y1, 1.0e-6);
-        const double nd_omega = p->L_atm / p->u_0;
-        const double nue_air = 1.5e-5;
-        for (int j = 0; j < jm; j++)
-            for (int k = 0; k < km; k++) {
-                const double vs = f2[OF2_VEL_STAR][(size_t)j * km + k];
-                f[OF_TKE][OR_IDX(0, j, k)] = vs * vs / (sqrt(0.028) * p->u_0 * p->u_0);
-                f[OF_NUE][OR_IDX(0, j, k)] = 0.0;
-                if (p->turb_model == 1) {
-                    f[OF_DIS][OR_IDX(0, j, k)] = 0.0;
-                } else if (p->turb_model == 2) {
-                    const double om = 6.0 * nue_air / (0.075 * y1_safe * y1_safe);
-                    f[OF_DIS][OR_IDX(0, j, k)] = om * nd_omega;
-                } else if (p->turb_model == 3) {
-                    const double om = 60.0 * nue_air / (0.0333 * y1_safe * y1_safe);
-                    f[OF_DIS][OR_IDX(0, j, k)] = om * nd_omega;
-                }
-            }
-    }
+    /* ---- TurbulenceAtm::apply_wall_bc (the per-iteration sequence only) ---- */
+    if (wall_bc) or_turb_wall_bc(im, jm, km, p, f, f2);
 
     /* ---- bcTheta, BC_Atm.h:750-796: pole copies ---- */
     for (int k = 0; k < km; k++)
@@ -159,5 +173,36 @@ void or_boundary_conditions(int im, int jm, int km, const or_params* p, double* 
                 smooth_seam(f[OF_V], jm, km, i, j);  smooth_seam(f[OF_VN], jm, km, i, j);
                 smooth_seam(f[OF_W], jm, km, i, j);  smooth_seam(f[OF_WN], jm, km, i, j);
             }
+
+    /* ---- bcScalarSurfSur (BC_Atm.h:1026-1123) and bcSolidGround (:23-547), flat terrain:
+     *      their land branches and the surface copies x[0] := x[i_mount = 0] change nothing;
+     *      bcSolidGround's value limits over every cell remain (:470-545) ---- */
+    {
+        const size_t n = (size_t)im * jm * km;
+        const int sign[5] = { OF_C, OF_CLOUD, OF_ICE, OF_TKE, OF_DIS };
+        for (int q = 0; q < 5; q++)
+            for (size_t e = 0; e < n; e++)
+                if (f[sign[q]][e] < 0.0) f[sign[q]][e] = 0.0;
+        const double tke_max_nd = 1000.0 / (p->u_0 * p->u_0);
+        const double nue_max = 1000.0 / (p->u_0 * p->L_atm);
+        const double prod_max = 1.0e4, dis_max = 1.0e6;
+        const double vel_max_nd = 100.0 / p->u_0;
+        const int vel[6] = { OF_U, OF_UN, OF_V, OF_VN, OF_W, OF_WN };
+        for (size_t e = 0; e < n; e++) {
+            f[OF_TKE][e] = or_safe_clamp(f[OF_TKE][e], 0.0, tke_max_nd);
+            f[OF_TKEN][e] = or_safe_clamp(f[OF_TKEN][e], 0.0, tke_max_nd);
+            f[OF_DIS][e] = or_safe_clamp(f[OF_DIS][e], 1.0e-10, dis_max);
+            f[OF_DISN][e] = or_safe_clamp(f[OF_DISN][e], 1.0e-10, dis_max);
+            f[OF_NUE][e] = or_safe_clamp(f[OF_NUE][e], 0.0, nue_max);
+            f[OF_PROD][e] = or_safe_clamp(f[OF_PROD][e], 0.0, prod_max);
+            f[OF_TKE_SOURCE][e] = or_safe_clamp(f[OF_TKE_SOURCE][e], -prod_max, prod_max);
+            f[OF_DIS_SOURCE][e] = or_safe_clamp(f[OF_DIS_SOURCE][e], -prod_max, prod_max);
+            for (int q = 0; q < 6; q++) {
+                const double v = f[vel[q]][e];
+                f[vel[q]][e] = !or_is_finite(v) ? 0.0 : (v < -vel_max_nd) ? -vel_max_nd
+                             : (v > vel_max_nd) ? vel_max_nd : v;
+            }
+        }
+    }
     or_geom_free(&g);
 }

@@ -154,7 +154,11 @@ void ref_delete(void* p) { delete (cAtmosphereModel*)p; }
 // without its file output, the printed diagnostics and the standard-atmosphere dew-point
 // diagnostic (standAtm_DewPoint_HumidRel, a 60-step bisection per cell that no hot-path
 // function reads), then the Held-Suarez target snapshot of run_3D_loop (:750-753).
-int ref_init_state(void* p)
+// ref_init_state_upto stops after stage `upto` (1 velocities, 2 temperature, 3 water and
+// the co2/densities fixed point, 4 cloud and ice, 5 saturation adjustment, 6 ice scheme,
+// 7 moist convection, 8 turbulence, 9 the diagnosis block from precipitationSum to
+// vegetationLand, 10 boundary conditions, 11 projection, 12 everything).
+int ref_init_state_upto(void* p, int upto)
 {
     cAtmosphereModel* m = (cAtmosphereModel*)p;
     m->m_current_time = m->m_time_list.insert(0).first;
@@ -178,22 +182,27 @@ int ref_init_state(void* p)
     AtomUtils::damp_wiggles(m->u, &m->i_topography, true, true, true);
     AtomUtils::damp_wiggles(m->v, &m->i_topography, true, true, true);
     AtomUtils::damp_wiggles(m->w, &m->i_topography, true, true, true);
+    if (upto <= 1) return 0;
     m->initTemperatureData(0);
     AtomUtils::damp_wiggles(m->t, &m->i_topography, true, true, true);
     m->t_top_init.assign(m->jm, std::vector<double>(m->km, 0.0));
     for (int j = 0; j < m->jm; j++)
         for (int k = 0; k < m->km; k++) m->t_top_init[j][k] = m->t.x[m->im - 1][j][k];
+    if (upto <= 2) return 0;
     m->initWaterWapour();
     for (int pass = 0; pass < 2; pass++) {
         ThermoAtm(*m).co2Atmosphere();
         ThermoAtm(*m).densities(true);
     }
+    if (upto <= 3) return 0;
     m->initCloudIce();
+    if (upto <= 4) return 0;
     SaturationAdjustment(*m).run();
     AtomUtils::damp_wiggles(m->ice, &m->i_topography, true, true, true);
     AtomUtils::damp_wiggles(m->c, &m->i_topography, true, true, true);
     AtomUtils::damp_wiggles(m->cloud, &m->i_topography, true, true, true);
     ThermoAtm(*m).precipitableWater();
+    if (upto <= 5) return 0;
     switch (m->CategoryIceScheme) {
         case 0: ZeroCatIceScheme(*m).run(); break;
         case 1: OneCatIceScheme(*m).run(); break;
@@ -203,15 +212,18 @@ int ref_init_state(void* p)
     }
     AtomUtils::damp_wiggles(m->P_rain, &m->i_topography, true, true, true);
     AtomUtils::damp_wiggles(m->P_snow, &m->i_topography, true, true, true);
+    if (upto <= 6) return 0;
     MoistConvection(*m).run(m->iter_n);
     for (Array* a : {&m->P_conv, &m->E_u, &m->M_u, &m->q_v_u, &m->q_c_u, &m->E_d, &m->M_d, &m->q_v_d})
         AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
+    if (upto <= 7) return 0;
     if (m->turb_model != "laminar") {
         TurbulenceAtm(*m).init();
         TurbulenceAtm(*m).run();
         for (Array* a : {&m->tke, &m->dis, &m->nue, &m->prod, &m->tke_source, &m->dis_source})
             AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
     }
+    if (upto <= 8) return 0;
     UtilsAtm(*m).precipitationSum();
     ThermoAtm(*m).co2Atmosphere();
     ThermoAtm(*m).co2Column(true);
@@ -221,18 +233,23 @@ int ref_init_state(void* p)
     ThermoAtm(*m).waterVapourEvaporation();
     ThermoAtm(*m).latentSensibleHeat();
     ThermoAtm(*m).vegetationLand();
+    if (upto <= 9) return 0;
     BC_Atm(*m).bcRadius();
     BC_Atm(*m).bcTheta();
     BC_Atm(*m).bcPhi();
     BC_Atm(*m).bcScalarSurfSur();
     BC_Atm(*m).bcSolidGround();
+    if (upto <= 10) return 0;
     PressureSolverAtm(*m).project_initial_velocity(200);
+    if (upto <= 11) return 0;
     UtilsAtm(*m).storeIntermediateData3D(1.0);
     for (int i = 0; i < m->im; i++)
         for (int j = 0; j < m->jm; j++)
             for (int k = 0; k < m->km; k++) m->t_eq.x[i][j][k] = m->t.x[i][j][k];
     return 0;
 }
+
+int ref_init_state(void* p) { return ref_init_state_upto(p, 99); }
 
 int ref_get3(void* p, const char* name, double* out)
 {
@@ -383,8 +400,7 @@ int ref_damp_wiggles(void* p, const char* name)
     AtomUtils::damp_wiggles(*a, &m->i_topography, true, true, true);
     return 0;
 }
-// the per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1442 (flat terrain:
-// bcScalarSurfSur and bcSolidGround change nothing and are left out)
+// the per-iteration boundary conditions of cAtmosphereModel.cpp:1439-1446
 void ref_bc(void* p)
 {
     cAtmosphereModel* m = (cAtmosphereModel*)p;
@@ -392,6 +408,8 @@ void ref_bc(void* p)
     if (m->turb_model != "laminar") TurbulenceAtm(*m).apply_wall_bc();
     BC_Atm(*m).bcTheta();
     BC_Atm(*m).bcPhi();
+    BC_Atm(*m).bcScalarSurfSur();
+    BC_Atm(*m).bcSolidGround();
 }
 // TurbulenceAtm::run, the moist iteration's call (cAtmosphereModel.cpp:1426); the closure
 // is the model's turb_model string, which TurbulenceAtm parses on construction

@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from athad_cond_b200._abi import FIELD, FIELD_NAMES, FIELD2D_NAMES, PROFILE_NAMES, Params
+from athad_cond_b200._abi import FIELD, FIELD_NAMES, FIELD2D_NAMES, PROFILE_NAMES, InitConfig, Params
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
@@ -30,6 +30,8 @@ def lib():
         assert _lib.or_params_size() == ctypes.sizeof(Params), "oracle params layout differs"
         _lib.or_nfields.restype = ctypes.c_int
         assert _lib.or_nfields() == len(FIELD_NAMES)
+        _lib.or_init_cfg_size.restype = ctypes.c_size_t
+        assert _lib.or_init_cfg_size() == ctypes.sizeof(InitConfig), "oracle init config layout differs"
         for name in ["or_saturation_pressure", "or_sublimation_pressure", "or_latent_heat",
                      "or_dew_point"]:
             fn = getattr(_lib, name)
@@ -96,6 +98,24 @@ class OracleState:
                    for n in FIELD2D_NAMES}
         self.prof = {n: np.array(state[n], dtype=np.float64, copy=True) if n in state else np.zeros(im)
                      for n in PROFILE_NAMES}
+
+    @classmethod
+    def initial(cls, im, jm, km, params: Params, cfg: InitConfig, compat=0, upto=99):
+        """The reference's initial state built by the oracle (or_init_state): RunTimeSlice up
+        to stage `upto` (OR_INIT_*, 99 = everything)."""
+        o = cls({"t": np.zeros((im, jm, km))}, params)
+        F, F2, P = o._args()
+        r = lib().or_init_state(im, jm, km, ctypes.byref(params), ctypes.byref(cfg), int(compat), int(upto),
+                                F, F2, P)
+        assert r == 0, f"or_init_state returned {r}"
+        return o
+
+    def tropopause_layers(self, cfg: InitConfig):
+        im, jm, _ = self.shape
+        out = np.zeros(jm)
+        lib().or_tropopause_layers(im, jm, ctypes.byref(self.params), ctypes.byref(cfg),
+                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
 
     def _args(self):
         self._F, self._kf = _ptrs(self.f, FIELD_NAMES, self.shape)

@@ -40,6 +40,7 @@ class Reference:
             getattr(L, n).restype = ctypes.c_int
         L.ref_project.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_densities.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_init_state_upto.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_moist.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_set_scalars.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_int]
@@ -64,8 +65,9 @@ class Reference:
             self.lib.ref_delete(self.h)
             self.h = None
 
-    def init_state(self):
-        self.lib.ref_init_state(self.h)
+    def init_state(self, upto: int = 99):
+        """RunTimeSlice's initial state, up to stage `upto` (99 = everything)."""
+        self.lib.ref_init_state_upto(self.h, int(upto))
 
     def get(self, name):
         out = np.empty(self.shape)

@@ -34,11 +34,15 @@ def test_library_exports_every_declared_symbol():
 
 def test_default_params_match_config():
     lib = _abi.load_library()
-    assert lib.athad_abi_version() == 9
+    assert lib.athad_abi_version() == 10
     assert lib.athad_params_size() == ctypes.sizeof(_abi.Params)
     a = _abi.default_params().as_dict()
     b = _abi.config_params().as_dict()
     assert a == b
+    c = _abi.InitConfig()
+    lib.athad_default_init_config(ctypes.byref(c))
+    d = _abi.config_init()
+    assert {n: getattr(c, n) for n, _ in c._fields_} == {n: getattr(d, n) for n, _ in d._fields_}
 
 
 def test_footprint_and_argument_checks():
