@@ -60,6 +60,9 @@ FIELD_NAMES = [
     "radiation", "epsilon",
     "TempStand", "TempDewPoint", "HumidityRel",
     "Q_Latent", "Q_Sensible",
+    "CoriolisForce", "BuoyancyForce", "PressureGradientForce",
+    "vbud_pgf", "vbud_cor", "vbud_advv", "vbud_advh", "vbud_diff", "vbud_other",
+    "wbud_pgf", "wbud_cor", "wbud_advv", "wbud_advh", "wbud_diff", "wbud_other",
 ]
 FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
 NFIELDS = len(FIELD_NAMES)
@@ -265,6 +268,8 @@ SIGNATURES = {
     "athad_batch_set_shape": (ctypes.c_int, [_P, ctypes.c_int32]),
     "athad_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_float)]),
+    "athad_thermo_arity": (ctypes.c_int32, [ctypes.c_int32]),
+    "athad_thermo_eval": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _D, _D]),
     "athad_density_profile_noalloc": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                      ctypes.c_size_t, _P, _P, _P]),
 }

@@ -159,11 +159,14 @@ class GpuAtmosphere:
         self._check(self.lib.athad_level_mean(self._h))
 
     def solveRungeKutta_Atmosphere_Turb(self, dt: float, diffusion_ramp: float = 1.0,
-                                        buoyancy_ramp: float = 1.0, write_diagnostics: bool = False,
+                                        buoyancy_ramp: float = 1.0, write_diagnostics: int = 0,
                                         store_n_level: bool = False):
         """RungeKutta_Atm_Turb.cpp:44-273 (call site cAtmosphereModel.cpp:1509); with
-        store_n_level the following storeIntermediateData3D is fused into the last stage."""
-        s = _abi.StepScalars(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0,
+        store_n_level the following storeIntermediateData3D is fused into the last stage.
+        write_diagnostics: 1 (or True) the right-hand side's diagnostic outputs (turbulence
+        production and sources, acting forces, Q_Latent, Q_Sensible), 2 the momentum budget
+        terms, 3 both."""
+        s = _abi.StepScalars(dt, diffusion_ramp, buoyancy_ramp, int(write_diagnostics),
                              1 if store_n_level else 0)
         self._check(self.lib.athad_rk4_step(self._h, ctypes.byref(s)))
 

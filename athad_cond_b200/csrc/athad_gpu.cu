@@ -106,10 +106,18 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c; return ATHAD_ERR_CUDA;
     }
+    if (cudaEventCreate(&c->ev_step0) != cudaSuccess || cudaEventCreate(&c->ev_step1) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->ev_step0) cudaEventDestroy(c->ev_step0);
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return ATHAD_ERR_CUDA;
+    }
     c->stream = c->own_stream;
     if (cudaMalloc((void**)&c->slab, L.bytes) != cudaSuccess) {
         cudaGetLastError();
         cudaStreamDestroy(c->own_stream);
+        cudaEventDestroy(c->ev_step0); cudaEventDestroy(c->ev_step1);
         delete c;
         return ATHAD_ERR_OOM;
     }
@@ -151,13 +159,15 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
         c->geof = (GeoF*)take((size_t)im * jm * sizeof(GeoF));
     }
     if ((size_t)(q - c->slab) > L.bytes) {
-        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream);
+        cudaEventDestroy(c->ev_step0); cudaEventDestroy(c->ev_step1); delete c;
         return ATHAD_ERR_INVALID;
     }
     // Every field starts at zero (the reference's Arrays are zero/one-initialised by
     // resetArrays; the caller uploads the state it wants).
     if (cudaMemsetAsync(c->slab, 0, L.bytes, c->stream) != cudaSuccess) {
-        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream);
+        cudaEventDestroy(c->ev_step0); cudaEventDestroy(c->ev_step1); delete c;
         return ATHAD_ERR_CUDA;
     }
 
@@ -308,7 +318,8 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     }
     if (s == ATHAD_OK) s = cuda_check(c, cudaStreamSynchronize(c->stream), "create sync");
     if (s != ATHAD_OK) {
-        cudaFree(c->slab); cudaStreamDestroy(c->own_stream); delete c;
+        cudaFree(c->slab); cudaStreamDestroy(c->own_stream);
+        cudaEventDestroy(c->ev_step0); cudaEventDestroy(c->ev_step1); delete c;
         return s;
     }
     *out = c;
@@ -329,6 +340,8 @@ athad_status athad_destroy(athad_ctx* ctx)
     mg_free(ctx->mg);
     cudaFree(ctx->slab);
     cudaStreamDestroy(ctx->own_stream);
+    cudaEventDestroy(ctx->ev_step0);
+    cudaEventDestroy(ctx->ev_step1);
     delete ctx;
     return ATHAD_OK;
 }
@@ -466,18 +479,74 @@ athad_status athad_store_n_level(athad_ctx* ctx)
 athad_status athad_level_mean(athad_ctx* ctx)
 {
     if (!ctx) return ATHAD_ERR_INVALID;
+    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters + kNonfiniteSlot, 0, sizeof(unsigned long long),
+                                                     ctx->stream), "level_mean counter");
+    if (s != ATHAD_OK) return s;
     launch_level_mean(ctx->L.d, ctx->field[ATHAD_T], ctx->sin_w, ctx->prof[ATHAD_PROF_T_REF_LEVEL], ctx->row_sum,
-                      ctx->stream);
+                      ctx->stream, ctx->counters + kNonfiniteSlot);
     ATHAD_CHECK_LAUNCH(ctx, "level_mean");
     return ATHAD_OK;
 }
 
 static athad_status rk4_step_mixed(athad_ctx* ctx, const athad_step_scalars* s);
 
+static athad_status rk4_step_fp64(athad_ctx* ctx, const athad_step_scalars* s);
+
+// the step between two events on the context's stream: athad_get_report's last_kernel_ms
 athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
 {
     if (!ctx || !s) return fail(ctx, ATHAD_ERR_INVALID, "rk4_step: bad argument");
-    if (ctx->p.precision == ATHAD_PRECISION_MIXED) return rk4_step_mixed(ctx, s);
+    athad_status st = cuda_check(ctx, cudaEventRecord(ctx->ev_step0, ctx->stream), "rk4_step event");
+    if (st != ATHAD_OK) return st;
+    st = (ctx->p.precision == ATHAD_PRECISION_MIXED) ? rk4_step_mixed(ctx, s) : rk4_step_fp64(ctx, s);
+    if (st != ATHAD_OK) return st;
+    if (s->write_diagnostics & 3) {
+        // the right-hand side's diagnostic outputs from the last stage's input state (the
+        // stage buffer A holds it after the step)
+        const athad_params& p = ctx->p;
+        RhsDiagArgs g;
+        std::memset(&g, 0, sizeof g);
+        g.d = ctx->L.d;
+        g.geo = ctx->geo;
+        g.t_ref = ctx->prof[ATHAD_PROF_T_REF_LEVEL];
+        g.p_dyn = ctx->field[ATHAD_P_DYN]; g.nue = ctx->field[ATHAD_NUE];
+        g.MC_v = ctx->field[ATHAD_MC_V]; g.MC_w = ctx->field[ATHAD_MC_W];
+        const int outs[17] = {ATHAD_CORIOLIS_FORCE, ATHAD_BUOYANCY_FORCE, ATHAD_PRESSURE_GRADIENT_FORCE,
+                              ATHAD_Q_LATENT, ATHAD_Q_SENSIBLE,
+                              ATHAD_VBUD_PGF, ATHAD_VBUD_COR, ATHAD_VBUD_ADVV, ATHAD_VBUD_ADVH, ATHAD_VBUD_DIFF,
+                              ATHAD_VBUD_OTHER, ATHAD_WBUD_PGF, ATHAD_WBUD_COR, ATHAD_WBUD_ADVV, ATHAD_WBUD_ADVH,
+                              ATHAD_WBUD_DIFF, ATHAD_WBUD_OTHER};
+        for (int q = 0; q < 17; q++) g.out[q] = ctx->field[outs[q]];
+        g.inv_2dr = 1.0 / (2.0 * ctx->dr); g.inv_2dthe = 1.0 / (2.0 * ctx->dthe); g.inv_2dphi = 1.0 / (2.0 * ctx->dphi);
+        g.inv_dr2 = 1.0 / (ctx->dr * ctx->dr); g.inv_dthe2 = 1.0 / (ctx->dthe * ctx->dthe);
+        g.inv_dphi2 = 1.0 / (ctx->dphi * ctx->dphi);
+        g.coeff_Coriolis = p.r_air * p.u_0 * p.omega;                 // RHS_Atm_Turb.cpp:365-376
+        g.coeff_buoy = p.r_air * p.g;
+        g.coeff_u_p = 0.5 * p.r_air * p.u_0 * p.u_0 / p.L_atm;
+        g.coeff_L = p.r_air * p.c_0 * p.lv * p.u_0 / p.L_atm;         // :474-475
+        g.coeff_S = p.lamda * p.t_0 / p.L_atm;
+        g.t_0 = p.t_0;
+        g.inv_re = 1.0 / p.re_turb;
+        g.diffusion_ramp = s->diffusion_ramp;
+        g.drag_pref = 1.0 / 86400.0 * p.L_atm / p.u_0 * s->dt;
+        g.force_nd = p.omega * ctx->shell_len / p.u_0;
+        g.coeff_MC_vel = p.L_atm / (p.u_0 * p.u_0);
+        g.nontrad = p.coriolis_nontrad;
+        g.flags = s->write_diagnostics & 3;
+        for (int n = 0; n < kNY; n++) {
+            if (ctx->p.precision == ATHAD_PRECISION_MIXED) g.Y32[n] = ctx->mA[n];
+            else g.Y64[n] = ctx->stA[n];
+        }
+        launch_rhs_diagnostics(g, ctx->stream);
+        ATHAD_CHECK_LAUNCH(ctx, "rhs diagnostics");
+    }
+    st = cuda_check(ctx, cudaEventRecord(ctx->ev_step1, ctx->stream), "rk4_step event");
+    if (st == ATHAD_OK) ctx->step_timed = true;
+    return st;
+}
+
+static athad_status rk4_step_fp64(athad_ctx* ctx, const athad_step_scalars* s)
+{
     const athad_params& p = ctx->p;
     athad_status st = athad_level_mean(ctx);
     if (st != ATHAD_OK) return st;
@@ -521,7 +590,7 @@ athad_status athad_rk4_step(athad_ctx* ctx, const athad_step_scalars* s)
     a.drag_pref = 1.0 / 86400.0 * p.L_atm / p.u_0 * s->dt;
     a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
     a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
-    a.write_diag = s->write_diagnostics;
+    a.write_diag = s->write_diagnostics & 1;
     a.store_n = s->store_n_level ? 1 : 0;
     for (int n = 0; n < kNY; n++) a.Yn_store[n] = ctx->field[ATHAD_TN + n];
     for (int stage = 1; stage <= 4; stage++) {
@@ -590,7 +659,7 @@ void athad::mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a)
     a.drag_pref = (float)(1.0 / 86400.0 * p.L_atm / p.u_0 * s->dt);
     a.turb_model = p.turb_model; a.wall_mode = p.wall_mode; a.nontrad = p.coriolis_nontrad;
     a.curvature = p.metric_curvature; a.tracer_diff_flux = p.tracer_diff_flux;
-    a.write_diag = s->write_diagnostics;
+    a.write_diag = s->write_diagnostics & 1;
     a.store_n = s->store_n_level ? 1 : 0;
     for (int n = 0; n < kNY; n++) a.Yn_store[n] = ctx->field[ATHAD_TN + n];
 }
@@ -743,14 +812,25 @@ athad_status athad_moist_convection(athad_ctx* ctx, int32_t iter_n)
 athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
 {
     if (!ctx || !out) return fail(ctx, ATHAD_ERR_INVALID, "get_report: bad argument");
-    unsigned long long h[3] = {0, 0, 0};
-    athad_status s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, ctx->stream), "report");
+    unsigned long long h[4] = {0, 0, 0, 0};
+    athad_status s = cuda_check(ctx, cudaMemcpyAsync(h, ctx->counters, 3 * sizeof(unsigned long long),
+                                                     cudaMemcpyDeviceToHost, ctx->stream), "report");
+    if (s == ATHAD_OK)
+        s = cuda_check(ctx, cudaMemcpyAsync(h + 3, ctx->counters + kNonfiniteSlot, sizeof(unsigned long long),
+                                            cudaMemcpyDeviceToHost, ctx->stream), "report");
     if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "report sync");
     if (s != ATHAD_OK) return s;
     std::memset(out, 0, sizeof *out);
     out->poisson_src_cells = (int64_t)h[0] * ctx->poisson_sweeps_since_reset;
     out->poisson_src_clamped = (int64_t)h[1] * ctx->poisson_sweeps_since_reset;
     out->satadj_ceiling_hits = (int64_t)h[2];
+    out->nonfinite_inputs = (int64_t)h[3];
+    if (ctx->step_timed) {
+        float ms = 0.0f;
+        s = cuda_check(ctx, cudaEventElapsedTime(&ms, ctx->ev_step0, ctx->ev_step1), "report step time");
+        if (s != ATHAD_OK) return s;
+        out->last_kernel_ms = ms;
+    }
     return ATHAD_OK;
 }
 

@@ -13,6 +13,7 @@ struct MGSolver;                 // pressure_solve hierarchy (k_mg.cu), built on
 void mg_free(MGSolver* s);
 
 constexpr int kNY = 11;   // prognostic fields t..dis
+constexpr int kNonfiniteSlot = 24;   // counters word of the level mean's non-finite count
 
 struct Layout {
     Dims d;
@@ -96,7 +97,9 @@ struct athad_ctx {
     double* cose = nullptr;
     double* row_sum = nullptr;
     double* row_cnt = nullptr;
-    unsigned long long* counters = nullptr;   // [0..1] poisson, [2] satadj ceiling
+    unsigned long long* counters = nullptr;   // 32 words: [0..1] poisson, [2] satadj ceiling,
+                                              // [3], [8..9] vapour ceiling, [12..15] min/max,
+                                              // [16..21] residuum, [kNonfiniteSlot] level mean
     int* polar_passes = nullptr;              // [jm] zonal filter passes per row
     TurbLevel* turb_lev = nullptr;            // [im] TurbulenceAtm per-level constants
     double* res_sin = nullptr;                // [jm] findResiduumAtm's max(0.55, sin theta_j)
@@ -119,6 +122,8 @@ struct athad_ctx {
     std::vector<double> height_h;             // [im] get_layer_height(i), float values (host copy)
     int64_t poisson_sweeps_since_reset = 0;
     MGSolver* mg = nullptr;
+    cudaEvent_t ev_step0 = nullptr, ev_step1 = nullptr;   // around the last athad_rk4_step
+    bool step_timed = false;
     std::string err;
 };
 

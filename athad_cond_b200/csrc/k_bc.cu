@@ -10,10 +10,10 @@
 // evaluated in the reference's order; the file is compiled without fused multiply-add, so
 // the results are bit-identical to the reference's.
 //
-// Fields: those of the reference's lists that the context holds (the heat diagnostics
-// Q_Latent and Q_Sensible included).  The reference's other diagnostic arrays in the same
-// lists (radiation, PrecipitableWaterLocal, the force diagnostics) are not state of the hot
-// path.  c43 and c13 are `const int` members
+// Fields: those of the reference's lists that the context holds (the right-hand side's
+// CoriolisForce and BuoyancyForce, the heat diagnostics Q_Latent and Q_Sensible and the
+// radiation flux included).  The reference's other arrays in the same lists, the outputs of
+// ThermoAtm::forces and precipitableWater, are not held.  c43 and c13 are `const int` members
 // initialised from 4.0/3.0 and 1.0/3.0 (cAtmosphereModel.h:158), i.e. 1 and 0.
 #include "kernels.cuh"
 
@@ -24,7 +24,8 @@ namespace {
 __constant__ int kBothCubic[] = {                       // BC_Atm.h:567-574, Pattern A
     ATHAD_S_C_C, ATHAD_S_V, ATHAD_S_C, ATHAD_S_I, ATHAD_S_R, ATHAD_S_S, ATHAD_S_G,
     ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_U_U, ATHAD_V_U, ATHAD_W_U,
-    ATHAD_MC_S, ATHAD_MC_S_U, ATHAD_MC_S_D, ATHAD_M_U, ATHAD_M_D, ATHAD_Q_LATENT, ATHAD_Q_SENSIBLE};
+    ATHAD_MC_S, ATHAD_MC_S_U, ATHAD_MC_S_D, ATHAD_M_U, ATHAD_M_D, ATHAD_Q_LATENT, ATHAD_Q_SENSIBLE,
+    ATHAD_CORIOLIS_FORCE, ATHAD_BUOYANCY_FORCE};
 __constant__ int kVnBot[] = {ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_P_CONV};   // :586-590, Pattern B
 __constant__ int kCubicBotVnTop[] = {                   // :599-603, Pattern C
     ATHAD_CLOUD, ATHAD_ICE, ATHAD_GR, ATHAD_CO2,
@@ -32,20 +33,20 @@ __constant__ int kCubicBotVnTop[] = {                   // :599-603, Pattern C
     ATHAD_TKE, ATHAD_DIS, ATHAD_NUE, ATHAD_PROD, ATHAD_TKE_SOURCE, ATHAD_DIS_SOURCE};
 __constant__ int kHydro[] = {ATHAD_P_STAT, ATHAD_R_HUMID, ATHAD_R_DRY};  // :656-665, Pattern D
 __constant__ int kTheta[] = {                           // :760-776
-    ATHAD_T, ATHAD_P_STAT, ATHAD_R_HUMID, ATHAD_R_DRY, ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_C,
+    ATHAD_T, ATHAD_RADIATION, ATHAD_P_STAT, ATHAD_R_HUMID, ATHAD_R_DRY, ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_C,
     ATHAD_CLOUD, ATHAD_ICE, ATHAD_GR, ATHAD_CO2, ATHAD_TKE, ATHAD_DIS, ATHAD_NUE, ATHAD_PROD,
     ATHAD_TKE_SOURCE, ATHAD_DIS_SOURCE,
     ATHAD_S_C_C, ATHAD_S_V, ATHAD_S_C, ATHAD_S_I, ATHAD_S_R, ATHAD_S_S, ATHAD_S_G,
     ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_U_U, ATHAD_V_U, ATHAD_W_U, ATHAD_MC_S, ATHAD_MC_S_U,
     ATHAD_MC_S_D, ATHAD_C_U, ATHAD_E_DD, ATHAD_E_L, ATHAD_E_P, ATHAD_G_P, ATHAD_Q_LATENT,
-    ATHAD_Q_SENSIBLE};
+    ATHAD_Q_SENSIBLE, ATHAD_CORIOLIS_FORCE, ATHAD_BUOYANCY_FORCE};
 __constant__ int kPhiAvg[] = {                          // :806-817
-    ATHAD_T, ATHAD_P_STAT, ATHAD_R_HUMID, ATHAD_R_DRY, ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_C,
+    ATHAD_T, ATHAD_RADIATION, ATHAD_P_STAT, ATHAD_R_HUMID, ATHAD_R_DRY, ATHAD_U, ATHAD_V, ATHAD_W, ATHAD_C,
     ATHAD_CLOUD, ATHAD_ICE, ATHAD_GR, ATHAD_CO2,
     ATHAD_S_C_C, ATHAD_S_V, ATHAD_S_C, ATHAD_S_I, ATHAD_S_R, ATHAD_S_S, ATHAD_S_G,
     ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_U_U, ATHAD_V_U, ATHAD_W_U, ATHAD_MC_S, ATHAD_MC_S_U,
     ATHAD_MC_S_D, ATHAD_C_U, ATHAD_E_DD, ATHAD_E_L, ATHAD_E_P, ATHAD_G_P, ATHAD_Q_LATENT,
-    ATHAD_Q_SENSIBLE};
+    ATHAD_Q_SENSIBLE, ATHAD_CORIOLIS_FORCE, ATHAD_BUOYANCY_FORCE};
 __constant__ int kPhiExtrap[] = {ATHAD_TKE, ATHAD_DIS, ATHAD_NUE, ATHAD_PROD, ATHAD_TKE_SOURCE,
                                  ATHAD_DIS_SOURCE};    // :822-825
 

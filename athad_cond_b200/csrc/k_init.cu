@@ -18,9 +18,10 @@
 // of latitude phi is lround((90 - phi) / dlat), dlat = 180/(jm-1) degrees per row, and the
 // southern hemisphere is j > (jm-1)/2 (VelocityInitializer.h:72, 196-201 at jm = 181).
 //
-// Left out, as outputs nothing in the model state reads: precipitableWater, forces,
-// vegetationLand (land only) and the standard-atmosphere dew-point diagnostic; the file
-// output and the printed diagnostics.
+// Left out, as outputs nothing in the model state reads: precipitableWater, the centrifugal
+// and pressure-gradient arrays of forces (its Coriolis and buoyancy arrays are the right-hand
+// side's too and are built), vegetationLand (land only) and the standard-atmosphere dew-point
+// diagnostic; the file output and the printed diagnostics.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -271,6 +272,28 @@ __global__ void __launch_bounds__(128) turb_init_kernel(TurbInitArgs a)
     a.tke[c0] = vs * vs / a.tke_wall_den;
     a.nue[c0] = 0.0;
     if (a.set_dis_wall) a.dis[c0] = a.dis_wall;
+}
+
+// ThermoAtm::forces (ThermoAtm.h:518-614), the two arrays it shares with the right-hand
+// side's outputs (CoriolisForce, BuoyancyForce) in the interior cells; before the first RK4
+// step the buoyancy reference (the level-mean temperature) does not exist and is 1
+__global__ void __launch_bounds__(256) init_forces_kernel(Dims d, const GeoIJ* geo, const double* sin_w,
+                                                          const double* u, const double* v, const double* w,
+                                                          const double* t, const double* r_humid,
+                                                          double* coriolis, double* buoyancy, double two_omega,
+                                                          double nontrad_d, double u_0, double r_air, double g)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = blockIdx.y, i = row / d.jm, j = row % d.jm;
+    if (k < 1 || k >= d.km - 1 || i < 1 || i >= d.im - 1 || j < 1 || j >= d.jm - 1) return;
+    const long long q = (long long)row * d.pitch + k;
+    const double sinthe = sin_w[j], costhe = geo[row].costhe;
+    const double w_ijk = w[q] * u_0;
+    const double Cor_r = -nontrad_d * two_omega * sinthe * w_ijk;
+    const double Cor_the = two_omega * costhe * w_ijk;
+    const double Cor_phi = -two_omega * (costhe * v[q] + nontrad_d * sinthe * u[q]) * u_0;
+    coriolis[q] = 1.0 * r_air * sqrt(Cor_r * Cor_r + Cor_the * Cor_the + Cor_phi * Cor_phi);
+    buoyancy[q] = 1.0e-3 * 1.0 * r_humid[q] * g * (t[q] - 1.0);
 }
 
 // UtilsAtm::precipitationSum (UtilsAtm.h:51-65)
@@ -688,6 +711,11 @@ athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* cfg)
     ATHAD_TRY(athad_co2_column(ctx, &rep));
     ATHAD_TRY(athad_water_budget(ctx, &rep, nullptr));
     ATHAD_TRY(athad_densities(ctx, 0));
+    init_forces_kernel<<<rows_grid, 256, 0, st>>>(d, ctx->geo, ctx->sin_w, ctx->field[ATHAD_U], ctx->field[ATHAD_V],
+                                                  ctx->field[ATHAD_W], ctx->field[ATHAD_T], ctx->field[ATHAD_R_HUMID],
+                                                  ctx->field[ATHAD_CORIOLIS_FORCE], ctx->field[ATHAD_BUOYANCY_FORCE],
+                                                  2.0 * p.omega, p.coriolis_nontrad ? 1.0 : 0.0, p.u_0, p.r_air, p.g);
+    ATHAD_CHECK_LAUNCH(ctx, "initial_state forces");
     ATHAD_TRY(athad_water_vapour_evaporation(ctx));
     ATHAD_TRY(athad_latent_sensible_heat(ctx));
 

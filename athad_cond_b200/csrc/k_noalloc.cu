@@ -12,9 +12,12 @@
 // fixed size: every GPU that loads this library keeps it until the process exits.  Host
 // code cannot use the array's name as a device address, so the address is looked up once
 // per device with cudaGetSymbolAddress, on that device's first call (make that first call
-// before any stream capture).  All calls share the array: calls that overlap on the GPU
-// (different streams or host threads) race on it.  Every entry a call reads is written
-// earlier in the same call, so nothing needs clearing between calls.
+// before any stream capture).  The address is kept for the life of the process, so
+// resetting a device (cudaDeviceReset) between calls is not supported.  All calls share the
+// array: calls that overlap on the GPU (different streams or host threads) race on it.
+// Every entry a call reads is written earlier in the same call, so nothing needs clearing
+// between calls.  A CUDA error already pending when the call starts is left pending and
+// reported (ATHAD_ERR_CUDA) before anything is launched.
 #include <cmath>
 #include <mutex>
 
@@ -100,6 +103,7 @@ extern "C" athad_status athad_density_profile_noalloc(const double* r_humid, int
     if (!r_humid || !rho_base || !dlnrho_dr) return ATHAD_ERR_INVALID;
     if (im < 2 || jm < 1 || km < 1 || pitch < (size_t)km) return ATHAD_ERR_INVALID;
     if (im > ATHAD_NOALLOC_MAX_IM || (long long)im * jm > ATHAD_NOALLOC_MAX_ROWS) return ATHAD_ERR_INVALID;
+    if (cudaPeekAtLastError() != cudaSuccess) return ATHAD_ERR_CUDA;   // an earlier call's error
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();

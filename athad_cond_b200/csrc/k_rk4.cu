@@ -24,8 +24,11 @@ namespace athad {
 // per (i, j) row over all SMs: a 32-lane strided partial sum reduced by xor butterfly; then
 // one CTA per level stages its row sums in shared memory (jm <= 6144) and one thread adds
 // rows j and jm-1-j before weighting, so the mean of a mirrored field is identical.
+// The same pass counts the non-finite values of t (nonfinite, may be null): a row whose sum
+// is finite holds none, so only rows with a non-finite sum are scanned.
 __global__ void __launch_bounds__(256) level_rows_kernel(Dims d, const double* __restrict__ t,
-                                                         double* __restrict__ rows)
+                                                         double* __restrict__ rows,
+                                                         unsigned long long* __restrict__ nonfinite)
 {
     const int lane = threadIdx.x & 31;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -35,6 +38,12 @@ __global__ void __launch_bounds__(256) level_rows_kernel(Dims d, const double* _
     for (int k = lane; k < d.km; k += 32) s += __ldg(r + k);
     for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
     if (lane == 0) rows[row] = s;
+    if (nonfinite && !is_finite_bits(s)) {
+        unsigned int n = 0;
+        for (int k = lane; k < d.km; k += 32) n += is_finite_bits(__ldg(r + k)) ? 0u : 1u;
+        for (int off = 16; off >= 1; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
+        if (lane == 0 && n) atomicAdd(nonfinite, (unsigned long long)n);
+    }
 }
 
 __global__ void __launch_bounds__(128) level_combine_kernel(Dims d, const double* __restrict__ rows,
@@ -61,10 +70,10 @@ __global__ void __launch_bounds__(128) level_combine_kernel(Dims d, const double
 }
 
 void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
-                       double* row_sum, cudaStream_t st)
+                       double* row_sum, cudaStream_t st, unsigned long long* nonfinite)
 {
     const int rows = d.im * d.jm;
-    level_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(d, t, row_sum);
+    level_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(d, t, row_sum, nonfinite);
     level_combine_kernel<<<d.im, 128, d.jm * sizeof(double), st>>>(d, row_sum, sin_w, out);
 }
 

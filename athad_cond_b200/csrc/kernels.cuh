@@ -42,8 +42,26 @@ struct RK4Args {
     int store_n;               // fuse storeIntermediateData3D into stage 4
 };
 
+// The right-hand side's diagnostic outputs (k_rhsdiag.cu): out[0..2] CoriolisForce,
+// BuoyancyForce, PressureGradientForce, [3..4] Q_Latent, Q_Sensible (flags bit 0),
+// [5..10] vbud_*, [11..16] wbud_* (flags bit 1); the last stage's input state in FP64 or FP32.
+struct RhsDiagArgs {
+    Dims d;
+    const GeoIJ* geo;
+    const double* t_ref;
+    const double* p_dyn; const double* nue; const double* MC_v; const double* MC_w;
+    const double* Y64[11];      // the state read: FP64 (Y32[0] null) or FP32 stage buffers
+    const float* Y32[11];
+    double* out[17];
+    double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
+    double coeff_Coriolis, coeff_buoy, coeff_u_p, coeff_L, coeff_S, t_0;
+    double inv_re, diffusion_ramp, drag_pref, force_nd, coeff_MC_vel;
+    int nontrad, flags;
+};
+void launch_rhs_diagnostics(const RhsDiagArgs& a, cudaStream_t st);
+
 void launch_level_mean(const Dims& d, const double* t, const double* sin_w, double* out,
-                       double* row_sum, cudaStream_t st);
+                       double* row_sum, cudaStream_t st, unsigned long long* nonfinite = nullptr);
 void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st);
 
 // Mixed-precision RK4 step (k_rk4m.cu).  FP32 geometry factors (rounded from GeoIJ, so

@@ -159,8 +159,18 @@ typedef enum athad_field {
     /* standAtm_DewPoint_HumidRel outputs (ThermoAtm.h:400-516): the standard-atmosphere
      * temperature [deg C], the dew point [deg C] and the relative humidity [%] */
     ATHAD_TEMP_STAND, ATHAD_TEMP_DEW_POINT, ATHAD_HUMIDITY_REL,
-    /* latentSensibleHeat outputs (ThermoAtm.h:36-112) */
+    /* latentSensibleHeat outputs (ThermoAtm.h:36-112), overwritten in the interior by the
+     * right-hand side's own heat diagnostics on athad_rk4_step's diagnostic steps
+     * (RHS_Atm_Turb.cpp:471-491) */
     ATHAD_Q_LATENT, ATHAD_Q_SENSIBLE,
+    /* the right-hand side's acting forces (RHS_Atm_Turb.cpp:447-456), written on diagnostic
+     * steps */
+    ATHAD_CORIOLIS_FORCE, ATHAD_BUOYANCY_FORCE, ATHAD_PRESSURE_GRADIENT_FORCE,
+    /* the terms of rhs_v and rhs_w (pressure gradient, Coriolis, vertical and horizontal
+     * advection, diffusion, the rest), written on momentum-budget steps
+     * (RHS_Atm_Turb.cpp:1031-1057, vbud_* and wbud_*) */
+    ATHAD_VBUD_PGF, ATHAD_VBUD_COR, ATHAD_VBUD_ADVV, ATHAD_VBUD_ADVH, ATHAD_VBUD_DIFF, ATHAD_VBUD_OTHER,
+    ATHAD_WBUD_PGF, ATHAD_WBUD_COR, ATHAD_WBUD_ADVV, ATHAD_WBUD_ADVH, ATHAD_WBUD_DIFF, ATHAD_WBUD_OTHER,
     ATHAD_NFIELDS
 } athad_field;
 
@@ -195,7 +205,13 @@ typedef struct athad_step_scalars {
     double dt;               /* dt = dt_visc (or dt_inviscid in the spin-up)           */
     double diffusion_ramp;   /* diffusion_ramp in [0,1]                                */
     double buoyancy_ramp;    /* min(1, total_iter_count / 300)                         */
-    int32_t write_diagnostics; /* 1: store prod/tke_source/dis_source of stage 4       */
+    int32_t write_diagnostics; /* bit 0: store the right-hand side's diagnostic outputs of
+                                * stage 4 - prod, tke_source, dis_source, the acting forces
+                                * and Q_Latent, Q_Sensible in the interior cells (the
+                                * reference writes them in every call; they are output
+                                * only); bit 1: the momentum budget terms vbud_*, wbud_*
+                                * (the reference's checkpoint iterations,
+                                * cAtmosphereModel.cpp:1502-1503)                       */
     int32_t store_n_level;   /* 1: storeIntermediateData3D (UtilsAtm.h:25-49) fused into
                               * the last stage (the precipitation fluxes copied right
                               * after it): the caller runs nothing between the RK4 step
@@ -208,8 +224,10 @@ typedef struct athad_report {
     int64_t poisson_src_cells;     /* fluid cells of the last pressure sweep(s)          */
     int64_t poisson_src_clamped;   /* of which the divergence source hit p_dyn_cap       */
     int64_t satadj_ceiling_hits;   /* c > 1 - co2 clamps in clampAndFade                  */
-    int64_t nonfinite_inputs;      /* non-finite values found by the last input check    */
-    double  last_kernel_ms;        /* device time of the last timed entry point          */
+    int64_t nonfinite_inputs;      /* non-finite values of t seen by the last level mean (every
+                                    * athad_rk4_step forms one from its input t)           */
+    double  last_kernel_ms;        /* device time of the last athad_rk4_step (CUDA events on
+                                    * the context's stream); 0 before the first            */
 } athad_report;
 
 /* What the vapour ceiling removed in one call (cAtmosphereModel.cpp:1369-1391). */
@@ -327,11 +345,11 @@ void athad_default_init_config(athad_init_config* c);
  * parabolic sea-surface temperature with the dry adiabat (InitValues_Atm.cpp:466-620), the
  * saturated water profile (:843-926), two passes of co2Atmosphere and densities(true), the
  * cloud and ice profile (:930-1117), the saturation adjustment, the ice scheme, the moist
- * convection, the turbulence initialisation, the diagnosis block, the boundary conditions
- * and the 200-sweep initial projection, with every damp_wiggles between them.  Overwrites
- * every field, 2-D field and profile, the tropopause levels and the budgets' first-call
- * references; leaves out the outputs no field reads (precipitableWater, forces,
- * standAtm_DewPoint_HumidRel).  Rows are evaluated on the northern half and mirrored, so the
+ * convection, the turbulence initialisation, the diagnosis block (with ThermoAtm::forces'
+ * Coriolis and buoyancy arrays), the boundary conditions and the 200-sweep initial
+ * projection, with every damp_wiggles between them.  Overwrites every field, 2-D field and
+ * profile, the tropopause levels and the budgets' first-call references; leaves out the
+ * outputs no field reads (precipitableWater, standAtm_DewPoint_HumidRel).  Rows are evaluated on the northern half and mirrored, so the
  * state is exactly north-south symmetric; the anchor row of latitude phi is
  * lround((90 - phi) (jm - 1) / 180), the reference's row at jm = 181.  Waits for the device. */
 athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* config);
@@ -564,6 +582,32 @@ athad_status athad_batch_set_shape(athad_batch* b, int32_t shape);
 athad_status athad_batch_autotune(athad_batch* b, int32_t reps, int32_t* best_shape,
                                   float* ms_per_shape);
 
+/* ---- the device thermodynamics, for the known-answer tests ---------------------- */
+
+/* The saturation and mixture functions the column kernels evaluate on the device
+ * (SaturationH2O.h:68-303, MixtureAtm.h:123-225), evaluated on the GPU for n input tuples so
+ * the reference's self-test values (test/saturation_selftest.cpp,
+ * test/cond_column_selftest.cpp) can be checked against the device code.  Arguments per
+ * function, in order: */
+typedef enum athad_thermo_fn {
+    ATHAD_THERMO_SATURATION_PRESSURE = 1,      /* T -> p_sat [hPa] (-1 where none)          */
+    ATHAD_THERMO_SUBLIMATION_PRESSURE,         /* T -> p_subl [hPa]                         */
+    ATHAD_THERMO_LATENT_HEAT,                  /* T -> L [J/kg]                             */
+    ATHAD_THERMO_SATURATION_MASS_FRACTION,     /* E, p, M_other -> q_sat                    */
+    ATHAD_THERMO_DEW_POINT,                    /* e [hPa] -> T_dew [K]                      */
+    ATHAD_THERMO_CP_OF,                        /* c, co2, T, M_bg -> cp [J/(kg K)]          */
+    ATHAD_THERMO_M_NONWATER,                   /* c, co2, M_bg -> M [kg/mol]                */
+    ATHAD_THERMO_MOIST_LAPSE,                  /* T, p, M_other, cp, R_mix, g -> lapse [K/m] */
+    ATHAD_THERMO_R_OF,                         /* c, co2, R_bg -> R [J/(kg K)]              */
+    ATHAD_THERMO_SATURATION_MASS_FRACTION_AT,  /* T, p, M_other -> q_sat                    */
+    ATHAD_THERMO_DQSAT_DT                      /* T, p, M_other -> dq_sat/dT [1/K]          */
+} athad_thermo_fn;
+/* Inputs per tuple (0 for an unknown function). */
+int32_t athad_thermo_arity(int32_t fn);
+/* in: n tuples of athad_thermo_arity(fn) doubles (host memory); out: n doubles (host).
+ * Synchronous; allocates device memory for the call. */
+athad_status athad_thermo_eval(int32_t fn, int32_t n, const double* in, double* out);
+
 /* ---- allocation-free entry point --------------------------------------------- */
 
 /* Largest grid athad_density_profile_noalloc accepts: im*jm (i, j) rows, im levels. */
@@ -582,9 +626,11 @@ athad_status athad_batch_autotune(athad_batch* b, int32_t reps, int32_t* best_sh
  * of 2 * ATHAD_NOALLOC_MAX_ROWS doubles (2 MiB) that every GPU loading the library keeps
  * until exit.  Grids beyond im*jm > ATHAD_NOALLOC_MAX_ROWS or im > ATHAD_NOALLOC_MAX_IM are
  * rejected with ATHAD_ERR_INVALID.  The first call on a device looks up the scratch
- * address (make it before any stream capture).  All calls share the scratch, so calls that
- * overlap on the GPU race; calls ordered on one stream do not.  Asynchronous: the outputs
- * are ready when the stream is. */
+ * address (make it before any stream capture) and keeps it for the life of the process:
+ * cudaDeviceReset between calls is not supported.  All calls share the scratch, so calls
+ * that overlap on the GPU race; calls ordered on one stream do not.  A CUDA error pending
+ * from earlier work is reported as ATHAD_ERR_CUDA without launching.  Asynchronous: the
+ * outputs are ready when the stream is. */
 athad_status athad_density_profile_noalloc(const double* r_humid, int32_t im, int32_t jm,
                                            int32_t km, size_t pitch, double* rho_base,
                                            double* dlnrho_dr, void* cuda_stream);

@@ -74,6 +74,9 @@ enum {
     OF_RADIATION, OF_EPSILON,
     OF_TEMP_STAND, OF_TEMP_DEW_POINT, OF_HUMIDITY_REL,
     OF_Q_LATENT, OF_Q_SENSIBLE,
+    OF_CORIOLIS_FORCE, OF_BUOYANCY_FORCE, OF_PRESSURE_GRADIENT_FORCE,
+    OF_VBUD_PGF, OF_VBUD_COR, OF_VBUD_ADVV, OF_VBUD_ADVH, OF_VBUD_DIFF, OF_VBUD_OTHER,
+    OF_WBUD_PGF, OF_WBUD_COR, OF_WBUD_ADVV, OF_WBUD_ADVH, OF_WBUD_DIFF, OF_WBUD_OTHER,
     OF_NFIELDS
 };
 enum { OF2_T_TOP_INIT = 0, OF2_P_STAT_LANDSCAPE, OF2_EVAPORATION, OF2_Q_SENSIBLE, OF2_VEL_STAR,

@@ -5,10 +5,11 @@
  * (cAtmosphereModel.cpp:1439-1446), flat terrain: every cell is air, so the last two keep
  * only bcSolidGround's value limits over every cell (BC_Atm.h:470-545).
  *
- * Only the fields the device context holds are treated; the reference's diagnostic
- * arrays in the same lists (radiation, PrecipitableWaterLocal, CoriolisForce,
- * CentrifugalForce, BuoyancyForce, PresGradForce) are not state of the hot path; Q_Latent
- * and Q_Sensible (latentSensibleHeat's outputs) are treated.  c43 and c13 are `const int` members initialised from 4.0/3.0 and 1.0/3.0
+ * Only the fields the device context holds are treated: the reference's lists also hold
+ * the output-only arrays of ThermoAtm::forces (CentrifugalForce, PresGradForce) and
+ * precipitableWater (PrecipitableWaterLocal); the right-hand side's CoriolisForce and
+ * BuoyancyForce, the heat diagnostics Q_Latent and Q_Sensible and the radiation flux are
+ * treated.  c43 and c13 are `const int` members initialised from 4.0/3.0 and 1.0/3.0
  * (cAtmosphereModel.h:158), i.e. 1 and 0, and are applied as such.
  */
 #include "or_internal.h"
@@ -17,7 +18,7 @@ static const int bc_both_cubic[] = {            /* BC_Atm.h:567-574, Pattern A *
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U,
     OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_M_U, OF_M_D, OF_Q_LATENT, OF_Q_SENSIBLE
+    OF_M_U, OF_M_D, OF_Q_LATENT, OF_Q_SENSIBLE, OF_CORIOLIS_FORCE, OF_BUOYANCY_FORCE
 };
 static const int bc_vn_bot[] = { OF_U, OF_V, OF_W, OF_P_CONV };   /* :586-590, Pattern B */
 static const int bc_cubic_bot_vn_top[] = {      /* :599-603, Pattern C */
@@ -27,17 +28,19 @@ static const int bc_cubic_bot_vn_top[] = {      /* :599-603, Pattern C */
 };
 static const int bc_hydro[] = { OF_P_STAT, OF_R_HUMID, OF_R_DRY };  /* :656-665, Pattern D */
 static const int bc_theta[] = {                 /* :760-776 */
-    OF_T, OF_P_STAT, OF_R_HUMID, OF_R_DRY, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR,
+    OF_T, OF_RADIATION, OF_P_STAT, OF_R_HUMID, OF_R_DRY, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR,
     OF_CO2, OF_TKE, OF_DIS, OF_NUE, OF_PROD, OF_TKE_SOURCE, OF_DIS_SOURCE,
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U, OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE
+    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE,
+    OF_CORIOLIS_FORCE, OF_BUOYANCY_FORCE
 };
 static const int bc_phi_avg[] = {               /* :806-817 */
-    OF_T, OF_P_STAT, OF_R_HUMID, OF_R_DRY, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR, OF_CO2,
+    OF_T, OF_RADIATION, OF_P_STAT, OF_R_HUMID, OF_R_DRY, OF_U, OF_V, OF_W, OF_C, OF_CLOUD, OF_ICE, OF_GR, OF_CO2,
     OF_S_C_C, OF_S_V, OF_S_C, OF_S_I, OF_S_R, OF_S_S, OF_S_G,
     OF_Q_V_U, OF_Q_C_U, OF_U_U, OF_V_U, OF_W_U, OF_MC_S, OF_MC_S_U, OF_MC_S_D,
-    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE
+    OF_C_U, OF_E_DD, OF_E_L, OF_E_P, OF_G_P, OF_Q_LATENT, OF_Q_SENSIBLE,
+    OF_CORIOLIS_FORCE, OF_BUOYANCY_FORCE
 };
 static const int bc_phi_extrap[] = { OF_TKE, OF_DIS, OF_NUE, OF_PROD, OF_TKE_SOURCE, OF_DIS_SOURCE };  /* :822-825 */
 

@@ -186,6 +186,10 @@ typedef struct rhs_out {
     double k[NY];
     double aux[3];
     double prod, tke_source, dis_source;
+    /* the right-hand side's diagnostic outputs (RHS_Atm_Turb.cpp:448-491, 1031-1057):
+     * CoriolisForce, BuoyancyForce, PressureGradientForce, Q_Latent, Q_Sensible and the six
+     * terms each of rhs_v and rhs_w (pgf, cor, advv, advh, diff, other) */
+    double force[3], q_latent, q_sensible, vbud[6], wbud[6];
 } rhs_out;
 
 /* RHS_Atmosphere_Turb for one interior cell, RHS_Atm_Turb.cpp:31-1080, flat terrain.
@@ -356,7 +360,7 @@ static void rhs_cell(const or_geom* g, const or_params* p, const or_step* s, int
     const double u_exp = u_ijk * exp_rm, v_invrm = v_ijk * inv_rm, w_invrs = w_ijk * inv_rmsinthe;
     const double pressure_t = coeff_energy_p * (u_exp * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
     const double inv_dr = 2.0 * G->inv_2dr, inv_dthe = 2.0 * G->inv_2dthe, inv_dphi = 2.0 * G->inv_2dphi;
-    double tr[NY];
+    double tr[NY], adv_r[NY], adv_t[NY], adv_p[NY];
     for (int n = 0; n < NY; n++) {
         const double* F = Y[n];
         double ar = d1r[n], at = d1t[n], ap = d1p[n];
@@ -365,6 +369,7 @@ static void rhs_cell(const or_geom* g, const or_params* p, const or_step* s, int
             at = minmod(F[c] - F[c - sJ], F[c + sJ] - F[c]) * inv_dthe;
             ap = minmod(F[c] - F[c - 1], F[c + 1] - F[c]) * inv_dphi;
         }
+        adv_r[n] = ar; adv_t[n] = at; adv_p[n] = ap;
         tr[n] = u_exp * ar + v_invrm * at + w_invrs * ap;
     }
     if (p->metric_curvature) {   /* :823-828 */
@@ -457,6 +462,67 @@ static void rhs_cell(const or_geom* g, const or_params* p, const or_step* s, int
     o->prod = prod;
     o->tke_source = tke_source;
     o->dis_source = dis_source;
+
+    /* diagnostic outputs: acting forces (:447-456) */
+    const double coeff_Coriolis = p->r_air * p->u_0 * p->omega, coeff_buoy = p->r_air * p->g;
+    const double coeff_u_p = 0.5 * p->r_air * p->u_0 * p->u_0 / p->L_atm;
+    o->force[0] = coriolis * coeff_Coriolis
+        * sqrt((pow(coriolis_rad, 2) + pow(coriolis_the, 2) + pow(coriolis_phi, 2)) / 3.0);
+    o->force[1] = 1.0 * coeff_buoy * (t_ijk - t_ref[i]);
+    o->force[2] = -coeff_u_p
+        * sqrt((pow(dpdr, 2) + pow(dpdthe * inv_rm, 2) + pow(dpdphi * inv_rmsinthe, 2)) / 3.0);
+    /* latent heat of the advected condensate (:458-488): the thresholds are saturation mass
+     * fractions at p_hydro, which nothing writes (0), so the rain branch is on below the
+     * critical point (q = 0) and off above it (no saturation: q = 1); the ice branch (the
+     * sublimation curve never reports "no saturation") always on */
+    const double t_u = t_ijk * p->t_0;
+    const double q_rain = or_saturation_mass_fraction(or_saturation_pressure(t_u), 0.0, 0.0);
+    const double q_ice = or_saturation_mass_fraction(or_sublimation_pressure(t_u), 0.0, 0.0);
+    const double c_ijk = Y[Y_C][c];
+    double q_lat = (c_ijk >= 0.85 * q_rain)
+        ? u_ijk * d1r[Y_CL] + v_ijk * inv_rm * d1t[Y_CL] + w_ijk * inv_rmsinthe * d1p[Y_CL] : 0.0;
+    const double q_lat_ice = (c_ijk >= 0.85 * q_ice)
+        ? u_ijk * d1r[Y_IC] + v_ijk * inv_rm * d1t[Y_IC] + w_ijk * inv_rmsinthe * d1p[Y_IC] : 0.0;
+    const double coeff_S = p->lamda * p->t_0 / p->L_atm;
+    const double coeff_L = p->r_air * p->c_0 * p->lv * p->u_0 / p->L_atm;
+    o->q_latent = coeff_L * (q_lat + q_lat_ice);
+    o->q_sensible = coeff_S * (d2r[Y_T] + d1r[Y_T] * 2.0 * inv_rm + d2t[Y_T] * inv_rm2
+        + d1t[Y_T] * G->costhe_inv_rm2sinthe + d2p[Y_T] * inv_rm2sinthe2);
+    /* momentum budget terms of rhs_v and rhs_w (:1031-1057) */
+    o->vbud[0] = -dpdthe_invrm;
+    o->vbud[1] = coriolis * force_nd * coriolis_the;
+    o->vbud[2] = -(u_exp * adv_r[Y_V]);
+    o->vbud[3] = -(v_invrm * adv_t[Y_V] + w_invrs * adv_p[Y_V]);
+    o->vbud[4] = diffusion_v;
+    o->vbud[5] = coeff_MC_vel * f[OF_MC_V][c] - surf_drag * v_ijk;
+    o->wbud[0] = -dpdphi_invrs;
+    o->wbud[1] = coriolis * force_nd * coriolis_phi;
+    o->wbud[2] = -(u_exp * adv_r[Y_W]);
+    o->wbud[3] = -(v_invrm * adv_t[Y_W] + w_invrs * adv_p[Y_W]);
+    o->wbud[4] = diffusion_w;
+    o->wbud[5] = coeff_MC_vel * f[OF_MC_W][c] - surf_drag * w_ijk;
+}
+
+/* write_diagnostics: bit 0 the turbulence production and sources, the acting forces and
+ * the heat diagnostics; bit 1 the momentum budget terms (the reference's vbudget_capture /
+ * wbudget_capture, set on its checkpoint iterations, cAtmosphereModel.cpp:1502-1503) */
+static void store_diagnostics(double* const* f, size_t c, const rhs_out* o, int flags)
+{
+    if (flags & 1) {
+        f[OF_PROD][c] = o->prod;
+        f[OF_TKE_SOURCE][c] = o->tke_source;
+        f[OF_DIS_SOURCE][c] = o->dis_source;
+        f[OF_CORIOLIS_FORCE][c] = o->force[0];
+        f[OF_BUOYANCY_FORCE][c] = o->force[1];
+        f[OF_PRESSURE_GRADIENT_FORCE][c] = o->force[2];
+        f[OF_Q_LATENT][c] = o->q_latent;
+        f[OF_Q_SENSIBLE][c] = o->q_sensible;
+    }
+    if (flags & 2)
+        for (int q = 0; q < 6; q++) {
+            f[OF_VBUD_PGF + q][c] = o->vbud[q];
+            f[OF_WBUD_PGF + q][c] = o->wbud[q];
+        }
 }
 
 /* stage update, RungeKutta_Atm_Turb.cpp:167-182 (and its copies for stages 2-4) */
@@ -536,11 +602,7 @@ int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int com
                     f[OF_AUX_U][c] = o4.aux[0];
                     f[OF_AUX_V][c] = o4.aux[1];
                     f[OF_AUX_W][c] = o4.aux[2];
-                    if (s->write_diagnostics) {
-                        f[OF_PROD][c] = o4.prod;
-                        f[OF_TKE_SOURCE][c] = o4.tke_source;
-                        f[OF_DIS_SOURCE][c] = o4.dis_source;
-                    }
+                    store_diagnostics(f, c, &o4, s->write_diagnostics);
                 }
             }
         }
@@ -584,11 +646,7 @@ int or_rk4(int im, int jm, int km, const or_params* p, const or_step* s, int com
                         f[OF_AUX_U][c] = o.aux[0];
                         f[OF_AUX_V][c] = o.aux[1];
                         f[OF_AUX_W][c] = o.aux[2];
-                        if (s->write_diagnostics) {
-                            f[OF_PROD][c] = o.prod;
-                            f[OF_TKE_SOURCE][c] = o.tke_source;
-                            f[OF_DIS_SOURCE][c] = o.dis_source;
-                        }
+                        store_diagnostics(f, c, &o, s->write_diagnostics);
                     }
                 }
             }

@@ -3,8 +3,8 @@
  * athad_oracle.h): cAtmosphereModel::RunTimeSlice for Ma = 0 (cAtmosphereModel.cpp:468-668)
  * on any grid, flat terrain, followed by run_3D_loop's Held-Suarez snapshot t_eq := t
  * (:750-753).  Its file output, printed diagnostics and the output-only arrays
- * (precipitableWater, forces, vegetationLand, standAtm_DewPoint_HumidRel) are left out: no
- * field of the model state reads them.
+ * (precipitableWater, forces' centrifugal and pressure-gradient arrays, vegetationLand,
+ * standAtm_DewPoint_HumidRel) are left out: no field of the model state reads them.
  *
  * Grid generalisation (the reference fixes 61 x 181 x 361 at 1 degree):
  *   - VelocityInitializer's anchor row of latitude phi, lround(90 - phi)
@@ -472,6 +472,31 @@ static void turbulence_init_fields(int im, int jm, int km, const or_params* p, c
     or_turb_wall_bc(im, jm, km, p, f, f2);
 }
 
+/* ThermoAtm::forces (ThermoAtm.h:518-614), the two arrays it shares with the right-hand side's
+ * outputs: CoriolisForce and BuoyancyForce of the interior cells (its centrifugal and
+ * pressure-gradient arrays are output only).  Coriolis and buoyancy are the configuration's
+ * 1; before the first RK4 step the level-mean temperature does not exist and the buoyancy
+ * reference is 1. */
+static void forces(int im, int jm, int km, const or_params* p, const or_geom* g, double* const* f)
+{
+    const double two_omega = 2.0 * p->omega;
+    const double nontrad_d = p->coriolis_nontrad ? 1.0 : 0.0;
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 1; j < jm - 1; j++) {
+            const double sinthe = g->sin_w[j], costhe = g->cos_t[j];
+            for (int k = 1; k < km - 1; k++) {
+                const size_t q = OR_IDX(i, j, k);
+                const double w_ijk = f[OF_W][q] * p->u_0;
+                const double Cor_r = -nontrad_d * two_omega * sinthe * w_ijk;
+                const double Cor_the = two_omega * costhe * w_ijk;
+                const double Cor_phi = -two_omega * (costhe * f[OF_V][q] + nontrad_d * sinthe * f[OF_U][q]) * p->u_0;
+                f[OF_CORIOLIS_FORCE][q] = 1.0 * p->r_air
+                    * sqrt(Cor_r * Cor_r + Cor_the * Cor_the + Cor_phi * Cor_phi);
+                f[OF_BUOYANCY_FORCE][q] = 1.0e-3 * 1.0 * f[OF_R_HUMID][q] * p->g * (f[OF_T][q] - 1.0);
+            }
+        }
+}
+
 static void precipitation_sum(int im, int jm, int km, double* const* f)   /* UtilsAtm.h:51-65 */
 {
     const size_t n = (size_t)im * jm * km;
@@ -577,6 +602,7 @@ int or_init_state(int im, int jm, int km, const or_params* p, const or_init_cfg*
         or_co2_column(im, jm, km, p, f, f2, out);                   /* :632 (co2_total) */
     }
     or_densities(im, jm, km, p, cm, 0, f, f2, prof);                /* :634 */
+    forces(im, jm, km, p, &g, f);                                   /* :635 */
     or_water_vapour_evaporation(im, jm, km, p, f, f2);              /* :637 */
     or_latent_sensible_heat(im, jm, km, p, cm, f);                  /* :638 */
     if (upto <= OR_INIT_DIAGNOSE) goto done;

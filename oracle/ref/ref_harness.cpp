@@ -93,6 +93,9 @@ Array* field3(cAtmosphereModel* m, const std::string& n)
     F(TempStand) F(TempDewPoint) F(HumidityRel) F(Q_Latent) F(Q_Sensible)
     F(rhs_t) F(rhs_u) F(rhs_v) F(rhs_w) F(rhs_c) F(rhs_cloud) F(rhs_ice) F(rhs_g) F(rhs_co2)
     F(rhs_tke) F(rhs_dis) F(h) F(p_hydro)
+    F(CoriolisForce) F(BuoyancyForce) F(PressureGradientForce)
+    F(vbud_pgf) F(vbud_cor) F(vbud_advv) F(vbud_advh) F(vbud_diff) F(vbud_other)
+    F(wbud_pgf) F(wbud_cor) F(wbud_advv) F(wbud_advh) F(wbud_diff) F(wbud_other)
 #undef F
     return nullptr;
 }
@@ -339,6 +342,14 @@ void ref_set_scalars(void* p, double dt, double diffusion_ramp, double buoyancy_
     m->buoyancy_ramp = buoyancy_ramp;
     m->total_iter_count = total_iter_count;
     m->iter_n = iter_n;
+}
+
+// the momentum-budget capture of the right-hand side (vbudget_capture / wbudget_capture)
+void ref_set_budget_capture(void* p, int on)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)p;
+    m->vbudget_capture = (on != 0);
+    m->wbudget_capture = (on != 0);
 }
 
 // a few derived constants, for the tests to compare with their own derivation

@@ -126,7 +126,7 @@ class OracleState:
     def rk4(self, dt=4e-5, diffusion_ramp=1.0, buoyancy_ramp=1.0, write_diagnostics=False, compat=0):
         F, _, P = self._args()
         im, jm, km = self.shape
-        s = Step(dt, diffusion_ramp, buoyancy_ramp, 1 if write_diagnostics else 0, 0)
+        s = Step(dt, diffusion_ramp, buoyancy_ramp, int(write_diagnostics), 0)
         r = lib().or_rk4(im, jm, km, ctypes.byref(self.params), ctypes.byref(s), compat, F, P)
         assert r == 0
 

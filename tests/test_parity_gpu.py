@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from athad_cond_b200 import GpuAtmosphere, make_state, mirror
-from athad_cond_b200._abi import FIELD_NAMES, config_params, Wall, Turb
+from athad_cond_b200._abi import FIELD_NAMES, Precision, config_params, Wall, Turb
 from oracle_binding import OracleState
 
 pytestmark = pytest.mark.gpu
@@ -50,6 +50,41 @@ def test_rk4_step_matches_oracle(grid, wall):
             assert e <= 1e-12, (n, e)
         tr = g.download_profile("t_ref_level")
         assert np.array_equal(tr, o.prof["t_ref_level"])
+
+
+DIAGNOSTICS = ["prod", "tke_source", "dis_source", "CoriolisForce", "BuoyancyForce",
+               "PressureGradientForce", "Q_Latent", "Q_Sensible",
+               "vbud_pgf", "vbud_cor", "vbud_advv", "vbud_advh", "vbud_diff", "vbud_other",
+               "wbud_pgf", "wbud_cor", "wbud_advv", "wbud_advh", "wbud_diff", "wbud_other"]
+
+
+@pytest.mark.parametrize("precision", [Precision.FP64, Precision.MIXED])
+def test_rk4_step_diagnostic_outputs(precision):
+    """The right-hand side's diagnostic outputs (acting forces, heat diagnostics, momentum
+    budget terms) on a diagnostic step: within 1e-12 of the oracle in FP64 (the same IEEE
+    operations; CUDA's saturation curve only decides the latent-heat branch), exactly mirror
+    symmetric (v-terms antisymmetric).  The mixed form forms them in FP64 from its FP32 stage
+    state, whose rounding the first and second differences amplify: checked for symmetry
+    and finiteness, and the smooth ones (buoyancy, Coriolis) within 1e-5."""
+    grid = (11, 21, 41)
+    p = config_params()
+    p.precision = int(precision)
+    st = make_state(*grid, seed=17, symmetric=True)
+    o = OracleState(st, p)
+    o.rk4(dt=4e-5, diffusion_ramp=1.0, buoyancy_ramp=0.5, write_diagnostics=3)
+    with gpu_with(st, p) as g:
+        g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5, write_diagnostics=3)
+        for n in DIAGNOSTICS:
+            a = g.download(n)
+            assert np.isfinite(a).all(), n
+            e = relerr(a, o.f[n])
+            if precision == Precision.FP64:
+                assert e <= 1e-12, (n, e)
+            elif n in ("BuoyancyForce", "CoriolisForce"):
+                assert e <= 1e-5, (n, e)
+            anti = n.startswith("vbud") or n == "v"
+            assert np.array_equal(a, mirror(a, anti)), n
+            assert float(np.max(np.abs(a))) > 0.0, n
 
 
 @pytest.mark.parametrize("turb", [Turb.K_EPSILON, Turb.K_OMEGA])
@@ -253,3 +288,26 @@ def test_pressure_boundaries_and_ceiling_bit_exact(grid):
             a = g.download("p_dyn")
         assert np.array_equal(a, o.f["p_dyn"], equal_nan=True), it
         assert np.max(np.abs(a)) <= (10.0 if it <= 300 else 3.0)
+
+
+@pytest.mark.parametrize("precision", [Precision.FP64, Precision.MIXED])
+def test_report_counts_nonfinite_temperature_and_times_the_step(precision):
+    """athad_get_report: the level mean of each RK4 step counts the non-finite cells of its
+    input t; last_kernel_ms is the step's device time."""
+    grid = (11, 21, 41)
+    p = config_params()
+    p.precision = int(precision)
+    st = make_state(*grid, seed=11)
+    with GpuAtmosphere(*grid, p) as g:
+        g.upload_state(st)
+        assert g.report()["last_kernel_ms"] == 0.0
+        g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5)
+        r = g.report()
+        assert r["nonfinite_inputs"] == 0 and r["last_kernel_ms"] > 0.0
+        t = st["t"].copy()
+        t[3, 5, 7] = np.nan
+        t[4, 10, 0] = np.inf
+        t[9, 20, 40] = -np.inf
+        g.upload("t", t)
+        g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, 0.5)
+        assert g.report()["nonfinite_inputs"] == 3

@@ -19,6 +19,7 @@ semantics, must reproduce every hot-path function bit for bit:
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
+import ctypes
 import os
 
 import numpy as np
@@ -101,6 +102,29 @@ def test_rk4_step_bit_exact(ref):
     assert_identical(R, o, ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
                             "aux_u", "aux_v", "aux_w"])
     assert np.array_equal(R.getp("t_ref_level"), o.prof["t_ref_level"])
+
+
+DIAGNOSTICS = ["prod", "tke_source", "dis_source", "CoriolisForce", "BuoyancyForce",
+               "PressureGradientForce", "Q_Latent", "Q_Sensible",
+               "vbud_pgf", "vbud_cor", "vbud_advv", "vbud_advh", "vbud_diff", "vbud_other",
+               "wbud_pgf", "wbud_cor", "wbud_advv", "wbud_advh", "wbud_diff", "wbud_other"]
+
+
+def test_rk4_step_diagnostic_outputs_bit_exact(ref):
+    """The right-hand side's diagnostic outputs of the last stage (RHS_Atm_Turb.cpp:447-491,
+    1031-1057), with the momentum-budget capture of a checkpoint iteration."""
+    R, o = fresh(ref)
+    R.set_scalars(DT, 1.0, 0.3, 90, 90)
+    R.lib.ref_set_budget_capture.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    R.lib.ref_set_budget_capture(R.h, 1)
+    R.lib.ref_rk4(R.h)
+    R.lib.ref_set_budget_capture(R.h, 0)
+    o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS, write_diagnostics=3)
+    interior = (slice(1, -1), slice(1, -1), slice(1, -1))
+    for n in DIAGNOSTICS:
+        a, b = R.get(n)[interior], o.f[n][interior]
+        assert np.array_equal(a, b), (n, float(np.max(np.abs(a - b))))
+    assert float(np.max(np.abs(o.f["CoriolisForce"]))) > 0.0 and float(np.max(np.abs(o.f["Q_Sensible"]))) > 0.0
 
 
 def test_pressure_sweep_bit_exact(ref):

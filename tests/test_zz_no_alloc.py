@@ -21,7 +21,7 @@ import pytest
 import torch
 
 from athad_cond_b200 import GpuAtmosphere, make_state, load_library
-from athad_cond_b200._abi import NOALLOC_MAX_ROWS, Status, config_params
+from athad_cond_b200._abi import NOALLOC_MAX_IM, NOALLOC_MAX_ROWS, Status, config_params
 
 pytestmark = pytest.mark.gpu
 
@@ -58,12 +58,34 @@ def noalloc_profile(lib, g, grid):
 def test_noalloc_profile_matches_context_path_two_calls():
     lib = load_library()
     torch.cuda.init()
-    for grid, seed in (((41, 181, 361), 101), ((21, 91, 181), 202)):
+    # odd jm (an equator row) and even jm (every row paired with its mirror)
+    for grid, seed in (((41, 181, 361), 101), ((21, 91, 181), 202), ((11, 20, 41), 303)):
         g, rho_ctx, dln_ctx = context_profile(grid, seed)
         rho, dln = noalloc_profile(lib, g, grid)
         g.close()
         assert relerr(rho, rho_ctx) <= 1e-11
         assert relerr(dln, dln_ctx) <= 1e-11
+
+
+def test_noalloc_accepts_the_largest_grid():
+    """im = ATHAD_NOALLOC_MAX_IM levels with im*jm = ATHAD_NOALLOC_MAX_ROWS rows exactly."""
+    lib = load_library()
+    im, jm, km = NOALLOC_MAX_IM, NOALLOC_MAX_ROWS // NOALLOC_MAX_IM, 8
+    r = torch.rand((im, jm, km), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+    r += 0.5
+    rho = torch.empty(im, dtype=torch.float64, device="cuda")
+    dln = torch.empty(im, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    st = lib.athad_density_profile_noalloc(ctypes.c_void_p(r.data_ptr()), im, jm, km, km,
+                                           ctypes.c_void_p(rho.data_ptr()), ctypes.c_void_p(dln.data_ptr()),
+                                           ctypes.c_void_p(stream.cuda_stream))
+    assert st == Status.OK
+    stream.synchronize()
+    # every positive cell counts with its cos-latitude weight: the row means of a field that
+    # is 0.5 + U[0, 1) lie in (0.5, 1.5)
+    rb = rho.cpu().numpy()
+    assert np.isfinite(rb).all() and (rb > 0.5).all() and (rb < 1.5).all()
+    assert np.isfinite(dln.cpu().numpy()).all()
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
