@@ -244,6 +244,7 @@ SIGNATURES = {
     "athad_water_vapour_evaporation": (ctypes.c_int, [_P]),
     "athad_latent_sensible_heat": (ctypes.c_int, [_P]),
     "athad_update_skin_temperature": (ctypes.c_int, [_P, ctypes.c_double, _D]),
+    "athad_forces": (ctypes.c_int, [_P]),
     "athad_co2_column": (ctypes.c_int, [_P, ctypes.POINTER(BudgetReport)]),
     "athad_water_budget": (ctypes.c_int, [_P, ctypes.POINTER(BudgetReport), _D]),
     "athad_checkpoint_begin": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),

@@ -278,6 +278,11 @@ class GpuAtmosphere:
         """Radiation mode 2's apply_radiative_heating (cAtmosphereModel.cpp:864-879)."""
         self._check(self.lib.athad_radiative_heating(self._h, float(omega_rad)))
 
+    def forces(self):
+        """ThermoAtm::forces' Coriolis and buoyancy arrays (ThermoAtm.h:518-614; call sites
+        cAtmosphereModel.cpp:635, 1419)."""
+        self._check(self.lib.athad_forces(self._h))
+
     def two_cat_ice_scheme(self):
         """TwoCatIceScheme::run (TwoCatIceScheme.h:89-109; call site cAtmosphereModel.cpp:1238)."""
         self._check(self.lib.athad_two_cat_ice_scheme(self._h))

@@ -425,6 +425,7 @@ athad_status athad_upload_profile(athad_ctx* ctx, athad_profile f, const double*
 {
     if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NPROFILES) return fail(ctx, ATHAD_ERR_INVALID, "upload_profile: bad argument");
     if (n != (size_t)ctx->grid.im) return fail(ctx, ATHAD_ERR_INVALID, "upload_profile: size mismatch");
+    if (f == ATHAD_PROF_T_REF_LEVEL) ctx->level_mean_valid = true;
     return cuda_check(ctx, cudaMemcpyAsync(ctx->prof[f], host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
                       "upload_profile");
 }
@@ -485,6 +486,7 @@ athad_status athad_level_mean(athad_ctx* ctx)
     launch_level_mean(ctx->L.d, ctx->field[ATHAD_T], ctx->sin_w, ctx->prof[ATHAD_PROF_T_REF_LEVEL], ctx->row_sum,
                       ctx->stream, ctx->counters + kNonfiniteSlot);
     ATHAD_CHECK_LAUNCH(ctx, "level_mean");
+    ctx->level_mean_valid = true;
     return ATHAD_OK;
 }
 

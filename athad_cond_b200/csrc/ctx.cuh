@@ -106,6 +106,8 @@ struct athad_ctx {
     double* rad_d = nullptr;                  // [im] rad.z
     int* i_trop = nullptr;                    // [jm] tropopause level per row (standAtm)
     bool trop_set = false;
+    bool level_mean_valid = false;            // t_ref_level computed (or uploaded) since creation
+                                              // or the last initial state
     double residuum_old = 1.0e-5;             // cAtmosphereModel.h:164
     // the budgets' first-call references (cAtmosphereModel.h:89-109; <= 0 / empty = unset)
     double q_co2_ref = -1.0, q_h2o_ref = -1.0, q_h2o_fixed_ref = -1.0;
@@ -151,4 +153,6 @@ void mixed_args(athad_ctx* ctx, const athad_step_scalars* s, RK4MArgs& a);
 // the boundary conditions of athad_boundary_conditions, with (wall_bc = 1) or without the
 // turbulence wall values
 athad_status boundary_conditions(athad_ctx* ctx, int wall_bc);
+// ThermoAtm::forces' Coriolis and buoyancy arrays (k_init.cu); t_ref null: reference 1
+void launch_forces(athad_ctx* ctx, const double* t_ref);
 }

@@ -274,14 +274,17 @@ __global__ void __launch_bounds__(128) turb_init_kernel(TurbInitArgs a)
     if (a.set_dis_wall) a.dis[c0] = a.dis_wall;
 }
 
+}  // namespace
+
 // ThermoAtm::forces (ThermoAtm.h:518-614), the two arrays it shares with the right-hand
-// side's outputs (CoriolisForce, BuoyancyForce) in the interior cells; before the first RK4
-// step the buoyancy reference (the level-mean temperature) does not exist and is 1
-__global__ void __launch_bounds__(256) init_forces_kernel(Dims d, const GeoIJ* geo, const double* sin_w,
-                                                          const double* u, const double* v, const double* w,
-                                                          const double* t, const double* r_humid,
-                                                          double* coriolis, double* buoyancy, double two_omega,
-                                                          double nontrad_d, double u_0, double r_air, double g)
+// side's outputs (CoriolisForce, BuoyancyForce) in the interior cells; the buoyancy
+// reference is the level-mean temperature t_ref, or 1 where none exists yet (t_ref null:
+// before the first RK4 step)
+__global__ void __launch_bounds__(256) forces_kernel(Dims d, const GeoIJ* geo, const double* sin_w,
+                                                     const double* u, const double* v, const double* w,
+                                                     const double* t, const double* r_humid, const double* t_ref,
+                                                     double* coriolis, double* buoyancy, double two_omega,
+                                                     double nontrad_d, double u_0, double r_air, double g)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int row = blockIdx.y, i = row / d.jm, j = row % d.jm;
@@ -293,8 +296,20 @@ __global__ void __launch_bounds__(256) init_forces_kernel(Dims d, const GeoIJ* g
     const double Cor_the = two_omega * costhe * w_ijk;
     const double Cor_phi = -two_omega * (costhe * v[q] + nontrad_d * sinthe * u[q]) * u_0;
     coriolis[q] = 1.0 * r_air * sqrt(Cor_r * Cor_r + Cor_the * Cor_the + Cor_phi * Cor_phi);
-    buoyancy[q] = 1.0e-3 * 1.0 * r_humid[q] * g * (t[q] - 1.0);
+    buoyancy[q] = 1.0e-3 * 1.0 * r_humid[q] * g * (t[q] - (t_ref ? t_ref[i] : 1.0));
 }
+
+void launch_forces(athad_ctx* ctx, const double* t_ref)
+{
+    const Dims& d = ctx->L.d;
+    const athad_params& p = ctx->p;
+    forces_kernel<<<dim3((d.km + 255) / 256, d.im * d.jm), 256, 0, ctx->stream>>>(
+        d, ctx->geo, ctx->sin_w, ctx->field[ATHAD_U], ctx->field[ATHAD_V], ctx->field[ATHAD_W],
+        ctx->field[ATHAD_T], ctx->field[ATHAD_R_HUMID], t_ref, ctx->field[ATHAD_CORIOLIS_FORCE],
+        ctx->field[ATHAD_BUOYANCY_FORCE], 2.0 * p.omega, p.coriolis_nontrad ? 1.0 : 0.0, p.u_0, p.r_air, p.g);
+}
+
+namespace {
 
 // UtilsAtm::precipitationSum (UtilsAtm.h:51-65)
 __global__ void __launch_bounds__(256) precipitation_sum_kernel(Dims d, const double* r, const double* sn,
@@ -524,6 +539,14 @@ void athad_default_init_config(athad_init_config* c)
     c->q_bg = m_bg / M_mean;
 }
 
+athad_status athad_forces(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    athad::launch_forces(ctx, ctx->level_mean_valid ? ctx->prof[ATHAD_PROF_T_REF_LEVEL] : nullptr);
+    ATHAD_CHECK_LAUNCH(ctx, "forces");
+    return ATHAD_OK;
+}
+
 athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* cfg)
 {
     using namespace athad;
@@ -564,6 +587,7 @@ athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* cfg)
     ctx->q_co2_ref = ctx->q_h2o_ref = ctx->q_h2o_fixed_ref = -1.0;   // co2Column(true), waterBudget(true) below
     ctx->air_levels.clear();
     ctx->h2o_levels.clear();
+    ctx->level_mean_valid = false;
 
     // host tables: tropopause levels, velocity profiles, surface temperature, layer steps
     const std::vector<double>& h = ctx->height_h;
@@ -711,10 +735,7 @@ athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* cfg)
     ATHAD_TRY(athad_co2_column(ctx, &rep));
     ATHAD_TRY(athad_water_budget(ctx, &rep, nullptr));
     ATHAD_TRY(athad_densities(ctx, 0));
-    init_forces_kernel<<<rows_grid, 256, 0, st>>>(d, ctx->geo, ctx->sin_w, ctx->field[ATHAD_U], ctx->field[ATHAD_V],
-                                                  ctx->field[ATHAD_W], ctx->field[ATHAD_T], ctx->field[ATHAD_R_HUMID],
-                                                  ctx->field[ATHAD_CORIOLIS_FORCE], ctx->field[ATHAD_BUOYANCY_FORCE],
-                                                  2.0 * p.omega, p.coriolis_nontrad ? 1.0 : 0.0, p.u_0, p.r_air, p.g);
+    launch_forces(ctx, nullptr);   // no level mean exists yet
     ATHAD_CHECK_LAUNCH(ctx, "initial_state forces");
     ATHAD_TRY(athad_water_vapour_evaporation(ctx));
     ATHAD_TRY(athad_latent_sensible_heat(ctx));

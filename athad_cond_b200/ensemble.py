@@ -19,7 +19,9 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._abi import Params, Precision, config_params
+import ctypes
+
+from ._abi import InitConfig, Params, Precision, config_init, config_params
 
 R_STAR = 8.314462618
 M_H2O, M_CO2, M_N2 = 0.018015, 0.044010, 0.028014
@@ -56,7 +58,7 @@ def resolve(x_h2o: float, x_co2: float, x_n2: float) -> dict:
     M_mean = m_h2o + m_co2 + m_bg
     M_bg = (m_bg / x_n2) if x_n2 > 0 else M_N2
     return {"M_mean": M_mean, "R_mix": R_STAR / M_mean, "q_H2O": m_h2o / M_mean,
-            "q_CO2": m_co2 / M_mean, "M_bg": M_bg, "R_bg": R_STAR / M_bg}
+            "q_CO2": m_co2 / M_mean, "q_bg": m_bg / M_mean, "M_bg": M_bg, "R_bg": R_STAR / M_bg}
 
 
 @dataclass
@@ -103,6 +105,19 @@ def condition_params(cond: Condition, precision: Precision = Precision.MIXED) ->
     p.M_bg = cond.surf["M_bg"]
     p.R_bg = cond.surf["R_bg"]
     return p
+
+
+def init_config(cond: Condition) -> InitConfig:
+    """athad_init_config of a condition point: the sea surface at T_sea on the equator with the
+    configuration's 10 K equator-to-pole contrast (513.15 / 503.15 K), the CO2 share of the
+    non-water surface air; the cli/config_cond.xml values otherwise."""
+    c = config_init()
+    c.struct_size = ctypes.sizeof(InitConfig)
+    c.t_surf_equator = cond.T_sea
+    c.t_surf_pole = cond.T_sea - 10.0
+    c.q_CO2 = cond.surf["q_CO2"]
+    c.q_bg = cond.surf["q_bg"]
+    return c
 
 
 def state_params(cond: Condition) -> dict:

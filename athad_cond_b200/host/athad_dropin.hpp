@@ -163,8 +163,23 @@ public:
         up(ATHAD_S_G, m.S_g); up(ATHAD_S_V, m.S_v);
         up(ATHAD_MC_T, m.MC_t); up(ATHAD_MC_Q, m.MC_q); up(ATHAD_MC_V, m.MC_v); up(ATHAD_MC_W, m.MC_w);
         up_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
-        athad_step_scalars s{m.dt, m.diffusion_ramp, m.buoyancy_ramp, 1, 0};
+        // the right-hand side's outputs are written in the interior: the boundary cells keep
+        // the model's values
+        up(ATHAD_CORIOLIS_FORCE, m.CoriolisForce); up(ATHAD_BUOYANCY_FORCE, m.BuoyancyForce);
+        up(ATHAD_PRESSURE_GRADIENT_FORCE, m.PressureGradientForce);
+        up(ATHAD_Q_LATENT, m.Q_Latent); up(ATHAD_Q_SENSIBLE, m.Q_Sensible);
+        const bool budget = m.vbudget_capture || m.wbudget_capture;
+        athad_step_scalars s{m.dt, m.diffusion_ramp, m.buoyancy_ramp, budget ? 3 : 1, 0};
         check(ctx_, athad_rk4_step(ctx_, &s), "rk4_step");
+        down(ATHAD_CORIOLIS_FORCE, m.CoriolisForce); down(ATHAD_BUOYANCY_FORCE, m.BuoyancyForce);
+        down(ATHAD_PRESSURE_GRADIENT_FORCE, m.PressureGradientForce);
+        down(ATHAD_Q_LATENT, m.Q_Latent); down(ATHAD_Q_SENSIBLE, m.Q_Sensible);
+        if (budget) {
+            down(ATHAD_VBUD_PGF, m.vbud_pgf); down(ATHAD_VBUD_COR, m.vbud_cor); down(ATHAD_VBUD_ADVV, m.vbud_advv);
+            down(ATHAD_VBUD_ADVH, m.vbud_advh); down(ATHAD_VBUD_DIFF, m.vbud_diff); down(ATHAD_VBUD_OTHER, m.vbud_other);
+            down(ATHAD_WBUD_PGF, m.wbud_pgf); down(ATHAD_WBUD_COR, m.wbud_cor); down(ATHAD_WBUD_ADVV, m.wbud_advv);
+            down(ATHAD_WBUD_ADVH, m.wbud_advh); down(ATHAD_WBUD_DIFF, m.wbud_diff); down(ATHAD_WBUD_OTHER, m.wbud_other);
+        }
         down(ATHAD_T, m.t); down(ATHAD_U, m.u); down(ATHAD_V, m.v); down(ATHAD_W, m.w);
         down(ATHAD_C, m.c); down(ATHAD_CLOUD, m.cloud); down(ATHAD_ICE, m.ice); down(ATHAD_GR, m.gr);
         down(ATHAD_CO2, m.co2); down(ATHAD_TKE, m.tke); down(ATHAD_DIS, m.dis);
@@ -264,7 +279,8 @@ public:
         X(ATHAD_V_U, v_u) X(ATHAD_W_U, w_u) X(ATHAD_MC_S, s) X(ATHAD_MC_S_U, s_u) X(ATHAD_MC_S_D, s_d) \
         X(ATHAD_M_U, M_u) X(ATHAD_M_D, M_d) X(ATHAD_C_U, c_u) X(ATHAD_E_DD, e_d) X(ATHAD_E_L, e_l) \
         X(ATHAD_E_P, e_p) X(ATHAD_G_P, g_p) X(ATHAD_P_CONV, P_conv) X(ATHAD_Q_LATENT, Q_Latent) \
-        X(ATHAD_Q_SENSIBLE, Q_Sensible)
+        X(ATHAD_Q_SENSIBLE, Q_Sensible) X(ATHAD_CORIOLIS_FORCE, CoriolisForce) \
+        X(ATHAD_BUOYANCY_FORCE, BuoyancyForce) X(ATHAD_RADIATION, radiation)
 #define ATHAD_BC_UP(F, N) up(F, m.N);
 #define ATHAD_BC_DOWN(F, N) down(F, m.N);
         ATHAD_BC_FIELDS(ATHAD_BC_UP)
@@ -339,6 +355,18 @@ public:
         down(ATHAD_PROD, m.prod); down(ATHAD_TKE_SOURCE, m.tke_source);
         down(ATHAD_DIS_SOURCE, m.dis_source);
         down2(ATHAD_2D_VEL_STAR, m.vel_star);
+    }
+
+    // ThermoAtm(m).forces() (cAtmosphereModel.cpp:635, 1419): its Coriolis and buoyancy
+    // arrays (the centrifugal and pressure-gradient ones are output only and stay the
+    // host's); the buoyancy reference is the model's level mean once it has one
+    void Forces(Model& m)
+    {
+        up(ATHAD_U, m.u); up(ATHAD_V, m.v); up(ATHAD_W, m.w); up(ATHAD_T, m.t); up(ATHAD_R_HUMID, m.r_humid);
+        up(ATHAD_CORIOLIS_FORCE, m.CoriolisForce); up(ATHAD_BUOYANCY_FORCE, m.BuoyancyForce);
+        up_profile(ATHAD_PROF_T_REF_LEVEL, m.t_ref_level);
+        check(ctx_, athad_forces(ctx_), "forces");
+        down(ATHAD_CORIOLIS_FORCE, m.CoriolisForce); down(ATHAD_BUOYANCY_FORCE, m.BuoyancyForce);
     }
 
     // ThermoAtm(m).standAtm_DewPoint_HumidRel() (cAtmosphereModel.cpp:636, 1420), flat
@@ -435,6 +463,173 @@ private:
     int im_, jm_, km_;
     std::vector<double> buf_;
     athad_ctx* ctx_ = nullptr;
+};
+
+// Every 3-D field a context holds and the model member it mirrors (athad_field order).
+#define ATHAD_ALL_FIELDS(X) \
+    X(ATHAD_T, t) X(ATHAD_U, u) X(ATHAD_V, v) X(ATHAD_W, w) X(ATHAD_C, c) X(ATHAD_CLOUD, cloud) \
+    X(ATHAD_ICE, ice) X(ATHAD_GR, gr) X(ATHAD_CO2, co2) X(ATHAD_TKE, tke) X(ATHAD_DIS, dis) \
+    X(ATHAD_TN, tn) X(ATHAD_UN, un) X(ATHAD_VN, vn) X(ATHAD_WN, wn) X(ATHAD_CN, cn) \
+    X(ATHAD_CLOUDN, cloudn) X(ATHAD_ICEN, icen) X(ATHAD_GRN, grn) X(ATHAD_CO2N, co2n) \
+    X(ATHAD_TKEN, tken) X(ATHAD_DISN, disn) X(ATHAD_P_DYN, p_dyn) X(ATHAD_NUE, nue) \
+    X(ATHAD_T_EQ, t_eq) X(ATHAD_P_STAT, p_stat) X(ATHAD_R_HUMID, r_humid) X(ATHAD_S_C, S_c) \
+    X(ATHAD_S_R, S_r) X(ATHAD_S_I, S_i) X(ATHAD_S_S, S_s) X(ATHAD_S_G, S_g) X(ATHAD_S_V, S_v) \
+    X(ATHAD_MC_T, MC_t) X(ATHAD_MC_Q, MC_q) X(ATHAD_MC_V, MC_v) X(ATHAD_MC_W, MC_w) \
+    X(ATHAD_AUX_U, aux_u) X(ATHAD_AUX_V, aux_v) X(ATHAD_AUX_W, aux_w) X(ATHAD_PROD, prod) \
+    X(ATHAD_TKE_SOURCE, tke_source) X(ATHAD_DIS_SOURCE, dis_source) X(ATHAD_S_C_C, S_c_c) \
+    X(ATHAD_P_RAIN, P_rain) X(ATHAD_P_SNOW, P_snow) X(ATHAD_P_GRAUPEL, P_graupel) \
+    X(ATHAD_PRECIPITATION, Precipitation) X(ATHAD_R_DRY, r_dry) X(ATHAD_MC_S, s) \
+    X(ATHAD_MC_S_U, s_u) X(ATHAD_MC_S_D, s_d) X(ATHAD_M_U, M_u) X(ATHAD_M_D, M_d) \
+    X(ATHAD_Q_V_U, q_v_u) X(ATHAD_Q_C_U, q_c_u) X(ATHAD_Q_V_D, q_v_d) X(ATHAD_U_U, u_u) \
+    X(ATHAD_V_U, v_u) X(ATHAD_W_U, w_u) X(ATHAD_U_D, u_d) X(ATHAD_V_D, v_d) X(ATHAD_W_D, w_d) \
+    X(ATHAD_E_U, E_u) X(ATHAD_D_U, D_u) X(ATHAD_E_D, E_d) X(ATHAD_D_D, D_d) X(ATHAD_C_U, c_u) \
+    X(ATHAD_E_L, e_l) X(ATHAD_E_DD, e_d) X(ATHAD_E_P, e_p) X(ATHAD_G_P, g_p) X(ATHAD_P_CONV, P_conv) \
+    X(ATHAD_CLOUD_BASE, CloudBase) X(ATHAD_LEVEL_FREE_SINKING, LevelFreeSinking) \
+    X(ATHAD_DEEP_BEG, Deep_beg) X(ATHAD_DEEP_END, Deep_end) X(ATHAD_P_RAINN, P_rainn) \
+    X(ATHAD_P_SNOWN, P_snown) X(ATHAD_RADIATION, radiation) X(ATHAD_EPSILON, epsilon) \
+    X(ATHAD_TEMP_STAND, TempStand) X(ATHAD_TEMP_DEW_POINT, TempDewPoint) \
+    X(ATHAD_HUMIDITY_REL, HumidityRel) X(ATHAD_Q_LATENT, Q_Latent) X(ATHAD_Q_SENSIBLE, Q_Sensible) \
+    X(ATHAD_CORIOLIS_FORCE, CoriolisForce) X(ATHAD_BUOYANCY_FORCE, BuoyancyForce) \
+    X(ATHAD_PRESSURE_GRADIENT_FORCE, PressureGradientForce) \
+    X(ATHAD_VBUD_PGF, vbud_pgf) X(ATHAD_VBUD_COR, vbud_cor) X(ATHAD_VBUD_ADVV, vbud_advv) \
+    X(ATHAD_VBUD_ADVH, vbud_advh) X(ATHAD_VBUD_DIFF, vbud_diff) X(ATHAD_VBUD_OTHER, vbud_other) \
+    X(ATHAD_WBUD_PGF, wbud_pgf) X(ATHAD_WBUD_COR, wbud_cor) X(ATHAD_WBUD_ADVV, wbud_advv) \
+    X(ATHAD_WBUD_ADVH, wbud_advh) X(ATHAD_WBUD_DIFF, wbud_diff) X(ATHAD_WBUD_OTHER, wbud_other)
+#define ATHAD_ALL_FIELDS2D(X) \
+    X(ATHAD_2D_P_STAT_LANDSCAPE, p_stat_landscape) X(ATHAD_2D_EVAPORATION, Evaporation) \
+    X(ATHAD_2D_Q_SENSIBLE, Q_sensible_2D) X(ATHAD_2D_VEL_STAR, vel_star) X(ATHAD_2D_EPSILON, epsilon_2D) \
+    X(ATHAD_2D_ALBEDO, albedo) X(ATHAD_2D_EVAPORATION_DALTON, Evaporation_Dalton) \
+    X(ATHAD_2D_EVAPORATION_MEYER, Evaporation_Meyer) X(ATHAD_2D_EVAPORATION_ROHWER, Evaporation_Rohwer) \
+    X(ATHAD_2D_C_FIX, c_fix) X(ATHAD_2D_CO2_TOTAL, co2_total)
+
+// What one iteration of the resident loop reads back: the figures the reference prints.
+struct IterationReport {
+    athad_residuum_report residuum;
+    bool moist = false;                  // the moist block ran (iter_n % 2 == 0)
+    athad_budget_report h2o_post_rk4{}, co2{}, h2o{};
+    double t_skin = 0.0;
+};
+
+// The device-resident drop-in of cAtmosphereModel::run_3D_loop's body
+// (cAtmosphereModel.cpp:1156-1661): the model's state is uploaded once (Attach), every module
+// of an iteration then runs on the device in the reference's order and cadence with nothing
+// crossing PCIe but the few figures the reference prints, and Sync downloads the state into
+// the model on the iterations whose output the reference writes (its `checkpoint`, the restart
+// dumps).  The patched loop keeps the reference's own loop header (iteration counters, the
+// diffusion and buoyancy ramps, dt) and its output code:
+//
+//     athad_dropin::Device<cAtmosphereModel> dev(*this);
+//     athad_dropin::ResidentLoop<cAtmosphereModel> loop(dev, *this);
+//     for (iter_n = iter_start; iter_n <= nm; iter_n++) {
+//         total_iter_count++; ... diffusion_ramp, dt, buoyancy_ramp as the reference ...
+//         auto report = loop.Iteration(*this);
+//         if (iter_n % checkpoint == 0) loop.Sync(*this);   // before the file output
+//         ... the reference's printing and output ...
+//     }
+//
+// Configuration of cli/config_cond.xml: flat terrain, radiation mode 2 (omega_rad 0.05), no
+// inviscid spin-up (moist block every 2nd iteration).  The zonal-mean momentum-budget
+// differencing of checkpoint iterations (:1471-1520) is the caller's, from synced fields;
+// the right-hand side's budget terms are captured on those iterations.
+template <class Model>
+class ResidentLoop {
+public:
+    ResidentLoop(Device<Model>& dev, Model& m, double omega_rad = 0.05) : dev_(dev), omega_rad_(omega_rad)
+    {
+        Attach(m);
+    }
+
+    // Uploads the model's whole state: every field the context holds, the 2-D fields, the
+    // lid snapshot, the profiles and the tropopause levels.
+    void Attach(Model& m)
+    {
+#define ATHAD_UP3(F, N) dev_.up(F, m.N);
+#define ATHAD_UP2(F, N) dev_.up2(F, m.N);
+        ATHAD_ALL_FIELDS(ATHAD_UP3)
+        ATHAD_ALL_FIELDS2D(ATHAD_UP2)
+#undef ATHAD_UP3
+#undef ATHAD_UP2
+        athad_ctx* ctx = dev_.handle();
+        const int jm = m.jm, km = m.km;
+        std::vector<double> tt((size_t)jm * km, 0.0);
+        if ((int)m.t_top_init.size() == jm)
+            for (int j = 0; j < jm; j++)
+                for (int k = 0; k < km; k++) tt[(size_t)j * km + k] = m.t_top_init[j][k];
+        check(ctx, athad_upload_2d(ctx, ATHAD_2D_T_TOP_INIT, tt.data(), tt.size()), "t_top_init");
+        dev_.up_profile(ATHAD_PROF_T_REF_LEVEL, m.t_ref_level);
+        dev_.up_profile(ATHAD_PROF_RHO_BASE, m.m_rho_base);
+        dev_.up_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+        check(ctx, athad_set_tropopause_layers(ctx, m.tropopause_layers.data(),
+                                               (int32_t)m.tropopause_layers.size()), "set_tropopause_layers");
+        check(ctx, athad_synchronize(ctx), "attach");
+    }
+
+    // One iteration for m.iter_n with the model's m.dt, m.diffusion_ramp, m.buoyancy_ramp and
+    // m.total_iter_count; sets m.residuum_old and m.t_skin as the reference does.
+    IterationReport Iteration(Model& m)
+    {
+        athad_ctx* ctx = dev_.handle();
+        IterationReport r;
+        const int it = m.iter_n;
+        if (it % 4 == 0)                                                  // :1156-1159
+            check(ctx, athad_pressure_sweep(ctx, 1, m.total_iter_count), "pressure_sweep");
+        if (it % 2 == 0) {                                                // :1182-1434
+            r.moist = true;
+            check(ctx, athad_water_budget(ctx, &r.h2o_post_rk4, nullptr), "water_budget");
+            check(ctx, athad_saturation_adjust(ctx), "saturation_adjust");
+            for (athad_field f : {ATHAD_T, ATHAD_ICE, ATHAD_C, ATHAD_CLOUD}) damp(ctx, f);
+            check(ctx, athad_two_cat_ice_scheme(ctx), "two_cat_ice_scheme");
+            for (athad_field f : {ATHAD_P_RAIN, ATHAD_P_SNOW}) damp(ctx, f);
+            check(ctx, athad_moist_convection(ctx, it), "moist_convection");
+            for (athad_field f : {ATHAD_P_CONV, ATHAD_E_U, ATHAD_M_U, ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_E_D,
+                                  ATHAD_M_D, ATHAD_Q_V_D, ATHAD_MC_T, ATHAD_MC_V, ATHAD_MC_W})
+                damp(ctx, f);
+            check(ctx, athad_moist_caps(ctx), "moist_caps");
+            check(ctx, athad_vapour_ceiling(ctx, nullptr), "vapour_ceiling");
+            check(ctx, athad_co2_column(ctx, &r.co2), "co2_column");
+            check(ctx, athad_water_budget(ctx, &r.h2o, nullptr), "water_budget");
+            check(ctx, athad_densities(ctx, 0), "densities");
+            check(ctx, athad_forces(ctx), "forces");
+            check(ctx, athad_stand_atm_dew_point(ctx), "stand_atm_dew_point");
+            check(ctx, athad_water_vapour_evaporation(ctx), "water_vapour_evaporation");
+            check(ctx, athad_latent_sensible_heat(ctx), "latent_sensible_heat");
+            check(ctx, athad_turbulence_run(ctx), "turbulence_run");
+            for (athad_field f : {ATHAD_TKE, ATHAD_DIS, ATHAD_NUE, ATHAD_PROD, ATHAD_TKE_SOURCE, ATHAD_DIS_SOURCE})
+                damp(ctx, f);
+        }
+        check(ctx, athad_boundary_conditions(ctx), "boundary_conditions");   // :1439-1446
+        const int budget = (m.checkpoint > 0 && it % m.checkpoint == 0) ? 2 : 0;   // :1471, 1502
+        athad_step_scalars s{m.dt, m.diffusion_ramp, m.buoyancy_ramp, 1 | budget, 0};
+        check(ctx, athad_rk4_step(ctx, &s), "rk4_step");                  // :1509
+        check(ctx, athad_post_rk4_filters(ctx), "post_rk4_filters");      // :1524-1575
+        check(ctx, athad_find_residuum(ctx, &r.residuum), "find_residuum");   // :1645
+        r.residuum.residuum_prev = m.residuum_old;
+        m.residuum_old = r.residuum.residuum;
+        check(ctx, athad_store_n_level(ctx), "store_n_level");           // :1647
+        check(ctx, athad_radiative_heating(ctx, omega_rad_), "radiative_heating");   // :1656
+        check(ctx, athad_update_skin_temperature(ctx, m.t_skin_relax, &r.t_skin), "skin");   // :1661
+        m.t_skin = r.t_skin;
+        return r;
+    }
+
+    // Downloads the whole device state into the model (for the reference's output code).
+    void Sync(Model& m)
+    {
+#define ATHAD_DOWN3(F, N) dev_.down(F, m.N);
+#define ATHAD_DOWN2(F, N) dev_.down2(F, m.N);
+        ATHAD_ALL_FIELDS(ATHAD_DOWN3)
+        ATHAD_ALL_FIELDS2D(ATHAD_DOWN2)
+#undef ATHAD_DOWN3
+#undef ATHAD_DOWN2
+        dev_.down_profile(ATHAD_PROF_T_REF_LEVEL, m.t_ref_level);
+        dev_.down_profile(ATHAD_PROF_RHO_BASE, m.m_rho_base);
+        dev_.down_profile(ATHAD_PROF_DLNRHO_DR, m.m_dlnrho_dr);
+    }
+
+private:
+    static void damp(athad_ctx* ctx, athad_field f) { check(ctx, athad_damp_wiggles(ctx, f), "damp_wiggles"); }
+    Device<Model>& dev_;
+    double omega_rad_;
 };
 
 }  // namespace athad_dropin

@@ -12,17 +12,23 @@ Per iteration, in the reference's order:
          :1244 damp_wiggles(P_rain, P_snow), :1247 MoistConvection,
          :1249-1263 damp_wiggles of the convection fields, :1265-1334 precipitationSum and
          the caps, :1369-1391 the vapour ceiling, :1416 co2Column, :1417 waterBudget,
-         :1418 densities, :1420 standAtm_DewPoint_HumidRel, :1421 waterVapourEvaporation,
-         :1422 latentSensibleHeat, :1426-1433 TurbulenceAtm::run and its damp_wiggles
-  :1439  boundary conditions                              every iteration
-  :1509  RK4 step; :1524-1575 polar zonal and radial Shapiro filters; :1645 findResiduumAtm;
-  :1647  storeIntermediateData3D; :1656 radiative heating; :1661 updateSkinTemperature
+         :1418 densities, :1419 forces, :1420 standAtm_DewPoint_HumidRel,
+         :1421 waterVapourEvaporation, :1422 latentSensibleHeat, :1426-1433
+         TurbulenceAtm::run and its damp_wiggles
+  :1439  boundary conditions (bcRadius, the turbulence wall values, bcTheta, bcPhi,
+         bcScalarSurfSur, bcSolidGround)                  every iteration
+  :1509  RK4 step, with the right-hand side's diagnostic outputs every iteration (the
+         reference writes them in every call) and its momentum-budget terms on checkpoint
+         iterations (:1471, 1502); :1524-1575 polar zonal and radial Shapiro filters;
+  :1645  findResiduumAtm; :1647 storeIntermediateData3D; :1656 radiative heating;
+  :1661  updateSkinTemperature
 
-The orographic, steep-massif and coastal filters, bcScalarSurfSur and bcSolidGround act on
-land cells only and do nothing on flat terrain; forces (output-only force fields),
-vegetationLand (land only), the momentum budgets (vbudget/wbudget diagnostics) and the file
-output are not run.  The residuum, the budgets and the skin temperature each read a few
-numbers back, so an iteration synchronises with the device four times.
+The orographic, steep-massif and coastal filters act on land cells only and do nothing on
+flat terrain; forces' centrifugal and pressure-gradient arrays (output only),
+vegetationLand (land only), the zonal-mean momentum-budget differencing of checkpoint
+iterations and the file output are not run.  The residuum, the budgets and the skin
+temperature each read a few numbers back, so an iteration synchronises with the device four
+times.
 """
 from __future__ import annotations
 
@@ -44,12 +50,15 @@ class ModelLoop:
     temperature's relaxation (0.25); omega_rad: radiation mode 2's blend (0.05);
     tropopause_layers: cAtmosphereModel::tropopause_layers (jm level indices; default the
     configuration's, the tropopause above the 120 km lid on every row, i.e. im - 1);
-    first_iter: the first iter_n (iterations counted from 1, as run_3D_loop counts them)."""
+    first_iter: the first iter_n (iterations counted from 1, as run_3D_loop counts them);
+    checkpoint: the output cadence (cli/config_cond.xml: 20), whose iterations capture the
+    momentum-budget terms."""
 
     def __init__(self, g: GpuAtmosphere, dt: float = 4e-5, buoyancy_ramp_iters: int = 300,
                  t_skin_relax: float = 0.25, omega_rad: float = 0.05, tropopause_layers=None,
-                 first_iter: int = 1):
+                 first_iter: int = 1, checkpoint: int = 20):
         self.g = g
+        self.checkpoint = checkpoint
         self.dt = dt
         self.ramp_iters = buoyancy_ramp_iters
         self.t_skin_relax = t_skin_relax
@@ -85,6 +94,7 @@ class ModelLoop:
             out["co2"] = g.co2_column()
             out["h2o"] = g.water_budget()
             g.densities()
+            g.forces()
             g.stand_atm_dew_point()
             g.water_vapour_evaporation()
             g.latent_sensible_heat()
@@ -93,7 +103,8 @@ class ModelLoop:
                 g.damp_wiggles(n)
         g.boundary_conditions()
         ramp = min(1.0, self.total_iter_count / self.ramp_iters) if self.ramp_iters > 0 else 1.0
-        g.solveRungeKutta_Atmosphere_Turb(self.dt, 1.0, ramp)
+        budget = 2 if (self.checkpoint > 0 and it % self.checkpoint == 0) else 0
+        g.solveRungeKutta_Atmosphere_Turb(self.dt, 1.0, ramp, write_diagnostics=1 | budget)
         g.post_rk4_filters()
         out["residuum"] = g.find_residuum()
         g.storeIntermediateData3D()

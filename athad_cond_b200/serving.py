@@ -29,8 +29,7 @@ import numpy as np
 
 from . import _abi
 from .context import GpuAtmosphere, GpuBatch
-from .ensemble import Condition, condition_params, draw_condition, state_params
-from .synthetic import make_state_device
+from .ensemble import Condition, condition_params, draw_condition, init_config
 
 GRIDS = [(21, 91, 181), (41, 181, 361), (41, 91, 181)]
 
@@ -123,13 +122,7 @@ class Server:
             return False
         ctx = GpuAtmosphere(*req.grid, condition_params(req.cond))
         ctx.set_stream(self.stream.cuda_stream)
-        with self.torch.cuda.stream(self.stream):
-            st = make_state_device(*req.grid, seed=req.seed, params=state_params(req.cond))
-            for name, t in st.items():
-                if t.dim() == 3:
-                    ctx.upload_tensor(name, t)
-            ev = st["Evaporation"].cpu().numpy()
-        ctx.upload_2d("Evaporation", ev)
+        ctx.initial_state(init_config(req.cond))   # the reference's deterministic initial state
         self.used += fp
         req.admitted = now
         self.runs.append(_Run(req, ctx, fp))

@@ -508,6 +508,14 @@ athad_status athad_latent_sensible_heat(athad_ctx* ctx);
  * NULL, receives it.  Nothing changes where the reference returns early (t_skin_relax <= 0,
  * no positive albedo, no positive absorbed flux).  Waits for the device. */
 athad_status athad_update_skin_temperature(athad_ctx* ctx, double t_skin_relax, double* t_skin);
+/* ThermoAtm::forces (ThermoAtm.h:518-614; call sites cAtmosphereModel.cpp:635, 1419): the
+ * two arrays it shares with the right-hand side's outputs, ATHAD_CORIOLIS_FORCE and
+ * ATHAD_BUOYANCY_FORCE of the interior cells (its centrifugal and pressure-gradient arrays
+ * are output only and not held).  The buoyancy reference is the level-mean temperature
+ * once one exists (an athad_rk4_step, athad_level_mean or an upload of
+ * ATHAD_PROF_T_REF_LEVEL since the context's creation or initial state), else 1, as the
+ * reference's empty t_ref_level gives before its first RK4 step. */
+athad_status athad_forces(athad_ctx* ctx);
 /* ThermoAtm::co2Column (ThermoAtm.h:1096-1137; call sites cAtmosphereModel.cpp:632, 1416):
  * ATHAD_2D_CO2_TOTAL and the CO2 budget.  Waits for the device. */
 athad_status athad_co2_column(athad_ctx* ctx, athad_budget_report* out);

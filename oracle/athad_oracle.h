@@ -227,6 +227,11 @@ void or_tropopause_layers(int im, int jm, const or_params* p, const or_init_cfg*
 int or_init_state(int im, int jm, int km, const or_params* p, const or_init_cfg* c, int compat, int upto,
                   double* const* f, double* const* f2, double* const* prof);
 
+/* ThermoAtm::forces (ThermoAtm.h:518-614): CoriolisForce and BuoyancyForce of the interior
+ * cells; t_ref the level-mean temperature, NULL before the first RK4 step (reference 1) */
+void or_forces(int im, int jm, int km, const or_params* p, int compat, double* const* f,
+               const double* t_ref);
+
 /* storeIntermediateData3D, UtilsAtm.h:25-49 */
 void or_store_n_level(int im, int jm, int km, double* const* f);
 

@@ -475,9 +475,10 @@ static void turbulence_init_fields(int im, int jm, int km, const or_params* p, c
 /* ThermoAtm::forces (ThermoAtm.h:518-614), the two arrays it shares with the right-hand side's
  * outputs: CoriolisForce and BuoyancyForce of the interior cells (its centrifugal and
  * pressure-gradient arrays are output only).  Coriolis and buoyancy are the configuration's
- * 1; before the first RK4 step the level-mean temperature does not exist and the buoyancy
- * reference is 1. */
-static void forces(int im, int jm, int km, const or_params* p, const or_geom* g, double* const* f)
+ * 1; the buoyancy reference is the level-mean temperature t_ref, or 1 where none exists yet
+ * (t_ref NULL: before the first RK4 step). */
+static void forces(int im, int jm, int km, const or_params* p, const or_geom* g, double* const* f,
+                   const double* t_ref)
 {
     const double two_omega = 2.0 * p->omega;
     const double nontrad_d = p->coriolis_nontrad ? 1.0 : 0.0;
@@ -492,9 +493,19 @@ static void forces(int im, int jm, int km, const or_params* p, const or_geom* g,
                 const double Cor_phi = -two_omega * (costhe * f[OF_V][q] + nontrad_d * sinthe * f[OF_U][q]) * p->u_0;
                 f[OF_CORIOLIS_FORCE][q] = 1.0 * p->r_air
                     * sqrt(Cor_r * Cor_r + Cor_the * Cor_the + Cor_phi * Cor_phi);
-                f[OF_BUOYANCY_FORCE][q] = 1.0e-3 * 1.0 * f[OF_R_HUMID][q] * p->g * (f[OF_T][q] - 1.0);
+                f[OF_BUOYANCY_FORCE][q] = 1.0e-3 * 1.0 * f[OF_R_HUMID][q] * p->g
+                                        * (f[OF_T][q] - (t_ref ? t_ref[i] : 1.0));
             }
         }
+}
+
+void or_forces(int im, int jm, int km, const or_params* p, int compat, double* const* f,
+               const double* t_ref)
+{
+    or_geom g;
+    or_geom_init(&g, im, jm, km, p, compat);
+    forces(im, jm, km, p, &g, f, t_ref);
+    or_geom_free(&g);
 }
 
 static void precipitation_sum(int im, int jm, int km, double* const* f)   /* UtilsAtm.h:51-65 */
@@ -602,7 +613,7 @@ int or_init_state(int im, int jm, int km, const or_params* p, const or_init_cfg*
         or_co2_column(im, jm, km, p, f, f2, out);                   /* :632 (co2_total) */
     }
     or_densities(im, jm, km, p, cm, 0, f, f2, prof);                /* :634 */
-    forces(im, jm, km, p, &g, f);                                   /* :635 */
+    forces(im, jm, km, p, &g, f, NULL);                             /* :635 */
     or_water_vapour_evaporation(im, jm, km, p, f, f2);              /* :637 */
     or_latent_sensible_heat(im, jm, km, p, cm, f);                  /* :638 */
     if (upto <= OR_INIT_DIAGNOSE) goto done;

@@ -72,6 +72,37 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
     return 0;
 }
 
+// n iterations of run_3D_loop's body through the device-resident drop-in
+// (athad_dropin::ResidentLoop) on the model, with the reference's loop header for each
+// (cAtmosphereModel.cpp:1103-1131: total_iter_count, no inviscid spin-up, dt_visc, the
+// buoyancy ramp), the state synced back into the model at the end.  residua: n values (the
+// residuum of each iteration); t_skin: n values.  Returns 0, or -1 with the message in err.
+int dropin_resident(void* model, int n, int first_iter, int wall, double* residua, double* t_skin,
+                    char* err, int errlen)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)model;
+    try {
+        Dev d(*m, wall ? ATHAD_WALL_REFERENCE : ATHAD_WALL_MIRROR);
+        athad_dropin::ResidentLoop<cAtmosphereModel> loop(d, *m);
+        for (int q = 0; q < n; q++) {
+            m->iter_n = first_iter + q;
+            m->total_iter_count++;
+            m->diffusion_ramp = 1.0;
+            m->dt = m->dt_visc;
+            m->buoyancy_ramp = (m->buoyancy_ramp_iters > 0)
+                ? std::min(1.0, (double)m->total_iter_count / m->buoyancy_ramp_iters) : 1.0;
+            athad_dropin::IterationReport r = loop.Iteration(*m);
+            residua[q] = r.residuum.residuum;
+            t_skin[q] = r.t_skin;
+        }
+        loop.Sync(*m);
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return -1;
+    }
+    return 0;
+}
+
 // the model's budget references: m_q_co2_ref, m_q_h2o_ref, m_q_h2o_fixed_ref
 void dropin_budget_refs(void* model, double* out)
 {

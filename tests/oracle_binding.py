@@ -262,6 +262,14 @@ class OracleState:
         lev = (ctypes.c_int * jm)(*[int(x) for x in i_trop])
         lib().or_stand_atm_dew_point(im, jm, km, ctypes.byref(self.params), F, lev)
 
+    def forces(self, compat=0, with_level_mean=True):
+        """or_forces: ThermoAtm::forces' Coriolis and buoyancy arrays; the buoyancy reference
+        the level mean of prof (or 1 without one)."""
+        F, _, P = self._args()
+        im, jm, km = self.shape
+        tr = P[0] if with_level_mean else None
+        lib().or_forces(im, jm, km, ctypes.byref(self.params), int(compat), F, tr)
+
     def moist_caps(self):
         F, _, _ = self._args()
         im, jm, km = self.shape

@@ -116,6 +116,21 @@ class Reference:
         if r != 0:
             raise RuntimeError(err.value.decode())
 
+    def resident(self, n: int, first_iter: int = 1, wall: int = 0):
+        """n iterations of run_3D_loop's body through the product's device-resident drop-in
+        on this model (athad_dropin::ResidentLoop); returns each iteration's residuum and
+        skin temperature."""
+        f = self.lib.dropin_resident
+        D = ctypes.POINTER(ctypes.c_double)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, ctypes.c_char_p, ctypes.c_int]
+        f.restype = ctypes.c_int
+        res, skin = np.zeros(n), np.zeros(n)
+        err = ctypes.create_string_buffer(512)
+        r = f(self.h, n, first_iter, wall, res.ctypes.data_as(D), skin.ctypes.data_as(D), err, 512)
+        if r != 0:
+            raise RuntimeError(err.value.decode())
+        return res, skin
+
     def post_rk4_filters(self):
         self.lib.ref_post_rk4_filters(self.h)
 

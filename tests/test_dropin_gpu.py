@@ -273,3 +273,42 @@ def test_dropin_mass_budgets(model):
     assert np.array_equal(R.get2("co2_total"), co2_total)
     for g, key in zip(got, ("q_co2_ref", "q_h2o_ref", "q_h2o_fixed_ref")):
         assert abs(g - want[key]) <= 1e-12 * want[key], key
+
+
+F2D = ["t_top_init", "p_stat_landscape", "Evaporation", "Q_sensible_2D", "vel_star", "epsilon_2D",
+       "albedo", "Evaporation_Dalton", "Evaporation_Meyer", "Evaporation_Rohwer", "c_fix", "co2_total"]
+
+
+def test_dropin_resident_loop_equals_the_device_loop(model):
+    """The device-resident drop-in (athad_dropin::ResidentLoop: the model's state uploaded
+    once, every module of run_3D_loop's body on the device, the state synced back at the end)
+    run for 20 iterations on the reference's own model is bit for bit the Python ModelLoop
+    from the same state: the same entry points in the same order, checkpoint iteration 20
+    (the momentum-budget capture) included.  The residuum and the skin temperature each
+    iteration reports agree too."""
+    from athad_cond_b200 import GpuAtmosphere
+    from athad_cond_b200._abi import config_params
+    from athad_cond_b200.loop import ModelLoop
+    R, snap = model
+    reset(R, snap)
+    two = {n: R.get2(n) for n in F2D}
+    prof = {n: R.getp(n) for n in ("t_ref_level", "rho_base", "dlnrho_dr")}
+    n_iter = 20
+    with GpuAtmosphere(*R.shape, config_params()) as g:
+        g.upload_state(dict(snap))
+        for n, a in two.items():
+            g.upload_2d(n, a)
+        for n, a in prof.items():
+            if a is not None:
+                g.upload_profile(n, a)
+        loop = ModelLoop(g)
+        reps = loop.run(n_iter)
+        want = {n: g.download(n) for n in FIELD_NAMES}
+    res, skin = R.resident(n_iter)
+    got = {n: R.get(n) for n in FIELD_NAMES}
+    reset(R, snap)
+    bad = [n for n in FIELD_NAMES if not np.array_equal(got[n], want[n])]
+    assert not bad, bad
+    assert res.tolist() == [r["residuum"]["residuum"] for r in reps]
+    assert skin.tolist() == [r["t_skin"] for r in reps]
+

@@ -7,9 +7,9 @@
     magnitude, and the device state exactly mirror symmetric;
   * the same for 4 iterations on configuration 2's 41 x 181 x 361 grid;
   * the whole model iteration (athad_cond_b200.loop.ModelLoop: boundary conditions,
-    filters, turbulence, ice scheme, radiation, surface fluxes, caps, diagnostics and the
-    skin temperature around the hot path) for 10 iterations against the oracle driving the
-    same module sequence.
+    filters, turbulence, ice scheme, radiation, surface fluxes, caps, diagnostics, the force
+    fields, the right-hand side's outputs and the skin temperature around the hot path) for
+    10 iterations against the oracle driving the same module sequence.
 The oracle runs the same initial state (or_init_state, the device semantics); it is pinned
 against the reference in tests/test_pin_initial_state.py and tests/test_pin_reference.py.
 """
@@ -79,7 +79,7 @@ def test_fp64_hot_path_from_the_initial_state(grid, iterations):
     assert not bad, (bad, err)
 
 
-def oracle_loop_iteration(o, it, total, tropopause, omega_rad=0.05, t_skin_relax=0.25):
+def oracle_loop_iteration(o, it, total, tropopause, omega_rad=0.05, t_skin_relax=0.25, checkpoint=20):
     """cAtmosphereModel::run_3D_loop's module sequence on the oracle, in ModelLoop's order."""
     if it % 4 == 0:
         o.pressure_sweep(1, total)
@@ -96,6 +96,7 @@ def oracle_loop_iteration(o, it, total, tropopause, omega_rad=0.05, t_skin_relax
         o.moist_caps()
         o.vapour_ceiling()
         o.densities()
+        o.forces()
         o.stand_atm_dew_point(tropopause)
         o.water_vapour_evaporation()
         o.latent_sensible_heat()
@@ -103,7 +104,8 @@ def oracle_loop_iteration(o, it, total, tropopause, omega_rad=0.05, t_skin_relax
         for n in TURBULENCE_FIELDS:
             o.damp_wiggles(n)
     o.boundary_conditions()
-    o.rk4(dt=DT, buoyancy_ramp=min(1.0, total / 300.0))
+    budget = 2 if it % checkpoint == 0 else 0
+    o.rk4(dt=DT, buoyancy_ramp=min(1.0, total / 300.0), write_diagnostics=1 | budget)
     o.post_rk4_filters()
     o.store_n_level()
     o.radiative_heating(omega_rad)
@@ -128,7 +130,8 @@ def test_model_loop_matches_oracle_for_ten_iterations():
             oracle_loop_iteration(o, it, it, trop)
             skins.append((rep["t_skin"], o.params.t_skin))
         names = FIELDS + ["nue", "P_rain", "P_snow", "Precipitation", "TempDewPoint", "HumidityRel",
-                          "Q_Sensible", "radiation", "S_v", "S_c", "MC_t", "MC_q"]
+                          "Q_Latent", "Q_Sensible", "radiation", "S_v", "S_c", "MC_t", "MC_q",
+                          "CoriolisForce", "BuoyancyForce", "PressureGradientForce", "prod"]
         err = errors(g, o, names)
     bad = {n: e for n, e in err.items() if not e <= TOL}
     assert not bad, (bad, err)
