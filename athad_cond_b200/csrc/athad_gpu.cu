@@ -764,7 +764,6 @@ static ColumnArgs column_args(athad_ctx* ctx)
     a.M_bg = p.M_bg; a.R_bg = p.R_bg; a.R_mix = p.R_mix; a.r_air = p.r_air; a.g = p.g; a.t_skin = p.t_skin;
     a.c_h2o_dry_top = p.c_h2o_dry_top;
     a.inv_2dr = 1.0 / (2.0 * ctx->dr); a.inv_dr = 1.0 / ctx->dr;
-    a.mixed = (p.precision == ATHAD_PRECISION_MIXED) ? 1 : 0;
     return a;
 }
 

@@ -98,17 +98,6 @@ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double i
     if (!(den > 0.0)) return 0.0;
     return x * M_H2O * M_other / (den * den) * L * (invT * invT) * (1.0 / R_H2O);
 }
-__device__ __forceinline__ float dqsat_f(double E, float L, float T, double p, double inv_p, float M_other)
-{
-    if (E == NO_SATURATION || !(p > 0.0) || E >= p || !(T > 0.0f)) return 0.0f;
-    const float x = (float)(E * inv_p);
-    const float mh = (float)M_H2O;
-    const float den = x * mh + (1.0f - x) * M_other;
-    if (!(den > 0.0f)) return 0.0f;
-    const float A = x * mh * M_other / (den * den);
-    return A * L / ((float)R_H2O * T * T);
-}
-
 // The mixture heat capacity of the Newton step (MixtureAtm.h:123-178) with the three
 // Shomate polynomials sharing t, t^2, t^3 and 1/t^2, and products by the reciprocal molar
 // masses: one division instead of six.
@@ -123,35 +112,18 @@ __device__ __forceinline__ double cp_of_r(double c, double co2, double T, double
     const double bg = 28.98641 + 1.853978 * t + -9.647459 * t2 + 16.63537 * t3 + 0.000117 * it2;
     return q_v * (h2o * (1.0 / M_H2O)) + q_c * (co2s * (1.0 / M_CO2)) + q_b * (bg * inv_M_b);
 }
-__device__ __forceinline__ float cp_of_fr(float c, float co2, float T, float inv_M_b)
-{
-    float q_v = fminf(fmaxf(c, 0.0f), 1.0f), q_c = fminf(fmaxf(co2, 0.0f), 1.0f);
-    const float sum = q_v + q_c;
-    if (sum > 1.0f) { q_v /= sum; q_c /= sum; }
-    const float q_b = fmaxf(0.0f, 1.0f - q_v - q_c);
-    float t = (T < 298.0f) ? 298.0f : T;
-    t = (t > 2000.0f) ? 2000.0f : t;
-    t *= 1.0e-3f;
-    const float t2 = t * t, t3 = t2 * t, it2 = 1.0f / t2;
-    const float h2o = 30.09200f + 6.832514f * t + 6.793435f * t2 + -2.534480f * t3 + 0.082139f * it2;
-    const float co2s = 24.99735f + 55.18696f * t + -33.69137f * t2 + 7.948387f * t3 + -0.136638f * it2;
-    const float bg = 28.98641f + 1.853978f * t + -9.647459f * t2 + 16.63537f * t3 + 0.000117f * it2;
-    return q_v * (h2o * (float)(1.0 / M_H2O)) + q_c * (co2s * (float)(1.0 / M_CO2)) + q_b * (bg * inv_M_b);
-}
 
 // adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
 // Neither reads a neighbour, so the two passes of the reference fuse into one.
+// FP64 in both precision forms: with the Newton step's latent heats, heat capacities and
+// derivative factors in FP32, cells converged to values 1e-7 apart from the FP64 form's
+// and moved its discontinuous branches (the supersaturation test, the moist-lapse switch of
+// the densities) in a few cells within 300 iterations; in FP64 the mixed form stays within
+// 1e-9 of the FP64 form in c and cloud over the same iterations.
 #ifndef ATHAD_SATADJ_MIN_BLOCKS
-#define ATHAD_SATADJ_MIN_BLOCKS 7         // FP64 form: 72 registers, 7 CTAs of 128 threads per SM
+#define ATHAD_SATADJ_MIN_BLOCKS 7         // 72 registers, 7 CTAs of 128 threads per SM
 #endif
-#ifndef ATHAD_SATADJ_MIN_BLOCKS_MIXED
-#define ATHAD_SATADJ_MIN_BLOCKS_MIXED 8   // mixed form: 64 registers, 8 CTAs (41x181x361 state
-#endif                                    // after 40 iterations: 6 -> 8 CTAs, 1.96 -> 1.89 ms)
-// MIXED: the Newton step's latent heats, heat capacities, derivative factors, gain and
-// damping in FP32; the saturation curves and mass fractions, the state it updates and the
-// clamp-and-fade pass in FP64.
-template <bool MIXED>
-__global__ void __launch_bounds__(128, MIXED ? ATHAD_SATADJ_MIN_BLOCKS_MIXED : ATHAD_SATADJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS)
 saturation_adjust_kernel(const ColumnArgs a)
 {
     const Dims& d = a.d;
@@ -189,11 +161,9 @@ saturation_adjust_kernel(const ColumnArgs a)
                     // and the ice curve is evaluated only where a term uses it — where the
                     // deposition weight DEP is 0 and there is no ice its terms are exactly
                     // zero, so skipping them changes no bit.
-                    double L_T = MIXED ? (double)thermo_f::latent_heat((float)T) : latent_heat(T);
+                    double L_T = latent_heat(T);
                     const double inv_p = 1.0 / p_local;
-                    const float co2_f = (float)co2, M_other_f = (float)M_other;
                     const double inv_M_b = 1.0 / a.M_bg;
-                    const float inv_M_b_f = (float)inv_M_b;
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
                         const double DEP = 1.0 - CND;
@@ -206,8 +176,7 @@ saturation_adjust_kernel(const ColumnArgs a)
                         q_v_b += d_q_v;
                         q_c_b = smax(0.0, q_c_b - d_cnd);
                         q_i_b = smax(0.0, q_i_b - d_dep);
-                        const double cp_loc = MIXED ? (double)cp_of_fr((float)q_v_b, co2_f, (float)T, inv_M_b_f)
-                                                    : cp_of_r(q_v_b, co2, T, inv_M_b);
+                        const double cp_loc = cp_of_r(q_v_b, co2, T, inv_M_b);
                         T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
                         const double invT = 1.0 / T;
                         const double E_sat = p_sat_r(T, invT);
@@ -218,25 +187,13 @@ saturation_adjust_kernel(const ColumnArgs a)
                         const double q_Ice = need_ice ? q_sat_r(E_Ice, p_local, inv_p, M_other) : 0.0;
                         const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
                                                                   : ((T >= a.t_0) ? q_sat : q_Ice);
-                        double omega;
-                        if (MIXED) {
-                            const float Tf = (float)T;
-                            const float cp_g = cp_of_fr((float)q_v_b, co2_f, Tf, inv_M_b_f);
-                            const float L_cnd = thermo_f::latent_heat(Tf);
-                            const float L_dep = L_cnd + 3.337e5f;
-                            float Gain = (float)CND * (L_cnd / cp_g) * dqsat_f(E_sat, L_cnd, Tf, p_local, inv_p, M_other_f);
-                            if (need_ice) Gain += (float)DEP * (L_dep / cp_g) * dqsat_f(E_Ice, L_dep, Tf, p_local, inv_p, M_other_f);
-                            L_T = (double)L_cnd;
-                            omega = (double)(1.0f / (1.0f + Gain));
-                        } else {
-                            const double cp_g = cp_of_r(q_v_b, co2, T, inv_M_b);
-                            const double L_cnd = latent_heat(T);
-                            const double L_dep = L_cnd + 3.337e5;
-                            double Gain = CND * (L_cnd / cp_g) * dqsat_r(E_sat, L_cnd, T, invT, p_local, inv_p, M_other);
-                            if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_r(E_Ice, L_dep, T, invT, p_local, inv_p, M_other);
-                            L_T = L_cnd;
-                            omega = 1.0 / (1.0 + Gain);
-                        }
+                        const double cp_g = cp_of_r(q_v_b, co2, T, inv_M_b);
+                        const double L_cnd = latent_heat(T);
+                        const double L_dep = L_cnd + 3.337e5;
+                        double Gain = CND * (L_cnd / cp_g) * dqsat_r(E_sat, L_cnd, T, invT, p_local, inv_p, M_other);
+                        if (need_ice) Gain += DEP * (L_dep / cp_g) * dqsat_r(E_Ice, L_dep, T, invT, p_local, inv_p, M_other);
+                        L_T = L_cnd;
+                        const double omega = 1.0 / (1.0 + Gain);
                         q_v_hyp = q_v_b + omega * (q_v_target - q_v_b);
                         if (fabs(q_v_b / q_v_hyp - 1.0) <= 1.0e-6) break;
                     }
@@ -296,8 +253,7 @@ saturation_adjust_kernel(const ColumnArgs a)
 void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st)
 {
     const dim3 block(128), grid((a.d.km + 127) / 128, a.d.jm, a.d.im);
-    if (a.mixed) saturation_adjust_kernel<true><<<grid, block, 0, st>>>(a);
-    else saturation_adjust_kernel<false><<<grid, block, 0, st>>>(a);
+    saturation_adjust_kernel<<<grid, block, 0, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -182,7 +182,6 @@ struct ColumnArgs {
     double t_0, t_00, t_max_phys, cloud_cap, M_bg, R_bg, R_mix, r_air, g, t_skin, c_h2o_dry_top;
     double inv_2dr, inv_dr;
     int set_water_profile;
-    int mixed;                  // saturation adjustment: FP32 Newton-step coefficients
 };
 void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st);
 void launch_densities(const ColumnArgs& a, cudaStream_t st);

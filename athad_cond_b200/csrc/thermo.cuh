@@ -192,50 +192,4 @@ ATHAD_HD double dew_point(double e)
 
 }  // namespace thermo
 
-// FP32 versions of the parts of the saturation adjustment's Newton step that are not the
-// saturation curve itself (latent heat, heat capacity, the derivative factor), used by the
-// mixed-precision form; p_sat, p_subl and q_sat stay FP64.
-namespace thermo_f {
-
-ATHAD_HD float latent_heat(float T)
-{
-    const float Tc = (float)thermo::T_CRIT;
-    if (T >= Tc) return 0.0f;
-    const float x = (Tc - T) / (Tc - 273.15f);
-    return (x > 0.0f) ? 2.501e6f * expf(0.38f * logf(x)) : 0.0f;
-}
-
-ATHAD_HD float shomate(float T, float A, float B, float Cc, float D, float E)
-{
-    float t = (T < 298.0f) ? 298.0f : T;
-    t = (t > 2000.0f) ? 2000.0f : t;
-    t *= 1.0e-3f;
-    const float t2 = t * t;
-    return A + B * t + Cc * t2 + D * t2 * t + E / t2;
-}
-
-ATHAD_HD float cp_of(float c, float co2, float T, float M_b)
-{
-    float q_v = fminf(fmaxf(c, 0.0f), 1.0f), q_c = fminf(fmaxf(co2, 0.0f), 1.0f);
-    const float sum = q_v + q_c;
-    if (sum > 1.0f) { q_v /= sum; q_c /= sum; }
-    const float q_b = fmaxf(0.0f, 1.0f - q_v - q_c);
-    return q_v * (shomate(T, 30.09200f, 6.832514f, 6.793435f, -2.534480f, 0.082139f) / (float)thermo::M_H2O)
-         + q_c * (shomate(T, 24.99735f, 55.18696f, -33.69137f, 7.948387f, -0.136638f) / (float)thermo::M_CO2)
-         + q_b * (shomate(T, 28.98641f, 1.853978f, -9.647459f, 16.63537f, 0.000117f) / M_b);
-}
-
-// dq_sat/dT from a FP64 saturation pressure (SaturationH2O.h:230-255)
-ATHAD_HD float dqsat_dT_from(double E, float L, float T, double p, float M_other)
-{
-    if (E == thermo::NO_SATURATION || !(p > 0.0) || E >= p || !(T > 0.0f)) return 0.0f;
-    const float x = (float)(E / p);
-    const float mh = (float)thermo::M_H2O;
-    const float den = x * mh + (1.0f - x) * M_other;
-    if (!(den > 0.0f)) return 0.0f;
-    const float A = x * mh * M_other / (den * den);
-    return A * L / ((float)thermo::R_H2O * T * T);
-}
-
-}  // namespace thermo_f
 }  // namespace athad
