@@ -709,10 +709,9 @@ athad_status athad_pressure_sweep(athad_ctx* ctx, int32_t n_sweeps, int32_t tota
     if (!ctx || n_sweeps < 0) return fail(ctx, ATHAD_ERR_INVALID, "pressure_sweep: bad argument");
     if (n_sweeps == 0) return ATHAD_OK;
     PoissonArgs a = poisson_args(ctx, total_iter_count);
-    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), ctx->stream), "counters");
+    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters + 1, 0, sizeof(unsigned long long), ctx->stream), "counters");
     if (s != ATHAD_OK) return s;
-    launch_poisson_prepare(a, ctx->stream);
-    ATHAD_CHECK_LAUNCH(ctx, "poisson prepare");
+    a.aux_lid = 1;
     for (int i = 0; i < n_sweeps; i++) {
         launch_poisson_sweep(a, ctx->stream);
         ATHAD_CHECK_LAUNCH(ctx, "poisson sweep");
@@ -822,8 +821,9 @@ athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
     if (s == ATHAD_OK) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "report sync");
     if (s != ATHAD_OK) return s;
     std::memset(out, 0, sizeof *out);
-    out->poisson_src_cells = (int64_t)h[0] * ctx->poisson_sweeps_since_reset;
-    out->poisson_src_clamped = (int64_t)h[1] * ctx->poisson_sweeps_since_reset;
+    const int64_t fluid = (int64_t)(ctx->L.d.im - 2) * (ctx->L.d.jm - 2) * (ctx->L.d.km - 2);
+    out->poisson_src_cells = fluid * ctx->poisson_sweeps_since_reset;
+    out->poisson_src_clamped = (int64_t)h[1];                // counted in every sweep
     out->satadj_ceiling_hits = (int64_t)h[2];
     out->nonfinite_inputs = (int64_t)h[3];
     if (ctx->step_timed) {

@@ -62,4 +62,31 @@ ATHAD_HD long long idx3(const Dims& d, int i, int j, int k)
     return ((long long)i * d.jm + j) * d.pitch + k;
 }
 
+// Programmatic dependent launch (sm_90 and later): a kernel launched with launch_dependent
+// may be scheduled while the kernel before it in the stream is still running; it calls
+// pdl_wait() before its first global memory access, which returns once that kernel has
+// completed and its writes are visible, so stream order holds for every access.  The
+// kernel before it calls pdl_trigger() to let the dependent's CTAs onto the SMs its last
+// wave frees instead of after its completion.  Both are no-ops in a kernel launched
+// without the attribute (the batched RK4 kernels, the kernels shared with other paths).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                    cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace athad

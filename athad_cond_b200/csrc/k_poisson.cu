@@ -3,11 +3,13 @@
 // Replaces PressureSolverAtm::run (PressureSolverAtm.h:27-594) for flat terrain, and the
 // gradient correction of PressureSolverAtm::project_initial_velocity (:713-749).
 //
-// The provisional velocity aux_u/v/w does not change while the pressure relaxes, so its
-// clamped divergence (the Poisson source) is formed once per call into a scratch field;
-// every red-black sweep then streams p and that source only.  Within one colour every
-// cell reads only cells of the other colour, so the in-place update is order-independent
-// and the result equals the serial red-black sweep bit for bit.
+// Each colour kernel forms the clamped divergence of aux_u/v/w (the Poisson source) of its
+// own cells as it updates them, from the same operands as the reference: the model's
+// cadence runs one sweep per call, and a source field written by one launch and read by
+// the next two cost more than the aux reads it saves (24 us of a 68 us call at
+// 41 x 181 x 361).  Within one colour every cell reads only cells of the other colour, so
+// the in-place update is order-independent and the result equals the serial red-black
+// sweep bit for bit.
 #include <algorithm>
 
 #include "kernels.cuh"
@@ -25,59 +27,68 @@ __device__ __forceinline__ double aux_u_lid(const PoissonArgs& a, double inner, 
     return a.anelastic ? 0.0 : c43 * inner - c13 * second;
 }
 
+// the aux values of the planes i = 0 and im-1 at (j, k), formed from the interior
+__device__ __forceinline__ void aux_lid_cell(const PoissonArgs& a, int i, int j, int k)
+{
+    const Dims& d = a.d;
+    const double c43 = 1.0, c13 = 0.0;
+    const long long cb = idx3(d, i, j, k);
+    const long long s = (i == 0) ? d.plane : -d.plane;   // toward the interior
+    a.aux_u[cb] = aux_u_lid(a, a.aux_u[cb + s], a.aux_u[cb + 2 * s]);
+    a.aux_v[cb] = c43 * a.aux_v[cb + s] - c13 * a.aux_v[cb + 2 * s];
+    a.aux_w[cb] = c43 * a.aux_w[cb + s] - c13 * a.aux_w[cb + 2 * s];
+}
+
+// the clamped divergence source of fluid cell c = (i, j, k); it reads aux_u/v/w of the
+// interior only (the lid through aux_u_lid)
+__device__ __forceinline__ double cell_source(const PoissonArgs& a, const PoiIJ& P, int i, long long c,
+                                              bool& clamped)
+{
+    const Dims& d = a.d;
+    const long long sI = d.plane, sJ = d.pitch;
+    const double u_c = __ldg(a.aux_u + c);
+    const double u_up = (i + 1 == d.im - 1) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c - sI)) : __ldg(a.aux_u + c + sI);
+    const double u_dn = (i - 1 == 0) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c + sI)) : __ldg(a.aux_u + c - sI);
+    const double du_dr = (u_up - u_dn) * a.inv_2dr;
+    const double dv_dthe = (__ldg(a.aux_v + c + sJ) - __ldg(a.aux_v + c - sJ)) * a.inv_2dthe;
+    const double dw_dphi = (__ldg(a.aux_w + c + 1) - __ldg(a.aux_w + c - 1)) * a.inv_2dphi;
+    double div_src = du_dr * P.exp_rm + dv_dthe * P.inv_rm + dw_dphi * P.inv_rmsinthe;
+    if (a.anelastic) div_src += u_c * __ldg(a.dlnrho + i) * P.exp_rm;
+    if (a.metric_div) div_src += (2.0 * u_c + __ldg(a.aux_v + c) * P.costhe / P.sinthe) * P.inv_rm;
+    const double src_max = P.denom * 2.0;   // p_dyn_cap = 2 (:148)
+    clamped = false;
+    if (!is_finite_bits(div_src)) div_src = 0.0;
+    else if (div_src > src_max) { div_src = src_max; clamped = true; }
+    else if (div_src < -src_max) { div_src = -src_max; clamped = true; }
+    return div_src;
+}
+
+// clamped sources are rare, so a warp adds its count only when it has one: no atomics and
+// no block barrier on the common path (the fluid cells, (im-2)(jm-2)(km-2) per sweep, are
+// counted by the host)
+__device__ __forceinline__ void count_clamped(const PoissonArgs& a, bool clamped)
+{
+    const unsigned nc = __popc(__ballot_sync(0xffffffffu, clamped));
+    if ((threadIdx.x & 31) == 0 && nc && a.counters) atomicAdd(a.counters + 1, (unsigned long long)nc);
+}
+
+// The source into a scratch field for the Poisson solve (athad_pressure_solve), with the
+// aux boundary
 __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
-    const long long sI = d.plane, sJ = d.pitch;
-    if ((i == 0 || i == d.im - 1) && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1) {
-        const double c43 = 1.0, c13 = 0.0;
-        const long long cb = idx3(d, i, j, k);
-        const long long s = (i == 0) ? sI : -sI;   // toward the interior
-        a.aux_u[cb] = aux_u_lid(a, a.aux_u[cb + s], a.aux_u[cb + 2 * s]);
-        a.aux_v[cb] = c43 * a.aux_v[cb + s] - c13 * a.aux_v[cb + 2 * s];
-        a.aux_w[cb] = c43 * a.aux_w[cb + s] - c13 * a.aux_w[cb + 2 * s];
-    }
-    bool fluid = (k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1 && i >= 1 && i < d.im - 1);
+    if ((i == 0 || i == d.im - 1) && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1) aux_lid_cell(a, i, j, k);
+    const bool fluid = (k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1 && i >= 1 && i < d.im - 1);
     bool clamped = false;
     if (fluid) {
         const long long c = idx3(d, i, j, k);
         const PoiIJ P = a.poi[i * d.jm + j];
-        const double u_c = __ldg(a.aux_u + c);
-        const double u_up = (i + 1 == d.im - 1) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c - sI)) : __ldg(a.aux_u + c + sI);
-        const double u_dn = (i - 1 == 0) ? aux_u_lid(a, u_c, __ldg(a.aux_u + c + sI)) : __ldg(a.aux_u + c - sI);
-        const double du_dr = (u_up - u_dn) * a.inv_2dr;
-        const double dv_dthe = (__ldg(a.aux_v + c + sJ) - __ldg(a.aux_v + c - sJ)) * a.inv_2dthe;
-        const double dw_dphi = (__ldg(a.aux_w + c + 1) - __ldg(a.aux_w + c - 1)) * a.inv_2dphi;
-        double div_src = du_dr * P.exp_rm + dv_dthe * P.inv_rm + dw_dphi * P.inv_rmsinthe;
-        if (a.anelastic) div_src += __ldg(a.aux_u + c) * __ldg(a.dlnrho + i) * P.exp_rm;
-        if (a.metric_div)
-            div_src += (2.0 * __ldg(a.aux_u + c) + __ldg(a.aux_v + c) * P.costhe / P.sinthe) * P.inv_rm;
-        const double src_max = P.denom * 2.0;   // p_dyn_cap = 2 (:148)
-        if (!is_finite_bits(div_src)) div_src = 0.0;
-        else if (div_src > src_max) { div_src = src_max; clamped = true; }
-        else if (div_src < -src_max) { div_src = -src_max; clamped = true; }
-        a.src[c] = div_src;
+        a.src[c] = cell_source(a, P, i, c, clamped);
     }
-    // counters aggregated per CTA: one global atomic per counter and CTA instead of one
-    // per warp, which would serialise on the two addresses
-    __shared__ unsigned cnt[2];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    if (tid < 2) cnt[tid] = 0u;
-    __syncthreads();
-    const unsigned nf = __popc(__ballot_sync(0xffffffffu, fluid));
-    const unsigned nc = __popc(__ballot_sync(0xffffffffu, clamped));
-    if ((tid & 31) == 0) {
-        if (nf) atomicAdd(&cnt[0], nf);
-        if (nc) atomicAdd(&cnt[1], nc);
-    }
-    __syncthreads();
-    if (tid == 0 && a.counters) {
-        if (cnt[0]) atomicAdd(a.counters + 0, (unsigned long long)cnt[0]);
-        if (cnt[1]) atomicAdd(a.counters + 1, (unsigned long long)cnt[1]);
-    }
+    count_clamped(a, clamped);
 }
 
 // one colour of the red-black sweep, PressureSolverAtm.h:225-486 (update :475-480); thread
@@ -86,22 +97,29 @@ __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
 template <int COLOUR>
 __global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
 {
+    pdl_trigger();
+    pdl_wait();
     const Dims& d = a.d;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((i + j + COLOUR) & 1);
-    if (k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1) return;
-    const long long c = idx3(d, i, j, k);
-    const PoiIJ P = a.poi[i * d.jm + j];
-    const long long sI = d.plane, sJ = d.pitch;
-    const double* p = a.p;
-    const double pip = p[c + sI], pim = p[c - sI];
-    const double num_a = a.anelastic ? P.exp_2_rm * __ldg(a.dlnrho + i) * a.inv_2dr : 0.0;
-    a.p[c] = ((pip + pim) * P.num1
-            + (p[c + sJ] + p[c - sJ]) * P.num2
-            + (p[c + 1] + p[c - 1]) * P.num3
-            + (pip - pim) * num_a
-            - __ldg(a.src + c)) * P.inv_denom;
+    const bool fluid = !(k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1);
+    bool clamped = false;
+    if (fluid) {
+        const long long c = idx3(d, i, j, k);
+        const PoiIJ P = a.poi[i * d.jm + j];
+        const double src = cell_source(a, P, i, c, clamped);
+        const long long sI = d.plane, sJ = d.pitch;
+        const double* p = a.p;
+        const double pip = p[c + sI], pim = p[c - sI];
+        const double num_a = a.anelastic ? P.exp_2_rm * __ldg(a.dlnrho + i) * a.inv_2dr : 0.0;
+        a.p[c] = ((pip + pim) * P.num1
+                + (p[c + sJ] + p[c - sJ]) * P.num2
+                + (p[c + 1] + p[c - 1]) * P.num3
+                + (pip - pim) * num_a
+                - src) * P.inv_denom;
+    }
+    count_clamped(a, clamped);
 }
 
 // The three boundary passes (radial, pole, seam, PressureSolverAtm.h:504-552) in one launch.
@@ -138,6 +156,8 @@ __device__ __forceinline__ double bc_final(const Dims& d, const double* p, int i
 
 __global__ void __launch_bounds__(128) poisson_bc_kernel(PoissonArgs a)
 {
+    pdl_trigger();
+    pdl_wait();
     const Dims& d = a.d;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
@@ -155,6 +175,8 @@ __global__ void __launch_bounds__(128) poisson_bc_kernel(PoissonArgs a)
         k = side ? d.km - 1 : 0; i = r / d.jm; j = r % d.jm;
     }
     a.p[idx3(d, i, j, k)] = bc_final(d, a.p, i, j, k);
+    if (a.aux_lid && blockIdx.z == 0 && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1)
+        aux_lid_cell(a, i, j, k);   // the aux radial boundary, PressureSolverAtm.h:106-121
 }
 
 static void launch_bcs(const PoissonArgs& a, cudaStream_t st)
@@ -163,7 +185,7 @@ static void launch_bcs(const PoissonArgs& a, cudaStream_t st)
     int most = 2 * d.jm * d.km;
     most = std::max(most, 2 * d.im * d.km);
     most = std::max(most, 2 * d.im * d.jm);
-    poisson_bc_kernel<<<dim3((most + 127) / 128, 1, 3), 128, 0, st>>>(a);
+    launch_dependent(poisson_bc_kernel, dim3((most + 127) / 128, 1, 3), dim3(128), 0, st, a);
 }
 
 // |p_dyn| ceiling (:583-594); writes only where the value changes.  A thread takes four
@@ -179,6 +201,7 @@ __device__ __forceinline__ bool ceiling_of(double v, double cap, double& out)
 
 __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
 {
+    pdl_wait();
     const Dims& d = a.d;
     const long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
     if (q >= (long long)d.im * d.plane) return;
@@ -205,11 +228,13 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     const Dims& d = a.d;
     const dim3 block(32, 8), grid((d.km + 31) / 32, (d.jm + 7) / 8, d.im);
     const dim3 half_grid(((d.km + 1) / 2 + 31) / 32, (d.jm + 7) / 8, d.im);
+    // each launch after the first waits for the one before it (pdl_wait) but is scheduled
+    // during its tail
     poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
-    poisson_colour_kernel<1><<<half_grid, block, 0, st>>>(a);
+    launch_dependent(poisson_colour_kernel<1>, half_grid, block, 0, st, a);
     launch_bcs(a, st);
     const long long quads = (long long)d.im * d.plane / 4;
-    poisson_ceiling_kernel<<<(unsigned)((quads + 255) / 256), 256, 0, st>>>(a);
+    launch_dependent(poisson_ceiling_kernel, dim3((unsigned)((quads + 255) / 256)), dim3(256), 0, st, a);
 }
 
 // the boundary conditions of a sweep alone (radial, pole, seam), PressureSolverAtm.h:504-552

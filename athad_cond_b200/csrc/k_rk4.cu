@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(256) level_rows_kernel(Dims d, const double* _
                                                          double* __restrict__ rows,
                                                          unsigned long long* __restrict__ nonfinite)
 {
+    pdl_trigger();
     const int lane = threadIdx.x & 31;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (row >= d.im * d.jm) return;
@@ -50,6 +51,8 @@ __global__ void __launch_bounds__(128) level_combine_kernel(Dims d, const double
                                                             const double* __restrict__ sin_w,
                                                             double* __restrict__ out)
 {
+    pdl_trigger();
+    pdl_wait();
     extern __shared__ double r[];   // [jm] row sums of level i
     const int i = blockIdx.x;
     for (int j = threadIdx.x; j < d.jm; j += blockDim.x) r[j] = rows[(long long)i * d.jm + j];
@@ -74,7 +77,8 @@ void launch_level_mean(const Dims& d, const double* t, const double* sin_w, doub
 {
     const int rows = d.im * d.jm;
     level_rows_kernel<<<(rows + 7) / 8, 256, 0, st>>>(d, t, row_sum, nonfinite);
-    level_combine_kernel<<<d.im, 128, d.jm * sizeof(double), st>>>(d, row_sum, sin_w, out);
+    launch_dependent(level_combine_kernel, dim3(d.im), dim3(128), d.jm * sizeof(double), st,
+                     d, (const double*)row_sum, sin_w, out);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -153,6 +157,48 @@ __device__ __forceinline__ void stage_update(const RK4Args& a, int n, long long 
 #define ATHAD_RK4_BY 4
 #endif
 
+// Shared-memory staging of the stencil tiles (ATHAD_RK4_SMEM=1): the CTA's BY x BX cells of
+// level i with a one-cell ring in j and k, for the 11 stage fields and p_dyn, loaded once
+// per launch; the centre, meridional and zonal neighbours then come from shared memory and
+// only the radial neighbours (levels i +- 1) from global memory (L1/L2).  Same results bit
+// for bit.  Off: measured at 41x181x361 (FP64 step, reference initial state) 1.743 ms
+// against 1.744 ms without it at 32 x 4 and 7 CTAs per SM, 1.76 ms at 6 CTAs, 1.94 ms with
+// 32 x 8 tiles (a third less halo, half the CTAs per SM): the DRAM traffic is already
+// 1.17x the algorithmic bytes, the neighbours the tiles would serve hit L1/L2 today, and
+// the staging adds a barrier and its own loads.
+#ifndef ATHAD_RK4_SMEM
+#define ATHAD_RK4_SMEM 0
+#endif
+constexpr int kTileJ = ATHAD_RK4_BY + 2, kTileK = ATHAD_RK4_BX + 2, kTileFields = 12;
+constexpr int kTileCells = kTileJ * kTileK;
+
+__device__ __forceinline__ const double* stage_field(const RK4Args& a, int n)
+{
+    return (n < 11) ? a.Yin[n] : a.p_dyn;
+}
+
+// every thread of the CTA takes part (before any thread returns); levels 0 and im-1 hold
+// boundary cells only and stage nothing
+__device__ __forceinline__ void stage_tiles(const RK4Args& a, double (*tile)[kTileJ][kTileK], int i)
+{
+    const Dims& d = a.d;
+    if (i <= 0 || i >= d.im - 1) return;
+    const int j0 = blockIdx.y * ATHAD_RK4_BY - 1, k0 = blockIdx.x * ATHAD_RK4_BX - 1;
+    const int tid = threadIdx.y * ATHAD_RK4_BX + threadIdx.x;
+    constexpr int kThreads = ATHAD_RK4_BX * ATHAD_RK4_BY;
+#pragma unroll
+    for (int e0 = 0; e0 < kTileCells; e0 += kThreads) {
+        const int e = e0 + tid;
+        if (e >= kTileCells) break;
+        const int tj = e / kTileK, tk = e - tj * kTileK;
+        const int jj = j0 + tj, kk = k0 + tk;
+        if (jj < 0 || jj >= d.jm || kk < 0 || kk >= d.km) continue;
+        const long long g = idx3(d, i, jj, kk);
+#pragma unroll
+        for (int n = 0; n < kTileFields; n++) tile[n][tj][tk] = __ldg(stage_field(a, n) + g);
+    }
+}
+
 #ifndef ATHAD_RK4_TRACER_UNROLL
 #define ATHAD_RK4_TRACER_UNROLL 5    // 41x181x361: 1.92 ms per step with 1, 1.64 ms with 5
 #endif
@@ -162,10 +208,17 @@ template <int STAGE>
 __global__ void __launch_bounds__(ATHAD_RK4_BX * ATHAD_RK4_BY, ATHAD_RK4_MIN_BLOCKS * 128 / (ATHAD_RK4_BX * ATHAD_RK4_BY))
 rk4_stage_kernel(const RK4Args a)
 {
+    pdl_trigger();
+    pdl_wait();
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
+#if ATHAD_RK4_SMEM
+    __shared__ double tile[kTileFields][kTileJ][kTileK];
+    stage_tiles(a, tile, i);
+    __syncthreads();
+#endif
     if (k >= d.km || j >= d.jm) return;
     const long long c = idx3(d, i, j, k);
     const bool interior = (i > 0 && i < d.im - 1 && j > 0 && j < d.jm - 1 && k > 0 && k < d.km - 1);
@@ -189,6 +242,20 @@ rk4_stage_kernel(const RK4Args a)
     const long long sI = d.plane, sJ = d.pitch;
     const GeoIJ* G = a.geo + (i * d.jm + j);
     const double exp_rm = G->exp_rm, inv_rm = G->inv_rm, inv_rmsinthe = G->inv_rmsinthe;
+#if ATHAD_RK4_SMEM
+    const int ty = threadIdx.y + 1, tx = threadIdx.x + 1;
+    auto star = [&](int n) {
+        Star s;
+        s.c = tile[n][ty][tx];
+        s.jp = tile[n][ty + 1][tx]; s.jm = tile[n][ty - 1][tx];
+        s.kp = tile[n][ty][tx + 1]; s.km = tile[n][ty][tx - 1];
+        const double* F = stage_field(a, n);
+        s.ip = __ldg(F + c + sI); s.im = __ldg(F + c - sI);
+        return s;
+    };
+#else
+    auto star = [&](int n) { return load_star(stage_field(a, n), c, sI, sJ); };
+#endif
 
     const double u_ijk = __ldg(a.Yin[1] + c), v_ijk = __ldg(a.Yin[2] + c), w_ijk = __ldg(a.Yin[3] + c);
     const double nue_ijk = __ldg(a.nue + c);
@@ -198,9 +265,9 @@ rk4_stage_kernel(const RK4Args a)
     // ---- turbulence: production from the velocity shear (RHS_Atm_Turb.cpp:528-561) ----
     double prod;
     {
-        const Star U = load_star(a.Yin[1], c, sI, sJ);
-        const Star V = load_star(a.Yin[2], c, sI, sJ);
-        const Star W = load_star(a.Yin[3], c, sI, sJ);
+        const Star U = star(1);
+        const Star V = star(2);
+        const Star W = star(3);
         const double dudr_s = d1r(U, a) * exp_rm, dvdr_s = d1r(V, a) * exp_rm, dwdr_s = d1r(W, a) * exp_rm;
         const double dudthe_s = d1t(U, a) * inv_rm, dvdthe_s = d1t(V, a) * inv_rm, dwdthe_s = d1t(W, a) * inv_rm;
         const double dudphi_s = d1p(U, a) * inv_rmsinthe, dvdphi_s = d1p(V, a) * inv_rmsinthe,
@@ -229,8 +296,8 @@ rk4_stage_kernel(const RK4Args a)
     {
         const double exp_2_rm = G->exp_2_rm, inv_rm2 = G->inv_rm2, inv_rm2sinthe2 = G->inv_rm2sinthe2;
         const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
-        const Star TK = load_star(a.Yin[9], c, sI, sJ);
-        const Star DI = load_star(a.Yin[10], c, sI, sJ);
+        const Star TK = star(9);
+        const Star DI = star(10);
         const double tke_ijk = TK.c, dis_ijk = DI.c;
         const double dtkedr = d1r(TK, a), dtkedthe = d1t(TK, a), dtkedphi = d1p(TK, a);
         const double ddisdr = d1r(DI, a), ddisdthe = d1t(DI, a), ddisdphi = d1p(DI, a);
@@ -312,10 +379,10 @@ rk4_stage_kernel(const RK4Args a)
         const double inv_rm2sinthe = G->inv_rm2sinthe;
         const double cos_rm2sin = G->costhe_inv_rm2sinthe, two_over_rm_exp = G->two_over_rm_exp;
         const double sinthe = G->sinthe, costhe = G->costhe, v_metric = G->v_metric;
-        const double* P = a.p_dyn;
-        const double dpdr = (__ldg(P + c + sI) - __ldg(P + c - sI)) * a.inv_2dr;
-        const double dpdthe = (__ldg(P + c + sJ) - __ldg(P + c - sJ)) * a.inv_2dthe;
-        const double dpdphi = (__ldg(P + c + 1) - __ldg(P + c - 1)) * a.inv_2dphi;
+        const Star P = star(11);
+        const double dpdr = (P.ip - P.im) * a.inv_2dr;
+        const double dpdthe = (P.jp - P.jm) * a.inv_2dthe;
+        const double dpdphi = (P.kp - P.km) * a.inv_2dphi;
         const double dpdr_exp = dpdr * exp_rm, dpdthe_invrm = dpdthe * inv_rm, dpdphi_invrs = dpdphi * inv_rmsinthe;
         const double nontrad = a.nontrad ? 1.0 : 0.0;
         const double cotanthe = a.curvature ? costhe / sinthe : 0.0;
@@ -325,7 +392,7 @@ rk4_stage_kernel(const RK4Args a)
         const double surf_drag = a.drag_pref * drag_profile;
         double dudthe, dudphi, dvdphi, part_v;
         {   // u
-            const Star U = load_star(a.Yin[1], c, sI, sJ);
+            const Star U = star(1);
             dudthe = d1t(U, a);
             dudphi = d1p(U, a);
             double tr_u = u_exp * ar(U, a) + v_invrm * at(U, a) + w_invrs * ap(U, a);
@@ -342,7 +409,7 @@ rk4_stage_kernel(const RK4Args a)
             if (STAGE == 4) a.aux_u[c] = rhs_u + dpdr_exp;
         }
         {   // v: every term but the w-shear one, which closes the sum below
-            const Star V = load_star(a.Yin[2], c, sI, sJ);
+            const Star V = star(2);
             dvdphi = d1p(V, a);
             part_v = V.c;   // placeholder for register reuse
             double tr_v = u_exp * ar(V, a) + v_invrm * at(V, a) + w_invrs * ap(V, a);
@@ -363,7 +430,7 @@ rk4_stage_kernel(const RK4Args a)
             if (STAGE == 4) a.aux_v[c] = rhs_v + dpdthe_invrm;
         }
         {   // w
-            const Star W = load_star(a.Yin[3], c, sI, sJ);
+            const Star W = star(3);
             double tr_w = u_exp * ar(W, a) + v_invrm * at(W, a) + w_invrs * ap(W, a);
             if (a.curvature) tr_w += (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
             const double diffusion_w = (d2r(W, a) * exp_2_rm + d1r(W, a) * two_over_rm_exp
@@ -381,7 +448,7 @@ rk4_stage_kernel(const RK4Args a)
         }
         // ---- temperature (RHS_Atm_Turb.cpp:752, 829, 866-868, 963-992) ----
         {
-            const Star T = load_star(a.Yin[0], c, sI, sJ);
+            const Star T = star(0);
             const double t_ijk = T.c;
             const double r_h = __ldg(a.r_humid + c);
             const double pressure_t = a.coeff_energy_p * (u_exp * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
@@ -411,7 +478,7 @@ rk4_stage_kernel(const RK4Args a)
         const double r_h = __ldg(a.r_humid + c);
 #pragma unroll kTracerUnroll64
         for (int n = 4; n <= 8; n++) {
-            const Star Q = load_star(a.Yin[n], c, sI, sJ);
+            const Star Q = star(n);
             const double coef = (n == 8) ? a.diff_co2_re_inv : a.diff_prec_re_inv;
             const double tr = (n <= 6) ? (u_exp * ar(Q, a) + v_invrm * at(Q, a) + w_invrs * ap(Q, a))
                                        : (u_exp * d1r(Q, a) + v_invrm * d1t(Q, a) + w_invrs * d1p(Q, a));
@@ -436,10 +503,10 @@ void launch_rk4_stage(int stage, const RK4Args& a, cudaStream_t st)
     const dim3 block(ATHAD_RK4_BX, ATHAD_RK4_BY, 1);
     const dim3 grid((a.d.km + ATHAD_RK4_BX - 1) / ATHAD_RK4_BX, (a.d.jm + ATHAD_RK4_BY - 1) / ATHAD_RK4_BY, a.d.im);
     switch (stage) {
-        case 1: rk4_stage_kernel<1><<<grid, block, 0, st>>>(a); break;
-        case 2: rk4_stage_kernel<2><<<grid, block, 0, st>>>(a); break;
-        case 3: rk4_stage_kernel<3><<<grid, block, 0, st>>>(a); break;
-        default: rk4_stage_kernel<4><<<grid, block, 0, st>>>(a); break;
+        case 1: launch_dependent(rk4_stage_kernel<1>, grid, block, 0, st, a); break;
+        case 2: launch_dependent(rk4_stage_kernel<2>, grid, block, 0, st, a); break;
+        case 3: launch_dependent(rk4_stage_kernel<3>, grid, block, 0, st, a); break;
+        default: launch_dependent(rk4_stage_kernel<4>, grid, block, 0, st, a); break;
     }
 }
 

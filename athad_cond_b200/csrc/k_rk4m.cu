@@ -436,6 +436,8 @@ __global__ void __launch_bounds__(ATHAD_RK4M_BX * ATHAD_RK4M_BY,
     * 128 / (ATHAD_RK4M_BX * ATHAD_RK4M_BY))
 rk4m_stage_kernel(const RK4MArgs a)
 {
+    pdl_trigger();
+    pdl_wait();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (k >= a.d.km || j >= a.d.jm) return;
@@ -447,10 +449,10 @@ void launch_rk4m_stage(int stage, const RK4MArgs& a, cudaStream_t st)
     const dim3 block(ATHAD_RK4M_BX, ATHAD_RK4M_BY, 1);
     const dim3 grid((a.d.km + ATHAD_RK4M_BX - 1) / ATHAD_RK4M_BX, (a.d.jm + ATHAD_RK4M_BY - 1) / ATHAD_RK4M_BY, a.d.im);
     switch (stage) {
-        case 1: rk4m_stage_kernel<1><<<grid, block, 0, st>>>(a); break;
-        case 2: rk4m_stage_kernel<2><<<grid, block, 0, st>>>(a); break;
-        case 3: rk4m_stage_kernel<3><<<grid, block, 0, st>>>(a); break;
-        default: rk4m_stage_kernel<4><<<grid, block, 0, st>>>(a); break;
+        case 1: launch_dependent(rk4m_stage_kernel<1>, grid, block, 0, st, a); break;
+        case 2: launch_dependent(rk4m_stage_kernel<2>, grid, block, 0, st, a); break;
+        case 3: launch_dependent(rk4m_stage_kernel<3>, grid, block, 0, st, a); break;
+        default: launch_dependent(rk4m_stage_kernel<4>, grid, block, 0, st, a); break;
     }
 }
 

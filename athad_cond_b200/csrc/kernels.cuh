@@ -155,13 +155,15 @@ struct PoissonArgs {
     double* aux_u; double* aux_v; double* aux_w;
     double* src;                // clamped divergence source (scratch field)
     double* p;
-    unsigned long long* counters;   // [2] fluid cells, clamped sources
+    unsigned long long* counters;   // [2] counters[1]: clamped sources
     double inv_2dr, inv_2dthe, inv_2dphi;
     int anelastic, metric_div;
+    int aux_lid;                // the boundary passes also write the aux radial boundary
     double ceiling;
 };
-void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st);   // aux BC + source
-void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st);     // colours + BCs + ceiling
+void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st);   // aux BC + source field
+void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st);     // colours (with their
+                                                                      // sources) + BCs + ceiling
 void launch_poisson_bcs(const PoissonArgs& a, cudaStream_t st);       // BCs only
 void launch_project_correct(const PoissonArgs& a, double* u, double* v, double* w, cudaStream_t st);
 

@@ -263,12 +263,14 @@ def test_fused_time_level_copy_equals_separate_copy(precision):
             assert np.array_equal(a.download(n), b.download(n)), n
 
 
-@pytest.mark.parametrize("grid", GRIDS)
+@pytest.mark.parametrize("grid", GRIDS + [(4, 5, 5), (6, 7, 9)])
 def test_pressure_boundaries_and_ceiling_bit_exact(grid):
     """The boundary passes (radial, pole, seam) and the |p| ceiling in the reference's order,
     with p far beyond the ceiling next to the seam, the poles and the lid, and non-finite
     values beside them: the seam average is formed from unclamped values and clamped after,
-    a non-finite neighbour turns an extrapolation into NaN and the ceiling into 0."""
+    a non-finite neighbour turns an extrapolation into NaN and the ceiling into 0.  The
+    smallest grid the context accepts (4 x 5 x 5) included: there every interior cell is one
+    the boundary passes read."""
     p = config_params()
     st = make_state(*grid, seed=17)
     im, jm, km = grid
