@@ -709,10 +709,9 @@ athad_status athad_pressure_sweep(athad_ctx* ctx, int32_t n_sweeps, int32_t tota
     if (!ctx || n_sweeps < 0) return fail(ctx, ATHAD_ERR_INVALID, "pressure_sweep: bad argument");
     if (n_sweeps == 0) return ATHAD_OK;
     PoissonArgs a = poisson_args(ctx, total_iter_count);
-    athad_status s = cuda_check(ctx, cudaMemsetAsync(ctx->counters + 1, 0, sizeof(unsigned long long), ctx->stream), "counters");
-    if (s != ATHAD_OK) return s;
     a.aux_lid = 1;
     for (int i = 0; i < n_sweeps; i++) {
+        a.first_sweep = (i == 0) ? 1 : 0;
         launch_poisson_sweep(a, ctx->stream);
         ATHAD_CHECK_LAUNCH(ctx, "poisson sweep");
     }
@@ -823,7 +822,7 @@ athad_status athad_get_report(athad_ctx* ctx, athad_report* out)
     std::memset(out, 0, sizeof *out);
     const int64_t fluid = (int64_t)(ctx->L.d.im - 2) * (ctx->L.d.jm - 2) * (ctx->L.d.km - 2);
     out->poisson_src_cells = fluid * ctx->poisson_sweeps_since_reset;
-    out->poisson_src_clamped = (int64_t)h[1];                // counted in every sweep
+    out->poisson_src_clamped = (int64_t)h[0];                // counted in every sweep
     out->satadj_ceiling_hits = (int64_t)h[2];
     out->nonfinite_inputs = (int64_t)h[3];
     if (ctx->step_timed) {

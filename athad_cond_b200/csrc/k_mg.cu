@@ -739,12 +739,10 @@ extern "C" athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int
     std::memset(&pa, 0, sizeof pa);
     pa.d = d; pa.poi = ctx->poi; pa.dlnrho = ctx->prof[ATHAD_PROF_DLNRHO_DR];
     pa.aux_u = ctx->field[ATHAD_AUX_U]; pa.aux_v = ctx->field[ATHAD_AUX_V]; pa.aux_w = ctx->field[ATHAD_AUX_W];
-    pa.src = ctx->src; pa.p = ctx->field[ATHAD_P_DYN]; pa.counters = ctx->counters;
+    pa.src = ctx->src; pa.p = ctx->field[ATHAD_P_DYN]; pa.counters = nullptr;   // clamps not counted
     pa.inv_2dr = 1.0 / (2.0 * ctx->dr); pa.inv_2dthe = 1.0 / (2.0 * ctx->dthe); pa.inv_2dphi = 1.0 / (2.0 * ctx->dphi);
     pa.anelastic = 0; pa.metric_div = ctx->p.metric_divergence;
     pa.ceiling = 0.0;
-    athad_status stt = cuda_check(ctx, cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), st), "counters");
-    if (stt != ATHAD_OK) return stt;
     launch_poisson_prepare(pa, st);
     const dim3 g0 = cells_grid(L0.nk, L0.nj, L0.ni);
     const double count = (double)L0.ni * L0.nj * L0.nk;
@@ -762,7 +760,7 @@ extern "C" athad_status athad_pressure_solve(athad_ctx* ctx, double rel_tol, int
     dot(s, s->r, s->z, 0, st);                                        // rz
     ATHAD_CHECK_LAUNCH(ctx, "pressure_solve setup");
     double h[5] = {0, 0, 0, 0, 0};
-    stt = cuda_check(ctx, cudaMemcpyAsync(h, s->scal, sizeof h, cudaMemcpyDeviceToHost, st), "pressure_solve norm");
+    athad_status stt = cuda_check(ctx, cudaMemcpyAsync(h, s->scal, sizeof h, cudaMemcpyDeviceToHost, st), "pressure_solve norm");
     if (stt == ATHAD_OK) stt = cuda_check(ctx, cudaStreamSynchronize(st), "pressure_solve");
     if (stt != ATHAD_OK) { cudaEventDestroy(t0); cudaEventDestroy(t1); return stt; }
 

@@ -3,13 +3,11 @@
 // Replaces PressureSolverAtm::run (PressureSolverAtm.h:27-594) for flat terrain, and the
 // gradient correction of PressureSolverAtm::project_initial_velocity (:713-749).
 //
-// Each colour kernel forms the clamped divergence of aux_u/v/w (the Poisson source) of its
-// own cells as it updates them, from the same operands as the reference: the model's
-// cadence runs one sweep per call, and a source field written by one launch and read by
-// the next two cost more than the aux reads it saves (24 us of a 68 us call at
-// 41 x 181 x 361).  Within one colour every cell reads only cells of the other colour, so
-// the in-place update is order-independent and the result equals the serial red-black
-// sweep bit for bit.
+// A sweep is the clamped divergence of aux_u/v/w (the Poisson source, from the reference's
+// operands) into a scratch field, the two colours, the boundary passes and the ceiling:
+// five launches, each after the first issued as a programmatic dependent launch.  Within
+// one colour every cell reads only cells of the other colour, so the in-place update is
+// order-independent and the result equals the serial red-black sweep bit for bit.
 #include <algorithm>
 
 #include "kernels.cuh"
@@ -72,10 +70,11 @@ __device__ __forceinline__ void count_clamped(const PoissonArgs& a, bool clamped
     if ((threadIdx.x & 31) == 0 && nc && a.counters) atomicAdd(a.counters + 1, (unsigned long long)nc);
 }
 
-// The source into a scratch field for the Poisson solve (athad_pressure_solve), with the
-// aux boundary
+// The source into a scratch field (the sweep's colours and the Poisson solve read it), with
+// the aux boundary
 __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
 {
+    pdl_trigger();
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -94,8 +93,19 @@ __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
 // one colour of the red-black sweep, PressureSolverAtm.h:225-486 (update :475-480); thread
 // kk of row (i, j) takes the kk-th cell of the colour, k = 2 kk + ((i + j + COLOUR) & 1),
 // so every lane of a warp updates a cell
+// ATHAD_POISSON_SRC_FIELD 1: the source formed by its own launch into a scratch field that
+// both colours read; 0: each colour forms its cells' sources from aux_u/v/w.  The pressure
+// call at 41x181x361 inside the model iteration (PDL on, mixed form, 300 iterations):
+// 59.1 us with the source field, 68.8 us forming the sources in the colours (46 registers,
+// 5 CTAs of 256 per SM), 63.7 us at 8 CTAs (spills), 60.0 us at 6.
+#ifndef ATHAD_POISSON_SRC_FIELD
+#define ATHAD_POISSON_SRC_FIELD 1
+#endif
+#ifndef ATHAD_POISSON_MIN_BLOCKS
+#define ATHAD_POISSON_MIN_BLOCKS 1
+#endif
 template <int COLOUR>
-__global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
+__global__ void __launch_bounds__(256, ATHAD_POISSON_MIN_BLOCKS) poisson_colour_kernel(PoissonArgs a)
 {
     pdl_trigger();
     pdl_wait();
@@ -108,7 +118,11 @@ __global__ void __launch_bounds__(256) poisson_colour_kernel(PoissonArgs a)
     if (fluid) {
         const long long c = idx3(d, i, j, k);
         const PoiIJ P = a.poi[i * d.jm + j];
+#if ATHAD_POISSON_SRC_FIELD
+        const double src = __ldg(a.src + c);
+#else
         const double src = cell_source(a, P, i, c, clamped);
+#endif
         const long long sI = d.plane, sJ = d.pitch;
         const double* p = a.p;
         const double pip = p[c + sI], pim = p[c - sI];
@@ -203,6 +217,14 @@ __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
 {
     pdl_wait();
     const Dims& d = a.d;
+    // the sweep's clamped sources into the call's count (counters[0]), the accumulator
+    // cleared for the next sweep: every launch that added to it has completed, and the
+    // next source launch waits for this one, so no memset precedes a call
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.counters) {
+        const unsigned long long n = a.counters[1];
+        a.counters[0] = a.first_sweep ? n : a.counters[0] + n;
+        a.counters[1] = 0ull;
+    }
     const long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
     if (q >= (long long)d.im * d.plane) return;
     const int k0 = (int)(q % d.pitch);
@@ -230,7 +252,12 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     const dim3 half_grid(((d.km + 1) / 2 + 31) / 32, (d.jm + 7) / 8, d.im);
     // each launch after the first waits for the one before it (pdl_wait) but is scheduled
     // during its tail
+#if ATHAD_POISSON_SRC_FIELD
+    poisson_src_kernel<<<grid, block, 0, st>>>(a);
+    launch_dependent(poisson_colour_kernel<0>, half_grid, block, 0, st, a);
+#else
     poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
+#endif
     launch_dependent(poisson_colour_kernel<1>, half_grid, block, 0, st, a);
     launch_bcs(a, st);
     const long long quads = (long long)d.im * d.plane / 4;

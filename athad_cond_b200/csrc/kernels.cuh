@@ -155,10 +155,12 @@ struct PoissonArgs {
     double* aux_u; double* aux_v; double* aux_w;
     double* src;                // clamped divergence source (scratch field)
     double* p;
-    unsigned long long* counters;   // [2] counters[1]: clamped sources
+    unsigned long long* counters;   // [2] clamped sources: [1] accumulated by the source
+                                    // launch, [0] the call's total (folded by the ceiling)
     double inv_2dr, inv_2dthe, inv_2dphi;
     int anelastic, metric_div;
     int aux_lid;                // the boundary passes also write the aux radial boundary
+    int first_sweep;            // the ceiling starts the call's count instead of adding
     double ceiling;
 };
 void launch_poisson_prepare(const PoissonArgs& a, cudaStream_t st);   // aux BC + source field

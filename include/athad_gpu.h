@@ -221,8 +221,10 @@ typedef struct athad_step_scalars {
 
 /* Counters a call leaves behind (read with athad_get_report). */
 typedef struct athad_report {
-    int64_t poisson_src_cells;     /* fluid cells of the last pressure sweep(s)          */
-    int64_t poisson_src_clamped;   /* of which the divergence source hit p_dyn_cap       */
+    int64_t poisson_src_cells;     /* fluid cells of the last pressure call, summed over
+                                    * its sweeps                                          */
+    int64_t poisson_src_clamped;   /* of which the divergence source hit p_dyn_cap (the
+                                    * pressure solve's sources are not counted)          */
     int64_t satadj_ceiling_hits;   /* c > 1 - co2 clamps in clampAndFade                  */
     int64_t nonfinite_inputs;      /* non-finite values of t seen by the last level mean (every
                                     * athad_rk4_step forms one from its input t)           */
