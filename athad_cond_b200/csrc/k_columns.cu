@@ -100,17 +100,24 @@ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double i
 }
 // The mixture heat capacity of the Newton step (MixtureAtm.h:123-178) with the three
 // Shomate polynomials sharing t, t^2, t^3 and 1/t^2, and products by the reciprocal molar
-// masses: one division instead of six.
-__device__ __forceinline__ double cp_of_r(double c, double co2, double T, double inv_M_b)
+// masses: one division instead of six.  Split in two: the specific heats of the three
+// components at T (shomate_r), and their mixture (cp_mix), so a Newton step that moves the
+// composition but not T reuses the first.
+struct SpecificHeats { double h2o, co2, bg; };
+__device__ __forceinline__ SpecificHeats shomate_r(double T, double inv_M_b)
 {
-    double q_v, q_c, q_b;
-    split(c, co2, q_v, q_c, q_b);
     const double t = smin(smax(T, 298.0), 2000.0) * 1.0e-3;
     const double t2 = t * t, t3 = t2 * t, it2 = 1.0 / t2;
     const double h2o = 30.09200 + 6.832514 * t + 6.793435 * t2 + -2.534480 * t3 + 0.082139 * it2;
     const double co2s = 24.99735 + 55.18696 * t + -33.69137 * t2 + 7.948387 * t3 + -0.136638 * it2;
     const double bg = 28.98641 + 1.853978 * t + -9.647459 * t2 + 16.63537 * t3 + 0.000117 * it2;
-    return q_v * (h2o * (1.0 / M_H2O)) + q_c * (co2s * (1.0 / M_CO2)) + q_b * (bg * inv_M_b);
+    return {h2o * (1.0 / M_H2O), co2s * (1.0 / M_CO2), bg * inv_M_b};
+}
+__device__ __forceinline__ double cp_mix(double c, double co2, const SpecificHeats& h)
+{
+    double q_v, q_c, q_b;
+    split(c, co2, q_v, q_c, q_b);
+    return q_v * h.h2o + q_c * h.co2 + q_b * h.bg;
 }
 
 // adjustSaturation (:62-287) followed, for the same cell, by clampAndFade (:303-459).
@@ -164,6 +171,7 @@ saturation_adjust_kernel(const ColumnArgs a)
                     double L_T = latent_heat(T);
                     const double inv_p = 1.0 / p_local;
                     const double inv_M_b = 1.0 / a.M_bg;
+                    SpecificHeats sh = shomate_r(T, inv_M_b);   // at the T of the step's start
                     for (int iter = 1; iter <= 20; iter++) {
                         const double CND = smax(0.0, smin(1.0, (T - a.t_00) * t_range_inv));
                         const double DEP = 1.0 - CND;
@@ -176,7 +184,7 @@ saturation_adjust_kernel(const ColumnArgs a)
                         q_v_b += d_q_v;
                         q_c_b = smax(0.0, q_c_b - d_cnd);
                         q_i_b = smax(0.0, q_i_b - d_dep);
-                        const double cp_loc = cp_of_r(q_v_b, co2, T, inv_M_b);
+                        const double cp_loc = cp_mix(q_v_b, co2, sh);
                         T -= (L_T * d_cnd + (L_T + 3.337e5) * d_dep) / cp_loc;
                         const double invT = 1.0 / T;
                         const double E_sat = p_sat_r(T, invT);
@@ -187,7 +195,8 @@ saturation_adjust_kernel(const ColumnArgs a)
                         const double q_Ice = need_ice ? q_sat_r(E_Ice, p_local, inv_p, M_other) : 0.0;
                         const double q_v_target = (q_sum > 1e-12) ? (q_c_b * q_sat + q_i_b * q_Ice) / q_sum
                                                                   : ((T >= a.t_0) ? q_sat : q_Ice);
-                        const double cp_g = cp_of_r(q_v_b, co2, T, inv_M_b);
+                        sh = shomate_r(T, inv_M_b);   // the updated T: the next step starts from it
+                        const double cp_g = cp_mix(q_v_b, co2, sh);
                         const double L_cnd = latent_heat(T);
                         const double L_dep = L_cnd + 3.337e5;
                         double Gain = CND * (L_cnd / cp_g) * dqsat_r(E_sat, L_cnd, T, invT, p_local, inv_p, M_other);
@@ -258,7 +267,10 @@ void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st)
 
 // ---------------------------------------------------------------------------------------
 // densities: one thread per column, ThermoAtm.h:1484-1614
-__global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs a)
+#ifndef ATHAD_DENS_BLOCK
+#define ATHAD_DENS_BLOCK 128   // columns per CTA
+#endif
+__global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(const ColumnArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,6 +279,10 @@ __global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs 
     const double p_sl_factor = 1e-2 * a.r_air * a.R_mix;
     double T_prev = smax(180.0, a.t[idx3(d, 0, j, k)] * a.t_0);
     double p_prev = p_sl_factor * T_prev;
+    // saturation_pressure_auto(T_prev): formed once per level and carried to the next,
+    // where T_prev is this level's T (the values, and the results, are the same as
+    // evaluating it at each use)
+    double E_prev = saturation_pressure_auto(T_prev);
     double q_sat_min = 1.0;
     double q_v_p = 0.0, q_c_p = 0.0;   // c and co2 of level i-1 (after any rewrite)
     for (int i = 0; i < d.im; i++) {
@@ -281,9 +297,9 @@ __global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs 
             const double dz = a.height[i] - a.height[i - 1];
             const double cp_loc = cp_of(q_v_p, q_c_p, T_prev, a.M_bg);
             const double M_nw = M_nonwater(q_v_p, q_c_p, a.M_bg);
-            const double q_s = saturation_mass_fraction_at(T_prev, p_prev, M_nw);
+            const double q_s = saturation_mass_fraction(E_prev, p_prev, M_nw);
             const double gamma = (q_v_p >= 0.99 * q_s)
-                ? moist_lapse(T_prev, p_prev, M_nw, cp_loc, R_loc, a.g)
+                ? moist_lapse_E(T_prev, E_prev, p_prev, M_nw, cp_loc, R_loc, a.g)
                 : a.g / cp_loc;
             const double T_ad = T_prev - gamma * dz;
             T_i = smax(a.t_skin, T_ad);
@@ -293,9 +309,10 @@ __global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs 
         a.t[c] = T_i / a.t_0;
         a.p_stat[c] = p_i;
         double q_v_now = q_v;
+        const double E_i = (i == 0) ? E_prev : saturation_pressure_auto(T_i);
         if (a.set_water_profile && i > 0) {
             const double M_nw_i = M_nonwater(q_v, q_c, a.M_bg);
-            const double q_s_i = saturation_mass_fraction_at(T_i, p_i, M_nw_i);
+            const double q_s_i = saturation_mass_fraction(E_i, p_i, M_nw_i);
             if (q_s_i < q_sat_min) q_sat_min = q_s_i;
             q_v_now = smax(q_sat_min, a.c_h2o_dry_top);
             a.c[c] = q_v_now;
@@ -304,7 +321,7 @@ __global__ void __launch_bounds__(128) densities_column_kernel(const ColumnArgs 
         a.r_humid[c] = 1e2 * p_i / (R_loc * T_i * water_factor);
         const double R_dry_loc = R_of(0.0, q_c, a.R_bg);
         a.r_dry[c] = 1e2 * p_i / (R_dry_loc * T_i);
-        T_prev = T_i; p_prev = p_i;
+        T_prev = T_i; p_prev = p_i; E_prev = E_i;
         q_v_p = q_v_now; q_c_p = q_c;
     }
     const long long c2 = (long long)j * d.pitch + k;
@@ -418,7 +435,7 @@ __global__ void densities_dlnrho_kernel(const ColumnArgs a)
 void launch_densities(const ColumnArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
-    densities_column_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
+    densities_column_kernel<<<dim3((d.km + ATHAD_DENS_BLOCK - 1) / ATHAD_DENS_BLOCK, d.jm), ATHAD_DENS_BLOCK, 0, st>>>(a);
     const int rows = d.im * d.jm;
     densities_rowsum_kernel<<<(rows + 7) / 8, 256, 0, st>>>(a);
     const size_t smem = 2 * (size_t)d.jm * sizeof(double);

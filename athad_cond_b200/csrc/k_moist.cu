@@ -178,12 +178,13 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
             const long long c = IDX(i, j, k);
             const double t_u = p->F[ATHAD_T][c] * t_0;
             const double w = 1.0 / (1.0 + exp(-(t_u - MC_T00) / 2.0));
+            const double qsc = QSC(i);   // T, p_stat and c are not written in this loop
             p->F[ATHAD_Q_V_U][c] = p->F[ATHAD_C][c] + MC_Q_V_U_ADD;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * QSC(i) && t_u >= MC_T00)
-                p->F[ATHAD_Q_C_U][c] = p->F[ATHAD_Q_V_U][c] - MC_SCALE * QSC(i);
+            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * qsc && t_u >= MC_T00)
+                p->F[ATHAD_Q_C_U][c] = p->F[ATHAD_Q_V_U][c] - MC_SCALE * qsc;
             if (p->F[ATHAD_Q_V_U][c] <= 0.0) p->F[ATHAD_Q_V_U][c] = 0.0;
             if (p->F[ATHAD_Q_C_U][c] <= 0.0) p->F[ATHAD_Q_C_U][c] = 0.0;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * QSC(i) && w > 0.01 && p->F[ATHAD_P_STAT][c] <= MC_F_CB * p0) {
+            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * qsc && w > 0.01 && p->F[ATHAD_P_STAT][c] <= MC_F_CB * p0) {
                 i_base = i;
                 p->F[ATHAD_CLOUD_BASE][c] = p->height[i] * w;
                 break;
@@ -373,79 +374,96 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
         }
         if (interior) cloud_base_update(X, j, k, i_deep_beg, i_lfs, &i_base);
 
-        /* updraftRecurrence, :1032-1163 (interior columns) */
+        /* updraftRecurrence, :1032-1163 (interior columns).  The updraft values of level i-1
+           that level i reads (M_u, q_v_u, q_c_u, v_u, w_u, s_u as this loop left them; E_u,
+           D_u, g_p as the entrainment left them or this loop zeroed them) are carried in
+           registers from one level to the next instead of being stored and loaded again:
+           the same values, so the same results. */
         if (interior && !(i_base < 0 || i_lfs <= i_base)) {
+            const long long cb = IDX(i_base, j, k);
+            double Mu_m = p->F[ATHAD_M_U][cb], qvu_m = p->F[ATHAD_Q_V_U][cb], qcu_m = p->F[ATHAD_Q_C_U][cb];
+            double vu_m = p->F[ATHAD_V_U][cb], wu_m = p->F[ATHAD_W_U][cb], su_m = p->F[ATHAD_MC_S_U][cb];
+            double eu_m = p->F[ATHAD_E_U][cb], du_m = p->F[ATHAD_D_U][cb], gp_m = p->F[ATHAD_G_P][cb];
+            const double inv_a_u = 1.0 / (MC_A_U * p->u_0);
+            const double cap = MC_W_CONV_MAX / p->u_0;
             for (int i = i_base + 1; i <= i_lfs - 1; i++) {
                 const long long c = IDX(i, j, k), cm = IDX(i - 1, j, k);
                 const double t_u = p->F[ATHAD_T][cm] * t_0;
                 const double r_h_prev = p->F[ATHAD_R_HUMID][cm];
                 const double step_prev = p->step[i - 1];
                 const double r_h_i = p->F[ATHAD_R_HUMID][c];
-                const double d_Mu = p->F[ATHAD_E_U][cm] - p->F[ATHAD_D_U][cm];
-                p->F[ATHAD_M_U][c] = clamp_M(p->F[ATHAD_M_U][cm] + d_Mu * step_prev);
-                if (t_u <= MC_T00M2) p->F[ATHAD_M_U][c] = 0.0;
-                const double M_u_prev = p->F[ATHAD_M_U][cm];
-                const double dq_v = M_u_prev * p->F[ATHAD_Q_V_U][cm]
-                    + step_prev * (p->F[ATHAD_E_U][cm] * p->F[ATHAD_C][cm] - p->F[ATHAD_D_U][cm] * p->F[ATHAD_Q_V_U][cm]);
-                const double dq_c = M_u_prev * p->F[ATHAD_Q_C_U][cm]
-                    + step_prev * (-p->F[ATHAD_D_U][cm] * p->F[ATHAD_CLOUD][cm] - r_h_prev * p->F[ATHAD_G_P][cm]);
-                const double dv = M_u_prev * p->F[ATHAD_V_U][cm] + step_prev * p->F[ATHAD_E_U][cm] * p->F[ATHAD_V][cm];
-                const double dw = M_u_prev * p->F[ATHAD_W_U][cm] + step_prev * p->F[ATHAD_E_U][cm] * p->F[ATHAD_W][cm];
-                const double ds = (M_u_prev * p->F[ATHAD_MC_S_U][cm]
-                    + step_prev * (p->F[ATHAD_E_U][cm] * p->F[ATHAD_MC_S][cm] - p->F[ATHAD_D_U][cm] * p->F[ATHAD_MC_S_U][cm])) / p->s_0;
-                const double M_u_i = p->F[ATHAD_M_U][c];
-                if (fabs(M_u_i) > MC_COEFF_RECURR) {
-                    const double inv = 1.0 / M_u_i;
-                    p->F[ATHAD_Q_V_U][c] = dq_v * inv;
-                    p->F[ATHAD_Q_C_U][c] = dq_c * inv;
-                    p->F[ATHAD_V_U][c] = dv * inv;
-                    p->F[ATHAD_W_U][c] = dw * inv;
-                    p->F[ATHAD_MC_S_U][c] = ds * inv;
+                const double d_Mu = eu_m - du_m;
+                double Mu = clamp_M(Mu_m + d_Mu * step_prev);
+                if (t_u <= MC_T00M2) Mu = 0.0;
+                const double M_u_prev = Mu_m;
+                const double dq_v = M_u_prev * qvu_m
+                    + step_prev * (eu_m * p->F[ATHAD_C][cm] - du_m * qvu_m);
+                const double dq_c = M_u_prev * qcu_m
+                    + step_prev * (-du_m * p->F[ATHAD_CLOUD][cm] - r_h_prev * gp_m);
+                const double dv = M_u_prev * vu_m + step_prev * eu_m * p->F[ATHAD_V][cm];
+                const double dw = M_u_prev * wu_m + step_prev * eu_m * p->F[ATHAD_W][cm];
+                const double ds = (M_u_prev * su_m
+                    + step_prev * (eu_m * p->F[ATHAD_MC_S][cm] - du_m * su_m)) / p->s_0;
+                double qvu, qcu, vu, wu, su;
+                if (fabs(Mu) > MC_COEFF_RECURR) {
+                    const double inv = 1.0 / Mu;
+                    qvu = dq_v * inv;
+                    qcu = dq_c * inv;
+                    vu = dv * inv;
+                    wu = dw * inv;
+                    su = ds * inv;
                 } else {
-                    p->F[ATHAD_MC_S_U][c] = p->F[ATHAD_MC_S][c];
-                    p->F[ATHAD_Q_V_U][c] = p->F[ATHAD_C][c];
-                    p->F[ATHAD_Q_C_U][c] = 0.0;
-                    p->F[ATHAD_V_U][c] = p->F[ATHAD_V][c];
-                    p->F[ATHAD_W_U][c] = p->F[ATHAD_W][c];
+                    su = p->F[ATHAD_MC_S][c];
+                    qvu = p->F[ATHAD_C][c];
+                    qcu = 0.0;
+                    vu = p->F[ATHAD_V][c];
+                    wu = p->F[ATHAD_W][c];
                 }
-                p->F[ATHAD_C_U][c] = 0.0;
-                if (fabs(p->F[ATHAD_M_U][c]) > MC_COEFF_RECURR) {
-                    double T_u = p->F[ATHAD_MC_S_U][c] * p->s_0 / p->cp_l;
+                double cu = 0.0;
+                if (fabs(Mu) > MC_COEFF_RECURR) {
+                    double T_u = su * p->s_0 / p->cp_l;
                     const double p_u = p->F[ATHAD_P_STAT][c];
                     double dcond_tot = 0.0;
                     for (int it = 0; it < 2; ++it) {
                         const double E_s = saturation_pressure_auto(T_u);
                         const double q_sat_u = safe_q_sat(X, E_s, p_u, p->F[ATHAD_C][c]);
-                        const double dq = p->F[ATHAD_Q_V_U][c] - q_sat_u;
+                        const double dq = qvu - q_sat_u;
                         if (dq <= 0.0) break;
                         const double L_u = (T_u >= t_0) ? p->lv : p->ls;
                         const double M_o_u = M_nonwater(p->F[ATHAD_C][c], p->F[ATHAD_CO2][c], p->M_bg);
-                        const double dqsdT = dqsat_dT(T_u, p_u, M_o_u);
+                        const double dqsdT = dqsat_dT_from(E_s, latent_heat_auto(T_u), T_u, p_u, M_o_u);
                         const double G = (L_u / p->cp_l) * dqsdT;
                         const double dcond = dq / (1.0 + G);
-                        p->F[ATHAD_Q_V_U][c] -= dcond;
-                        p->F[ATHAD_Q_C_U][c] += dcond;
+                        qvu -= dcond;
+                        qcu += dcond;
                         T_u += (L_u / p->cp_l) * dcond;
                         dcond_tot += dcond;
                     }
-                    p->F[ATHAD_MC_S_U][c] = p->cp_l * T_u / p->s_0;
-                    p->F[ATHAD_C_U][c] = dcond_tot * p->F[ATHAD_M_U][c] / (smax(r_h_i, 0.01) * p->step[i]);
+                    su = p->cp_l * T_u / p->s_0;
+                    cu = dcond_tot * Mu / (smax(r_h_i, 0.01) * p->step[i]);
                 }
-                const double inv_a_u = 1.0 / (MC_A_U * p->u_0);
-                p->F[ATHAD_U_U][c] = p->F[ATHAD_U][c] + p->F[ATHAD_M_U][c] * inv_a_u / safe_r_humid(r_h_i);
-                const double cap = MC_W_CONV_MAX / p->u_0;
-                p->F[ATHAD_U_U][c] = smax(-cap, smin(p->F[ATHAD_U_U][c], cap));
-                if (p->F[ATHAD_Q_V_U][c] <= 0.0) p->F[ATHAD_Q_V_U][c] = 0.0;
-                if (p->F[ATHAD_Q_C_U][c] <= 0.0) p->F[ATHAD_Q_C_U][c] = 0.0;
-                if (p->F[ATHAD_Q_C_U][c] > MC_Q_C_U_MAX) p->F[ATHAD_Q_C_U][c] = MC_Q_C_U_MAX;
-                if (p->F[ATHAD_MC_S_U][c] <= 0.0) p->F[ATHAD_MC_S_U][c] = 0.0;
+                double uu = p->F[ATHAD_U][c] + Mu * inv_a_u / safe_r_humid(r_h_i);
+                uu = smax(-cap, smin(uu, cap));
+                if (qvu <= 0.0) qvu = 0.0;
+                if (qcu <= 0.0) qcu = 0.0;
+                if (qcu > MC_Q_C_U_MAX) qcu = MC_Q_C_U_MAX;
+                if (su <= 0.0) su = 0.0;
+                double eu = p->F[ATHAD_E_U][c], du = p->F[ATHAD_D_U][c], gp = p->F[ATHAD_G_P][c];
                 if (t_u <= MC_T00) {
-                    p->F[ATHAD_E_U][c] = 0.0; p->F[ATHAD_D_U][c] = 0.0; p->F[ATHAD_M_U][c] = 0.0;
-                    p->F[ATHAD_Q_V_U][c] = 0.0; p->F[ATHAD_Q_C_U][c] = 0.0;
-                    p->F[ATHAD_U_U][c] = 0.0; p->F[ATHAD_V_U][c] = 0.0; p->F[ATHAD_W_U][c] = 0.0;
-                    p->F[ATHAD_MC_S_U][c] = 1.0;
-                    p->F[ATHAD_G_P][c] = 0.0; p->F[ATHAD_C_U][c] = 0.0; p->F[ATHAD_E_L][c] = 0.0;
+                    eu = 0.0; du = 0.0; Mu = 0.0;
+                    qvu = 0.0; qcu = 0.0;
+                    uu = 0.0; vu = 0.0; wu = 0.0;
+                    su = 1.0;
+                    gp = 0.0; cu = 0.0;
+                    p->F[ATHAD_E_U][c] = 0.0; p->F[ATHAD_D_U][c] = 0.0; p->F[ATHAD_G_P][c] = 0.0;
+                    p->F[ATHAD_E_L][c] = 0.0;
                 }
+                p->F[ATHAD_M_U][c] = Mu;
+                p->F[ATHAD_Q_V_U][c] = qvu; p->F[ATHAD_Q_C_U][c] = qcu;
+                p->F[ATHAD_V_U][c] = vu; p->F[ATHAD_W_U][c] = wu;
+                p->F[ATHAD_MC_S_U][c] = su; p->F[ATHAD_C_U][c] = cu; p->F[ATHAD_U_U][c] = uu;
+                Mu_m = Mu; qvu_m = qvu; qcu_m = qcu; vu_m = vu; wu_m = wu; su_m = su;
+                eu_m = eu; du_m = du; gp_m = gp;
             }
         }
 
@@ -519,53 +537,68 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
             }
         }
 
-        /* downdraftRecurrence, :1168-1254 (every column) */
-        for (int i = i_lfs - 1; i >= 0; i--) {
-            const long long c = IDX(i, j, k), cp = IDX(i + 1, j, k);
-            const double t_u = p->F[ATHAD_T][c] * t_0;
-            const double step_ip1 = p->step[i + 1];
-            const double r_h_ip1 = p->F[ATHAD_R_HUMID][cp], r_h_i = p->F[ATHAD_R_HUMID][c];
-            const double d_Md = p->F[ATHAD_E_D][c] - p->F[ATHAD_D_D][c];
-            p->F[ATHAD_M_D][c] = clamp_M(p->F[ATHAD_M_D][cp] - d_Md * step_ip1);
-            if (t_u <= MC_T00M2) p->F[ATHAD_M_D][c] = 0.0;
-            const double L_latent = (t_u >= t_0) ? p->lv : p->ls;
-            const double M_d_ip1 = p->F[ATHAD_M_D][cp];
-            const double dq_v = M_d_ip1 * p->F[ATHAD_Q_V_D][cp]
-                - step_ip1 * (p->F[ATHAD_E_D][cp] * p->F[ATHAD_C][cp] - p->F[ATHAD_D_D][cp] * p->F[ATHAD_Q_V_D][cp]
-                              + r_h_ip1 * p->F[ATHAD_E_DD][cp]);
-            const double dv = M_d_ip1 * p->F[ATHAD_V_D][cp]
-                - step_ip1 * (p->F[ATHAD_E_D][cp] * p->F[ATHAD_V][cp] - p->F[ATHAD_D_D][cp] * p->F[ATHAD_V_D][cp]);
-            const double dw = M_d_ip1 * p->F[ATHAD_W_D][cp]
-                - step_ip1 * (p->F[ATHAD_E_D][cp] * p->F[ATHAD_W][cp] - p->F[ATHAD_D_D][cp] * p->F[ATHAD_W_D][cp]);
-            const double ds = (M_d_ip1 * p->F[ATHAD_MC_S_D][cp]
-                - step_ip1 * (p->F[ATHAD_E_D][cp] * p->F[ATHAD_MC_S][cp] - p->F[ATHAD_D_D][cp] * p->F[ATHAD_MC_S_D][cp]
-                              - L_latent * r_h_ip1 * p->F[ATHAD_E_DD][cp])) / p->s_0;
-            const double M_d_i = p->F[ATHAD_M_D][c];
-            if (fabs(M_d_i) > MC_COEFF_RECURR) {
-                const double inv = 1.0 / M_d_i;
-                p->F[ATHAD_Q_V_D][c] = dq_v * inv;
-                p->F[ATHAD_V_D][c] = dv * inv;
-                p->F[ATHAD_W_D][c] = dw * inv;
-                p->F[ATHAD_MC_S_D][c] = ds * inv;
-            } else {
-                p->F[ATHAD_Q_V_D][c] = p->F[ATHAD_C][c];
-                p->F[ATHAD_V_D][c] = p->F[ATHAD_V][c];
-                p->F[ATHAD_W_D][c] = p->F[ATHAD_W][c];
-                p->F[ATHAD_MC_S_D][c] = p->F[ATHAD_MC_S][c];
-            }
+        /* downdraftRecurrence, :1168-1254 (every column).  The downdraft values of level
+           i+1 that level i reads are carried in registers, as in the updraft recurrence. */
+        {
+            const long long c0 = IDX(i_lfs, j, k);
+            double Md_p = p->F[ATHAD_M_D][c0], qvd_p = p->F[ATHAD_Q_V_D][c0];
+            double vd_p = p->F[ATHAD_V_D][c0], wd_p = p->F[ATHAD_W_D][c0], sd_p = p->F[ATHAD_MC_S_D][c0];
+            double ed_p = p->F[ATHAD_E_D][c0], dd_p = p->F[ATHAD_D_D][c0], edd_p = p->F[ATHAD_E_DD][c0];
+            double pconv_p = p->F[ATHAD_P_CONV][c0], rh_p = p->F[ATHAD_R_HUMID][c0];
             const double inv_a_d = 1.0 / (MC_A_D * p->u_0);
-            p->F[ATHAD_U_D][c] = p->F[ATHAD_U][c] + p->F[ATHAD_M_D][c] * inv_a_d / safe_r_humid(r_h_i);
-            if (p->F[ATHAD_Q_V_D][c] <= 0.0) p->F[ATHAD_Q_V_D][c] = 0.0;
-            if (p->F[ATHAD_MC_S_D][c] <= 0.0) p->F[ATHAD_MC_S_D][c] = 0.0;
-            if (t_u <= MC_T00) {
-                p->F[ATHAD_E_D][c] = 0.0; p->F[ATHAD_D_D][c] = 0.0; p->F[ATHAD_M_D][c] = 0.0;
-                p->F[ATHAD_Q_V_D][c] = 0.0;
-                p->F[ATHAD_U_D][c] = 0.0; p->F[ATHAD_V_D][c] = 0.0; p->F[ATHAD_W_D][c] = 0.0;
-                p->F[ATHAD_MC_S_D][c] = 1.0; p->F[ATHAD_E_DD][c] = 0.0; p->F[ATHAD_E_P][c] = 0.0;
+            for (int i = i_lfs - 1; i >= 0; i--) {
+                const long long c = IDX(i, j, k), cp = IDX(i + 1, j, k);
+                const double t_u = p->F[ATHAD_T][c] * t_0;
+                const double step_ip1 = p->step[i + 1];
+                const double r_h_ip1 = rh_p, r_h_i = p->F[ATHAD_R_HUMID][c];
+                double ed = p->F[ATHAD_E_D][c], dd = p->F[ATHAD_D_D][c];
+                const double d_Md = ed - dd;
+                double Md = clamp_M(Md_p - d_Md * step_ip1);
+                if (t_u <= MC_T00M2) Md = 0.0;
+                const double L_latent = (t_u >= t_0) ? p->lv : p->ls;
+                const double M_d_ip1 = Md_p;
+                const double dq_v = M_d_ip1 * qvd_p
+                    - step_ip1 * (ed_p * p->F[ATHAD_C][cp] - dd_p * qvd_p + r_h_ip1 * edd_p);
+                const double dv = M_d_ip1 * vd_p - step_ip1 * (ed_p * p->F[ATHAD_V][cp] - dd_p * vd_p);
+                const double dw = M_d_ip1 * wd_p - step_ip1 * (ed_p * p->F[ATHAD_W][cp] - dd_p * wd_p);
+                const double ds = (M_d_ip1 * sd_p
+                    - step_ip1 * (ed_p * p->F[ATHAD_MC_S][cp] - dd_p * sd_p - L_latent * r_h_ip1 * edd_p)) / p->s_0;
+                double qvd, vd, wd, sd;
+                if (fabs(Md) > MC_COEFF_RECURR) {
+                    const double inv = 1.0 / Md;
+                    qvd = dq_v * inv;
+                    vd = dv * inv;
+                    wd = dw * inv;
+                    sd = ds * inv;
+                } else {
+                    qvd = p->F[ATHAD_C][c];
+                    vd = p->F[ATHAD_V][c];
+                    wd = p->F[ATHAD_W][c];
+                    sd = p->F[ATHAD_MC_S][c];
+                }
+                double ud = p->F[ATHAD_U][c] + Md * inv_a_d / safe_r_humid(r_h_i);
+                if (qvd <= 0.0) qvd = 0.0;
+                if (sd <= 0.0) sd = 0.0;
+                double edd = p->F[ATHAD_E_DD][c], ep = p->F[ATHAD_E_P][c];
+                if (t_u <= MC_T00) {
+                    ed = 0.0; dd = 0.0; Md = 0.0;
+                    qvd = 0.0;
+                    ud = 0.0; vd = 0.0; wd = 0.0;
+                    sd = 1.0; edd = 0.0; ep = 0.0;
+                    p->F[ATHAD_E_D][c] = 0.0; p->F[ATHAD_D_D][c] = 0.0;
+                    p->F[ATHAD_E_DD][c] = 0.0; p->F[ATHAD_E_P][c] = 0.0;
+                }
+                p->F[ATHAD_M_D][c] = Md; p->F[ATHAD_Q_V_D][c] = qvd;
+                p->F[ATHAD_U_D][c] = ud; p->F[ATHAD_V_D][c] = vd; p->F[ATHAD_W_D][c] = wd;
+                p->F[ATHAD_MC_S_D][c] = sd;
+                double pconv = 0.0;
+                if (i > 0) {
+                    pconv = smax(0.0, pconv_p + p->step[i] * r_h_i * (p->F[ATHAD_G_P][c] - edd - ep));
+                    p->F[ATHAD_P_CONV][c] = pconv;
+                }
+                Md_p = Md; qvd_p = qvd; vd_p = vd; wd_p = wd; sd_p = sd;
+                ed_p = ed; dd_p = dd; edd_p = edd; pconv_p = pconv; rh_p = r_h_i;
             }
-            if (i > 0)
-                p->F[ATHAD_P_CONV][c] = smax(0.0, p->F[ATHAD_P_CONV][cp] + p->step[i] * p->F[ATHAD_R_HUMID][c]
-                                          * (p->F[ATHAD_G_P][c] - p->F[ATHAD_E_DD][c] - p->F[ATHAD_E_P][c]));
         }
         p->F[ATHAD_P_CONV][IDX(0, j, k)] = p->F[ATHAD_P_CONV][IDX(1, j, k)];
     }

@@ -109,7 +109,18 @@ ATHAD_HD double dqsat_dT(double T, double p, double M_other)   // :257-260
     return dqsat_dT_from(saturation_pressure_auto(T), latent_heat_auto(T), T, p, M_other);
 }
 
-// full moist lapse rate (SaturationH2O.h:280-293)
+// full moist lapse rate (SaturationH2O.h:280-293), with E = saturation_pressure_auto(T)
+// when the caller has formed it already
+ATHAD_HD double moist_lapse_E(double T, double E, double p, double M_other, double cp, double R_mix, double g)
+{
+    if (!(cp > 0.0) || !(T > 0.0) || !(R_mix > 0.0)) return 0.0;
+    const double A = sat_deriv_factor_at(E, p, M_other);
+    if (!(A > 0.0)) return g / cp;
+    const double L = latent_heat_auto(T);
+    const double num = 1.0 + L * A / (R_mix * T);
+    const double den = cp + L * L * A / (R_H2O * T * T);
+    return (den > 0.0) ? g * num / den : g / cp;
+}
 ATHAD_HD double moist_lapse(double T, double p, double M_other, double cp, double R_mix, double g)
 {
     if (!(cp > 0.0) || !(T > 0.0) || !(R_mix > 0.0)) return 0.0;

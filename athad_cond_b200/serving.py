@@ -88,7 +88,12 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int | None = None, max_slots: int = 64, dt: float = 4e-5,
                  use_graph: bool = True, shape: int | None = None, keep_fields=("t",),
-                 stream=None):
+                 stream=None, graph_after: int = 0, rebuild_every: int = 1):
+        """graph_after: iterations a batch runs without CUDA graphs before it captures them
+        (a batch that changes members every few iterations would capture every cadence
+        pattern anew each time).  rebuild_every: fewest iterations between two rebuilds of
+        the batch; runs that finish in between are set inactive and leave, and waiting
+        requests join, at the next rebuild."""
         import torch
         self.torch = torch
         self.lib = _abi.load_library()
@@ -107,6 +112,10 @@ class Server:
         self.batch: GpuBatch | None = None
         self.iterations = 0
         self.rebuilds = 0
+        self.graph_after = int(graph_after)
+        self.rebuild_every = max(1, int(rebuild_every))
+        self.since_rebuild = 0
+        self.host_s = {"admit": 0.0, "retire": 0.0, "rebuild": 0.0, "iteration": 0.0}
 
     # ---- admission ----
     def footprint(self, req: Request) -> int:
@@ -129,13 +138,15 @@ class Server:
         return True
 
     def _retire(self, run: _Run, now: float):
-        run.req.result = {n: run.ctx.download(n) for n in self.keep_fields}
+        if not run.req.result:
+            run.req.result = {n: run.ctx.download(n) for n in self.keep_fields}
         run.req.finished = now
         run.ctx.close()
         self.used -= run.footprint
         self.runs.remove(run)
 
     def _rebuild(self):
+        self.since_rebuild = 0
         if self.batch is not None:
             self.batch.close()
             self.batch = None
@@ -158,15 +169,32 @@ class Server:
         waiting: list = []
         pi = 0
         done = []
+        leaving: list = []     # finished, inactive in the batch until the next rebuild
+        clk = time.perf_counter
         while pi < len(pending) or waiting or self.runs:
             now = now_fn()
             while pi < len(pending) and pending[pi].arrival <= now:
                 waiting.append(pending[pi])
                 pi += 1
+            active = len(self.runs) - len(leaving)
+            may_rebuild = self.batch is None or active == 0 or self.since_rebuild >= self.rebuild_every
             changed = False
-            while waiting and self._admit(waiting[0], now):
-                waiting.pop(0)
-                changed = True
+            if may_rebuild:
+                if leaving:
+                    t = clk()
+                    if self.batch is not None:
+                        self.batch.close()
+                        self.batch = None
+                    for r in leaving:
+                        self._retire(r, r.req.finished)
+                    leaving = []
+                    changed = True
+                    self.host_s["retire"] += clk() - t
+                t = clk()
+                while waiting and self._admit(waiting[0], now):
+                    waiting.pop(0)
+                    changed = True
+                self.host_s["admit"] += clk() - t
             if not self.runs:
                 if waiting:
                     raise RuntimeError(f"request {waiting[0].rid} does not fit the HBM budget alone")
@@ -174,23 +202,37 @@ class Server:
                     time.sleep(max(0.0, min(0.05, pending[pi].arrival - now)))
                 continue
             if changed or self.batch is None:
+                t = clk()
                 self._rebuild()
-            self.batch.iteration(graph=self.use_graph)
+                self.host_s["rebuild"] += clk() - t
+            t = clk()
+            self.batch.iteration(graph=self.use_graph and self.since_rebuild >= self.graph_after)
+            self.host_s["iteration"] += clk() - t
             self.iterations += 1
+            self.since_rebuild += 1
             for r in self.runs:
-                r.next_iter += 1
-            finished = [r for r in self.runs if r.next_iter > r.req.steps]
+                if r not in leaving:
+                    r.next_iter += 1
+            finished = [r for r in self.runs if r not in leaving and r.next_iter > r.req.steps]
             if finished:
+                t = clk()
                 self.batch.synchronize()
                 now = now_fn()
                 for r in finished:
-                    self._retire(r, now)
+                    r.req.result = {n: r.ctx.download(n) for n in self.keep_fields}
+                    r.req.finished = now
+                    self.batch.set_active(self.runs.index(r), False)
+                    leaving.append(r)
                     done.append(r.req)
-                self._rebuild()
+                self.host_s["retire"] += clk() - t
         if self.batch is not None:
             self.batch.close()
             self.batch = None
-        return report(done, now_fn(), self.dt)
+        for r in leaving:
+            self._retire(r, r.req.finished)
+        rep = report(done, now_fn(), self.dt)
+        rep["host_seconds"] = dict(self.host_s)
+        return rep
 
 
 def report(done: list, wall: float, dt: float = 4e-5) -> dict:

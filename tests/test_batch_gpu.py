@@ -147,3 +147,46 @@ def test_batch_rejects_fp64_members_and_duplicates():
         GpuBatch([gm, gm])
     g64.close()
     gm.close()
+
+
+def test_configuration4_members_in_the_mix_equal_members_alone():
+    """Members drawn as the 64-member ensemble draws them (grids 21-41 x 61-181 x 121-361,
+    condition points over p_surf 40-100 bar and T_sea 503-523 K), each from the reference
+    initial state for its grid and condition point: six batched iterations (graph, the
+    cadence of each member's own iteration counter) equal the same iterations of each member
+    alone through the single-context entry points, bit for bit."""
+    from athad_cond_b200.ensemble import draw_ensemble, condition_params, init_config
+    specs = draw_ensemble(64)
+    largest = sorted(range(len(specs)), key=lambda q: -int(np.prod(specs[q].grid)))
+    picks = list(dict.fromkeys(largest[:2] + [0, 1, 2]))[:4]   # the two largest and the first
+    chosen = [specs[q] for q in picks]
+
+    def build(s):
+        g = GpuAtmosphere(*s.grid, condition_params(s.cond, Precision.MIXED))
+        g.initial_state(init_config(s.cond))
+        return g
+
+    first = [1, 2, 3, 4]
+    ms = [build(s) for s in chosen]
+    with GpuBatch(ms, first_iter=first) as b:
+        for _ in range(6):
+            b.iteration(graph=True)
+        b.synchronize()
+    for q, s in enumerate(chosen):
+        mix = {n: ms[q].download(n) for n in CHECK}
+        ms[q].close()
+        g = build(s)
+        for it in range(first[q], first[q] + 6):
+            if it % 4 == 0:
+                g.PressureSolverAtm_run(total_iter_count=it)
+            if it % 2 == 0:
+                g.SaturationAdjustment_run()
+                g.MoistConvection_run(it)
+                g.densities()
+            g.solveRungeKutta_Atmosphere_Turb(4e-5, 1.0, min(1.0, it / 300.0))
+            g.storeIntermediateData3D()
+        for n in CHECK:
+            a = g.download(n)
+            assert np.isfinite(mix[n]).all(), (s.grid, n)
+            assert np.array_equal(mix[n], a), (s.grid, n)
+        g.close()
