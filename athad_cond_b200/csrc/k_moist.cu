@@ -338,33 +338,41 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
                 p->F[ATHAD_Q_V_U][IDX(ib, j, k)] = smax(p->F[ATHAD_C][IDX(ib, j, k)] + dq_sfp, 0.0);
             }
             M_d_LFS = clamp_M(MC_GAM_D * p->F[ATHAD_M_U][IDX(ib, j, k)]);
+            double Mu_m = p->F[ATHAD_M_U][IDX(ib, j, k)];   // level i-1 as this loop left it
             for (int i = ib + 1; i <= il; i++) {
                 const long long c = IDX(i, j, k);
                 const double height_i = p->height[i];
                 const double t_u = p->F[ATHAD_T][c] * t_0, r_h_i = p->F[ATHAD_R_HUMID][c];
                 double dcdr, dcdthe, dcdphi, c_ijk;
                 entrainment_gradients(X, i, j, k, &dcdr, &dcdthe, &dcdphi, &c_ijk);
+                const double Mu_c = p->F[ATHAD_M_U][c];   // the previous pass's mass flux here
+                double eu;
                 if ((pb - pl) >= MC_F_DIFF * p0)
-                    p->F[ATHAD_E_U][c] = -r_h_i / c_ijk * (p->F[ATHAD_U][c] * dcdr + p->F[ATHAD_V][c] * dcdthe + p->F[ATHAD_W][c] * dcdphi)
-                                 + MC_EPS_U * p->F[ATHAD_M_U][c];
+                    eu = -r_h_i / c_ijk * (p->F[ATHAD_U][c] * dcdr + p->F[ATHAD_V][c] * dcdthe + p->F[ATHAD_W][c] * dcdphi)
+                         + MC_EPS_U * Mu_c;
                 else
-                    p->F[ATHAD_E_U][c] = 0.0;
-                if (t_u <= MC_T00M2) p->F[ATHAD_E_U][c] = 0.0;
-                p->F[ATHAD_D_U][c] = (i <= il) ? MC_EPS_U * p->F[ATHAD_M_U][c] : 0.0;
+                    eu = 0.0;
+                if (t_u <= MC_T00M2) eu = 0.0;
+                double du = (i <= il) ? MC_EPS_U * Mu_c : 0.0;
                 if (ip > 1 && i == il)
-                    p->F[ATHAD_D_U][c] = MC_DEL_U * p->F[ATHAD_M_U][c] + MC_B_U * p->F[ATHAD_M_U][c] / p->step[i];
+                    du = MC_DEL_U * Mu_c + MC_B_U * Mu_c / p->step[i];
                 if (ip > 1 && i == il - 1)
-                    p->F[ATHAD_D_U][c] = MC_DEL_U * p->F[ATHAD_M_U][c] + (1.0 - MC_B_U) * p->F[ATHAD_M_U][c] / p->step[i];
-                if (t_u <= MC_T00M2) p->F[ATHAD_D_U][c] = 0.0;
-                const double d_Mu = p->F[ATHAD_E_U][c] - p->F[ATHAD_D_U][c];
-                p->F[ATHAD_M_U][c] = clamp_M(p->F[ATHAD_M_U][IDX(i - 1, j, k)] + d_Mu * p->step[i]);
+                    du = MC_DEL_U * Mu_c + (1.0 - MC_B_U) * Mu_c / p->step[i];
+                if (t_u <= MC_T00M2) du = 0.0;
+                const double d_Mu = eu - du;
+                const double Mu = clamp_M(Mu_m + d_Mu * p->step[i]);
+                p->F[ATHAD_E_U][c] = eu;
+                p->F[ATHAD_D_U][c] = du;
+                p->F[ATHAD_M_U][c] = Mu;
+                Mu_m = Mu;
                 p->F[ATHAD_C_U][c] = 0.0;
                 if (ip == 1) {
                     p->F[ATHAD_E_L][c] = 0.0;
                 } else {
                     const double r_h_floor = smax(r_h_i, 0.01);
-                    p->F[ATHAD_E_L][c] = p->F[ATHAD_D_U][c] * p->F[ATHAD_Q_C_U][c] / r_h_floor;
-                    if (p->F[ATHAD_E_L][c] <= 0.0) p->F[ATHAD_E_L][c] = 0.0;
+                    double el = du * p->F[ATHAD_Q_C_U][c] / r_h_floor;
+                    if (el <= 0.0) el = 0.0;
+                    p->F[ATHAD_E_L][c] = el;
                 }
                 const double K_p = (height_i > height_base + delta_i_c) ? MC_BET_P : 0.0;
                 if (t_u >= t_0) p->F[ATHAD_G_P][c] = (ip == 1) ? 0.0 : K_p * p->F[ATHAD_Q_C_U][c];
@@ -610,28 +618,33 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
         p->F[ATHAD_M_U][c] = !is_finite_bits(vu) ? 0.0 : (vu < -3.0) ? -3.0 : (vu > 3.0) ? 3.0 : vu;
         p->F[ATHAD_M_D][c] = !is_finite_bits(vd) ? 0.0 : (vd < -3.0) ? -3.0 : (vd > 3.0) ? 3.0 : vd;
     }
+    // the four mass fluxes at a level; level i+1's are level i's upper fluxes and the next
+    // level's lower ones, so each is formed once and carried (same operands, same values)
+    auto flux_at = [&](long long c, double& fs, double& fq, double& fv, double& fw) {
+        const double Mu = p->F[ATHAD_M_U][c], Md = p->F[ATHAD_M_D][c];
+        fs = Mu * (p->F[ATHAD_MC_S_U][c] - p->F[ATHAD_MC_S][c]) + Md * (p->F[ATHAD_MC_S_D][c] - p->F[ATHAD_MC_S][c]);
+        fq = Mu * (p->F[ATHAD_Q_V_U][c] - p->F[ATHAD_C][c]) + Md * (p->F[ATHAD_Q_V_D][c] - p->F[ATHAD_C][c]);
+        fv = Mu * (p->F[ATHAD_V_U][c] - p->F[ATHAD_V][c]) + Md * (p->F[ATHAD_V_D][c] - p->F[ATHAD_V][c]);
+        fw = Mu * (p->F[ATHAD_W_U][c] - p->F[ATHAD_W][c]) + Md * (p->F[ATHAD_W_D][c] - p->F[ATHAD_W][c]);
+    };
+    double fs0, fq0, fv0, fw0;
+    flux_at(IDX(0, j, k), fs0, fq0, fv0, fw0);
     for (int i = 0; i < im - 1; i++) {
         const long long c = IDX(i, j, k), cp = IDX(i + 1, j, k);
         const double L_latent = (p->F[ATHAD_T][c] * t_0 >= t_0) ? p->lv : p->ls;
         const double inv_step_rh = 1.0 / (p->step[i] * smax(p->F[ATHAD_R_HUMID][c], 0.01));
-        const double Mu1 = p->F[ATHAD_M_U][cp], Md1 = p->F[ATHAD_M_D][cp], Mu0 = p->F[ATHAD_M_U][c], Md0 = p->F[ATHAD_M_D][c];
-        const double fs1 = Mu1 * (p->F[ATHAD_MC_S_U][cp] - p->F[ATHAD_MC_S][cp]) + Md1 * (p->F[ATHAD_MC_S_D][cp] - p->F[ATHAD_MC_S][cp]);
-        const double fs0 = Mu0 * (p->F[ATHAD_MC_S_U][c] - p->F[ATHAD_MC_S][c]) + Md0 * (p->F[ATHAD_MC_S_D][c] - p->F[ATHAD_MC_S][c]);
+        double fs1, fq1, fv1, fw1;
+        flux_at(cp, fs1, fq1, fv1, fw1);
         const double conv_src = p->F[ATHAD_C_U][c] - p->F[ATHAD_E_DD][c] - p->F[ATHAD_E_L][c] - p->F[ATHAD_E_P][c];
         double v = -(fs1 - fs0) * inv_step_rh * t_0 + (L_latent / p->cp_l) * conv_src * t_0;
         p->F[ATHAD_MC_T][c] = !is_finite_bits(v) ? 0.0 : (v < -0.01) ? -0.01 : (v > 0.01) ? 0.01 : v;
-        const double fq1 = Mu1 * (p->F[ATHAD_Q_V_U][cp] - p->F[ATHAD_C][cp]) + Md1 * (p->F[ATHAD_Q_V_D][cp] - p->F[ATHAD_C][cp]);
-        const double fq0 = Mu0 * (p->F[ATHAD_Q_V_U][c] - p->F[ATHAD_C][c]) + Md0 * (p->F[ATHAD_Q_V_D][c] - p->F[ATHAD_C][c]);
         v = -(fq1 - fq0) * inv_step_rh - conv_src;
         p->F[ATHAD_MC_Q][c] = !is_finite_bits(v) ? 0.0 : (v < -2.0e-5) ? -2.0e-5 : (v > 2.0e-5) ? 2.0e-5 : v;
-        const double fv1 = Mu1 * (p->F[ATHAD_V_U][cp] - p->F[ATHAD_V][cp]) + Md1 * (p->F[ATHAD_V_D][cp] - p->F[ATHAD_V][cp]);
-        const double fv0 = Mu0 * (p->F[ATHAD_V_U][c] - p->F[ATHAD_V][c]) + Md0 * (p->F[ATHAD_V_D][c] - p->F[ATHAD_V][c]);
         v = -(fv1 - fv0) * inv_step_rh * p->u_0;
         p->F[ATHAD_MC_V][c] = !is_finite_bits(v) ? 0.0 : (v < -0.01) ? -0.01 : (v > 0.01) ? 0.01 : v;
-        const double fw1 = Mu1 * (p->F[ATHAD_W_U][cp] - p->F[ATHAD_W][cp]) + Md1 * (p->F[ATHAD_W_D][cp] - p->F[ATHAD_W][cp]);
-        const double fw0 = Mu0 * (p->F[ATHAD_W_U][c] - p->F[ATHAD_W][c]) + Md0 * (p->F[ATHAD_W_D][c] - p->F[ATHAD_W][c]);
         v = -(fw1 - fw0) * inv_step_rh * p->u_0;
         p->F[ATHAD_MC_W][c] = !is_finite_bits(v) ? 0.0 : (v < -0.01) ? -0.01 : (v > 0.01) ? 0.01 : v;
+        fs0 = fs1; fq0 = fq1; fv0 = fv1; fw0 = fw1;
     }
 }
 

@@ -42,6 +42,27 @@ __device__ __forceinline__ float fminmod(float a, float b)
     return (a * b <= 0.0f) ? 0.0f : (fabsf(a) < fabsf(b) ? a : b);
 }
 
+// Single-use operands of a stage can be loaded with the streaming hint so they do not
+// displace the stencil fields' lines from L1: ATHAD_RK4M_STREAM bit 1 the time level n, bit 2
+// the packed forcing, bit 4 the accumulator.  Off: all three on made the mixed step 2 %
+// slower at 41x181x361 (1.033 -> 1.055 ms; the FP64 step gains and uses it, k_rk4.cu).
+#ifndef ATHAD_RK4M_STREAM
+#define ATHAD_RK4M_STREAM 0
+#endif
+template <int BIT, class T>
+__device__ __forceinline__ T ld_single(const T* p)
+{
+    if (ATHAD_RK4M_STREAM & BIT) return __ldcs(p);
+    return __ldg(p);
+}
+// the accumulator, which the launch also writes (same thread, same cell): a coherent load
+template <class T>
+__device__ __forceinline__ T ld_acc(const T* p)
+{
+    if (ATHAD_RK4M_STREAM & 4) return __ldcs(p);
+    return *p;
+}
+
 struct StarF {
     float c, ip, im, jp, jm, kp, km;
 };
@@ -88,7 +109,7 @@ template <int STAGE>
 __device__ __forceinline__ void stage_update(const RK4MArgs& a, int n, long long c, float kn)
 {
     if (STAGE == 1) {
-        const double yn = __ldg(a.Yn[n] + c);
+        const double yn = ld_single<1>(a.Yn[n] + c);
         a.Yn32[n][c] = (float)yn;
         a.K[n][c] = kn;
         double y = yn + (double)kn * a.half_dt;
@@ -97,16 +118,16 @@ __device__ __forceinline__ void stage_update(const RK4MArgs& a, int n, long long
         else if (n == 10) y = smax(1.0e-10, y);
         a.Yout[n][c] = (float)y;
     } else if (STAGE < 4) {
-        const float yn = __ldg(a.Yn32[n] + c);
-        a.K[n][c] = a.K[n][c] + 2.0f * kn;
+        const float yn = ld_single<1>(a.Yn32[n] + c);
+        a.K[n][c] = ld_acc(a.K[n] + c) + 2.0f * kn;
         float y = yn + kn * ((STAGE == 3) ? a.dt_f : a.half_dt_f);
         if (n >= 4 && n <= 7) y = fmaxs(0.0f, y);
         else if (n == 9) y = isfinite(y) ? fclamps(y, 0.0f, a.tke_max_nd) : 0.0f;
         else if (n == 10) y = fmaxs(1.0e-10f, y);
         a.Yout[n][c] = y;
     } else {
-        const double yn = __ldg(a.Yn[n] + c);
-        const float kk = a.K[n][c] + kn;
+        const double yn = ld_single<1>(a.Yn[n] + c);
+        const float kk = ld_acc(a.K[n] + c) + kn;
         double y = yn + (double)kk * a.dt_sixth;
         if (n >= 4 && n <= 7) y = smax(0.0, y);
         else if (n == 9) y = safe_clamp(y, 0.0, (double)a.tke_max_nd);
@@ -125,7 +146,7 @@ __device__ __forceinline__ float forcing(const RK4MArgs& a, int f, long long c, 
         a.F[f][c] = v;
         return v;
     }
-    return __ldg(a.F[f] + c);
+    return ld_single<2>(a.F[f] + c);
 }
 
 }  // namespace

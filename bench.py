@@ -59,8 +59,8 @@ RK4_BYTES_PER_POINT = {0: 8 * (1 + 59 + 70 + 70 + 62 + 11), 1: 8 + 472 + 264 + 2
 # sweep): source 24 + 8, sweep 24, ceiling 8
 PRESSURE_BYTES_PER_POINT = 64
 # DRAM bytes (read + write) of one RK4 step (level mean and the four stage launches, the
-# time-level copy fused) measured by ncu (profiles/rk4_stage_41x181x361.md): per form, grid
-RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.871e9, ("mixed", (41, 181, 361)): 3.871e9}
+# time-level copy fused) measured by ncu (one capture of each form's stage launches): per form, grid
+RK4_TRAFFIC = {("fp64", (41, 181, 361)): 6.680e9, ("mixed", (41, 181, 361)): 3.880e9}
 # fields compared between the two forms after the timed iterations: the 11 prognostics and
 # the diagnosed pressure and densities
 ERR_FIELDS = ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
@@ -188,7 +188,7 @@ def cpu_baseline(seconds_budget: float = 20.0):
                       f"(-O2, 1 thread), {el:.1f} s"}
 
 
-def reference_arm(args):
+def time_reference(max_iter: int = 4, budget_s: float | None = None):
     """The reference's own CPU implementation of the path, timed on this host's cores.
 
     The reference is built from its sources into oracle/_ref/stock with its own Makefile
@@ -198,56 +198,65 @@ def reference_arm(args):
     time-level copy every iteration), with all host threads.  It supports only its
     compiled-in 61 x 181 x 361 grid, so the sample runs there; the metric is per grid point.
     A bounded sample of iterations (at least two, so one moist iteration is included) keeps
-    the run within a few minutes.  Without the built reference it times the oracle instead."""
+    the run within a few minutes.  Returns (value, threads, sample, kind, grid), or None
+    without the built reference."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import ref_binding
-    metric = "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)"
     if not ref_binding.available("stock"):
+        return None
+    threads = len(os.sched_getaffinity(0))
+    cwd = os.getcwd()
+    os.chdir(os.environ.get("TMPDIR", "/tmp"))
+    # the reference prints its progress with printf; keep stdout for the JSON line
+    sys.stdout.flush()
+    saved_fd = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        R = ref_binding.Reference("stock", threads=threads)
+        t0 = time.perf_counter()
+        R.init_state()
+        t_init = time.perf_counter() - t0
+        im, jm, km = R.shape
+        it, el = 0, 0.0
+        budget = float(os.environ.get("ATHAD_REF_BUDGET_S", "90")) if budget_s is None else budget_s
+        t0 = time.perf_counter()
+        while True:
+            it += 1
+            R.set_scalars(4e-5, 1.0, min(1.0, it / 300.0), it, it)
+            if it % 4 == 0:
+                R.lib.ref_pressure(R.h)
+            if it % 2 == 0:
+                R.lib.ref_satadj(R.h)
+                R.lib.ref_moist(R.h, it)
+                R.lib.ref_densities(R.h, 0)
+            R.lib.ref_rk4(R.h)
+            R.lib.ref_store(R.h)
+            el = time.perf_counter() - t0
+            if it >= 2 and (el >= budget or it >= max_iter):
+                break
+        R.close()
+    finally:
+        os.dup2(saved_fd, 1)
+        os.close(saved_fd)
+        os.close(devnull)
+        os.chdir(cwd)
+    sample = (f"{it} model iterations of the reference's own {im}x{jm}x{km} grid through its own "
+              f"functions, built with its Makefile flags (-ffast-math, no -O), OMP_NUM_THREADS={threads}, "
+              f"{el:.1f} s (initial state {t_init:.1f} s, not timed)")
+    return im * jm * km * it / el, threads, sample, "reference", [im, jm, km]
+
+
+def reference_arm(args):
+    """The reference arm: the reference's own CPU path (time_reference); without the built
+    reference it times the oracle instead."""
+    metric = "grid-point RK4 steps/s (model iteration of the hot path, reference cadence)"
+    r = time_reference()
+    if r is None:
         b = cpu_baseline(seconds_budget=20.0)
         val, cores, sample, kind, grid = b["value"], 1, b["sample"], "port", list(GRID)
     else:
-        threads = len(os.sched_getaffinity(0))
-        cwd = os.getcwd()
-        os.chdir(os.environ.get("TMPDIR", "/tmp"))
-        # the reference prints its progress with printf; keep stdout for the JSON line
-        sys.stdout.flush()
-        saved_fd = os.dup(1)
-        devnull = os.open(os.devnull, os.O_WRONLY)
-        os.dup2(devnull, 1)
-        try:
-            R = ref_binding.Reference("stock", threads=threads)
-            t0 = time.perf_counter()
-            R.init_state()
-            t_init = time.perf_counter() - t0
-            im, jm, km = R.shape
-            it, el = 0, 0.0
-            budget = float(os.environ.get("ATHAD_REF_BUDGET_S", "90"))
-            t0 = time.perf_counter()
-            while True:
-                it += 1
-                R.set_scalars(4e-5, 1.0, min(1.0, it / 300.0), it, it)
-                if it % 4 == 0:
-                    R.lib.ref_pressure(R.h)
-                if it % 2 == 0:
-                    R.lib.ref_satadj(R.h)
-                    R.lib.ref_moist(R.h, it)
-                    R.lib.ref_densities(R.h, 0)
-                R.lib.ref_rk4(R.h)
-                R.lib.ref_store(R.h)
-                el = time.perf_counter() - t0
-                if it >= 2 and (el >= budget or it >= 4):
-                    break
-            R.close()
-        finally:
-            os.dup2(saved_fd, 1)
-            os.close(saved_fd)
-            os.close(devnull)
-            os.chdir(cwd)
-        val = im * jm * km * it / el
-        cores, kind, grid = threads, "reference", [im, jm, km]
-        sample = (f"{it} model iterations of the reference's own {im}x{jm}x{km} grid through its own "
-                  f"functions, built with its Makefile flags (-ffast-math, no -O), OMP_NUM_THREADS={threads}, "
-                  f"{el:.1f} s (initial state {t_init:.1f} s, not timed)")
+        val, cores, sample, kind, grid = r
     line = {"impl": "reference", "metric": metric, "value": val, "unit": "grid-point steps/s",
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "dtype": "f64", "data": "the reference initial state",
@@ -631,6 +640,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-envelope", action="store_true",
                     help="skip the FP64 one-ulp sensitivity run of the error report")
+    ap.add_argument("--no-native-reference", action="store_true",
+                    help="skip timing the reference itself beside the native-grid leg")
     ap.add_argument("--native-steps", type=int, default=100,
                     help="iterations of the leg on the reference's own 61x181x361 grid (0: skip)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
@@ -736,6 +747,15 @@ def main():
                          "e2e": rr["e2e_value"], "finite": rr["finite"]}
         native["grid"] = list(NATIVE_GRID)
         native["steps"] = args.native_steps
+        if rank == 0 and world == 1 and not args.no_native_reference:
+            # the reference itself on the same grid, state and cadence (four iterations, one
+            # full cadence cycle, on all host cores): the like-for-like ratio of this leg
+            r = time_reference(max_iter=4, budget_s=1.0e9)
+            if r is not None:
+                native["reference"] = {"value": r[0], "cores": r[1], "sample": r[2]}
+                native["vs_reference_native"] = {
+                    f"{f}_{k}": native[f][k] / r[0] for f in wanted for k in ("value", "e2e")
+                    if native[f].get(k)}
     base = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     if world > 1:
         import torch.distributed as tdist

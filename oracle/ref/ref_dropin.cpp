@@ -103,6 +103,25 @@ int dropin_resident(void* model, int n, int first_iter, int wall, double* residu
     return 0;
 }
 
+// the athad_params the adapter builds from the model (athad_dropin::params_from)
+void dropin_params(void* model, int wall, athad_params* out)
+{
+    *out = athad_dropin::params_from(*(cAtmosphereModel*)model, wall ? ATHAD_WALL_REFERENCE : ATHAD_WALL_MIRROR);
+}
+
+// the model's loop scalars the resident loop reads: dt_visc, buoyancy_ramp_iters,
+// t_skin_relax, checkpoint, total_iter_count, t_skin
+void dropin_loop_scalars(void* model, double* out)
+{
+    cAtmosphereModel* m = (cAtmosphereModel*)model;
+    out[0] = m->dt_visc;
+    out[1] = (double)m->buoyancy_ramp_iters;
+    out[2] = m->t_skin_relax;
+    out[3] = (double)m->checkpoint;
+    out[4] = (double)m->total_iter_count;
+    out[5] = m->t_skin;
+}
+
 // the model's budget references: m_q_co2_ref, m_q_h2o_ref, m_q_h2o_fixed_ref
 void dropin_budget_refs(void* model, double* out)
 {

@@ -131,6 +131,24 @@ class Reference:
             raise RuntimeError(err.value.decode())
         return res, skin
 
+    def dropin_params(self, wall: int = 0):
+        """The athad_params the C++ adapter builds from this model."""
+        from athad_cond_b200._abi import Params
+        p = Params()
+        f = self.lib.dropin_params
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Params)]
+        f(self.h, wall, ctypes.byref(p))
+        return p
+
+    def loop_scalars(self) -> dict:
+        """The model's scalars the resident loop reads."""
+        out = np.zeros(6)
+        f = self.lib.dropin_loop_scalars
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        f(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return {"dt": out[0], "buoyancy_ramp_iters": int(out[1]), "t_skin_relax": out[2],
+                "checkpoint": int(out[3]), "total_iter_count": int(out[4]), "t_skin": out[5]}
+
     def post_rk4_filters(self):
         self.lib.ref_post_rk4_filters(self.h)
 

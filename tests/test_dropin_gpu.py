@@ -287,21 +287,24 @@ def test_dropin_resident_loop_equals_the_device_loop(model):
     (the momentum-budget capture) included.  The residuum and the skin temperature each
     iteration reports agree too."""
     from athad_cond_b200 import GpuAtmosphere
-    from athad_cond_b200._abi import config_params
     from athad_cond_b200.loop import ModelLoop
     R, snap = model
     reset(R, snap)
     two = {n: R.get2(n) for n in F2D}
     prof = {n: R.getp(n) for n in ("t_ref_level", "rho_base", "dlnrho_dr")}
+    sc = R.loop_scalars()          # what the resident loop takes from the model
     n_iter = 20
-    with GpuAtmosphere(*R.shape, config_params()) as g:
+    with GpuAtmosphere(*R.shape, R.dropin_params()) as g:
         g.upload_state(dict(snap))
         for n, a in two.items():
             g.upload_2d(n, a)
         for n, a in prof.items():
             if a is not None:
                 g.upload_profile(n, a)
-        loop = ModelLoop(g)
+        loop = ModelLoop(g, dt=sc["dt"], buoyancy_ramp_iters=sc["buoyancy_ramp_iters"],
+                         t_skin_relax=sc["t_skin_relax"], tropopause_layers=R.tropopause_layers(),
+                         checkpoint=sc["checkpoint"])
+        loop.total_iter_count = sc["total_iter_count"]
         reps = loop.run(n_iter)
         want = {n: g.download(n) for n in FIELD_NAMES}
     res, skin = R.resident(n_iter)
