@@ -188,6 +188,10 @@ athad_status athad_batch_create(athad_ctx* const* members, int32_t n_members, co
         for (int r = 0; r < q; r++)
             if (members[r] == members[q]) return ATHAD_ERR_INVALID;
     }
+    // the batch runs the members on its own streams: what is queued on theirs (an initial
+    // state, an upload) must be complete first
+    for (int q = 0; q < n_members; q++)
+        if (cudaStreamSynchronize(members[q]->stream) != cudaSuccess) { cudaGetLastError(); return ATHAD_ERR_CUDA; }
     athad_batch* b = new (std::nothrow) athad_batch();
     if (!b) return ATHAD_ERR_OOM;
     b->m.assign(members, members + n_members);

@@ -567,7 +567,8 @@ typedef struct athad_batch_step {
 
 /* members: n_members distinct MIXED contexts on the current device; first_iter: each
  * member's next iteration number (NULL = all 1).  The batch holds small device tables
- * only. */
+ * only.  Creation waits for the work already queued on the members' streams (an initial
+ * state being built, an upload), since the batch runs the members on its own streams. */
 athad_status athad_batch_create(athad_ctx* const* members, int32_t n_members,
                                 const athad_batch_step* step, const int32_t* first_iter,
                                 athad_batch** out);
