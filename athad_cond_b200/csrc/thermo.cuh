@@ -188,17 +188,53 @@ ATHAD_HD double x_H2O_of(double c, double co2, double M_b)
 
 // SaturationH2O::dewPoint (SaturationH2O.h:189-202): bisection of the saturation curve
 // (liquid above the triple point, ice below) on [150 K, T_crit], 60 halvings
+// d ln p_sat / dT of saturation_pressure_auto, for the dew point's Newton step: the
+// Wagner-Pruss line above the triple point (ln p = ln p_c + (T_c/T) S(theta)), the IAPWS
+// sublimation curve below it (ln p = ln p_t + sum b_i vartheta^(m_i - 1))
+ATHAD_HD double dlnp_sat_dT(double T)
+{
+    if (T >= T_TRIPLE) {
+        const double theta = 1.0 - T / T_CRIT;
+        const double sq = sqrt(theta);
+        const double t2 = theta * theta, t3 = t2 * theta;
+        const double S = -7.85951783 * theta + 1.84408259 * theta * sq + -11.7866497 * t3
+                       + 22.6807411 * t3 * sq + -15.9618719 * t3 * theta + 1.80122502 * t3 * t3 * theta * sq;
+        const double dS = -7.85951783 + 1.5 * 1.84408259 * sq + 3.0 * -11.7866497 * t2
+                        + 3.5 * 22.6807411 * t2 * sq + 4.0 * -15.9618719 * t3 + 7.5 * 1.80122502 * t3 * t3 * sq;
+        return -(T_CRIT / (T * T)) * S - dS / T;
+    }
+    const double th = T / T_TRIPLE;
+    const double lt = log(th);
+    return (-0.212144006e2 * (0.333333333e-2 - 1.0) * exp((0.333333333e-2 - 2.0) * lt)
+            + 0.273203819e2 * (0.120666667e1 - 1.0) * exp((0.120666667e1 - 2.0) * lt)
+            + -0.610598130e1 * (0.170333333e1 - 1.0) * exp((0.170333333e1 - 2.0) * lt)) / T_TRIPLE;
+}
+
+// SaturationH2O::dewPoint (the temperature whose saturation pressure is e): the reference
+// bisects [150 K, T_crit] 60 times; here a Newton iteration on ln p_sat(T) = ln e, kept
+// inside the bisection bracket it narrows (a step leaving it bisects instead), stops when a
+// step moves T by under 1e-12 K.  Both end at the root to within a few ulps; the same
+// results below 150 K, at and above the critical pressure and for e <= 0.
 ATHAD_HD double dew_point(double e)
 {
     if (!(e > 0.0)) return 0.0;
     if (e >= 220640.0) return T_CRIT;
     double lo = 150.0, hi = T_CRIT;
     if (saturation_pressure_auto(lo) >= e) return lo;
+    const double ln_e = log(e);
+    // Clausius-Clapeyron start from the triple point (6.11657 hPa; L/R_v = 2.5e6 / 461.5 K)
+    double T = 1.0 / (1.0 / T_TRIPLE - log(e / 6.11657) / (2.5e6 / 461.5));
+    if (!(T > lo && T < hi)) T = 0.5 * (lo + hi);
     for (int it = 0; it < 60; it++) {
-        const double mid = 0.5 * (lo + hi);
-        if (saturation_pressure_auto(mid) < e) lo = mid; else hi = mid;
+        const double p = saturation_pressure_auto(T);
+        if (p < e) lo = T; else hi = T;
+        double Tn = T - (log(p) - ln_e) / dlnp_sat_dT(T);
+        if (fabs(Tn - T) <= 1.0e-12 && Tn >= lo && Tn <= hi) return Tn;   // converged
+        if (!(Tn > lo && Tn < hi)) Tn = 0.5 * (lo + hi);
+        T = Tn;
+        if (hi - lo <= 1.0e-12) break;
     }
-    return 0.5 * (lo + hi);
+    return T;
 }
 
 }  // namespace thermo
