@@ -31,9 +31,10 @@ __global__ void __launch_bounds__(128) zonal_rows_kernel(FilterArgs a, int nfiel
     const int np = const_passes >= 0 ? const_passes : a.polar_passes[j];
     if (np == 0) return;
     double* x = a.field[q] + idx3(d, i, j, 0);
+    const double* xs = a.src[q] ? a.src[q] + idx3(d, i, j, 0) : x;
     double* b0 = row;
     double* b1 = row + d.km;
-    for (int k = threadIdx.x; k < d.km; k += blockDim.x) b0[k] = x[k];
+    for (int k = threadIdx.x; k < d.km; k += blockDim.x) b0[k] = xs[k];
     __syncthreads();
     for (int pass = 0; pass < np; pass++) {
         for (int k = threadIdx.x; k < d.km; k += blockDim.x) {
@@ -113,8 +114,8 @@ void launch_damp_wiggles(const Dims& d, double* f, double* scratch, cudaStream_t
     FilterArgs a{};
     a.d = d;
     a.field[0] = scratch;
-    // along k: the row kernel with one pass, from f into scratch (the copy-in reads f)
-    cudaMemcpyAsync(scratch, f, d.fstride * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    a.src[0] = f;
+    // along k: the row kernel with one pass, reading f's rows and writing scratch
     zonal_rows_kernel<<<dim3(d.jm, d.im, 1), 128, 2 * d.km * sizeof(double), st>>>(a, 1, 1);
     wiggle_ji_kernel<<<dim3((d.km + 127) / 128, d.jm, d.im), 128, 0, st>>>(d, scratch, f);
 }

@@ -226,6 +226,8 @@ struct FilterArgs {
     Dims d;
     double* field[3];           // u, v, w for the post-RK4 filters
     const int* polar_passes;    // [jm] zonal passes per row
+    const double* src[3];       // the zonal passes read these rows instead of field[] (null:
+                                // in place)
 };
 void launch_post_rk4_filters(const FilterArgs& a, cudaStream_t st);
 void launch_damp_wiggles(const Dims& d, double* f, double* scratch, cudaStream_t st);
