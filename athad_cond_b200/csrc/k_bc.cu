@@ -170,32 +170,51 @@ __global__ void __launch_bounds__(128) bc_phi_kernel(BcArgs a)
 // bcScalarSurfSur and bcSolidGround (BC_Atm.h:1026-1123, 23-547) with flat terrain: their
 // land branches and the surface copies x[0] := x[i_mount = 0] change nothing, which leaves
 // bcSolidGround's value limits over every cell (:470-545), one (i, j) row per block row
-__global__ void __launch_bounds__(256) bc_limits_kernel(BcArgs a)
+// a limit stores only where it changes the value (bit for bit: -0.0 stays -0.0), so the
+// common case reads the fields and writes nothing
+__device__ __forceinline__ void store_if_changed(double* p, double old_v, double new_v)
+{
+    if (__double_as_longlong(old_v) != __double_as_longlong(new_v)) *p = new_v;
+}
+
+__global__ void __launch_bounds__(128) bc_limits_kernel(BcArgs a)
 {
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.km) return;
     const long long c = (long long)blockIdx.y * d.pitch + k;
     double* const* F = a.F;
-    const int sign[5] = {ATHAD_C, ATHAD_CLOUD, ATHAD_ICE, ATHAD_TKE, ATHAD_DIS};
+    const int sign[3] = {ATHAD_C, ATHAD_CLOUD, ATHAD_ICE};
 #pragma unroll
-    for (int q = 0; q < 5; q++)
+    for (int q = 0; q < 3; q++)
         if (F[sign[q]][c] < 0.0) F[sign[q]][c] = 0.0;
     const double prod_max = 1.0e4, dis_max = 1.0e6;
-    F[ATHAD_TKE][c] = safe_clamp(F[ATHAD_TKE][c], 0.0, a.tke_max_nd);
-    F[ATHAD_TKEN][c] = safe_clamp(F[ATHAD_TKEN][c], 0.0, a.tke_max_nd);
-    F[ATHAD_DIS][c] = safe_clamp(F[ATHAD_DIS][c], 1.0e-10, dis_max);
-    F[ATHAD_DISN][c] = safe_clamp(F[ATHAD_DISN][c], 1.0e-10, dis_max);
-    F[ATHAD_NUE][c] = safe_clamp(F[ATHAD_NUE][c], 0.0, a.nue_max);
-    F[ATHAD_PROD][c] = safe_clamp(F[ATHAD_PROD][c], 0.0, prod_max);
-    F[ATHAD_TKE_SOURCE][c] = safe_clamp(F[ATHAD_TKE_SOURCE][c], -prod_max, prod_max);
-    F[ATHAD_DIS_SOURCE][c] = safe_clamp(F[ATHAD_DIS_SOURCE][c], -prod_max, prod_max);
+    {   // tke and dis: non-negative, then clamped (a negative value becomes 0 first, which
+        // the clamp keeps, or 1e-10 for dis)
+        double v = F[ATHAD_TKE][c];
+        const double v0 = v;
+        if (v < 0.0) v = 0.0;
+        store_if_changed(F[ATHAD_TKE] + c, v0, safe_clamp(v, 0.0, a.tke_max_nd));
+        v = F[ATHAD_DIS][c];
+        const double w0 = v;
+        if (v < 0.0) v = 0.0;
+        store_if_changed(F[ATHAD_DIS] + c, w0, safe_clamp(v, 1.0e-10, dis_max));
+    }
+    struct Lim { int f; double lo, hi; };
+    const Lim lim[6] = {{ATHAD_TKEN, 0.0, a.tke_max_nd}, {ATHAD_DISN, 1.0e-10, dis_max},
+                        {ATHAD_NUE, 0.0, a.nue_max}, {ATHAD_PROD, 0.0, prod_max},
+                        {ATHAD_TKE_SOURCE, -prod_max, prod_max}, {ATHAD_DIS_SOURCE, -prod_max, prod_max}};
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const double v = F[lim[q].f][c];
+        store_if_changed(F[lim[q].f] + c, v, safe_clamp(v, lim[q].lo, lim[q].hi));
+    }
     const int vel[6] = {ATHAD_U, ATHAD_UN, ATHAD_V, ATHAD_VN, ATHAD_W, ATHAD_WN};
     const double vm = a.vel_max_nd;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
         const double v = F[vel[q]][c];
-        F[vel[q]][c] = !is_finite_bits(v) ? 0.0 : (v < -vm) ? -vm : (v > vm) ? vm : v;
+        store_if_changed(F[vel[q]] + c, v, !is_finite_bits(v) ? 0.0 : (v < -vm) ? -vm : (v > vm) ? vm : v);
     }
 }
 
@@ -207,7 +226,7 @@ void launch_boundary_conditions(const BcArgs& a, cudaStream_t st)
     bc_radius_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
     bc_theta_kernel<<<dim3((d.km + 127) / 128, d.im), 128, 0, st>>>(a);
     bc_phi_kernel<<<dim3((d.jm + 127) / 128, d.im), 128, 0, st>>>(a);
-    bc_limits_kernel<<<dim3((d.km + 255) / 256, d.im * d.jm), 256, 0, st>>>(a);
+    bc_limits_kernel<<<dim3((d.km + 127) / 128, d.im * d.jm), 128, 0, st>>>(a);
 }
 
 }  // namespace athad
