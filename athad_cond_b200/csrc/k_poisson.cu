@@ -79,6 +79,9 @@ __global__ void __launch_bounds__(256) poisson_src_kernel(PoissonArgs a)
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
+    // the sweep's "a value reached the ceiling" flag starts clear (the colours set it)
+    if (a.counters && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+        a.counters[5] = 0ull;
     if ((i == 0 || i == d.im - 1) && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1) aux_lid_cell(a, i, j, k);
     const bool fluid = (k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1 && i >= 1 && i < d.im - 1);
     bool clamped = false;
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(256, ATHAD_POISSON_MIN_BLOCKS) poisson_colour_
     const int i = blockIdx.z;
     const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((i + j + COLOUR) & 1);
     const bool fluid = !(k < 1 || k >= d.km - 1 || j < 1 || j >= d.jm - 1 || i < 1 || i >= d.im - 1);
-    bool clamped = false;
+    bool clamped = false, beyond = false;
     if (fluid) {
         const long long c = idx3(d, i, j, k);
         const PoiIJ P = a.poi[i * d.jm + j];
@@ -127,13 +130,18 @@ __global__ void __launch_bounds__(256, ATHAD_POISSON_MIN_BLOCKS) poisson_colour_
         const double* p = a.p;
         const double pip = p[c + sI], pim = p[c - sI];
         const double num_a = a.anelastic ? P.exp_2_rm * __ldg(a.dlnrho + i) * a.inv_2dr : 0.0;
-        a.p[c] = ((pip + pim) * P.num1
-                + (p[c + sJ] + p[c - sJ]) * P.num2
-                + (p[c + 1] + p[c - 1]) * P.num3
-                + (pip - pim) * num_a
-                - src) * P.inv_denom;
+        const double v = ((pip + pim) * P.num1
+                        + (p[c + sJ] + p[c - sJ]) * P.num2
+                        + (p[c + 1] + p[c - 1]) * P.num3
+                        + (pip - pim) * num_a
+                        - src) * P.inv_denom;
+        a.p[c] = v;
+        beyond = !(fabs(v) <= a.ceiling);      // non-finite included
     }
     count_clamped(a, clamped);
+    // one atomic per warp that has such a value (rare): the ceiling pass runs only then
+    if (__any_sync(0xffffffffu, beyond) && (threadIdx.x & 31) == 0 && a.counters)
+        atomicOr(a.counters + 5, 1ull);
 }
 
 // The three boundary passes (radial, pole, seam, PressureSolverAtm.h:504-552) in one launch.
@@ -225,6 +233,10 @@ __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
         a.counters[0] = a.first_sweep ? n : a.counters[0] + n;
         a.counters[1] = 0ull;
     }
+    // Every cell is a value the colours just formed or a boundary value copied or averaged
+    // from such values, so when no colour formed a value beyond the ceiling (or a
+    // non-finite one) the ceiling changes nothing and the launch ends here.
+    if (a.counters && a.counters[5] == 0ull) return;
     const long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
     if (q >= (long long)d.im * d.plane) return;
     const int k0 = (int)(q % d.pitch);

@@ -292,6 +292,34 @@ def test_pressure_boundaries_and_ceiling_bit_exact(grid):
         assert np.max(np.abs(a)) <= (10.0 if it <= 300 else 3.0)
 
 
+def test_pressure_ceiling_skipped_only_when_nothing_reaches_it():
+    """The ceiling pass ends early when no colour formed a value beyond the ceiling (every
+    boundary value is then a copy or average of such values).  Interior values well inside
+    the ceiling, and before the call values far beyond it and non-finite on the grid's edges
+    (cells that no interior cell reads, so the sweep itself stays inside the ceiling): the
+    boundary passes replace them, and the result is the oracle's bit for bit."""
+    grid = (11, 21, 41)
+    p = config_params()
+    st = make_state(*grid, seed=23)
+    im, jm, km = grid
+    rng = np.random.default_rng(4)
+    for n in ("aux_u", "aux_v", "aux_w"):
+        st[n] = 1e-4 * rng.standard_normal(st["t"].shape)
+    pd = 0.5 * rng.standard_normal(st["t"].shape)
+    pd[0, 0, :] = 1e6
+    pd[im - 1, jm - 1, :] = -1e6
+    pd[:, 0, km - 1] = np.inf
+    pd[0, :, 0] = np.nan
+    st["p_dyn"] = pd
+    o = OracleState(st, p)
+    o.pressure_sweep(n_sweeps=1, total_iter_count=400)
+    with gpu_with(st, p) as g:
+        g.PressureSolverAtm_run(total_iter_count=400, n_sweeps=1)
+        a = g.download("p_dyn")
+    assert np.array_equal(a, o.f["p_dyn"], equal_nan=True)
+    assert np.isfinite(a).all() and np.max(np.abs(a)) <= 3.0
+
+
 @pytest.mark.parametrize("precision", [Precision.FP64, Precision.MIXED])
 def test_report_counts_nonfinite_temperature_and_times_the_step(precision):
     """athad_get_report: the level mean of each RK4 step counts the non-finite cells of its
