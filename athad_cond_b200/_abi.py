@@ -84,7 +84,7 @@ class Grid(ctypes.Structure):
 _PARAM_INTS = [
     "turb_model", "wall_mode", "poisson_metric_fix", "anelastic", "tracer_diff_flux",
     "coriolis_nontrad", "metric_curvature", "metric_divergence",
-    "convection_perturbation", "convection_mode", "iter_prec", "precision",
+    "convection_perturbation", "convection_mode", "iter_prec", "precision", "category_ice_scheme",
 ]
 _PARAM_DOUBLES = [
     "metric_r0", "re_turb",
@@ -95,7 +95,7 @@ _PARAM_DOUBLES = [
     "M_bg", "R_bg", "R_mix",
     "abl_height", "t_000",
     "sigma", "kappa_H2O", "kappa_CO2", "kappa_bg", "geothermal_flux", "albedo_surface",
-    "albedo_cloud", "rad_equator_short", "rad_pole_short", "coeff_Dalton",
+    "albedo_cloud", "rad_equator_short", "rad_pole_short", "coeff_Dalton", "r_0_water",
 ]
 
 
@@ -233,6 +233,10 @@ SIGNATURES = {
     "athad_damp_wiggles": (ctypes.c_int, [_P, ctypes.c_int]),
     "athad_turbulence_run": (ctypes.c_int, [_P]),
     "athad_two_cat_ice_scheme": (ctypes.c_int, [_P]),
+    "athad_zero_cat_ice_scheme": (ctypes.c_int, [_P]),
+    "athad_one_cat_ice_scheme": (ctypes.c_int, [_P]),
+    "athad_three_cat_ice_scheme": (ctypes.c_int, [_P]),
+    "athad_ice_scheme": (ctypes.c_int, [_P]),
     "athad_multilayer_radiation": (ctypes.c_int, [_P]),
     "athad_radiative_heating": (ctypes.c_int, [_P, ctypes.c_double]),
     "athad_moist_caps": (ctypes.c_int, [_P]),
@@ -318,6 +322,7 @@ def config_params() -> Params:
     p.convection_perturbation = 1
     p.convection_mode = 1
     p.iter_prec = 3
+    p.category_ice_scheme = 2
     p.metric_r0 = -1.0
     p.re_turb = 0.4 * 0.1 / 1.5e-5
     vals = dict(r_air=40.8, g=9.8066, u_0=8.0, cp_l=1349.0, t_0=273.15, c_0=0.3464, L_atm=6287.5,
@@ -327,7 +332,7 @@ def config_params() -> Params:
                 co2_0=0.6233, s_0=274515.75, R_Air=296.8, R_WaterVapour=461.5, abl_height=10000.0,
                 t_000=253.15, sigma=5.67028e-08, kappa_H2O=0.01, kappa_CO2=0.001, kappa_bg=1e-06,
                 geothermal_flux=150.0, albedo_surface=0.08, albedo_cloud=0.5,
-                rad_equator_short=298.0, rad_pole_short=0.0, coeff_Dalton=0.7)
+                rad_equator_short=298.0, rad_pole_short=0.0, coeff_Dalton=0.7, r_0_water=997.0)
     for k, v in vals.items():
         setattr(p, k, v)
     comp = composition(CONFIG_X)

@@ -287,6 +287,23 @@ class GpuAtmosphere:
         """TwoCatIceScheme::run (TwoCatIceScheme.h:89-109; call site cAtmosphereModel.cpp:1238)."""
         self._check(self.lib.athad_two_cat_ice_scheme(self._h))
 
+    def zero_cat_ice_scheme(self):
+        """ZeroCatIceScheme::run (ZeroCatIceScheme.h:37-56; CategoryIceScheme 0)."""
+        self._check(self.lib.athad_zero_cat_ice_scheme(self._h))
+
+    def one_cat_ice_scheme(self):
+        """OneCatIceScheme::run (OneCatIceScheme.h:50-68; CategoryIceScheme 1)."""
+        self._check(self.lib.athad_one_cat_ice_scheme(self._h))
+
+    def three_cat_ice_scheme(self):
+        """ThreeCatIceScheme::run (ThreeCatIceScheme.h:70-89; CategoryIceScheme 3)."""
+        self._check(self.lib.athad_three_cat_ice_scheme(self._h))
+
+    def ice_scheme(self):
+        """The CategoryIceScheme switch (cAtmosphereModel.cpp:581-596, 1230-1245) on
+        params.category_ice_scheme: -1 nothing, 0..3 the schemes above."""
+        self._check(self.lib.athad_ice_scheme(self._h))
+
     def turbulence_run(self):
         """TurbulenceAtm::run (TurbulenceAtm.h:62-79; call site cAtmosphereModel.cpp:1426)."""
         self._check(self.lib.athad_turbulence_run(self._h))

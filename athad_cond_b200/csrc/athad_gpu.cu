@@ -32,6 +32,7 @@ void athad_default_params(athad_params* p)
     p->convection_perturbation = 1;
     p->convection_mode = 1;
     p->iter_prec = 3;
+    p->category_ice_scheme = 2;
     p->metric_r0 = -1.0;                 // derive r_Earth*1e3/metricShellLength()
     p->re_turb = 0.4 * 0.1 / 1.5e-5;     // TurbulenceAtm.h:26-35
     p->r_air = 40.8; p->g = 9.8066; p->u_0 = 8.0; p->cp_l = 1349.0; p->t_0 = 273.15;
@@ -46,6 +47,7 @@ void athad_default_params(athad_params* p)
     p->geothermal_flux = 150.0; p->albedo_surface = 0.08; p->albedo_cloud = 0.5;
     p->rad_equator_short = 298.0; p->rad_pole_short = 0.0;
     p->coeff_Dalton = 0.7;
+    p->r_0_water = 997.0;
     const double x[8] = {0.5578, 0.4109, 0.0313, 0.0, 0.0, 0.0, 0.0, 0.0};
     const double m_H2O = x[0] * thermo::M_H2O, m_CO2 = x[1] * thermo::M_CO2;
     const double m_bg = x[2] * 0.028014 + x[3] * 0.016043 + x[4] * 0.017031
@@ -88,6 +90,8 @@ athad_status athad_create(const athad_grid* grid, const athad_params* params, at
     if (params->turb_model < ATHAD_TURB_K_EPSILON || params->turb_model > ATHAD_TURB_K_OMEGA_SST)
         return ATHAD_ERR_UNSUPPORTED;
     if (params->precision != ATHAD_PRECISION_FP64 && params->precision != ATHAD_PRECISION_MIXED)
+        return ATHAD_ERR_UNSUPPORTED;
+    if (params->category_ice_scheme < -1 || params->category_ice_scheme > 3)
         return ATHAD_ERR_UNSUPPORTED;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return ATHAD_ERR_NO_DEVICE; }
@@ -1320,12 +1324,9 @@ athad_status athad_radiative_heating(athad_ctx* ctx, double omega_rad)
     return ATHAD_OK;
 }
 
-athad_status athad_two_cat_ice_scheme(athad_ctx* ctx)
+// the fields and constants of the ice / precipitation schemes
+static void ice_args(athad_ctx* ctx, IceArgs& a)
 {
-    if (!ctx) return ATHAD_ERR_INVALID;
-    if (ctx->L.d.im < 3 || ctx->L.d.jm < 3 || ctx->L.d.km < 3)
-        return fail(ctx, ATHAD_ERR_UNSUPPORTED, "two_cat_ice_scheme: grid too small");
-    IceArgs a;
     std::memset(&a, 0, sizeof a);
     a.d = ctx->L.d;
     double** F = ctx->field;
@@ -1336,10 +1337,95 @@ athad_status athad_two_cat_ice_scheme(athad_ctx* ctx)
     a.S_v = F[ATHAD_S_V]; a.S_c = F[ATHAD_S_C]; a.S_i = F[ATHAD_S_I]; a.S_r = F[ATHAD_S_R];
     a.S_s = F[ATHAD_S_S]; a.S_g = F[ATHAD_S_G]; a.S_c_c = F[ATHAD_S_C_C];
     a.step_f = ctx->step_f;
-    a.t_0 = ctx->p.t_0; a.t_000 = ctx->p.t_000; a.M_bg = ctx->p.M_bg;
+    const athad_params& p = ctx->p;
+    a.t_0 = p.t_0; a.t_000 = p.t_000; a.M_bg = p.M_bg; a.t_00 = p.t_00; a.ls = p.ls;
+}
+
+athad_status athad_two_cat_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (ctx->L.d.im < 3 || ctx->L.d.jm < 3 || ctx->L.d.km < 3)
+        return fail(ctx, ATHAD_ERR_UNSUPPORTED, "two_cat_ice_scheme: grid too small");
+    IceArgs a;
+    ice_args(ctx, a);
     launch_two_cat_ice(a, ctx->stream);
     ATHAD_CHECK_LAUNCH(ctx, "two_cat_ice_scheme");
     return ATHAD_OK;
+}
+
+// ZeroCat, OneCat and ThreeCat read the rain flux at level 23 (P_rain.x[23]) for their
+// convergence test
+static bool ice_level_23(athad_ctx* ctx, const char* what)
+{
+    if (ctx->L.d.im >= 24) return true;
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "%s: the scheme reads level 23, the grid needs im >= 24", what);
+    fail(ctx, ATHAD_ERR_UNSUPPORTED, msg);
+    return false;
+}
+
+athad_status athad_zero_cat_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (!ice_level_23(ctx, "zero_cat_ice_scheme")) return ATHAD_ERR_UNSUPPORTED;
+    IceArgs a;
+    ice_args(ctx, a);
+    launch_zero_cat_ice(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "zero_cat_ice_scheme");
+    return ATHAD_OK;
+}
+
+athad_status athad_one_cat_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (!ice_level_23(ctx, "one_cat_ice_scheme")) return ATHAD_ERR_UNSUPPORTED;
+    IceArgs a;
+    ice_args(ctx, a);
+    // the carry of S_au across columns, in RK4 stage buffers (free between RK4 steps; one
+    // double per interior column each)
+    a.sau_exit = ctx->stA[1]; a.sau_has = ctx->stA[2]; a.sau_entry = ctx->stA[3];
+    launch_one_cat_ice(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "one_cat_ice_scheme");
+    return ATHAD_OK;
+}
+
+athad_status athad_three_cat_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    if (!ice_level_23(ctx, "three_cat_ice_scheme")) return ATHAD_ERR_UNSUPPORTED;
+    IceArgs a;
+    ice_args(ctx, a);
+    // ThreeCatIceScheme.h:147-170, on the host once per call
+    const double N_r_0 = 8.0e+6, N_s_0 = 8.0e+5, N_g_0 = 4.0e6, v_s_0 = 130.0, v_r_0 = 4.9;
+    const double v_g_0 = 442.0, a_s_m = 0.038, a_g_m = 169.6;
+    const double gamma_4_5 = std::tgamma(4.5), gamma_4_0 = std::tgamma(4.0), gamma_3_25 = std::tgamma(3.25);
+    const double r0w = ctx->p.r_0_water;
+    a.A_r = r0w * M_PI * N_r_0;
+    a.A_s = 2.0 * a_s_m * N_s_0;
+    a.A_g = 2.0 * a_g_m * N_g_0;
+    const double B_rad = r0w * M_PI * N_r_0 * v_r_0 * gamma_4_5 / gamma_4_0;
+    const double B_s = N_s_0 * v_s_0 * a_s_m * gamma_3_25;
+    const double B_g = N_g_0 * v_g_0 * a_g_m * gamma_3_25;
+    a.B_rad_neg89 = std::pow(B_rad, -8.0 / 9.0);
+    a.B_s_neg1213 = std::pow(B_s, -12.0 / 13.0);
+    a.B_g_neg1213 = std::pow(B_g, -12.0 / 13.0);
+    a.E_sat_t_0_Pa = 1e2 * thermo::saturation_pressure(ctx->p.t_0);
+    launch_three_cat_ice(a, ctx->stream);
+    ATHAD_CHECK_LAUNCH(ctx, "three_cat_ice_scheme");
+    return ATHAD_OK;
+}
+
+athad_status athad_ice_scheme(athad_ctx* ctx)
+{
+    if (!ctx) return ATHAD_ERR_INVALID;
+    switch (ctx->p.category_ice_scheme) {
+    case -1: return ATHAD_OK;
+    case 0: return athad_zero_cat_ice_scheme(ctx);
+    case 1: return athad_one_cat_ice_scheme(ctx);
+    case 2: return athad_two_cat_ice_scheme(ctx);
+    case 3: return athad_three_cat_ice_scheme(ctx);
+    default: return fail(ctx, ATHAD_ERR_UNSUPPORTED, "ice_scheme: category_ice_scheme not in -1..3");
+    }
 }
 
 athad_status athad_turbulence_run(athad_ctx* ctx)

@@ -10,7 +10,8 @@
 //                        cloud-ice limiters and the capped flux integration;
 //   ice_bc_*_kernel      applyBoundaryConditions (:489-492): IceSchemeCommon::extrapolateBC
 //                        (IceSchemeCommon.h:27-52) of P_rain and P_snow, radial lid, poles,
-//                        then the seam with its average.
+//                        then the seam with its average (launch_precip_bc, shared with the
+//                        other schemes of k_ice_cat.cu, which choose the average per field).
 //
 // A column reads nothing of other columns, so the columns run independently.  The reference
 // keeps N_i, m_i, S_nuc and S_i_dep from one cell to the next where a branch does not
@@ -18,8 +19,7 @@
 // exp, log and the saturation curves are CUDA's.  The reference's pow calls become powers of
 // one root per cell (Rain^(1/18), Snow^(1/26)), cbrt and x * sqrt(x): the same exponents
 // within a few ulp.
-#include "kernels.cuh"
-#include "thermo.cuh"
+#include "ice_common.cuh"
 
 namespace athad {
 
@@ -37,44 +37,10 @@ constexpr double kCrFrz = 3.75e-2;
 constexpr double kTnuc = 267.15, kTd = 248.15, kThn = 236.15, kTrFrz = 271.15;
 constexpr int kIterPrecEnd = 3, kIcheck = 1;
 
-__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
-
-__device__ __forceinline__ double q_sat_at(const IceArgs& a, long long c, double E)
-{
-    return saturation_mass_fraction(E, a.p_stat[c], M_nonwater(a.c[c], a.co2[c], a.M_bg));
-}
-
-// IceSchemeCommon::evaporateWhereImpossible (IceSchemeCommon.h:121-190) on cell c
-__device__ void evaporate_cell(const IceArgs& a, long long c, double t_u)
-{
-    const double q_cond = dmax(0.0, a.cloud[c]) + dmax(0.0, a.ice[c]) + dmax(0.0, a.gr[c]);
-    if (q_cond > 0.0) {
-        const double c_max = dmax(0.0, 1.0 - a.co2[c]);
-        const double c_new = dmin(c_max, a.c[c] + q_cond);
-        const double q_used = dmax(0.0, c_new - a.c[c]);
-        a.c[c] = c_new;
-        a.cloud[c] = 0.0; a.ice[c] = 0.0; a.gr[c] = 0.0;
-        if (t_u < T_CRIT) {
-            const double cp_loc = cp_of(a.c[c], a.co2[c], t_u, a.M_bg);
-            if (cp_loc > 0.0) {
-                double T_new = t_u - latent_heat(t_u) * q_used / cp_loc;
-                if (T_new < 1.0) T_new = 1.0;
-                a.t[c] = T_new / a.t_0;
-            }
-        }
-    }
-    const double rho = dmax(1.0e-6, a.r_humid[c]);
-    const double q_p = dmax(0.0, a.P_rain[c]) / (1.6 * rho) + dmax(0.0, a.P_snow[c]) / (0.96 * rho)
-                     + dmax(0.0, a.P_graupel[c]) / (2.0 * rho);
-    if (q_p > 0.0) {
-        const double c_max = dmax(0.0, 1.0 - a.co2[c]);
-        a.c[c] = dmin(c_max, a.c[c] + q_p);
-    }
-    a.P_rain[c] = 0.0; a.P_snow[c] = 0.0; a.P_graupel[c] = 0.0; a.Precipitation[c] = 0.0;
-    a.S_v[c] = 0.0; a.S_c[c] = 0.0; a.S_i[c] = 0.0; a.S_r[c] = 0.0; a.S_s[c] = 0.0;
-    a.S_g[c] = 0.0; a.S_c_c[c] = 0.0;
-}
+using ice::dmax;
+using ice::dmin;
+using ice::q_sat_at;
+using ice::evaporate_cell;
 
 __global__ void __launch_bounds__(256) ice_init_kernel(IceArgs a)
 {
@@ -233,36 +199,43 @@ __global__ void __launch_bounds__(128) ice_columns_kernel(IceArgs a)
 }
 
 // extrapolateBC with c43 = 1, c13 = 0 (const int members, cAtmosphereModel.h:158), for the
-// field P[blockIdx.z] (P_rain, P_snow): radial lid, then poles, then the seam
-__global__ void ice_bc_lid_kernel(Dims d, double* P0, double* P1)
+// field b.P[blockIdx.z]: radial lid, then poles, then the seam (averaged where b.avg is set)
+struct PrecipBc { double* P[3]; int avg[3]; };
+
+__global__ void ice_bc_lid_kernel(Dims d, PrecipBc b)
 {
-    double* P = blockIdx.z ? P1 : P0;
+    double* P = b.P[blockIdx.z];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (k >= d.km) return;
     P[idx3(d, d.im - 1, j, k)] = 1.0 * P[idx3(d, d.im - 2, j, k)] - 0.0 * P[idx3(d, d.im - 3, j, k)];
 }
-__global__ void ice_bc_pole_kernel(Dims d, double* P0, double* P1)
+__global__ void ice_bc_pole_kernel(Dims d, PrecipBc b)
 {
-    double* P = blockIdx.z ? P1 : P0;
+    double* P = b.P[blockIdx.z];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (k >= d.km) return;
     P[idx3(d, i, 0, k)] = 1.0 * P[idx3(d, i, 1, k)] - 0.0 * P[idx3(d, i, 2, k)];
     P[idx3(d, i, d.jm - 1, k)] = 1.0 * P[idx3(d, i, d.jm - 2, k)] - 0.0 * P[idx3(d, i, d.jm - 3, k)];
 }
-__global__ void ice_bc_seam_kernel(Dims d, double* P0, double* P1)
+__global__ void ice_bc_seam_kernel(Dims d, PrecipBc b)
 {
-    double* P = blockIdx.z ? P1 : P0;
+    double* P = b.P[blockIdx.z];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j >= d.jm) return;
     double* row = P + idx3(d, i, j, 0);
     const double r0 = 1.0 * row[1] - 0.0 * row[2];
     const double r1 = 1.0 * row[d.km - 2] - 0.0 * row[d.km - 3];
-    const double m = (r0 + r1) * 0.5;
-    row[0] = m;
-    row[d.km - 1] = m;
+    if (b.avg[blockIdx.z]) {
+        const double m = (r0 + r1) * 0.5;
+        row[0] = m;
+        row[d.km - 1] = m;
+    } else {
+        row[0] = r0;
+        row[d.km - 1] = r1;
+    }
 }
 
 }  // namespace
@@ -272,9 +245,21 @@ void launch_two_cat_ice(const IceArgs& a, cudaStream_t st)
     const Dims& d = a.d;
     ice_init_kernel<<<148 * 8, 256, 0, st>>>(a);
     ice_columns_kernel<<<dim3((d.km + 127) / 128, d.jm), 128, 0, st>>>(a);
-    ice_bc_lid_kernel<<<dim3((d.km + 127) / 128, d.jm, 2), 128, 0, st>>>(d, a.P_rain, a.P_snow);
-    ice_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im, 2), 128, 0, st>>>(d, a.P_rain, a.P_snow);
-    ice_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im, 2), 128, 0, st>>>(d, a.P_rain, a.P_snow);
+    double* P[3] = {a.P_rain, a.P_snow, nullptr};
+    const int avg[3] = {1, 1, 0};
+    launch_precip_bc(d, P, avg, 2, st);
+}
+
+void launch_precip_bc(const Dims& d, double* const* P, const int* avg, int n, cudaStream_t st)
+{
+    PrecipBc b;
+    for (int q = 0; q < 3; q++) {
+        b.P[q] = (q < n) ? P[q] : nullptr;
+        b.avg[q] = (q < n) ? avg[q] : 0;
+    }
+    ice_bc_lid_kernel<<<dim3((d.km + 127) / 128, d.jm, n), 128, 0, st>>>(d, b);
+    ice_bc_pole_kernel<<<dim3((d.km + 127) / 128, d.im, n), 128, 0, st>>>(d, b);
+    ice_bc_seam_kernel<<<dim3((d.jm + 127) / 128, d.im, n), 128, 0, st>>>(d, b);
 }
 
 }  // namespace athad

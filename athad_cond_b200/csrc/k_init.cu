@@ -681,8 +681,9 @@ athad_status athad_initial_state(athad_ctx* ctx, const athad_init_config* cfg)
     // SaturationAdjustment and damp_wiggles(ice, c, cloud) (cAtmosphereModel.cpp:574-577)
     ATHAD_TRY(athad_saturation_adjust(ctx));
     for (int f : {ATHAD_ICE, ATHAD_C, ATHAD_CLOUD}) ATHAD_TRY(athad_damp_wiggles(ctx, (athad_field)f));
-    // the ice scheme (CategoryIceScheme 2) and damp_wiggles(P_rain, P_snow) (:581-596)
-    ATHAD_TRY(athad_two_cat_ice_scheme(ctx));
+    // the configured ice scheme (the CategoryIceScheme switch) and damp_wiggles(P_rain,
+    // P_snow) (:581-596)
+    ATHAD_TRY(athad_ice_scheme(ctx));
     for (int f : {ATHAD_P_RAIN, ATHAD_P_SNOW}) ATHAD_TRY(athad_damp_wiggles(ctx, (athad_field)f));
     // MoistConvection(iter_n = 0) and the smoothing of its outputs (:599-608)
     ATHAD_TRY(athad_moist_convection(ctx, 0));

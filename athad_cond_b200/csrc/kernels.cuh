@@ -262,8 +262,20 @@ struct IceArgs {
     double* S_v; double* S_c; double* S_i; double* S_r; double* S_s; double* S_g; double* S_c_c;
     const double* step_f;       // [im] float layer thickness, get_layer_height(i+1) - (i)
     double t_0, t_000, M_bg;
+    double t_00, ls;            // OneCat's and ThreeCat's temperature bands; ThreeCat's t_crit
+    // ThreeCat's constants, formed on the host as ThreeCatIceScheme.h:147-170 does: A_r, A_s,
+    // A_g, B_rad^(-8/9), B_s^(-12/13), B_g^(-12/13) and 100 * saturationPressure(t_0)
+    double A_r, A_s, A_g, B_rad_neg89, B_s_neg1213, B_g_neg1213, E_sat_t_0_Pa;
+    // OneCat's carry of S_au across columns: per column (serial order n = (k-1)*(jm-2) + j-1)
+    // the rate at its last cloudy cell, whether it has one, and the value it enters with
+    double* sau_exit; double* sau_has; double* sau_entry;
 };
 void launch_two_cat_ice(const IceArgs& a, cudaStream_t st);
+void launch_zero_cat_ice(const IceArgs& a, cudaStream_t st);
+void launch_one_cat_ice(const IceArgs& a, cudaStream_t st);
+void launch_three_cat_ice(const IceArgs& a, cudaStream_t st);
+// IceSchemeCommon::extrapolateBC of n <= 3 flux fields P[q], the seam averaged where avg[q]
+void launch_precip_bc(const Dims& d, double* const* P, const int* avg, int n, cudaStream_t st);
 
 // MultiLayerRadiation::run (k_rad.cu)
 struct RadArgs {

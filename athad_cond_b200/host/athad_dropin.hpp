@@ -68,6 +68,7 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.convection_perturbation = m.convection_perturbation;
     p.convection_mode = m.convection_mode;
     p.iter_prec = m.iter_prec;
+    p.category_ice_scheme = m.CategoryIceScheme;
     p.r_air = m.r_air; p.g = m.g; p.u_0 = m.u_0; p.cp_l = m.cp_l; p.t_0 = m.t_0; p.c_0 = m.c_0;
     p.L_atm = m.L_atm; p.zeta = m.zeta; p.omega = m.omega; p.lamda = m.lamda; p.lv = m.lv;
     p.ls = m.ls; p.pr_turb = m.pr_turb; p.sc_WaterVapour = m.sc_WaterVapour; p.sc_CO2 = m.sc_CO2;
@@ -81,6 +82,7 @@ athad_params params_from(const Model& m, athad_wall_mode wall = ATHAD_WALL_MIRRO
     p.albedo_cloud = m.albedo_cloud; p.rad_equator_short = m.rad_equator_short;
     p.rad_pole_short = m.rad_pole_short;
     p.coeff_Dalton = m.coeff_Dalton;
+    p.r_0_water = m.r_0_water;
     return p;
 }
 
@@ -319,7 +321,13 @@ public:
     }
 
     // TwoCatIceScheme(m).run() (cAtmosphereModel.cpp:589, 1238), flat terrain
-    void TwoCatIceSchemeRun(Model& m)
+    void TwoCatIceSchemeRun(Model& m) { IceSchemeCall(m, athad_two_cat_ice_scheme, "two_cat_ice_scheme"); }
+    // the whole CategoryIceScheme switch (cAtmosphereModel.cpp:581-596, 1230-1245) on the
+    // model's CategoryIceScheme, flat terrain
+    void IceSchemeRun(Model& m) { IceSchemeCall(m, athad_ice_scheme, "ice_scheme"); }
+
+private:
+    void IceSchemeCall(Model& m, athad_status (*fn)(athad_ctx*), const char* what)
     {
 #define ATHAD_ICE_FIELDS(X) X(ATHAD_T, t) X(ATHAD_C, c) X(ATHAD_CLOUD, cloud) X(ATHAD_ICE, ice) \
         X(ATHAD_GR, gr) X(ATHAD_P_RAIN, P_rain) X(ATHAD_P_SNOW, P_snow) X(ATHAD_P_GRAUPEL, P_graupel) \
@@ -330,12 +338,14 @@ public:
 #define ATHAD_ICE_DOWN(F, N) down(F, m.N);
         ATHAD_ICE_FIELDS(ATHAD_ICE_UP)
         up(ATHAD_CO2, m.co2); up(ATHAD_P_STAT, m.p_stat); up(ATHAD_R_HUMID, m.r_humid);
-        check(ctx_, athad_two_cat_ice_scheme(ctx_), "two_cat_ice_scheme");
+        check(ctx_, fn(ctx_), what);
         ATHAD_ICE_FIELDS(ATHAD_ICE_DOWN)
 #undef ATHAD_ICE_UP
 #undef ATHAD_ICE_DOWN
 #undef ATHAD_ICE_FIELDS
     }
+
+public:
 
     // MultiLayerRadiation(m).run() (cAtmosphereModel.cpp:831-1007), and radiation mode 2's
     // heating t := t (1 - omega) + MLR(t) omega (:864-879; omega_rad = 0.05, :801)
@@ -578,7 +588,7 @@ public:
             check(ctx, athad_water_budget(ctx, &r.h2o_post_rk4, nullptr), "water_budget");
             check(ctx, athad_saturation_adjust(ctx), "saturation_adjust");
             for (athad_field f : {ATHAD_T, ATHAD_ICE, ATHAD_C, ATHAD_CLOUD}) damp(ctx, f);
-            check(ctx, athad_two_cat_ice_scheme(ctx), "two_cat_ice_scheme");
+            check(ctx, athad_ice_scheme(ctx), "ice_scheme");
             for (athad_field f : {ATHAD_P_RAIN, ATHAD_P_SNOW}) damp(ctx, f);
             check(ctx, athad_moist_convection(ctx, it), "moist_convection");
             for (athad_field f : {ATHAD_P_CONV, ATHAD_E_U, ATHAD_M_U, ATHAD_Q_V_U, ATHAD_Q_C_U, ATHAD_E_D,

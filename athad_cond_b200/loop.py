@@ -83,7 +83,7 @@ class ModelLoop:
             g.SaturationAdjustment_run()
             for n in MOIST_FIELDS_AFTER_SATADJ:
                 g.damp_wiggles(n)
-            g.two_cat_ice_scheme()
+            g.ice_scheme()
             for n in ICE_FLUXES:
                 g.damp_wiggles(n)
             g.MoistConvection_run(it)

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ATHAD_ABI_VERSION 10
+#define ATHAD_ABI_VERSION 11
 
 typedef enum athad_status {
     ATHAD_OK              = 0,
@@ -96,6 +96,8 @@ typedef struct athad_params {
     int32_t  iter_prec;          /* XML, 3 */
     int32_t  precision;          /* athad_precision of the RK4 step (no counterpart in
                                   * the reference, which is FP64 only); default FP64 */
+    int32_t  category_ice_scheme;/* XML CategoryIceScheme, 2 (cli/config_cond.xml:18): the
+                                  * scheme athad_ice_scheme runs, -1 (none) or 0..3 */
     /* metric radius in rad.z units; 0 = off.  The reference default (ATM_METRIC_RADIUS
      * unset) is r_Earth*1e3/metricShellLength() (cAtmosphereModel.cpp:382-399); the
      * value 0 reproduces ATM_METRIC_RADIUS=0. */
@@ -120,6 +122,8 @@ typedef struct athad_params {
     double rad_equator_short, rad_pole_short;   /* TOA short-wave insolation [W/m2]     */
     double coeff_Dalton;         /* XML coeff_Dalton, 0.7 (cli/config_cond.xml:54): the
                                   * Dalton evaporation coefficient (AtomUtils::C_Dalton)   */
+    double r_0_water;            /* XML r_0_water [kg/m3], 997 (cAtmosphereDefaults.cpp.inc:33):
+                                  * the rain drop density of ThreeCatIceScheme            */
 } athad_params;
 
 /* 3-D fields, one per cAtmosphereModel Array member of the same name. */
@@ -438,6 +442,31 @@ athad_status athad_turbulence_run(athad_ctx* ctx);
  * Precipitation, and their boundary extrapolation; cells where no condensed phase can exist
  * evaporate their condensate (IceSchemeCommon.h:121-190). */
 athad_status athad_two_cat_ice_scheme(athad_ctx* ctx);
+/* ZeroCatIceScheme(*this).run() (ZeroCatIceScheme.h:37-56; CategoryIceScheme = 0), flat
+ * terrain: rain only.  Kessler autoconversion above 0.5 g/kg, accretion and evaporation give
+ * S_v, S_c and S_r; the rain flux is integrated top-down from S_r of the cell above, uncapped;
+ * P_snow keeps its restart value; P_rain is extrapolated with the seam average, P_snow
+ * without.  Up to two passes per column until the rain flux at i = 23 settles, so the grid
+ * needs im >= 24 (the reference reads level 23 whatever the grid; ATHAD_ERR_UNSUPPORTED
+ * below). */
+athad_status athad_zero_cat_ice_scheme(athad_ctx* ctx);
+/* OneCatIceScheme(*this).run() (OneCatIceScheme.h:50-68; CategoryIceScheme = 1), flat
+ * terrain: rain and snow with the COSMO one-category rates; snow grows through the shared
+ * ice throttle (IceSchemeCommon.h:203-237); fluxes capped at 3e-3 kg/(m2 s).  The reference
+ * walks the columns in one serial order (k outer, j inner) and keeps the autoconversion rate
+ * S_au from the last cell with cloud water where a cell has none, across columns; the library
+ * resolves that carry with a scan over the columns in the same order, so the result is the
+ * reference's.  The carry before the first cloudy cell of the grid, uninitialised in the
+ * reference, is 0 here.  im >= 24 as for athad_zero_cat_ice_scheme. */
+athad_status athad_one_cat_ice_scheme(athad_ctx* ctx);
+/* ThreeCatIceScheme(*this).run() (ThreeCatIceScheme.h:70-89; CategoryIceScheme = 3), flat
+ * terrain: rain, snow and graupel, the fluxes normalised by the surface flux (floored at
+ * 1e-6), the shared ice throttle, capped at 3e-3 kg/(m2 s); all three fluxes extrapolated
+ * with the seam average.  im >= 24 as for athad_zero_cat_ice_scheme. */
+athad_status athad_three_cat_ice_scheme(athad_ctx* ctx);
+/* The switch of cAtmosphereModel.cpp:581-596 and 1230-1245 on athad_params.
+ * category_ice_scheme: -1 runs nothing, 0..3 the schemes above. */
+athad_status athad_ice_scheme(athad_ctx* ctx);
 /* MultiLayerRadiation(*this).run() (MultiLayerRadiation.h:56-388; call sites
  * cAtmosphereModel.cpp:831-1007), flat terrain: per (j, k) column the grey long-wave
  * emissivities, four radiative-equilibrium sweeps and the surface energy balance.  Writes t

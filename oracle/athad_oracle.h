@@ -36,6 +36,7 @@ typedef struct or_params {
     int32_t  turb_model, wall_mode, poisson_metric_fix, anelastic, tracer_diff_flux;
     int32_t  coriolis_nontrad, metric_curvature, metric_divergence;
     int32_t  convection_perturbation, convection_mode, iter_prec, precision;   /* precision: unused by the oracle (FP64) */
+    int32_t  category_ice_scheme;
     double metric_r0, re_turb;
     double r_air, g, u_0, cp_l, t_0, c_0, L_atm, zeta, omega, lamda, lv, ls;
     double pr_turb, sc_WaterVapour, sc_CO2;
@@ -46,6 +47,7 @@ typedef struct or_params {
     double sigma, kappa_H2O, kappa_CO2, kappa_bg, geothermal_flux, albedo_surface, albedo_cloud;
     double rad_equator_short, rad_pole_short;
     double coeff_Dalton;
+    double r_0_water;
 } or_params;
 
 typedef struct or_step {
@@ -149,6 +151,12 @@ void or_turbulence_run(int im, int jm, int km, const or_params* p, int compat,
 /* TwoCatIceScheme::run, TwoCatIceScheme.h:89-109 (initArrays, computeColumns,
  * applyBoundaryConditions; applyTopography does nothing without land), flat terrain */
 void or_two_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
+/* ZeroCatIceScheme::run, OneCatIceScheme::run, ThreeCatIceScheme::run (im >= 24: the
+ * schemes read level 23); or_ice_scheme: the CategoryIceScheme switch (-1 .. 3) */
+void or_zero_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
+void or_one_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
+void or_three_cat_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
+void or_ice_scheme(int im, int jm, int km, const or_params* p, double* const* f);
 
 /* MultiLayerRadiation::run (MultiLayerRadiation.h:56-388): t := the radiative equilibrium;
  * radiation, epsilon, epsilon_2D, albedo.  or_radiative_heating: radiation mode 2's

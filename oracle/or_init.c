@@ -585,7 +585,7 @@ int or_init_state(int im, int jm, int km, const or_params* p, const or_init_cfg*
     or_damp_wiggles(im, jm, km, f[OF_CLOUD], cm);
     if (upto <= OR_INIT_SATADJ) goto done;
 
-    or_two_cat_ice_scheme(im, jm, km, p, f);                        /* :581-596 */
+    or_ice_scheme(im, jm, km, p, f);                                /* :581-596 */
     or_damp_wiggles(im, jm, km, f[OF_P_RAIN], cm);
     or_damp_wiggles(im, jm, km, f[OF_P_SNOW], cm);
     if (upto <= OR_INIT_ICE) goto done;

@@ -429,6 +429,10 @@ void ref_set_turb_model(void* p, const char* s) { ((cAtmosphereModel*)p)->turb_m
 // the moist iteration's ice scheme of the configuration (CategoryIceScheme = 2,
 // cAtmosphereModel.cpp:1238)
 void ref_two_cat_ice(void* p) { TwoCatIceScheme(*(cAtmosphereModel*)p).run(); }
+// the other CategoryIceScheme values' schemes, run on the model as they are
+void ref_zero_cat_ice(void* p) { ZeroCatIceScheme(*(cAtmosphereModel*)p).run(); }
+void ref_one_cat_ice(void* p) { OneCatIceScheme(*(cAtmosphereModel*)p).run(); }
+void ref_three_cat_ice(void* p) { ThreeCatIceScheme(*(cAtmosphereModel*)p).run(); }
 // MultiLayerRadiation::run, and radiation mode 2's apply_radiative_heating (the lambda of
 // cAtmosphereModel.cpp:864-879, which saves t, runs the radiation and blends t toward the
 // radiative equilibrium by omega_rad; restated here around the reference's own run())

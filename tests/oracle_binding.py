@@ -301,6 +301,14 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_two_cat_ice_scheme(im, jm, km, ctypes.byref(self.params), F)
 
+    def ice_scheme(self, category):
+        """or_zero/one/two/three_cat_ice_scheme: the CategoryIceScheme switch for `category`."""
+        F, _, _ = self._args()
+        im, jm, km = self.shape
+        name = ("or_zero_cat_ice_scheme", "or_one_cat_ice_scheme", "or_two_cat_ice_scheme",
+                "or_three_cat_ice_scheme")[category]
+        getattr(lib(), name)(im, jm, km, ctypes.byref(self.params), F)
+
     def damp_wiggles(self, name, compat=0):
         """or_damp_wiggles: AtomUtils::damp_wiggles; compat=1 the reference's summation order
         in the j pass, 0 the mirror-exact one of the device."""

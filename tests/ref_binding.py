@@ -175,6 +175,13 @@ class Reference:
         f.argtypes = [ctypes.c_void_p]
         f(self.h)
 
+    def ice_scheme(self, category):
+        """ZeroCat/OneCat/TwoCat/ThreeCatIceScheme(*m).run() for `category` 0..3."""
+        f = getattr(self.lib, ("ref_zero_cat_ice", "ref_one_cat_ice", "ref_two_cat_ice",
+                               "ref_three_cat_ice")[category])
+        f.argtypes = [ctypes.c_void_p]
+        f(self.h)
+
     def skin(self, relax: float) -> float:
         """cAtmosphereModel::updateSkinTemperature with t_skin_relax = relax: the new t_skin
         (relax = 0 reads it unchanged)."""

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_default_params_match_config():
     lib = _abi.load_library()
-    assert lib.athad_abi_version() == 10
+    assert lib.athad_abi_version() == 11
     assert lib.athad_params_size() == ctypes.sizeof(_abi.Params)
     a = _abi.default_params().as_dict()
     b = _abi.config_params().as_dict()

@@ -11,7 +11,8 @@ semantics, must reproduce every hot-path function bit for bit:
   * the per-iteration boundary conditions (bcRadius, apply_wall_bc, bcTheta, bcPhi);
   * the filters after the RK4 step and the moist iteration's damp_wiggles;
   * TurbulenceAtm::run (its in-place sweep on one thread) for the three closures;
-  * TwoCatIceScheme::run; MultiLayerRadiation::run and radiation mode 2's heating;
+  * TwoCatIceScheme::run, and the schemes of the other CategoryIceScheme values (ZeroCat,
+    OneCat, ThreeCat); MultiLayerRadiation::run and radiation mode 2's heating;
   * the diagnostics standAtm_DewPoint_HumidRel and findResiduumAtm;
   * the surface fluxes waterVapourEvaporation and latentSensibleHeat;
   * the mass budgets co2Column and waterBudget (their sums on one thread);
@@ -265,6 +266,51 @@ def test_two_cat_ice_scheme_bit_exact(ref):
         o.f[n][...] = a
     R.two_cat_ice()
     o.two_cat_ice_scheme()
+    assert_identical(R, o, ICE_FIELDS)
+
+
+def seed_precipitation_state(R, o, seed, cold_band):
+    """The reference's state after a saturation adjustment, with falling rain, snow and
+    graupel seeded from above, cloud ice and graupel present, and cloud water in every cell
+    of the k = 1 plane (OneCat's serial loop reads its carried autoconversion rate before any
+    assignment otherwise).  cold_band: levels 40-52 redrawn between 230 and 285 K with cloud
+    water and vapour around saturation, so that the sub-freezing branches act."""
+    im, jm, km = R.shape
+    R.lib.ref_satadj(R.h)
+    o.saturation_adjust(compat=1)
+    rng = np.random.default_rng(seed)
+    new = {}
+    for n in ("P_rainn", "P_snown", "P_graupel"):
+        new[n] = 2e-4 * rng.random((im, jm, km))
+    for n in ("ice", "gr"):
+        a = o.f[n].copy()
+        a[30:55] += np.where(rng.random((25, jm, km)) < 0.5, 0.0, 1e-5 * rng.random((25, jm, km)))
+        new[n] = a
+    cloud = o.f["cloud"].copy()
+    if cold_band:
+        t = o.f["t"].copy()
+        t[40:53] = (230.0 + 55.0 * rng.random((13, jm, km))) / 273.15
+        new["t"] = t
+        cloud[40:53] = np.where(rng.random((13, jm, km)) < 0.3, 0.0, 2e-3 * rng.random((13, jm, km)))
+        c = o.f["c"].copy()
+        c[40:53] *= 0.5 + rng.random((13, jm, km))
+        new["c"] = c
+    cloud[:, :, 1] = np.maximum(cloud[:, :, 1], 1e-5)
+    new["cloud"] = cloud
+    for n, a in new.items():
+        R.set(n, a)
+        o.f[n][...] = a
+
+
+@pytest.mark.parametrize("category", [0, 1, 3])
+@pytest.mark.parametrize("cold_band", [False, True])
+def test_other_ice_schemes_bit_exact(ref, category, cold_band):
+    """ZeroCat, OneCat and ThreeCatIceScheme::run on the reference's state with falling
+    precipitation seeded (and a sub-freezing band redrawn)."""
+    R, o = fresh(ref)
+    seed_precipitation_state(R, o, 60 + category, cold_band)
+    R.ice_scheme(category)
+    o.ice_scheme(category)
     assert_identical(R, o, ICE_FIELDS)
 
 
