@@ -32,11 +32,18 @@ using Dev = athad_dropin::Device<cAtmosphereModel>;
 extern "C" {
 
 // what: 0 RK4, 1 pressure sweep, 2 saturation adjustment, 3 moist convection,
-// 4 densities, 5 densities(set_water_profile).  wall: 0 mirror, 1 reference.
+// 4 densities, 5 densities(set_water_profile), ... 18 the CategoryIceScheme switch with the
+// model's CategoryIceScheme set to arg for the call.  wall: 0 mirror, 1 reference.
 // Returns 0, or -1 with the message in err.
 int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
 {
     cAtmosphereModel* m = (cAtmosphereModel*)model;
+    const int category = m->CategoryIceScheme;
+    if (what == 18) m->CategoryIceScheme = arg;
+    struct Restore {
+        cAtmosphereModel* m; int c;
+        ~Restore() { m->CategoryIceScheme = c; }
+    } restore{m, category};
     try {
         Dev d(*m, wall ? ATHAD_WALL_REFERENCE : ATHAD_WALL_MIRROR);
         switch (what) {
@@ -63,6 +70,7 @@ int dropin_run(void* model, int what, int arg, int wall, char* err, int errlen)
                 d.WaterBudget(*m);
                 break;
             }
+            case 18: d.IceSchemeRun(*m); break;
             default: return -1;
         }
     } catch (const std::exception& e) {

@@ -301,8 +301,13 @@ class OracleState:
         im, jm, km = self.shape
         lib().or_two_cat_ice_scheme(im, jm, km, ctypes.byref(self.params), F)
 
-    def ice_scheme(self, category):
-        """or_zero/one/two/three_cat_ice_scheme: the CategoryIceScheme switch for `category`."""
+    def ice_scheme(self, category=None):
+        """or_zero/one/two/three_cat_ice_scheme: the CategoryIceScheme switch for `category`
+        (default: params.category_ice_scheme; -1 runs nothing)."""
+        if category is None:
+            category = self.params.category_ice_scheme
+        if category < 0:
+            return
         F, _, _ = self._args()
         im, jm, km = self.shape
         name = ("or_zero_cat_ice_scheme", "or_one_cat_ice_scheme", "or_two_cat_ice_scheme",

@@ -196,6 +196,37 @@ def test_dropin_two_cat_ice_scheme(model):
         assert relerr(a, b) <= 1e-10, (n, relerr(a, b))
 
 
+@pytest.mark.parametrize("category", [0, 1, 3])
+def test_dropin_other_ice_schemes(model, category):
+    """The CategoryIceScheme switch through the adapter (IceSchemeRun, the model's category
+    set to 0, 1 or 3) against the reference's own scheme, on the reference's state after its
+    saturation adjustment with rain, snow and graupel seeded and cloud water in the k = 1
+    plane (OneCat's carried rate is then assigned before it is read): within 1e-10."""
+    R, snap = model
+    im, jm, km = R.shape
+    rng = np.random.default_rng(61 + category)
+    seeded = dict(snap)
+    for n in ("P_rainn", "P_snown", "P_graupel"):
+        seeded[n] = 2e-4 * rng.random((im, jm, km))
+    cloud = np.array(snap["cloud"], copy=True)
+    cloud[:, :, 1] = np.maximum(cloud[:, :, 1], 1e-5)
+    seeded["cloud"] = cloud
+    names = ["t", "c", "cloud", "ice", "gr", "P_rain", "P_snow", "P_graupel", "Precipitation",
+             "S_v", "S_c", "S_i", "S_r", "S_s", "S_g"]
+
+    def prep():
+        R.lib.ref_satadj(R.h)
+        c = R.get("cloud")
+        c[:, :, 1] = np.maximum(c[:, :, 1], 1e-5)
+        R.set("cloud", c)
+
+    out = run_both(R, seeded, lambda: (prep(), R.ice_scheme(category)),
+                   lambda: (prep(), R.dropin(18, category)), names)
+    reset(R, snap)
+    for n, (a, b) in out.items():
+        assert relerr(a, b) <= 1e-10, (n, relerr(a, b))
+
+
 def test_dropin_radiation(model):
     """MultiLayerRadiation::run and radiation mode 2's heating through the adapter against the
     reference's own calls, cloud and ice seeded: within 1e-12 (CUDA vs glibc pow/exp)."""

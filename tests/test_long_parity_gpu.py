@@ -87,7 +87,7 @@ def oracle_loop_iteration(o, it, total, tropopause, omega_rad=0.05, t_skin_relax
         o.saturation_adjust()
         for n in MOIST_FIELDS_AFTER_SATADJ:
             o.damp_wiggles(n)
-        o.two_cat_ice_scheme()
+        o.ice_scheme()
         for n in ICE_FLUXES:
             o.damp_wiggles(n)
         o.moist_convection(it)
