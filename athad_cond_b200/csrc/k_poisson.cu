@@ -176,38 +176,44 @@ __device__ __forceinline__ double bc_final(const Dims& d, const double* p, int i
     return bc_pole(d, p, i, j, k);
 }
 
+// one flat grid over the three face groups: the planes i = 0, im-1 (2 jm km cells), the rows
+// j = 0, jm-1 (2 im km) and the seam columns k = 0, km-1 (2 im jm)
 __global__ void __launch_bounds__(128) poisson_bc_kernel(PoissonArgs a)
 {
     pdl_trigger();
     pdl_wait();
     const Dims& d = a.d;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n_planes = 2LL * d.jm * d.km, n_rows = 2LL * d.im * d.km, n_seam = 2LL * d.im * d.jm;
     int i, j, k;
-    if (blockIdx.z == 0) {            // the planes i = 0, im-1
-        if (t >= 2 * d.jm * d.km) return;
-        const int side = t / (d.jm * d.km), r = t % (d.jm * d.km);
+    bool plane = false;
+    if (t < n_planes) {
+        const int side = (int)(t / ((long long)d.jm * d.km));
+        const int r = (int)(t % ((long long)d.jm * d.km));
         i = side ? d.im - 1 : 0; j = r / d.km; k = r % d.km;
-    } else if (blockIdx.z == 1) {     // the rows j = 0, jm-1
-        if (t >= 2 * d.im * d.km) return;
-        const int side = t / (d.im * d.km), r = t % (d.im * d.km);
+        plane = true;
+    } else if ((t -= n_planes) < n_rows) {
+        const int side = (int)(t / ((long long)d.im * d.km));
+        const int r = (int)(t % ((long long)d.im * d.km));
         j = side ? d.jm - 1 : 0; i = r / d.km; k = r % d.km;
-    } else {                          // the seam columns k = 0, km-1
-        if (t >= 2 * d.im * d.jm) return;
-        const int side = t / (d.im * d.jm), r = t % (d.im * d.jm);
+    } else if ((t -= n_rows) < n_seam) {
+        const int side = (int)(t / ((long long)d.im * d.jm));
+        const int r = (int)(t % ((long long)d.im * d.jm));
         k = side ? d.km - 1 : 0; i = r / d.jm; j = r % d.jm;
+    } else {
+        return;
     }
     a.p[idx3(d, i, j, k)] = bc_final(d, a.p, i, j, k);
-    if (a.aux_lid && blockIdx.z == 0 && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1)
+    if (a.aux_lid && plane && k >= 1 && k < d.km - 1 && j >= 1 && j < d.jm - 1)
         aux_lid_cell(a, i, j, k);   // the aux radial boundary, PressureSolverAtm.h:106-121
 }
 
+// aux_lid: also the aux radial boundary (a sweep whose source launch wrote it passes 0)
 static void launch_bcs(const PoissonArgs& a, cudaStream_t st)
 {
     const Dims& d = a.d;
-    int most = 2 * d.jm * d.km;
-    most = std::max(most, 2 * d.im * d.km);
-    most = std::max(most, 2 * d.im * d.jm);
-    launch_dependent(poisson_bc_kernel, dim3((most + 127) / 128, 1, 3), dim3(128), 0, st, a);
+    const long long n = 2LL * d.jm * d.km + 2LL * d.im * d.km + 2LL * d.im * d.jm;
+    launch_dependent(poisson_bc_kernel, dim3((unsigned)((n + 127) / 128)), dim3(128), 0, st, a);
 }
 
 // |p_dyn| ceiling (:583-594); writes only where the value changes.  A thread takes four
@@ -237,16 +243,18 @@ __global__ void __launch_bounds__(256) poisson_ceiling_kernel(PoissonArgs a)
     // from such values, so when no colour formed a value beyond the ceiling (or a
     // non-finite one) the ceiling changes nothing and the launch ends here.
     if (a.counters && a.counters[5] == 0ull) return;
-    const long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
-    if (q >= (long long)d.im * d.plane) return;
-    const int k0 = (int)(q % d.pitch);
-    const double2* p2 = reinterpret_cast<const double2*>(a.p + q);
-    const double2 v01 = p2[0], v23 = p2[1];
-    const double v[4] = {v01.x, v01.y, v23.x, v23.y};
+    const long long n = (long long)d.im * d.plane;
+    for (long long q = 4LL * ((long long)blockIdx.x * blockDim.x + threadIdx.x); q < n;
+         q += 4LL * gridDim.x * blockDim.x) {
+        const int k0 = (int)(q % d.pitch);
+        const double2* p2 = reinterpret_cast<const double2*>(a.p + q);
+        const double2 v01 = p2[0], v23 = p2[1];
+        const double v[4] = {v01.x, v01.y, v23.x, v23.y};
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-        double w;
-        if (k0 + e < d.km && ceiling_of(v[e], a.ceiling, w)) a.p[q + e] = w;
+        for (int e = 0; e < 4; e++) {
+            double w;
+            if (k0 + e < d.km && ceiling_of(v[e], a.ceiling, w)) a.p[q + e] = w;
+        }
     }
 }
 
@@ -271,9 +279,18 @@ void launch_poisson_sweep(const PoissonArgs& a, cudaStream_t st)
     poisson_colour_kernel<0><<<half_grid, block, 0, st>>>(a);
 #endif
     launch_dependent(poisson_colour_kernel<1>, half_grid, block, 0, st, a);
+#if ATHAD_POISSON_SRC_FIELD
+    PoissonArgs b = a;
+    b.aux_lid = 0;   // the source launch wrote the aux boundary (aux is constant in a sweep)
+    launch_bcs(b, st);
+#else
     launch_bcs(a, st);
+#endif
+    // one wave of CTAs, each striding over the grid: when no value reached the ceiling (the
+    // usual case) the launch costs one short wave
     const long long quads = (long long)d.im * d.plane / 4;
-    launch_dependent(poisson_ceiling_kernel, dim3((unsigned)((quads + 255) / 256)), dim3(256), 0, st, a);
+    const long long blocks = std::min<long long>((quads + 255) / 256, 148LL * 4);
+    launch_dependent(poisson_ceiling_kernel, dim3((unsigned)blocks), dim3(256), 0, st, a);
 }
 
 // the boundary conditions of a sweep alone (radial, pole, seam), PressureSolverAtm.h:504-552
