@@ -239,7 +239,12 @@ rk4_stage_kernel(const RK4Args a)
     const Dims& d = a.d;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    // the even stages walk the radial planes from the top down (ATHAD_RK4_SERPENTINE, kernels.cuh)
+#if ATHAD_RK4_SERPENTINE
+    const int i = (STAGE % 2 == 0) ? d.im - 1 - (int)blockIdx.z : (int)blockIdx.z;
+#else
     const int i = blockIdx.z;
+#endif
 #if ATHAD_RK4_SMEM
     __shared__ double tile[kTileFields][kTileJ][kTileK];
     stage_tiles(a, tile, i);

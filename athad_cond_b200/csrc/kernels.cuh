@@ -4,6 +4,13 @@
 
 #include "common.cuh"
 
+// The RK4 stage launches (single grid, both forms) walk the radial planes forward in the odd
+// stages and backward in the even ones, so that a stage starts on the planes the stage
+// before it wrote last; measured 0.6 % on the mixed step, neutral on FP64.
+#ifndef ATHAD_RK4_SERPENTINE
+#define ATHAD_RK4_SERPENTINE 1
+#endif
+
 namespace athad {
 
 // Argument block of the RK4 stage kernels.  Field pointers are pitched device arrays.
