@@ -220,6 +220,7 @@ SIGNATURES = {
     "athad_download_2d": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_upload_profile": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_download_profile": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
+    "athad_download_profile_async": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.c_size_t]),
     "athad_field_device_ptr": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_size_t)]),
     "athad_fill": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_double]),
     "athad_default_init_config": (None, [ctypes.POINTER(InitConfig)]),

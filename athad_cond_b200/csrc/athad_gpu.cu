@@ -444,6 +444,15 @@ athad_status athad_download_profile(athad_ctx* ctx, athad_profile f, double* hos
     return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "download_profile sync");
 }
 
+athad_status athad_download_profile_async(athad_ctx* ctx, athad_profile f, double* host, size_t n)
+{
+    if (!ctx || !host || (int)f < 0 || (int)f >= ATHAD_NPROFILES)
+        return fail(ctx, ATHAD_ERR_INVALID, "download_profile_async: bad argument");
+    if (n != (size_t)ctx->grid.im) return fail(ctx, ATHAD_ERR_INVALID, "download_profile_async: size mismatch");
+    return cuda_check(ctx, cudaMemcpyAsync(host, ctx->prof[f], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                           ctx->stream), "download_profile_async");
+}
+
 athad_status athad_field_device_ptr(athad_ctx* ctx, athad_field f, double** ptr, size_t* pitch)
 {
     if (!ctx || !ptr || (int)f < 0 || (int)f >= ATHAD_NFIELDS) return fail(ctx, ATHAD_ERR_INVALID, "field_device_ptr: bad argument");

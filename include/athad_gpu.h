@@ -314,6 +314,13 @@ athad_status athad_upload_2d(athad_ctx* ctx, athad_field2d f, const double* host
 athad_status athad_download_2d(athad_ctx* ctx, athad_field2d f, double* host, size_t n);
 athad_status athad_upload_profile(athad_ctx* ctx, athad_profile f, const double* host, size_t n);
 athad_status athad_download_profile(athad_ctx* ctx, athad_profile f, double* host, size_t n);
+/* athad_download_profile without the wait: the copy is enqueued on the context's stream and
+ * the call returns.  host should be page-locked (into pageable memory CUDA completes the copy
+ * before the call returns) and must stay valid until the stream has passed the copy
+ * (athad_synchronize, or an event the caller records on the stream after the call); the
+ * caller reads it only then.  A loop that reads each step's profile one step later keeps
+ * the device busy while the host enqueues the next step. */
+athad_status athad_download_profile_async(athad_ctx* ctx, athad_profile f, double* host, size_t n);
 /* Device address and row pitch (in elements, >= km) of a field: element (i,j,k) is at
  * ptr[(i*jm + j)*pitch + k].  For zero-copy adapters and device-side consumers. */
 athad_status athad_field_device_ptr(athad_ctx* ctx, athad_field f, double** ptr, size_t* pitch);

@@ -159,3 +159,27 @@ def test_stand_atm_dew_point_mirror_symmetric():
         for n in ("TempStand", "TempDewPoint", "HumidityRel"):
             a = g.download(n)
             assert np.array_equal(a, mirror(a, False)), n
+
+
+def test_download_profile_async_equals_the_waiting_download():
+    """athad_download_profile_async into page-locked memory: after the stream has passed the
+    copy the host array holds what athad_download_profile returns; a kernel enqueued after
+    the call does not change it."""
+    import ctypes
+    import torch
+    from athad_cond_b200._abi import PROFILE
+    grid = (11, 21, 41)
+    with GpuAtmosphere(*grid, config_params()) as g:
+        g.upload_state(make_state(*grid, seed=5))
+        g.computeLevelMeanTemperature()
+        want = g.download_profile("t_ref_level")
+        host = torch.full((grid[0],), -1.0, dtype=torch.float64).pin_memory()
+        ptr = ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        g._check(g.lib.athad_download_profile_async(g._h, PROFILE["t_ref_level"], ptr, grid[0]))
+        g.fill("t", 1.0)
+        g.computeLevelMeanTemperature()
+        g.synchronize()
+        assert np.array_equal(host.numpy(), want)
+        assert not np.array_equal(g.download_profile("t_ref_level"), want)
+        with pytest.raises(AthadError):
+            g._check(g.lib.athad_download_profile_async(g._h, PROFILE["t_ref_level"], ptr, grid[0] + 1))
