@@ -1,14 +1,15 @@
 """A whole model iteration on the device: cAtmosphereModel::run_3D_loop
 (atmosphere/cAtmosphereModel.cpp:1101-1700) for the configuration of cli/config_cond.xml
-(flat terrain, turb_model k_omega_SST, CategoryIceScheme 2, radiation_mode 2, no inviscid
-spin-up), every step through the C ABI on one context, the state resident in HBM.
+(flat terrain, turb_model k_omega_SST, the ice scheme of the params' category_ice_scheme
+(2), radiation_mode 2, no inviscid spin-up), every step through the C ABI on one context, the
+state resident in HBM.
 
 Per iteration, in the reference's order:
 
   :1156  pressure sweep                                   every 4th iteration
   :1162  moist block                                      every 2nd iteration
          :1216 waterBudget("post-RK4"), :1218 SaturationAdjustment,
-         :1225 damp_wiggles(t, ice, c, cloud), :1238 TwoCatIceScheme,
+         :1225 damp_wiggles(t, ice, c, cloud), :1230-1242 the CategoryIceScheme switch,
          :1244 damp_wiggles(P_rain, P_snow), :1247 MoistConvection,
          :1249-1263 damp_wiggles of the convection fields, :1265-1334 precipitationSum and
          the caps, :1369-1391 the vapour ceiling, :1416 co2Column, :1417 waterBudget,
