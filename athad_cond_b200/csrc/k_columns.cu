@@ -279,16 +279,23 @@ __global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(cons
     const double p_sl_factor = 1e-2 * a.r_air * a.R_mix;
     double T_prev = smax(180.0, a.t[idx3(d, 0, j, k)] * a.t_0);
     double p_prev = p_sl_factor * T_prev;
+    const double p_first = p_prev;
     // saturation_pressure_auto(T_prev): formed once per level and carried to the next,
     // where T_prev is this level's T (the values, and the results, are the same as
     // evaluating it at each use)
     double E_prev = saturation_pressure_auto(T_prev);
     double q_sat_min = 1.0;
     double q_v_p = 0.0, q_c_p = 0.0;   // c and co2 of level i-1 (after any rewrite)
+    double t_last = 0.0;
+    // The level recurrence is sequential, so each level's loads would sit on its critical
+    // path; the next level's c, co2, cloud and ice are loaded while this level computes.
+    // A level writes only its own cells, so the values are those the serial order reads.
+    long long c = idx3(d, 0, j, k);
+    double q_v = a.c[c], q_c = a.co2[c], cl = a.cloud[c], ic = a.ice[c];
     for (int i = 0; i < d.im; i++) {
-        const long long c = idx3(d, i, j, k);
-        const double q_v = a.c[c];
-        const double q_c = a.co2[c];
+        const long long c_next = c + (long long)d.jm * d.pitch;
+        double q_v_n = 0.0, q_c_n = 0.0, cl_n = 0.0, ic_n = 0.0;
+        if (i + 1 < d.im) { q_v_n = a.c[c_next]; q_c_n = a.co2[c_next]; cl_n = a.cloud[c_next]; ic_n = a.ice[c_next]; }
         const double R_loc = R_of(q_v, q_c, a.R_bg);
         double T_i, p_i;
         if (i == 0) {
@@ -306,7 +313,8 @@ __global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(cons
             const double T_mean = 0.5 * (T_prev + T_i);
             p_i = p_prev * exp(-a.g * dz / (R_loc * T_mean));
         }
-        a.t[c] = T_i / a.t_0;
+        t_last = T_i / a.t_0;
+        a.t[c] = t_last;
         a.p_stat[c] = p_i;
         double q_v_now = q_v;
         const double E_i = (i == 0) ? E_prev : saturation_pressure_auto(T_i);
@@ -317,16 +325,17 @@ __global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(cons
             q_v_now = smax(q_sat_min, a.c_h2o_dry_top);
             a.c[c] = q_v_now;
         }
-        const double water_factor = smax(0.5, 1.0 - a.cloud[c] - a.ice[c]);
+        const double water_factor = smax(0.5, 1.0 - cl - ic);
         a.r_humid[c] = 1e2 * p_i / (R_loc * T_i * water_factor);
         const double R_dry_loc = R_of(0.0, q_c, a.R_bg);
         a.r_dry[c] = 1e2 * p_i / (R_dry_loc * T_i);
         T_prev = T_i; p_prev = p_i; E_prev = E_i;
         q_v_p = q_v_now; q_c_p = q_c;
+        c = c_next; q_v = q_v_n; q_c = q_c_n; cl = cl_n; ic = ic_n;
     }
     const long long c2 = (long long)j * d.pitch + k;
-    a.t_top_init[c2] = a.t[idx3(d, d.im - 1, j, k)];
-    a.p_stat_landscape[c2] = a.p_stat[idx3(d, 0, j, k)];
+    a.t_top_init[c2] = t_last;           // the value stored at level im-1
+    a.p_stat_landscape[c2] = p_first;    // the value stored at level 0
 }
 
 // per-(i,j) row sums of the positive densities, fixed warp order (one warp per row)

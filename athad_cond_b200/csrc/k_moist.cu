@@ -57,6 +57,17 @@ __device__ __forceinline__ double clamp_M(double v)
 }
 __device__ __forceinline__ double safe_r_humid(double r) { return smax(r, 1e-6); }
 
+// a - b rounded on its own: where the serial order stores a product and subtracts the
+// reloaded value, the register form must not fuse the two into one multiply-add
+__device__ __forceinline__ double sub_rn(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+
 // safe_q_sat, :181-184: the reference CO2 mass fraction co2_0 with the local water
 __device__ __forceinline__ double safe_q_sat(const MoistArgs& X, double E, double p_u, double q_v)
 {
@@ -148,46 +159,78 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
     const double t_0 = p->t_0;
     const double p0 = p->F[ATHAD_P_STAT][IDX(0, j, k)];
 
-    /* precompute, :339-376 */
-    for (int i = 0; i < im; i++) {
-        const long long c = IDX(i, j, k);
-        p->F[ATHAD_MC_S][c] = p->cp_l * p->F[ATHAD_T][c] * t_0 / p->s_0;
-        p->F[ATHAD_M_U][c] = 0.0; p->F[ATHAD_M_D][c] = 0.0;
-        p->F[ATHAD_MC_S_U][c] = 0.0; p->F[ATHAD_Q_V_U][c] = 0.0; p->F[ATHAD_Q_C_U][c] = 0.0;
-        p->F[ATHAD_C_U][c] = 0.0; p->F[ATHAD_E_L][c] = 0.0; p->F[ATHAD_E_DD][c] = 0.0; p->F[ATHAD_E_P][c] = 0.0;
-        p->F[ATHAD_G_P][c] = 0.0; p->F[ATHAD_MC_S_D][c] = 0.0; p->F[ATHAD_Q_V_D][c] = 0.0; p->F[ATHAD_P_CONV][c] = 0.0;
+    /* precompute, :339-376.  T is not written here: the next level's value is loaded while
+       this level's stores go out. */
+    const long long plane_s = (long long)jm * d.pitch;   // IDX(i + 1, j, k) - IDX(i, j, k)
+    {
+        const double* T = p->F[ATHAD_T];
+        double t_cur = T[IDX(0, j, k)];
+        for (int i = 0; i < im; i++) {
+            const long long c = IDX(i, j, k);
+            const double t_nxt = (i + 1 < im) ? T[c + plane_s] : 0.0;
+            p->F[ATHAD_MC_S][c] = p->cp_l * t_cur * t_0 / p->s_0;
+            p->F[ATHAD_M_U][c] = 0.0; p->F[ATHAD_M_D][c] = 0.0;
+            p->F[ATHAD_MC_S_U][c] = 0.0; p->F[ATHAD_Q_V_U][c] = 0.0; p->F[ATHAD_Q_C_U][c] = 0.0;
+            p->F[ATHAD_C_U][c] = 0.0; p->F[ATHAD_E_L][c] = 0.0; p->F[ATHAD_E_DD][c] = 0.0; p->F[ATHAD_E_P][c] = 0.0;
+            p->F[ATHAD_G_P][c] = 0.0; p->F[ATHAD_MC_S_D][c] = 0.0; p->F[ATHAD_Q_V_D][c] = 0.0; p->F[ATHAD_P_CONV][c] = 0.0;
+            t_cur = t_nxt;
+        }
     }
     int i_base = 0, i_lfs = 0, i_deep_beg = -1, i_deep_end = -1;
     double M_d_LFS = 0.0, cape_col = 0.0, dT_sfp = 0.0, dq_sfp = 0.0;
 
-    /* findCloudBaseLFS, :627-777 (every column) */
-    for (int i = 0; i < im; i++)
-        if (p->F[ATHAD_P_STAT][IDX(i, j, k)] <= MC_F_BEG * p0) {
-            i_deep_beg = i;
-            p->F[ATHAD_DEEP_BEG][IDX(i, j, k)] = p->height[i];
-            break;
+    /* findCloudBaseLFS, :627-777 (every column).  Each level's loads are issued before the
+       previous level's values are used: the two searches read p_stat four levels at a time,
+       the cloud-base search loads the next level while this one computes.  The loops store
+       only at the level they are on, so every value is the one the serial order reads. */
+    {
+        const double* P = p->F[ATHAD_P_STAT];
+        for (int i0 = 0; i0 < im && i_deep_beg < 0; i0 += 4) {
+            double pv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) pv[q] = (i0 + q < im) ? P[IDX(i0 + q, j, k)] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (i_deep_beg < 0 && i0 + q < im && pv[q] <= MC_F_BEG * p0) i_deep_beg = i0 + q;
         }
-    for (int i = im - 1; i >= 0; i--)
-        if (p->F[ATHAD_P_STAT][IDX(i, j, k)] >= MC_F_END * p0) {
-            i_deep_end = i;
-            p->F[ATHAD_DEEP_END][IDX(i, j, k)] = p->height[i];
-            break;
+        if (i_deep_beg >= 0) p->F[ATHAD_DEEP_BEG][IDX(i_deep_beg, j, k)] = p->height[i_deep_beg];
+        for (int i0 = im - 1; i0 >= 0 && i_deep_end < 0; i0 -= 4) {
+            double pv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) pv[q] = (i0 - q >= 0) ? P[IDX(i0 - q, j, k)] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (i_deep_end < 0 && i0 - q >= 0 && pv[q] >= MC_F_END * p0) i_deep_end = i0 - q;
         }
+        if (i_deep_end >= 0) p->F[ATHAD_DEEP_END][IDX(i_deep_end, j, k)] = p->height[i_deep_end];
+    }
     if (i_deep_beg >= 0 && i_deep_end >= 0) {
-        for (int i = i_deep_beg; i < im; i++) {
-            const long long c = IDX(i, j, k);
-            const double t_u = p->F[ATHAD_T][c] * t_0;
-            const double w = 1.0 / (1.0 + exp(-(t_u - MC_T00) / 2.0));
-            const double qsc = QSC(i);   // T, p_stat and c are not written in this loop
-            p->F[ATHAD_Q_V_U][c] = p->F[ATHAD_C][c] + MC_Q_V_U_ADD;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * qsc && t_u >= MC_T00)
-                p->F[ATHAD_Q_C_U][c] = p->F[ATHAD_Q_V_U][c] - MC_SCALE * qsc;
-            if (p->F[ATHAD_Q_V_U][c] <= 0.0) p->F[ATHAD_Q_V_U][c] = 0.0;
-            if (p->F[ATHAD_Q_C_U][c] <= 0.0) p->F[ATHAD_Q_C_U][c] = 0.0;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * qsc && w > 0.01 && p->F[ATHAD_P_STAT][c] <= MC_F_CB * p0) {
-                i_base = i;
-                p->F[ATHAD_CLOUD_BASE][c] = p->height[i] * w;
-                break;
+        {
+            const long long c0 = IDX(i_deep_beg, j, k);
+            double Tn = p->F[ATHAD_T][c0], Pn = p->F[ATHAD_P_STAT][c0];
+            double Cn = p->F[ATHAD_C][c0], QCn = p->F[ATHAD_Q_C_U][c0];
+            for (int i = i_deep_beg; i < im; i++) {
+                const long long c = IDX(i, j, k);
+                const double Tc = Tn, Pc = Pn, Cc = Cn;
+                double qcu = QCn;
+                if (i + 1 < im) {
+                    Tn = p->F[ATHAD_T][c + plane_s]; Pn = p->F[ATHAD_P_STAT][c + plane_s];
+                    Cn = p->F[ATHAD_C][c + plane_s]; QCn = p->F[ATHAD_Q_C_U][c + plane_s];
+                }
+                const double t_u = Tc * t_0;
+                const double w = 1.0 / (1.0 + exp(-(t_u - MC_T00) / 2.0));
+                const double qsc = safe_q_sat(X, saturation_pressure_auto(Tc * t_0 + MC_T_ADD_U), Pc, Cc);
+                double qvu = Cc + MC_Q_V_U_ADD;
+                if (qvu >= MC_SCALE * qsc && t_u >= MC_T00) qcu = qvu - MC_SCALE * qsc;
+                if (qvu <= 0.0) qvu = 0.0;
+                if (qcu <= 0.0) qcu = 0.0;
+                p->F[ATHAD_Q_V_U][c] = qvu;
+                p->F[ATHAD_Q_C_U][c] = qcu;
+                if (qvu >= MC_SCALE * qsc && w > 0.01 && Pc <= MC_F_CB * p0) {
+                    i_base = i;
+                    p->F[ATHAD_CLOUD_BASE][c] = p->height[i] * w;
+                    break;
+                }
             }
         }
         if (i_base > 0) {   /* LNB by theta_e, :711-759 */
@@ -256,67 +299,89 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
         }
     }
 
-    /* initUpdraft, :490-622 (interior columns) */
+    /* initUpdraft, :490-622 (interior columns).  Every value a level reads is loaded before
+       the level stores anything (a level stores only its own cells, and of the fields it
+       reads only q_c_u, which it reads first), and the mass flux of the level below is
+       carried in a register. */
     if (interior && i_deep_beg != -1 && i_deep_end != -1) {
         const int ib = i_base, il = i_lfs;
-        const double pb = p->F[ATHAD_P_STAT][IDX(ib, j, k)], pl = p->F[ATHAD_P_STAT][IDX(il, j, k)];
-        p->F[ATHAD_M_U][IDX(i_deep_beg, j, k)] =
-            clamp_M(p->F[ATHAD_R_HUMID][IDX(i_deep_beg, j, k)] * MC_C_MB * sqrt(2.0 * cape_col));
+        const double pb = p->F[ATHAD_P_STAT][IDX(ib, j, k)], pl_p = p->F[ATHAD_P_STAT][IDX(il, j, k)];
+        const double Mu_beg = clamp_M(p->F[ATHAD_R_HUMID][IDX(i_deep_beg, j, k)] * MC_C_MB * sqrt(2.0 * cape_col));
+        p->F[ATHAD_M_U][IDX(i_deep_beg, j, k)] = Mu_beg;
+        double Mu_m = Mu_beg;
         for (int i = i_deep_beg + 1; i <= i_deep_end; i++) {
             const long long c = IDX(i, j, k);
-            const double t_u = p->F[ATHAD_T][c] * t_0, t_u_add = t_u + dT_sfp;
-            const double r_h_i = p->F[ATHAD_R_HUMID][c], p_u = p->F[ATHAD_P_STAT][c];
-            const double q_sat_add = safe_q_sat(X, saturation_pressure_auto(t_u_add), p_u, p->F[ATHAD_C][c]);
-            p->F[ATHAD_Q_V_U][c] = p->F[ATHAD_C][c] + dq_sfp;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * q_sat_add && t_u >= MC_T00)
-                p->F[ATHAD_Q_C_U][c] = p->F[ATHAD_Q_V_U][c] - MC_SCALE * q_sat_add;
-            if (p->F[ATHAD_Q_V_U][c] <= 0.0) p->F[ATHAD_Q_V_U][c] = 0.0;
-            if (p->F[ATHAD_Q_C_U][c] <= 0.0) p->F[ATHAD_Q_C_U][c] = 0.0;
+            const double Tc = p->F[ATHAD_T][c], r_h_i = p->F[ATHAD_R_HUMID][c], p_u = p->F[ATHAD_P_STAT][c];
+            const double Cc = p->F[ATHAD_C][c];
+            double qcu = p->F[ATHAD_Q_C_U][c];
+            const double Uc = p->F[ATHAD_U][c], Vc = p->F[ATHAD_V][c], Wc = p->F[ATHAD_W][c];
             double dcdr, dcdthe, dcdphi, c_ijk;
             entrainment_gradients(X, i, j, k, &dcdr, &dcdthe, &dcdphi, &c_ijk);
-            if ((pb - pl) >= MC_F_DIFF * p0)
-                p->F[ATHAD_E_U][c] = -r_h_i / c_ijk * (p->F[ATHAD_U][c] * dcdr + p->F[ATHAD_V][c] * dcdthe + p->F[ATHAD_W][c] * dcdphi);
+            const double t_u = Tc * t_0, t_u_add = t_u + dT_sfp;
+            const double q_sat_add = safe_q_sat(X, saturation_pressure_auto(t_u_add), p_u, Cc);
+            double qvu = Cc + dq_sfp;
+            if (qvu >= MC_SCALE * q_sat_add && t_u >= MC_T00) qcu = qvu - MC_SCALE * q_sat_add;
+            if (qvu <= 0.0) qvu = 0.0;
+            if (qcu <= 0.0) qcu = 0.0;
+            p->F[ATHAD_Q_V_U][c] = qvu;
+            p->F[ATHAD_Q_C_U][c] = qcu;
+            double eu;
+            if ((pb - pl_p) >= MC_F_DIFF * p0)
+                eu = -r_h_i / c_ijk * (Uc * dcdr + Vc * dcdthe + Wc * dcdphi);
             else
-                p->F[ATHAD_E_U][c] = 0.0;
-            if (t_u <= MC_T00M2) p->F[ATHAD_E_U][c] = 0.0;
+                eu = 0.0;
+            if (t_u <= MC_T00M2) eu = 0.0;
+            p->F[ATHAD_E_U][c] = eu;
             p->F[ATHAD_D_U][c] = 0.0;
-            const double d_Mu = p->F[ATHAD_E_U][c] - p->F[ATHAD_D_U][c];
-            p->F[ATHAD_M_U][c] = clamp_M(p->F[ATHAD_M_U][IDX(i - 1, j, k)] + d_Mu * p->step[i]);
+            const double d_Mu = eu - 0.0;
+            const double Mu = clamp_M(Mu_m + d_Mu * p->step[i]);
+            p->F[ATHAD_M_U][c] = Mu;
+            Mu_m = Mu;
             p->F[ATHAD_MC_S][c] = p->cp_l * t_u / p->s_0;
             p->F[ATHAD_MC_S_U][c] = p->cp_l * t_u_add / p->s_0;
-            p->F[ATHAD_U_U][c] = MC_VEL * p->F[ATHAD_U][c];
-            p->F[ATHAD_V_U][c] = MC_VEL * p->F[ATHAD_V][c];
-            p->F[ATHAD_W_U][c] = MC_VEL * p->F[ATHAD_W][c];
+            p->F[ATHAD_U_U][c] = MC_VEL * Uc;
+            p->F[ATHAD_V_U][c] = MC_VEL * Vc;
+            p->F[ATHAD_W_U][c] = MC_VEL * Wc;
         }
-        M_d_LFS = clamp_M(MC_GAM_D * p->F[ATHAD_M_U][IDX(i_deep_beg, j, k)]);
+        M_d_LFS = clamp_M(MC_GAM_D * Mu_beg);
         p->F[ATHAD_M_D][IDX(il, j, k)] = M_d_LFS;
+        const double inv_a_u = 1.0 / (MC_A_U * p->u_0);
+        const double cap = MC_W_CONV_MAX / p->u_0;
+        Mu_m = Mu_beg;   // level i_deep_end takes the flux of i_deep_beg below
         for (int i = i_deep_end + 1; i <= il - 1; i++) {
             const long long c = IDX(i, j, k);
-            const double inv_a_u = 1.0 / (MC_A_U * p->u_0);
-            const double t_u = p->F[ATHAD_T][c] * t_0, r_h_i = p->F[ATHAD_R_HUMID][c];
-            const double t_u_add = t_u + dT_sfp, p_u = p->F[ATHAD_P_STAT][c];
-            const double q_sat_add = safe_q_sat(X, saturation_pressure_auto(t_u_add), p_u, p->F[ATHAD_C][c]);
-            if (i == i_deep_end + 1) p->F[ATHAD_M_U][IDX(i - 1, j, k)] = p->F[ATHAD_M_U][IDX(i_deep_beg, j, k)];
-            p->F[ATHAD_MC_S][c] = p->cp_l * t_u / p->s_0;
-            p->F[ATHAD_MC_S_U][c] = p->cp_l * t_u / p->s_0;
-            p->F[ATHAD_Q_V_U][c] = p->F[ATHAD_C][c] + dq_sfp;
-            if (p->F[ATHAD_Q_V_U][c] >= MC_SCALE * q_sat_add && t_u_add >= MC_T00)
-                p->F[ATHAD_Q_C_U][c] = p->F[ATHAD_Q_V_U][c] - MC_SCALE * q_sat_add;
+            const double Tc = p->F[ATHAD_T][c], r_h_i = p->F[ATHAD_R_HUMID][c], p_u = p->F[ATHAD_P_STAT][c];
+            const double Cc = p->F[ATHAD_C][c];
+            const double Uc = p->F[ATHAD_U][c], Vc = p->F[ATHAD_V][c], Wc = p->F[ATHAD_W][c];
             double dcdr, dcdthe, dcdphi, c_ijk;
             entrainment_gradients(X, i, j, k, &dcdr, &dcdthe, &dcdphi, &c_ijk);
-            if ((pb - pl) >= MC_F_DIFF * p0)
-                p->F[ATHAD_E_U][c] = -r_h_i / c_ijk * (p->F[ATHAD_U][c] * dcdr + p->F[ATHAD_V][c] * dcdthe + p->F[ATHAD_W][c] * dcdphi);
+            const double t_u = Tc * t_0;
+            const double t_u_add = t_u + dT_sfp;
+            const double q_sat_add = safe_q_sat(X, saturation_pressure_auto(t_u_add), p_u, Cc);
+            if (i == i_deep_end + 1) p->F[ATHAD_M_U][IDX(i - 1, j, k)] = Mu_beg;
+            p->F[ATHAD_MC_S][c] = p->cp_l * t_u / p->s_0;
+            p->F[ATHAD_MC_S_U][c] = p->cp_l * t_u / p->s_0;
+            const double qvu = Cc + dq_sfp;
+            p->F[ATHAD_Q_V_U][c] = qvu;
+            if (qvu >= MC_SCALE * q_sat_add && t_u_add >= MC_T00)
+                p->F[ATHAD_Q_C_U][c] = qvu - MC_SCALE * q_sat_add;
+            double eu;
+            if ((pb - pl_p) >= MC_F_DIFF * p0)
+                eu = -r_h_i / c_ijk * (Uc * dcdr + Vc * dcdthe + Wc * dcdphi);
             else
-                p->F[ATHAD_E_U][c] = 0.0;
-            if (t_u <= MC_T00M2) p->F[ATHAD_E_U][c] = 0.0;
+                eu = 0.0;
+            if (t_u <= MC_T00M2) eu = 0.0;
+            p->F[ATHAD_E_U][c] = eu;
             p->F[ATHAD_D_U][c] = 0.0;
-            const double d_Mu = p->F[ATHAD_E_U][c] - p->F[ATHAD_D_U][c];
-            p->F[ATHAD_M_U][c] = clamp_M(p->F[ATHAD_M_U][IDX(i - 1, j, k)] + d_Mu * p->step[i]);
-            p->F[ATHAD_U_U][c] = p->F[ATHAD_U][c] + p->F[ATHAD_M_U][c] * inv_a_u / safe_r_humid(r_h_i);
-            const double cap = MC_W_CONV_MAX / p->u_0;
-            p->F[ATHAD_U_U][c] = smax(-cap, smin(p->F[ATHAD_U_U][c], cap));
-            p->F[ATHAD_V_U][c] = p->F[ATHAD_V][c];
-            p->F[ATHAD_W_U][c] = p->F[ATHAD_W][c];
+            const double d_Mu = eu - 0.0;
+            const double Mu = clamp_M(Mu_m + d_Mu * p->step[i]);
+            p->F[ATHAD_M_U][c] = Mu;
+            Mu_m = Mu;
+            double uu = Uc + Mu * inv_a_u / safe_r_humid(r_h_i);
+            uu = smax(-cap, smin(uu, cap));
+            p->F[ATHAD_U_U][c] = uu;
+            p->F[ATHAD_V_U][c] = Vc;
+            p->F[ATHAD_W_U][c] = Wc;
         }
     }
     if (interior) cloud_base_update(X, j, k, i_deep_beg, i_lfs, &i_base);
@@ -346,6 +411,7 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
                 double dcdr, dcdthe, dcdphi, c_ijk;
                 entrainment_gradients(X, i, j, k, &dcdr, &dcdthe, &dcdphi, &c_ijk);
                 const double Mu_c = p->F[ATHAD_M_U][c];   // the previous pass's mass flux here
+                const double qcu_c = p->F[ATHAD_Q_C_U][c];  // not written by this loop
                 double eu;
                 if ((pb - pl) >= MC_F_DIFF * p0)
                     eu = -r_h_i / c_ijk * (p->F[ATHAD_U][c] * dcdr + p->F[ATHAD_V][c] * dcdthe + p->F[ATHAD_W][c] * dcdphi)
@@ -370,12 +436,12 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
                     p->F[ATHAD_E_L][c] = 0.0;
                 } else {
                     const double r_h_floor = smax(r_h_i, 0.01);
-                    double el = du * p->F[ATHAD_Q_C_U][c] / r_h_floor;
+                    double el = du * qcu_c / r_h_floor;
                     if (el <= 0.0) el = 0.0;
                     p->F[ATHAD_E_L][c] = el;
                 }
                 const double K_p = (height_i > height_base + delta_i_c) ? MC_BET_P : 0.0;
-                if (t_u >= t_0) p->F[ATHAD_G_P][c] = (ip == 1) ? 0.0 : K_p * p->F[ATHAD_Q_C_U][c];
+                if (t_u >= t_0) p->F[ATHAD_G_P][c] = (ip == 1) ? 0.0 : K_p * qcu_c;
                 else p->F[ATHAD_G_P][c] = 0.0;
             }
             p->F[ATHAD_M_U][IDX(il, j, k)] = 0.0;
@@ -502,45 +568,62 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
                     sigma_p = fabs(p->F[ATHAD_M_U][IDX(ib, j, k)]) / (safe_r_humid(p->F[ATHAD_R_HUMID][IDX(ib, j, k)]) * w_u_cb);
                 sigma_p = smin(sigma_p, 1.0);
             }
+            // Every value a level reads is loaded before it stores anything (it stores only
+            // its own cells and reads nothing it stores); M_d of the level above is carried
+            // in a register.  The differences that the serial order forms from stored and
+            // reloaded products are formed without contraction into a fused multiply-add.
+            double Md_up = p->F[ATHAD_M_D][cl];
             for (int i = il - 1; i >= 0; i--) {
                 const long long c = IDX(i, j, k);
                 p_u = p->F[ATHAD_P_STAT][c];
                 t_u = p->F[ATHAD_T][c] * t_0;
                 const double r_h_i = p->F[ATHAD_R_HUMID][c];
+                const double Cc = p->F[ATHAD_C][c], CLc = p->F[ATHAD_CLOUD][c];
+                const double Md_old = p->F[ATHAD_M_D][c];
+                const double Uc = p->F[ATHAD_U][c], Vc = p->F[ATHAD_V][c], Wc = p->F[ATHAD_W][c];
+                const double precip_i = p->F[ATHAD_P_CONV][c];
+                const double ep_old = p->F[ATHAD_E_P][c];
                 p->F[ATHAD_MC_S_D][c] = p->cp_l * t_u / p->s_0;
-                const double q_sat = safe_q_sat(X, saturation_pressure_auto(t_u), p_u, p->F[ATHAD_C][c]);
-                p->F[ATHAD_Q_V_D][c] = 0.5 * (p->F[ATHAD_CLOUD][c] + MC_SCALE * q_sat);
-                p->F[ATHAD_E_D][c] = MC_EPS_D * fabs(p->F[ATHAD_M_D][c]);
-                p->F[ATHAD_D_D][c] = MC_DEL_D * fabs(p->F[ATHAD_M_D][c]);
-                const double d_Md = p->F[ATHAD_E_D][c] - p->F[ATHAD_D_D][c];
-                p->F[ATHAD_M_D][c] = clamp_M(p->F[ATHAD_M_D][IDX(i + 1, j, k)] - d_Md * p->step[i]);
+                const double q_sat = safe_q_sat(X, saturation_pressure_auto(t_u), p_u, Cc);
+                const double qvd = 0.5 * (CLc + MC_SCALE * q_sat);
+                p->F[ATHAD_Q_V_D][c] = qvd;
+                const double ed = MC_EPS_D * fabs(Md_old);
+                const double dd = MC_DEL_D * fabs(Md_old);
+                p->F[ATHAD_E_D][c] = ed;
+                p->F[ATHAD_D_D][c] = dd;
+                const double d_Md = sub_rn(ed, dd);
+                const double Md = clamp_M(Md_up - d_Md * p->step[i]);
+                p->F[ATHAD_M_D][c] = Md;
+                Md_up = Md;
                 const double inv_a_d = 1.0 / (MC_A_D * p->u_0);
-                p->F[ATHAD_U_D][c] = p->F[ATHAD_U][c] + p->F[ATHAD_M_D][c] * inv_a_d / safe_r_humid(r_h_i);
-                p->F[ATHAD_V_D][c] = p->F[ATHAD_V][c];
-                p->F[ATHAD_W_D][c] = p->F[ATHAD_W][c];
+                p->F[ATHAD_U_D][c] = Uc + Md * inv_a_d / safe_r_humid(r_h_i);
+                p->F[ATHAD_V_D][c] = Vc;
+                p->F[ATHAD_W_D][c] = Wc;
                 if (i <= ib) {
                     if (ip == 1) {
                         p->F[ATHAD_E_P][c] = 0.0;
                     } else {
-                        const double precip_i = p->F[ATHAD_P_CONV][c];
+                        double ep = ep_old;
                         if (precip_i > 0.0 && sigma_p > 0.0)
-                            p->F[ATHAD_E_P][c] = sigma_p * MC_ALF_1 * (q_sat - p->F[ATHAD_Q_V_D][c])
-                                         * sqrt(1e1 / MC_ALF_2 * precip_i / sigma_p);
-                        if (p->F[ATHAD_E_P][c] <= 0.0) p->F[ATHAD_E_P][c] = 0.0;
+                            ep = sigma_p * MC_ALF_1 * sub_rn(q_sat, qvd)
+                                 * sqrt(1e1 / MC_ALF_2 * precip_i / sigma_p);
+                        if (ep <= 0.0) ep = 0.0;
+                        p->F[ATHAD_E_P][c] = ep;
                     }
                 }
                 if (ip == 1) {
                     p->F[ATHAD_E_DD][c] = 0.0;
                 } else {
-                    const double precip_i = p->F[ATHAD_P_CONV][c];
+                    double edd;
                     if (precip_i > 0.0) {
                         const double P_16 = pow(precip_i, 1.0 / 6.0);
                         const double P_49 = pow(precip_i, 4.0 / 9.0);
-                        p->F[ATHAD_E_DD][c] = MC_A_EV * (1.0 + MC_B_EV * P_16) * (q_sat - p->F[ATHAD_Q_V_D][c]) * P_49;
+                        edd = MC_A_EV * (1.0 + MC_B_EV * P_16) * sub_rn(q_sat, qvd) * P_49;
                     } else {
-                        p->F[ATHAD_E_DD][c] = 0.0;
+                        edd = 0.0;
                     }
-                    if (p->F[ATHAD_E_DD][c] <= 0.0) p->F[ATHAD_E_DD][c] = 0.0;
+                    if (edd <= 0.0) edd = 0.0;
+                    p->F[ATHAD_E_DD][c] = edd;
                 }
             }
         }
@@ -557,6 +640,7 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
             for (int i = i_lfs - 1; i >= 0; i--) {
                 const long long c = IDX(i, j, k), cp = IDX(i + 1, j, k);
                 const double t_u = p->F[ATHAD_T][c] * t_0;
+                const double gp_c = p->F[ATHAD_G_P][c];   // not written by this loop
                 const double step_ip1 = p->step[i + 1];
                 const double r_h_ip1 = rh_p, r_h_i = p->F[ATHAD_R_HUMID][c];
                 double ed = p->F[ATHAD_E_D][c], dd = p->F[ATHAD_D_D][c];
@@ -601,7 +685,7 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
                 p->F[ATHAD_MC_S_D][c] = sd;
                 double pconv = 0.0;
                 if (i > 0) {
-                    pconv = smax(0.0, pconv_p + p->step[i] * r_h_i * (p->F[ATHAD_G_P][c] - edd - ep));
+                    pconv = smax(0.0, pconv_p + p->step[i] * r_h_i * (gp_c - edd - ep));
                     p->F[ATHAD_P_CONV][c] = pconv;
                 }
                 Md_p = Md; qvd_p = qvd; vd_p = vd; wd_p = wd; sd_p = sd;
@@ -611,31 +695,37 @@ __device__ void mc_column(const MoistArgs& X, int j, int k)
         p->F[ATHAD_P_CONV][IDX(0, j, k)] = p->F[ATHAD_P_CONV][IDX(1, j, k)];
     }
 
-    /* rhsForcing, :1304-1417 */
-    for (int i = 0; i < im; i++) {
-        const long long c = IDX(i, j, k);
-        const double vu = p->F[ATHAD_M_U][c], vd = p->F[ATHAD_M_D][c];
-        p->F[ATHAD_M_U][c] = !is_finite_bits(vu) ? 0.0 : (vu < -3.0) ? -3.0 : (vu > 3.0) ? 3.0 : vu;
-        p->F[ATHAD_M_D][c] = !is_finite_bits(vd) ? 0.0 : (vd < -3.0) ? -3.0 : (vd > 3.0) ? 3.0 : vd;
-    }
+    /* rhsForcing, :1304-1417.  The clamp of M_u and M_d to [-3, 3] (NaN to 0) is applied
+       where the flux of a level first reads them, each level once and before any use, as
+       the reference's separate pass leaves them. */
+    auto clamp3 = [](double v) { return !is_finite_bits(v) ? 0.0 : (v < -3.0) ? -3.0 : (v > 3.0) ? 3.0 : v; };
     // the four mass fluxes at a level; level i+1's are level i's upper fluxes and the next
     // level's lower ones, so each is formed once and carried (same operands, same values)
     auto flux_at = [&](long long c, double& fs, double& fq, double& fv, double& fw) {
-        const double Mu = p->F[ATHAD_M_U][c], Md = p->F[ATHAD_M_D][c];
-        fs = Mu * (p->F[ATHAD_MC_S_U][c] - p->F[ATHAD_MC_S][c]) + Md * (p->F[ATHAD_MC_S_D][c] - p->F[ATHAD_MC_S][c]);
-        fq = Mu * (p->F[ATHAD_Q_V_U][c] - p->F[ATHAD_C][c]) + Md * (p->F[ATHAD_Q_V_D][c] - p->F[ATHAD_C][c]);
-        fv = Mu * (p->F[ATHAD_V_U][c] - p->F[ATHAD_V][c]) + Md * (p->F[ATHAD_V_D][c] - p->F[ATHAD_V][c]);
-        fw = Mu * (p->F[ATHAD_W_U][c] - p->F[ATHAD_W][c]) + Md * (p->F[ATHAD_W_D][c] - p->F[ATHAD_W][c]);
+        const double Mu = clamp3(p->F[ATHAD_M_U][c]), Md = clamp3(p->F[ATHAD_M_D][c]);
+        const double su = p->F[ATHAD_MC_S_U][c], sm = p->F[ATHAD_MC_S][c], sd = p->F[ATHAD_MC_S_D][c];
+        const double qu = p->F[ATHAD_Q_V_U][c], qm = p->F[ATHAD_C][c], qd = p->F[ATHAD_Q_V_D][c];
+        const double vu = p->F[ATHAD_V_U][c], vm = p->F[ATHAD_V][c], vd = p->F[ATHAD_V_D][c];
+        const double wu = p->F[ATHAD_W_U][c], wm = p->F[ATHAD_W][c], wd = p->F[ATHAD_W_D][c];
+        p->F[ATHAD_M_U][c] = Mu;
+        p->F[ATHAD_M_D][c] = Md;
+        fs = Mu * (su - sm) + Md * (sd - sm);
+        fq = Mu * (qu - qm) + Md * (qd - qm);
+        fv = Mu * (vu - vm) + Md * (vd - vm);
+        fw = Mu * (wu - wm) + Md * (wd - wm);
     };
     double fs0, fq0, fv0, fw0;
     flux_at(IDX(0, j, k), fs0, fq0, fv0, fw0);
     for (int i = 0; i < im - 1; i++) {
         const long long c = IDX(i, j, k), cp = IDX(i + 1, j, k);
-        const double L_latent = (p->F[ATHAD_T][c] * t_0 >= t_0) ? p->lv : p->ls;
-        const double inv_step_rh = 1.0 / (p->step[i] * smax(p->F[ATHAD_R_HUMID][c], 0.01));
+        const double Tc = p->F[ATHAD_T][c], Rc = p->F[ATHAD_R_HUMID][c];
+        const double cu = p->F[ATHAD_C_U][c], edd = p->F[ATHAD_E_DD][c];
+        const double el = p->F[ATHAD_E_L][c], ep = p->F[ATHAD_E_P][c];
+        const double L_latent = (Tc * t_0 >= t_0) ? p->lv : p->ls;
+        const double inv_step_rh = 1.0 / (p->step[i] * smax(Rc, 0.01));
         double fs1, fq1, fv1, fw1;
         flux_at(cp, fs1, fq1, fv1, fw1);
-        const double conv_src = p->F[ATHAD_C_U][c] - p->F[ATHAD_E_DD][c] - p->F[ATHAD_E_L][c] - p->F[ATHAD_E_P][c];
+        const double conv_src = cu - edd - el - ep;
         double v = -(fs1 - fs0) * inv_step_rh * t_0 + (L_latent / p->cp_l) * conv_src * t_0;
         p->F[ATHAD_MC_T][c] = !is_finite_bits(v) ? 0.0 : (v < -0.01) ? -0.01 : (v > 0.01) ? 0.01 : v;
         v = -(fq1 - fq0) * inv_step_rh - conv_src;
