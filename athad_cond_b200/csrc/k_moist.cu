@@ -49,17 +49,20 @@ using namespace thermo;
 
 #define IDX(i, j, k) idx3(d, (i), (j), (k))
 
+// The column code is __host__ __device__: the kernel runs it on the device, and a host build
+// of this file runs the same source against the oracle on the CPU (tests/host_moist.cu).
+
 // clamp_M, MoistConvection.h:216-222
-__device__ __forceinline__ double clamp_M(double v)
+__host__ __device__ __forceinline__ double clamp_M(double v)
 {
     if (!is_finite_bits(v)) return 0.0;
     return (v < -MC_M_MAX) ? -MC_M_MAX : (v > MC_M_MAX) ? MC_M_MAX : v;
 }
-__device__ __forceinline__ double safe_r_humid(double r) { return smax(r, 1e-6); }
+__host__ __device__ __forceinline__ double safe_r_humid(double r) { return smax(r, 1e-6); }
 
 // a - b rounded on its own: where the serial order stores a product and subtracts the
 // reloaded value, the register form must not fuse the two into one multiply-add
-__device__ __forceinline__ double sub_rn(double a, double b)
+__host__ __device__ __forceinline__ double sub_rn(double a, double b)
 {
 #ifdef __CUDA_ARCH__
     return __dsub_rn(a, b);
@@ -69,13 +72,13 @@ __device__ __forceinline__ double sub_rn(double a, double b)
 }
 
 // safe_q_sat, :181-184: the reference CO2 mass fraction co2_0 with the local water
-__device__ __forceinline__ double safe_q_sat(const MoistArgs& X, double E, double p_u, double q_v)
+__host__ __device__ __forceinline__ double safe_q_sat(const MoistArgs& X, double E, double p_u, double q_v)
 {
     return saturation_mass_fraction(E, p_u, M_nonwater(q_v, X.co2_0, X.M_bg));
 }
 
 // cc_factor, :191-203
-__device__ double cc_factor(const MoistArgs& X, double T, double p)
+__host__ __device__ double cc_factor(const MoistArgs& X, double T, double p)
 {
     const double Et = (T >= X.t_0) ? saturation_pressure(T) : sublimation_pressure(T);
     const double Er = (288.15 >= X.t_0) ? saturation_pressure(288.15) : sublimation_pressure(288.15);
@@ -85,7 +88,7 @@ __device__ double cc_factor(const MoistArgs& X, double T, double p)
 }
 
 // entrainmentGradients, :238-297 (flat terrain)
-__device__ void entrainment_gradients(const MoistArgs& X, int i, int j, int k, double* dcdr,
+__host__ __device__ void entrainment_gradients(const MoistArgs& X, int i, int j, int k, double* dcdr,
                                       double* dcdthe, double* dcdphi, double* c_ijk)
 {
     const Dims& d = X.d;
@@ -106,7 +109,7 @@ __device__ void entrainment_gradients(const MoistArgs& X, int i, int j, int k, d
 }
 
 // simpsonCxEu, :1426-1455
-__device__ int simpson_cxeu(const MoistArgs& X, int j, int k, int i_beg, int i_end)
+__host__ __device__ int simpson_cxeu(const MoistArgs& X, int j, int k, int i_beg, int i_end)
 {
     const Dims& d = X.d;
     if (i_end <= i_beg) return -1;
@@ -133,7 +136,7 @@ __device__ int simpson_cxeu(const MoistArgs& X, int j, int k, int i_beg, int i_e
 }
 
 // CloudBaseUpdate for one column, :1462-1482
-__device__ void cloud_base_update(const MoistArgs& X, int j, int k, int i_deep_beg, int i_lfs, int* i_base)
+__host__ __device__ void cloud_base_update(const MoistArgs& X, int j, int k, int i_deep_beg, int i_lfs, int* i_base)
 {
     const Dims& d = X.d;
     if (i_deep_beg < 0 || i_lfs <= i_deep_beg) return;
@@ -150,7 +153,7 @@ __device__ void cloud_base_update(const MoistArgs& X, int j, int k, int i_deep_b
 #define QSC(ii) safe_q_sat(X, saturation_pressure_auto(p->F[ATHAD_T][IDX((ii), j, k)] * t_0 + MC_T_ADD_U), \
                            p->F[ATHAD_P_STAT][IDX((ii), j, k)], p->F[ATHAD_C][IDX((ii), j, k)])
 
-__device__ void mc_column(const MoistArgs& X, int j, int k)
+__host__ __device__ void mc_column(const MoistArgs& X, int j, int k)
 {
     const Dims& d = X.d;
     const int im = d.im, jm = d.jm, km = d.km;

@@ -125,6 +125,10 @@ void or_densities(int im, int jm, int km, const or_params* p, int compat,
 /* MoistConvection::run, MoistConvection.h:106-140 */
 int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, int iter_n,
                         double* const* f, double* const* f2);
+/* the geometry or_moist_convection uses: layer heights [im], level steps [im] (double
+ * differences, MoistConvection.h:300-309) and cos(theta_equator - theta_j) [jm] (:239) */
+int or_moist_geometry(int im, int jm, int km, const or_params* p, int compat, double* height,
+                      double* step, double* cose);
 
 /* the per-iteration boundary conditions, cAtmosphereModel.cpp:1439-1446: BC_Atm::bcRadius,
  * TurbulenceAtm::apply_wall_bc, BC_Atm::bcTheta, BC_Atm::bcPhi, BC_Atm::bcScalarSurfSur and

@@ -615,28 +615,49 @@ static void mc_column(const mc_ctx* X, int j, int k, int iter_prec_n)
     }
 }
 
+/* The layer heights, the level steps of MoistConvection::precompute (MoistConvection.h:300-309)
+   and cos(theta_equator - theta_j) of entrainmentGradients (:239) */
+static void mc_geometry(const or_geom* g, int im, int jm, int compat, double* height, double* step,
+                        double* cose)
+{
+    for (int i = 0; i < im; i++) height[i] = g->height[i];
+    for (int i = 0; i < im - 1; i++) step[i] = g->height[i + 1] - g->height[i];
+    step[im - 1] = (im >= 2) ? step[im - 2] : 0.0;
+    /* the equator row: the.z[90] at the reference's 181 rows (:239), (jm-1)/2 in general */
+    const int je = (jm - 1) / 2;
+    for (int j = 0; j < jm; j++) {
+        if (compat) cose[j] = cos(g->the[je] - g->the[j]);
+        else {
+            const int jj = (j < jm - 1 - j) ? j : jm - 1 - j;
+            cose[j] = cos(g->the[je] - g->the[jj]);
+        }
+    }
+}
+
+int or_moist_geometry(int im, int jm, int km, const or_params* p, int compat, double* height,
+                      double* step, double* cose)
+{
+    or_geom g;
+    or_geom_init(&g, im, jm, km, p, compat);
+    mc_geometry(&g, im, jm, compat, height, step, cose);
+    or_geom_free(&g);
+    return 0;
+}
+
 int or_moist_convection(int im, int jm, int km, const or_params* p, int compat, int iter_n,
                         double* const* f, double* const* f2)
 {
     (void)iter_n;
     or_geom g;
     or_geom_init(&g, im, jm, km, p, compat);
+    double* height = (double*)malloc(sizeof(double) * im);
     double* step = (double*)malloc(sizeof(double) * im);
     double* cose = (double*)malloc(sizeof(double) * jm);
-    for (int i = 0; i < im - 1; i++) step[i] = g.height[i + 1] - g.height[i];
-    step[im - 1] = (im >= 2) ? step[im - 2] : 0.0;
-    /* the equator row: the.z[90] at the reference's 181 rows (:239), (jm-1)/2 in general */
-    const int je = (jm - 1) / 2;
-    for (int j = 0; j < jm; j++) {
-        if (compat) cose[j] = cos(g.the[je] - g.the[j]);
-        else {
-            const int jj = (j < jm - 1 - j) ? j : jm - 1 - j;
-            cose[j] = cos(g.the[je] - g.the[jj]);
-        }
-    }
-    mc_ctx X = {im, jm, km, p, f, f2, g.height, step, cose};
+    mc_geometry(&g, im, jm, compat, height, step, cose);
+    mc_ctx X = {im, jm, km, p, f, f2, height, step, cose};
     for (int j = 0; j < jm; j++)
         for (int k = 0; k < km; k++) mc_column(&X, j, k, p->iter_prec);
+    free(height);
     free(step);
     free(cose);
     or_geom_free(&g);

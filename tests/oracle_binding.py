@@ -176,6 +176,16 @@ class OracleState:
         im, jm, km = self.shape
         return lib().or_moist_convection(im, jm, km, ctypes.byref(self.params), compat, iter_n, F, F2)
 
+    def moist_geometry(self, compat=0):
+        """The layer heights, level steps and cos(theta_equator - theta_j) that
+        moist_convection uses (or_moist_geometry)."""
+        im, jm, km = self.shape
+        h, s, c = np.zeros(im), np.zeros(im), np.zeros(jm)
+        P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        r = lib().or_moist_geometry(im, jm, km, ctypes.byref(self.params), compat, P(h), P(s), P(c))
+        assert r == 0
+        return h, s, c
+
     def store_n_level(self):
         F, _, _ = self._args()
         im, jm, km = self.shape
