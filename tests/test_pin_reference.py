@@ -20,6 +20,7 @@ semantics, must reproduce every hot-path function bit for bit:
 
 Skipped where the reference was not built (a machine without the reference sources).
 """
+import concurrent.futures
 import ctypes
 import os
 
@@ -50,6 +51,17 @@ def ref():
         R.close()
     finally:
         os.chdir(cwd)
+
+
+_ORACLE_THREAD = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+
+
+def side_by_side(reference_call, oracle_call):
+    """Run the oracle's call on a worker thread while the reference's runs on this one: both
+    are C calls that release the interpreter and work on their own copies of the state."""
+    done = _ORACLE_THREAD.submit(oracle_call)
+    reference_call()
+    done.result()
 
 
 def fresh(ref):
@@ -98,8 +110,7 @@ def test_rhs_cells_bit_exact(ref):
 def test_rk4_step_bit_exact(ref):
     R, o = fresh(ref)
     R.set_scalars(DT, 1.0, 0.3, 90, 90)
-    R.lib.ref_rk4(R.h)
-    o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS)
+    side_by_side(lambda: R.lib.ref_rk4(R.h), lambda: o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS))
     assert_identical(R, o, ["t", "u", "v", "w", "c", "cloud", "ice", "gr", "co2", "tke", "dis",
                             "aux_u", "aux_v", "aux_w"])
     assert np.array_equal(R.getp("t_ref_level"), o.prof["t_ref_level"])
@@ -118,9 +129,9 @@ def test_rk4_step_diagnostic_outputs_bit_exact(ref):
     R.set_scalars(DT, 1.0, 0.3, 90, 90)
     R.lib.ref_set_budget_capture.argtypes = [ctypes.c_void_p, ctypes.c_int]
     R.lib.ref_set_budget_capture(R.h, 1)
-    R.lib.ref_rk4(R.h)
+    side_by_side(lambda: R.lib.ref_rk4(R.h),
+                 lambda: o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS, write_diagnostics=3))
     R.lib.ref_set_budget_capture(R.h, 0)
-    o.rk4(dt=DT, buoyancy_ramp=0.3, compat=THREADS, write_diagnostics=3)
     interior = (slice(1, -1), slice(1, -1), slice(1, -1))
     for n in DIAGNOSTICS:
         a, b = R.get(n)[interior], o.f[n][interior]
@@ -174,8 +185,7 @@ def test_moist_convection_bit_exact_two_calls(ref):
     for n in ("Evaporation", "Q_sensible_2D"):
         o.f2[n][:] = R.get2(n)
     for it in (2, 4):
-        R.lib.ref_moist(R.h, it)
-        o.moist_convection(it, compat=1)
+        side_by_side(lambda: R.lib.ref_moist(R.h, it), lambda: o.moist_convection(it, compat=1))
         assert_identical(R, o, MC_FIELDS)
 
 
@@ -309,8 +319,7 @@ def test_other_ice_schemes_bit_exact(ref, category, cold_band):
     precipitation seeded (and a sub-freezing band redrawn)."""
     R, o = fresh(ref)
     seed_precipitation_state(R, o, 60 + category, cold_band)
-    R.ice_scheme(category)
-    o.ice_scheme(category)
+    side_by_side(lambda: R.ice_scheme(category), lambda: o.ice_scheme(category))
     assert_identical(R, o, ICE_FIELDS)
 
 
@@ -373,8 +382,8 @@ def test_stand_atm_dew_point_bit_exact(ref):
     for n, a in (("t", t), ("c", c)):
         R.set(n, a)
         o.f[n][...] = a
-    R.stand_atm()
-    o.stand_atm_dew_point(equator_rule(R.tropopause_layers()))
+    layers = equator_rule(R.tropopause_layers())
+    side_by_side(R.stand_atm, lambda: o.stand_atm_dew_point(layers))
     assert_identical(R, o, ["TempStand", "TempDewPoint", "HumidityRel"])
     hr = o.f["HumidityRel"]
     assert np.all(hr[5:8, 20:24, 100:110] == -1.0) and np.all(hr[10:12, 60:64, 200:210] == 0.0)
