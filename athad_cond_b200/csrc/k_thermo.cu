@@ -10,7 +10,8 @@
 namespace athad {
 namespace {
 
-__device__ double eval_one(int fn, const double* x)
+// __host__ __device__: tests/host_thermo.cu evaluates the same source on the host
+__host__ __device__ double eval_one(int fn, const double* x)
 {
     switch (fn) {
         case ATHAD_THERMO_SATURATION_PRESSURE:      return thermo::saturation_pressure(x[0]);
