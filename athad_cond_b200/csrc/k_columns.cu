@@ -14,7 +14,7 @@ namespace athad {
 using namespace thermo;
 
 // IceSchemeCommon::evaporateWhereImpossible, IceSchemeCommon.h:121-190
-__device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, double t_u,
+__host__ __device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, double t_u,
                                            double& cv, double& cld, double& ic, double& T_nd)
 {
     const double co2 = a.co2[c];
@@ -54,7 +54,7 @@ __device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, dou
 // 230-255) with the reciprocals they divide by formed once: 1/T per Newton step, shared by
 // the saturation and sublimation curves and the derivative factor, and 1/p per cell.  A
 // product by a reciprocal instead of a quotient moves a result by at most an ulp or two.
-__device__ __forceinline__ double p_sat_r(double T, double invT)
+__host__ __device__ __forceinline__ double p_sat_r(double T, double invT)
 {
     if (T >= T_CRIT) return NO_SATURATION;
     if (T <= 0.0) return 0.0;
@@ -69,7 +69,7 @@ __device__ __forceinline__ double p_sat_r(double T, double invT)
                      + 22.6807411 * t35 + -15.9618719 * t4 + 1.80122502 * t75;
     return 220640.0 * exp((T_CRIT * invT) * sum);
 }
-__device__ __forceinline__ double p_subl_r(double T, double invT)
+__host__ __device__ __forceinline__ double p_subl_r(double T, double invT)
 {
     if (T <= 0.0) return 0.0;
     const double lt = log(T * (1.0 / T_TRIPLE));
@@ -78,7 +78,7 @@ __device__ __forceinline__ double p_subl_r(double T, double invT)
                      + -0.610598130e1 * exp(0.170333333e1 * lt);
     return 6.11657 * exp(sum * (T_TRIPLE * invT));
 }
-__device__ __forceinline__ double q_sat_r(double E, double p, double inv_p, double M_other)
+__host__ __device__ __forceinline__ double q_sat_r(double E, double p, double inv_p, double M_other)
 {
     if (E == NO_SATURATION) return 1.0;
     if (!(p > 0.0)) return 0.0;
@@ -88,7 +88,7 @@ __device__ __forceinline__ double q_sat_r(double E, double p, double inv_p, doub
     const double den = num + (1.0 - x) * M_other;
     return (den > 0.0) ? num / den : 1.0;
 }
-__device__ __forceinline__ double dqsat_r(double E, double L, double T, double invT, double p, double inv_p,
+__host__ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double invT, double p, double inv_p,
                                           double M_other)
 {
     if (!(T > 0.0)) return 0.0;
@@ -104,7 +104,7 @@ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double i
 // components at T (shomate_r), and their mixture (cp_mix), so a Newton step that moves the
 // composition but not T reuses the first.
 struct SpecificHeats { double h2o, co2, bg; };
-__device__ __forceinline__ SpecificHeats shomate_r(double T, double inv_M_b)
+__host__ __device__ __forceinline__ SpecificHeats shomate_r(double T, double inv_M_b)
 {
     const double t = smin(smax(T, 298.0), 2000.0) * 1.0e-3;
     const double t2 = t * t, t3 = t2 * t, it2 = 1.0 / t2;
@@ -113,7 +113,7 @@ __device__ __forceinline__ SpecificHeats shomate_r(double T, double inv_M_b)
     const double bg = 28.98641 + 1.853978 * t + -9.647459 * t2 + 16.63537 * t3 + 0.000117 * it2;
     return {h2o * (1.0 / M_H2O), co2s * (1.0 / M_CO2), bg * inv_M_b};
 }
-__device__ __forceinline__ double cp_mix(double c, double co2, const SpecificHeats& h)
+__host__ __device__ __forceinline__ double cp_mix(double c, double co2, const SpecificHeats& h)
 {
     double q_v, q_c, q_b;
     split(c, co2, q_v, q_c, q_b);
@@ -130,15 +130,13 @@ __device__ __forceinline__ double cp_mix(double c, double co2, const SpecificHea
 #ifndef ATHAD_SATADJ_MIN_BLOCKS
 #define ATHAD_SATADJ_MIN_BLOCKS 7         // 72 registers, 7 CTAs of 128 threads per SM
 #endif
-__global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS)
-saturation_adjust_kernel(const ColumnArgs a)
+// One cell (i, j, k < km) of the fused pass; returns whether the vapour hit its 1 - co2 cap.
+// __host__ __device__: tests/host_columns.cu runs the same source on the host.
+__host__ __device__ __forceinline__ bool satadj_cell(const ColumnArgs& a, int i, int j, int k)
 {
     const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    const int i = blockIdx.z;
     bool hit = false;
-    if (k < d.km) {
+    {
         const long long c = idx3(d, i, j, k);
         double cv = a.c[c], cld = a.cloud[c], ic = a.ice[c], T_nd = a.t[c];
         const double co2 = a.co2[c], p_local = a.p_stat[c];
@@ -255,6 +253,17 @@ saturation_adjust_kernel(const ColumnArgs a)
         }
         a.c[c] = cv; a.cloud[c] = cld; a.ice[c] = ic; a.t[c] = T_nd;
     }
+    return hit;
+}
+
+__global__ void __launch_bounds__(128, ATHAD_SATADJ_MIN_BLOCKS)
+saturation_adjust_kernel(const ColumnArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    bool hit = false;
+    if (k < a.d.km) hit = satadj_cell(a, i, j, k);
     const unsigned nh = __popc(__ballot_sync(0xffffffffu, hit));
     if ((threadIdx.x & 31) == 0 && nh && a.counters) atomicAdd(a.counters, (unsigned long long)nh);
 }
@@ -270,12 +279,11 @@ void launch_saturation_adjust(const ColumnArgs& a, cudaStream_t st)
 #ifndef ATHAD_DENS_BLOCK
 #define ATHAD_DENS_BLOCK 128   // columns per CTA
 #endif
-__global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(const ColumnArgs a)
+// One (j, k) column, k < km.  __host__ __device__: tests/host_columns.cu runs the same source
+// on the host.
+__host__ __device__ __forceinline__ void densities_column(const ColumnArgs& a, int j, int k)
 {
     const Dims& d = a.d;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (k >= d.km) return;
     const double p_sl_factor = 1e-2 * a.r_air * a.R_mix;
     double T_prev = smax(180.0, a.t[idx3(d, 0, j, k)] * a.t_0);
     double p_prev = p_sl_factor * T_prev;
@@ -336,6 +344,14 @@ __global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(cons
     const long long c2 = (long long)j * d.pitch + k;
     a.t_top_init[c2] = t_last;           // the value stored at level im-1
     a.p_stat_landscape[c2] = p_first;    // the value stored at level 0
+}
+
+__global__ void __launch_bounds__(ATHAD_DENS_BLOCK) densities_column_kernel(const ColumnArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k >= a.d.km) return;
+    densities_column(a, j, k);
 }
 
 // per-(i,j) row sums of the positive densities, fixed warp order (one warp per row)

@@ -117,6 +117,11 @@ void or_project_initial_velocity(int im, int jm, int km, const or_params* p, int
 void or_saturation_adjust(int im, int jm, int km, const or_params* p, int compat,
                           double* const* f, int64_t* counters);
 
+/* the layer heights [im] and SaturationAdjustment's level steps [im] (computeSteps,
+ * SaturationAdjustment.h:56-60: float differences) that the two column passes use */
+int or_column_geometry(int im, int jm, int km, const or_params* p, int compat, double* height,
+                       double* step_f);
+
 /* ThermoAtm::densities, ThermoAtm.h:1436-1666 */
 void or_densities(int im, int jm, int km, const or_params* p, int compat,
                   int set_water_profile, double* const* f, double* const* f2,

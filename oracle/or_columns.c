@@ -46,6 +46,22 @@ void or_evaporate_where_impossible(const or_params* p, double* const* f, size_t 
 
 /* SaturationAdjustment::run = computeSteps, adjustSaturation, applyTopography (identity
  * with flat terrain), clampAndFade: SaturationAdjustment.h:25-459. */
+int or_column_geometry(int im, int jm, int km, const or_params* p, int compat, double* height,
+                       double* step_f)
+{
+    or_geom g;
+    or_geom_init(&g, im, jm, km, p, compat);
+    for (int i = 0; i < im; i++) {
+        height[i] = g.height[i];
+        /* computeSteps (SaturationAdjustment.h:56-60), as or_saturation_adjust forms it */
+        const float h1 = (i + 1 <= im - 1) ? (float)g.height[i + 1] : -1.0f;
+        const float h0 = (float)g.height[i];
+        step_f[i] = (double)(float)(h1 - h0);
+    }
+    or_geom_free(&g);
+    return 0;
+}
+
 void or_saturation_adjust(int im, int jm, int km, const or_params* p, int compat,
                           double* const* f, int64_t* counters)
 {

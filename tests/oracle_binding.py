@@ -186,6 +186,14 @@ class OracleState:
         assert r == 0
         return h, s, c
 
+    def column_geometry(self, compat=0):
+        """The layer heights and the saturation adjustment's level steps (or_column_geometry)."""
+        im, jm, km = self.shape
+        h, s = np.zeros(im), np.zeros(im)
+        P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        assert lib().or_column_geometry(im, jm, km, ctypes.byref(self.params), compat, P(h), P(s)) == 0
+        return h, s
+
     def store_n_level(self):
         F, _, _ = self._args()
         im, jm, km = self.shape
