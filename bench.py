@@ -349,7 +349,7 @@ def run_form(args, rank, world, device, precision, grid=None, steps=None, pertur
     torch.cuda.synchronize(device)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    rk_ev, ps_ev = [], []
+    rk_ev, ps_ev, col_ev = [], [], []
     with ClockSampler(device.index if device.index is not None else 0) as clk:
         ev0.record(stream)
         for _ in range(steps):
@@ -362,9 +362,15 @@ def run_form(args, rank, world, device, precision, grid=None, steps=None, pertur
                 pb.record(stream)
                 ps_ev.append((pa, pb))
             if it % 2 == 0:
+                ce = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                ce[0].record(stream)
                 g.SaturationAdjustment_run()
+                ce[1].record(stream)
                 g.MoistConvection_run(it)
+                ce[2].record(stream)
                 g.densities()
+                ce[3].record(stream)
+                col_ev.append(ce)
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -377,6 +383,9 @@ def run_form(args, rank, world, device, precision, grid=None, steps=None, pertur
     ms = ev0.elapsed_time(ev1)
     rk_ms = [a.elapsed_time(b) for a, b in rk_ev]
     ps_ms = [a.elapsed_time(b) for a, b in ps_ev]
+    # per call of the column passes (every 2nd iteration): saturation adjustment, moist
+    # convection, densities
+    col_ms = [[ce[q].elapsed_time(ce[q + 1]) for q in range(3)] for ce in col_ev]
     if dist:
         tdist.barrier()
     ms = max_over_ranks(ms, device)
@@ -387,6 +396,9 @@ def run_form(args, rank, world, device, precision, grid=None, steps=None, pertur
            "rk4_ms": rk_avg, "achieved": fields_per_point * pts / (rk_avg * 1e-3) / 1e9,
            "rk4_bytes_per_point": fields_per_point, "clocks": clk.summary(), "final": final,
            "pressure_ms": (sum(ps_ms) / len(ps_ms)) if ps_ms else None,
+           "column_ms": ({n: sum(c[q] for c in col_ms) / len(col_ms)
+                          for q, n in enumerate(("saturation_adjust", "moist_convection", "densities"))}
+                         if col_ms else None),
            "e2e_value": None, "h2d": 0, "d2h": 0, "finite": True}
     if args.no_e2e or not e2e:
         g.close()
@@ -848,6 +860,8 @@ def main():
             summary[f]["pressure_ms"] = rr["pressure_ms"]
             summary[f]["pressure_gbs"] = pgbs
             summary[f]["pressure_roofline_frac"] = pgbs / peak
+        if rr.get("column_ms"):
+            summary[f]["column_ms_per_call"] = rr["column_ms"]
     errors = None
     if "fp64" in runs and "mixed" in runs:
         err, frac = field_errors(runs["mixed"]["final"], runs["fp64"]["final"])
