@@ -15,7 +15,7 @@ using namespace thermo;
 
 // IceSchemeCommon::evaporateWhereImpossible, IceSchemeCommon.h:121-190
 __host__ __device__ void evaporate_where_impossible(const ColumnArgs& a, long long c, double t_u,
-                                           double& cv, double& cld, double& ic, double& T_nd)
+                                                    double& cv, double& cld, double& ic, double& T_nd)
 {
     const double co2 = a.co2[c];
     const double q_cond = smax(0.0, cld) + smax(0.0, ic) + smax(0.0, a.gr[c]);
@@ -88,8 +88,8 @@ __host__ __device__ __forceinline__ double q_sat_r(double E, double p, double in
     const double den = num + (1.0 - x) * M_other;
     return (den > 0.0) ? num / den : 1.0;
 }
-__host__ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double invT, double p, double inv_p,
-                                          double M_other)
+__host__ __device__ __forceinline__ double dqsat_r(double E, double L, double T, double invT, double p,
+                                                   double inv_p, double M_other)
 {
     if (!(T > 0.0)) return 0.0;
     if (E == NO_SATURATION || !(p > 0.0) || E >= p) return 0.0;

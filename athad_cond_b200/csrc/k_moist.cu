@@ -89,7 +89,7 @@ __host__ __device__ double cc_factor(const MoistArgs& X, double T, double p)
 
 // entrainmentGradients, :238-297 (flat terrain)
 __host__ __device__ void entrainment_gradients(const MoistArgs& X, int i, int j, int k, double* dcdr,
-                                      double* dcdthe, double* dcdphi, double* c_ijk)
+                                               double* dcdthe, double* dcdphi, double* c_ijk)
 {
     const Dims& d = X.d;
     const double* c = X.F[ATHAD_C];
